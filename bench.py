@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark: STKFMM near-field P2P on B200.
+
+Workload (one "step"): one U-list S2T pass of the LapPGrad kernel (single layer
+q ~ U(-0.5,0.5) and double layer d ~ N(0,1)^3 at the same points as the
+targets) over an adaptive octree of 1,048,576 points drawn from 64 Gaussian
+clusters (centres U[0.1,0.9]^3, sigma 0.02, clipped into [0,1)^3), max 256
+points per leaf, multipole order 10.  Seeded synthetic data stands in for the
+reference's TOML-configured point sets.
+
+Metric: P2P pair-interactions/s (SL and DL (target, source point) pairs counted
+separately, exact counts from the U-list), mixed precision (FP64 centre-relative
+displacement, FP32 kernel, Kahan FP32 accumulation) as the headline, the plain
+FP64 path beside it, and their ratio.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) each rank runs an independent replica (its own seed) on
+its own GPU: weak scaling, no collective on the data path; timing is the max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 1_048_576
+N_CLUSTERS = 64
+SIGMA = 0.02
+MAX_PTS = 256
+MULT_ORDER = 10
+KERNEL_LAPPGRAD = 1
+# FP32 flops per (target, source point) pair of the fused laplace_pgrad +
+# laplace_dipolepgrad micro-kernel (FMA = 2), counted from stk_ukernels.cuh:
+# displacement 3, r^2 5, Newton step on rsqrt 5, inverse powers 3, r.d 5,
+# q/r^3 1, radial coefficient 3, potential 4, gradient 15.  Plus 1 MUFU rsqrt.
+FLOPS_PER_POINT_PAIR_FUSED = 44
+WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clusters (sigma 0.02, centres "
+            "U[0.1,0.9]^3), max 256 pts/leaf, p=10, SL=DL=targets")
+
+
+def make_points(seed: int):
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.1, 0.9, size=(N_CLUSTERS, 3))
+    idx = rng.integers(0, N_CLUSTERS, size=N_POINTS)
+    pts = centres[idx] + rng.normal(0.0, SIGMA, size=(N_POINTS, 3))
+    pts = np.clip(pts, 0.0, np.nextafter(1.0, 0.0))
+    q = rng.uniform(-0.5, 0.5, size=(N_POINTS, 1))
+    d = rng.normal(size=(N_POINTS, 3))
+    return pts, q, d
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------- CPU baseline ----
+def sample_boxes(ul, budget_pairs, seed=1):
+    """Random target leaves of the U-list whose SL+DL pairs sum to ~budget_pairs."""
+    tb, te, off, ent = ul["trg_begin"], ul["trg_end"], ul["list_off"], ul["list_ent"]
+    sb, se = ul["sl_begin"], ul["sl_end"]
+    cnt = se - sb
+    nt = te - tb
+    ns = np.array([cnt[ent[off[b]:off[b + 1]] >> 5].sum() for b in range(len(tb))], dtype=np.int64)
+    cand = np.flatnonzero((nt > 0) & (ns > 0))
+    rng = np.random.default_rng(seed)
+    rng.shuffle(cand)
+    pick, tot = [], 0
+    for b in cand:
+        pick.append(b)
+        tot += 2 * int(nt[b]) * int(ns[b])
+        if tot >= budget_pairs:
+            break
+    pick = np.array(sorted(pick), dtype=np.int64)
+    return pick, tot
+
+
+def cpu_lists_run(ul, pts, q, d, boxes, use_ref):
+    """The reference's kernels (oracle/_ref, SimpleKernel) or the oracle port over sampled U-list boxes."""
+    from oracle import oracle as O
+    tb, te, off, ent = ul["trg_begin"][boxes], ul["trg_end"][boxes], ul["list_off"], ul["list_ent"]
+    noff = np.zeros(len(boxes) + 1, np.int64)
+    ents = []
+    for i, b in enumerate(boxes):
+        e = ent[off[b]:off[b + 1]]
+        ents.append(e)
+        noff[i + 1] = noff[i] + len(e)
+    ents = np.concatenate(ents) if ents else np.zeros(0, np.int32)
+    sp, tp = ul["sl_perm"], ul["trg_perm"]
+    src = pts[sp]
+    trg = pts[tp]
+    qs, ds = q[sp], d[sp]
+    if use_ref:
+        out = O.ref_lists(O.REF_LAP_SL_PGRAD, tb, te, noff, ents >> 5, ul["sl_begin"], ul["sl_end"], src, qs, trg)
+        O.ref_lists(O.REF_LAP_DL_PGRAD, tb, te, noff, ents >> 5, ul["dl_begin"], ul["dl_end"], src, ds, trg, out=out)
+    else:
+        out = O.lists(O.UK_LAPLACE_PGRAD, tb, te, noff, ents >> 5, ents & 31, ul["sl_begin"], ul["sl_end"], src, qs,
+                      trg)
+        O.lists(O.UK_LAPLACE_DIPOLEPGRAD, tb, te, noff, ents >> 5, ents & 31, ul["dl_begin"], ul["dl_end"], src, ds,
+                trg, out=out)
+    return out
+
+
+def cpu_baseline(ul, pts, q, d, target_seconds=12.0):
+    from oracle import oracle as O
+    O.build()
+    use_ref = O.ref_available()
+    cores = os.cpu_count() or 1
+    # calibrate on a small sample, then size the timed sample to ~target_seconds
+    boxes, pairs = sample_boxes(ul, 2e7)
+    t0 = time.perf_counter()
+    cpu_lists_run(ul, pts, q, d, boxes, use_ref)
+    rate = pairs / max(time.perf_counter() - t0, 1e-6)
+    boxes, pairs = sample_boxes(ul, rate * target_seconds, seed=2)
+    t0 = time.perf_counter()
+    cpu_lists_run(ul, pts, q, d, boxes, use_ref)
+    dt = time.perf_counter() - t0
+    kind = "reference" if use_ref else "port"
+    what = ("reference Test/SimpleKernel.cpp LaplaceSLPGrad+LaplaceDLPGrad (oracle/_ref)" if use_ref else
+            "oracle C port of laplace_pgrad+laplace_dipolepgrad")
+    return {"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+            "sample": "%s over the U-lists of %d randomly chosen target leaves (%.3g SL+DL pairs, %.1f s, OpenMP %d "
+                      "threads)" % (what, len(boxes), pairs, dt, cores)}
+
+
+# ---------------------------------------------------------------- arms ------
+def reference_arm(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import stkfmm_b200 as S
+    pts, q, d = make_points(0)
+    # the same adaptive tree / U-list as the GPU arm, built on the host (no GPU)
+    t = S.Octree(pts, MAX_PTS, 0, sl=pts, dl=pts, trg=pts)
+    ul = {}
+    off, ent = t.list("U")
+    ul["list_off"], ul["list_ent"] = off, ent
+    for k, nm in enumerate(("sl", "dl", "trg")):
+        perm, b, e = t.point_set(k)
+        ul[nm + "_perm"] = perm
+        if nm == "trg":
+            ul["trg_begin"], ul["trg_end"] = b, e
+        else:
+            ul[nm + "_begin"], ul[nm + "_end"] = b, e
+    from oracle import oracle as O
+    O.build()
+    use_ref = O.ref_available()
+    # each step: a bounded sample of the workload, sized so the whole run ends in a few minutes
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    boxes, pairs = sample_boxes(ul, 2e7)
+    t0 = time.perf_counter()
+    cpu_lists_run(ul, pts, q, d, boxes, use_ref)
+    rate = pairs / max(time.perf_counter() - t0, 1e-6)
+    boxes, pairs = sample_boxes(ul, rate * per_step, seed=3)
+    for _ in range(args.warmup):
+        cpu_lists_run(ul, pts, q, d, boxes, use_ref)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cpu_lists_run(ul, pts, q, d, boxes, use_ref)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    value = pairs / dt
+    cores = os.cpu_count() or 1
+    kind = "reference" if use_ref else "port"
+    line = {"impl": "reference", "metric": "P2P pair-interactions/s", "value": value, "unit": "pairs/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "step": "bounded sample: U-lists of %d target leaves (%.3g pairs)"
+                       % (len(boxes), pairs)},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind,
+                             "sample": "%s, %d target leaves, OpenMP %d threads" % (
+                                 "reference Test/SimpleKernel.cpp via oracle/_ref" if use_ref else "oracle port",
+                                 len(boxes), cores)},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def b200_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    import stkfmm_b200 as S
+    from stkfmm_b200._lib import lib
+
+    K = KERNEL_LAPPGRAD
+    pts, q, d = make_points(rank)
+    fmm = S.Stk3DFMM(MULT_ORDER, MAX_PTS, S.PAXIS.NONE, K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts)
+    t0 = time.perf_counter()
+    fmm.setup_tree(K)
+    tree_s = time.perf_counter() - t0
+    st = fmm.tree_stats(K)
+    pairs = st["u_pairs_sl"] + st["u_pairs_dl"]
+    point_pairs = st["u_pairs_sl"]
+
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    qd = torch.as_tensor(q).cuda()
+    dd = torch.as_tensor(d).cuda()
+    outs = {}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def run(prec, steps, warmup):
+        fmm.set_precision(prec)
+        out = torch.zeros((N_POINTS, 4), dtype=torch.float64, device="cuda")
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                fmm.evaluate_near_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+        stream.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        kern = []
+        barrier()
+        torch.cuda.synchronize()
+        tw0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush.zero_()  # L2 flush (256 MB write) between timed steps, outside the step events
+                out.zero_()
+                evs[i][0].record(stream)
+                fmm.evaluate_near_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+                evs[i][1].record(stream)
+                stream.synchronize()
+                kern.append(fmm.last_kernel_ms(K))
+        torch.cuda.synchronize()
+        barrier()
+        wall = time.perf_counter() - tw0
+        step_ms = [a.elapsed_time(b) for a, b in evs]
+        ms = sum(step_ms) / len(step_ms)
+        kms = sum(kern) / len(kern)
+        if ws > 1:
+            tt = torch.tensor([ms, kms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms, kms = float(tt[0]), float(tt[1])
+        outs[prec] = out
+        return ms, kms, wall
+
+    clocks = ClockSampler(dev) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    ms64, k64, _ = run(S.PRECISION.FP64, args.steps, args.warmup)
+    msmx, kmx, _ = run(S.PRECISION.MIXED, args.steps, args.warmup)
+    clk = clocks.stop() if clocks else None
+
+    value = ws * pairs / (msmx * 1e-3)
+    value64 = ws * pairs / (ms64 * 1e-3)
+    o64 = outs[S.PRECISION.FP64].double()
+    omx = outs[S.PRECISION.MIXED].double()
+    err_mx = float(torch.linalg.norm(omx - o64) / torch.linalg.norm(o64))
+    err_cols = [float(torch.linalg.norm(omx[:, c] - o64[:, c]) / torch.linalg.norm(o64[:, c])) for c in range(4)]
+
+    # ---- e2e: the C-ABI host call (pinned host buffers in and out, copies inside) ----
+    fmm.set_precision(S.PRECISION.MIXED)
+    qh = torch.as_tensor(q).pin_memory().numpy()
+    dh = torch.as_tensor(d).pin_memory().numpy()
+    oh = torch.zeros((N_POINTS, 4), dtype=torch.float64).pin_memory().numpy()
+    for _ in range(args.warmup):
+        fmm.evaluate_near(K, qh, oh, dh)
+    barrier()
+    e2e_t = []
+    for _ in range(args.steps):
+        oh[:] = 0.0
+        t0 = time.perf_counter()
+        fmm.evaluate_near(K, qh, oh, dh)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    if ws > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt[0])
+    e2e_val = ws * pairs / e2e_s
+
+    if rank != 0:
+        if ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    # ---- parity spot check of the timed FP64 output against the oracle ----
+    ul = fmm.ulist(K)
+    from oracle import oracle as O
+    O.build()
+    boxes, _ = sample_boxes(ul, 2e7, seed=5)
+    ref_sorted = cpu_lists_run(ul, pts, q, d, boxes, use_ref=False)
+    sel = np.concatenate([np.arange(ul["trg_begin"][b], ul["trg_end"][b]) for b in boxes])
+    gpu64 = o64.cpu().numpy()[ul["trg_perm"][sel]]
+    parity64 = float(np.linalg.norm(gpu64 - ref_sorted[sel]) / np.linalg.norm(ref_sorted[sel]))
+
+    # ---- roofline of the dominant kernel (the fused mixed P2P kernel) ----
+    peaks = np.zeros(5)
+    lib().stk_measure_peaks(peaks.ctypes.data_as(__import__("stkfmm_b200._lib", fromlist=["P_d"]).P_d))
+    achieved = point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (kmx * 1e-3) / 1e12
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tj):
+        try:
+            traffic = json.load(open(tj)).get("list_p2p_kernel<LAPLACE_SLDL_PGRAD,mixed>")
+        except Exception:
+            traffic = None
+
+    cpu = cpu_baseline(ul, pts, q, d) if ws == 1 else None
+
+    line = {
+        "metric": "P2P pair-interactions/s (U-list S2T, mixed precision; FP64 path beside it)",
+        "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 displacement, Kahan f32 accumulation)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_points": N_POINTS, "tree_nodes": st["nodes"], "leaves": st["leaves"],
+                   "depth": st["depth"], "u_entries": st["u_entries"], "pairs_per_step": pairs,
+                   "point_pairs_per_step": point_pairs, "l2": "256 MB write between timed steps (inputs < L2)",
+                   "parallelism": "replica per GPU" if ws > 1 else "1 GPU", "setup_tree_s": tree_s},
+        "fp64": {"value": value64, "unit": "pairs/s", "ms_per_step": ms64, "kernel_ms": k64},
+        "mixed_over_fp64": value / value64,
+        "rel_l2_mixed_vs_fp64": err_mx, "rel_l2_mixed_vs_fp64_per_component": err_cols,
+        "rel_l2_fp64_vs_oracle_sample": parity64,
+        "fmm_evals_per_s": None,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peaks[0]), "unit": "TFLOP/s",
+                     "frac": achieved / float(peaks[0]) if peaks[0] > 0 else None, "traffic": traffic,
+                     "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, mixed>", "kernel_ms": kmx,
+                     "flops_per_point_pair": FLOPS_PER_POINT_PAIR_FUSED,
+                     "peak_source": "measured FP32 FMA probe (stk_measure_peaks) on this GPU",
+                     "probe": {"fp32_tflops": float(peaks[0]), "fp64_tflops": float(peaks[1]),
+                               "mufu_rsqrt_gops": float(peaks[2]), "probe_sm_mhz": float(peaks[3])},
+                     "fp64_path": {"achieved": point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (k64 * 1e-3) / 1e12,
+                                   "peak": float(peaks[1]),
+                                   "frac": (point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (k64 * 1e-3) / 1e12)
+                                   / float(peaks[1]) if peaks[1] > 0 else None}},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes),
+                "d2h_bytes_per_step": int(N_POINTS * 4 * 8), "ms_per_step": e2e_s * 1e3,
+                "api": "Stk3DFMM_evaluate_near (C ABI, pinned host arrays)"},
+        "gpu_launches": 3 * args.steps * 2,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,236 @@
+/*
+ * stkfmm_b200.h -- C ABI of the B200 (sm_100a) STKFMM kernel-evaluation path.
+ *
+ * Drop-in boundary for STKFMM's direct kernel-evaluation hot path:
+ *   - the Stk3DFMM_* handle API of Lib/include/STKFMM/STKFMM.h:5-36 and
+ *     Lib/src/Stk3DFMM-c.cpp:5-67 (same names, argument order and
+ *     accumulate-into-output semantics; every call returns a status code
+ *     instead of printing and calling exit(1));
+ *   - STKFMM::evaluateKernel (Lib/include/STKFMM/STKFMM.hpp:108-110,
+ *     Lib/src/STKFMM.cpp:88-99, Lib/src/FMMData.cpp:252-283), which the
+ *     reference C ABI never exported;
+ *   - list-level P2P entry points over device-resident, leaf-sorted arrays, the
+ *     unit of work PVFMM's PtFMM_Evaluate performs per (target box, source box)
+ *     pair through Kernel<T>::ker_poten (Lib/src/FMMData.cpp:198, 280-281);
+ *   - ker_poten-signature shims, one per STKFMM micro-kernel, that a PVFMM build
+ *     could register in place of the CPU uKerEval bodies.
+ *
+ * Host pointers are plain double arrays owned by the caller (AoS xyz, AoS
+ * values), as in the reference.  Device pointers are only taken by the
+ * *_device / *_lists entry points and are never freed by the library.
+ * The library fails loudly (STK_ERR_NO_DEVICE) when no CUDA device is present:
+ * there is no CPU fallback.
+ */
+#ifndef STKFMM_B200_H_
+#define STKFMM_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum stk_status {
+    STK_OK = 0,
+    STK_ERR_INVALID_ARG = 1,  /* null pointer, negative size, bad enum value            */
+    STK_ERR_KERNEL = 2,       /* kernel not activated / no such sub-kernel (STKFMM.cpp:53-55) */
+    STK_ERR_STATE = 3,        /* call order: set_points / setup_tree missing              */
+    STK_ERR_SIZE = 4,         /* point / value counts disagree (FMMData.cpp:184-195)      */
+    STK_ERR_CUDA = 5,         /* a CUDA runtime call failed                               */
+    STK_ERR_NO_DEVICE = 6,    /* no CUDA device: this library has no CPU path             */
+    STK_ERR_OUT_OF_BOX = 7,   /* a point lies outside the FMM box on a free axis          */
+    STK_ERR_NOT_SUPPORTED = 8 /* kernel or feature not provided by this build             */
+};
+
+/* ---- enums of Lib/include/STKFMM/STKFMM_common.hpp ---------------------- */
+/* PAXIS (STKFMM_common.hpp:29-34) */
+enum stk_paxis { STK_PAXIS_NONE = 0, STK_PAXIS_PX = 1, STK_PAXIS_PXY = 2, STK_PAXIS_PXYZ = 3 };
+/* PPKERNEL (STKFMM_common.hpp:40-44) */
+enum stk_ppkernel { STK_SLS2T = 1, STK_DLS2T = 2, STK_L2T = 4 };
+/* KERNEL (STKFMM_common.hpp:46-62) */
+enum stk_kernel {
+    STK_LapPGrad = 1,
+    STK_LapPGradGrad = 2,
+    STK_LapQPGradGrad = 4,
+    STK_Stokes = 8,
+    STK_RPY = 16,
+    STK_StokesRegVel = 32,
+    STK_StokesRegVelOmega = 64,
+    STK_PVel = 128,
+    STK_PVelGrad = 256,
+    STK_PVelLaplacian = 512,
+    STK_Traction = 1024
+};
+
+/* Arithmetic of the P2P kernels.  FP64: plain double.  MIXED: FP64
+ * centre-relative displacement, FP32 kernel tensor (MUFU rsqrt + 1 Newton
+ * step), Kahan-compensated FP32 accumulation per target. */
+enum stk_precision { STK_FP64 = 0, STK_MIXED = 1 };
+
+/* Micro-kernels: one STKFMM uKerEval body each (sources -> targets dims). */
+enum stk_ukernel {
+    STK_UK_LAPLACE_P = 0,           /* 1 -> 1   LaplaceLayerKernel.hpp:41-65                */
+    STK_UK_LAPLACE_PGRAD = 1,       /* 1 -> 4   LaplaceLayerKernel.hpp:67-96                */
+    STK_UK_LAPLACE_DIPOLEP = 2,     /* 3 -> 1   LaplaceLayerKernel.hpp:98-113               */
+    STK_UK_LAPLACE_DIPOLEPGRAD = 3, /* 3 -> 4   LaplaceLayerKernel.hpp:115-136              */
+    STK_UK_STOKES_VEL = 4,          /* 3 -> 3   PVFMM stokes_vel, StokesLayerKernel.hpp:39-42 */
+    STK_UK_RPY_U = 5,               /* 4 -> 3   RPYKernel.hpp:17-45                         */
+    STK_UK_RPY_ULAPU = 6,           /* 4 -> 6   RPYKernel.hpp:52-90                         */
+    STK_UK_STK_ULAPU = 7,           /* 3 -> 6   RPYKernel.hpp:97-129                        */
+    STK_UK_STOKES_REGVEL = 8,       /* 4 -> 3   StokesRegSingleLayerKernel.hpp:17-41        */
+    STK_UK_STOKES_PVEL = 9,         /* 4 -> 4   StokesSingleLayerKernel.hpp:27-47           */
+    STK_UK_STOKES_DOUBLEPVEL = 10,  /* 9 -> 4   StokesDoubleLayerKernel.hpp:25-57           */
+    STK_UK_LAPLACE_SLDL_PGRAD = 11, /* 1+3 -> 4 laplace_pgrad + laplace_dipolepgrad at one point */
+    STK_UK_STOKES_SLDL_PVEL = 12    /* 4+9 -> 4 stokes_pvel + stokes_doublepvel at one point     */
+};
+
+/* ---- kernel descriptors --------------------------------------------------- */
+const char *stk_status_string(int status);
+/* dims = {kdimSL, kdimDL, kdimTrg}; replaces getKernelDimension (Lib/src/STKFMM.cpp:33-40) */
+int stk_get_kernel_dimension(unsigned kernel, int *dims);
+/* PVFMM kernel name of the S2T kernel (getKernelName, Lib/src/STKFMM.cpp:42-47) */
+const char *stk_get_kernel_name(unsigned kernel);
+/* micro-kernel that fills a PVFMM slot of a kernel: slot 0 s2t SL, 1 s2t DL,
+ * 2 s2m SL, 3 s2m DL, 4 m2m/m2l/l2l, 5 m2t, 6 l2t, 7 s2l SL, 8 s2l DL;
+ * -1 when the slot is empty.  Mirrors the BuildKernel compositions, e.g.
+ * RPYKernel.hpp:137-154, LaplaceLayerKernel.hpp:314-326. */
+int stk_kernel_slot(unsigned kernel, int slot);
+int stk_ukernel_dims(int ukernel, int *sdim, int *tdim);
+int stk_device_count(void);
+/* Throughput probes of the running GPU (no reference counterpart; roofline
+ * denominators of the P2P kernels): out[0] FP32 TFLOP/s (FMA = 2 flops),
+ * out[1] FP64 TFLOP/s, out[2] MUFU rsqrt Gop/s, out[3] SM clock MHz seen by the
+ * probe, out[4] SM count. */
+int stk_measure_peaks(double *out);
+
+/* ---- direct sum (STKFMM::evaluateKernel) --------------------------------- */
+/* trg_value += K(trg - src) src_value over all pairs, host arrays, raw
+ * coordinates (no box scaling), accumulate.  ppkernel picks the k_s2t SL
+ * (SLS2T), k_s2t DL (DLS2T) or k_l2t (L2T) sub-kernel as FMMData.cpp:261-268. */
+int stk_evaluate_kernel(unsigned kernel, unsigned ppkernel, int nsrc, const double *src_coord,
+                        const double *src_value, int ntrg, const double *trg_coord, double *trg_value,
+                        int precision);
+/* Same on device pointers and a caller's cudaStream_t (passed as void *). */
+int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, int nsrc, const double *d_src_coord,
+                               const double *d_src_value, int ntrg, const double *d_trg_coord,
+                               double *d_trg_value, int precision, void *stream);
+/* Direct sum of one micro-kernel on device pointers. */
+int stk_ukernel_direct_device(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
+                              int ntrg, const double *d_trg_coord, double *d_trg_value, int precision,
+                              void *stream);
+
+/* ---- list-level P2P ---------------------------------------------------------
+ * One micro-kernel over an explicit interaction list (device pointers):
+ *   target box b owns targets [trg_begin[b], trg_end[b]) of d_trg_coord / d_trg_value;
+ *   source box s owns sources [src_begin[s], src_end[s]) of d_src_coord / d_src_value;
+ *   list_off[b] .. list_off[b+1]-1 index list_ent, each entry
+ *   (source box << 5) | (sx+1) + 3(sy+1) + 9(sz+1), the source image shifted by
+ *   (sx, sy, sz) * period.  Index arrays are host arrays (the library builds the
+ *   cost-sorted work list from them).  Outputs accumulate. */
+int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
+                  const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
+                  const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value, int ntrg,
+                  const double *d_trg_coord, double *d_trg_value, double period, void *stream);
+
+/* ---- Stk3DFMM handle (Lib/include/STKFMM/STKFMM.h, Lib/src/Stk3DFMM-c.cpp) -- */
+typedef struct Stk3DFMM Stk3DFMM;
+/* Stk3DFMM-c.cpp:5-7; returns NULL on invalid arguments or when no device */
+Stk3DFMM *Stk3DFMM_create(int mult_order, int max_pts, int pbc, unsigned kernelComb);
+void Stk3DFMM_destroy(Stk3DFMM *fmm);
+/* Stk3DFMM-c.cpp:13-16 */
+int Stk3DFMM_set_points(Stk3DFMM *fmm, const int nSL, double *src_SL_coord, const int nTrg, double *trg_coord,
+                        const int nDL, double *src_DL_coord);
+/* Stk3DFMM-c.cpp:18-20 (not declared in the reference header) */
+int Stk3DFMM_get_kernel_dimension(unsigned kernel, int *dims);
+/* Stk3DFMM-c.cpp:22 */
+int Stk3DFMM_set_box(Stk3DFMM *fmm, double *origin, double len);
+/* Stk3DFMM-c.cpp:24 */
+int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
+/* Stk3DFMM-c.cpp:26 (not declared in the reference header) */
+int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
+/* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources); see stk_fmm_far_field_available */
+int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
+                          double *trg_value, const int nDL, double *src_DL_value);
+/* Stk3DFMM-c.cpp:33-35 */
+int Stk3DFMM_show_active_kernels(Stk3DFMM *fmm);
+
+/* additions with no reference C counterpart */
+/* STKFMM::evaluateKernel through the handle (STKFMM.cpp:88-99) */
+int Stk3DFMM_evaluate_kernel(Stk3DFMM *fmm, unsigned kernel, int nThreads, unsigned p2p, int nSrc,
+                             double *srcCoord, double *srcValue, int nTrg, double *trgCoord, double *trgValue);
+/* choose FP64 or MIXED for the P2P kernels of this handle (default FP64) */
+int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision);
+/* Near-field (U-list S2T) part of evaluate_fmm only, on the tree of setup_tree:
+ * trg_value += sum over U-list leaf pairs, in the caller's coordinates/units. */
+int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
+                           double *trg_value, const int nDL, double *src_DL_value);
+/* Same on device buffers in the caller's order (values as given, unit box only:
+ * STK_ERR_NOT_SUPPORTED otherwise), queued on `stream` (a cudaStream_t, or null for
+ * the handle's stream) without a host synchronisation. */
+int Stk3DFMM_evaluate_near_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value, double *d_trg_value,
+                                  const double *d_src_DL_value, void *stream);
+/* Device time (ms, CUDA events on the launching stream) of the P2P kernel
+ * launches of the last near-field evaluation of `kernel`. */
+int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms);
+/* Tree / list statistics of the last setup_tree for `kernel`:
+ * out[0] nodes, [1] leaves, [2] depth, [3] U-list entries, [4] U-list SL point pairs,
+ * [5] U-list DL point pairs, [6] V entries, [7] W entries, [8] X entries. */
+int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
+/* Copy the U-list of the last setup_tree (leaf-sorted indices, same layout as
+ * stk_p2p_lists).  Pass null arrays to query sizes: sizes = {n_leaf_boxes, n_entries, nSL, nDL, nTrg}. */
+int Stk3DFMM_get_ulist(Stk3DFMM *fmm, unsigned kernel, int *sizes, int *trg_begin, int *trg_end, int *list_off,
+                       int *list_ent, int *sl_begin, int *sl_end, int *dl_begin, int *dl_end, int *sl_perm,
+                       int *dl_perm, int *trg_perm);
+
+/* ---- host-only octree (no CUDA call) ------------------------------------------
+ * The tree and KIFMM lists that Stk3DFMM_setup_tree builds, in place of PVFMM's
+ * PtFMM_Tree::Initialize / InitFMM_Tree / SetupFMM (FMMData.cpp:107-167).  All
+ * coordinates must already lie in [0,1)^3 (scaled and wrapped).  List entries
+ * are (node << 5) | shift code, as for stk_p2p_lists. */
+typedef struct stk_octree stk_octree;
+stk_octree *stk_octree_build(const double *tree_pts, int n, int max_pts, int pbc, const double *sl, int nsl,
+                             const double *dl, int ndl, const double *trg, int ntrg);
+void stk_octree_free(stk_octree *t);
+/* out = {nodes, leaves, depth, U entries, V entries, W entries, X entries} */
+int stk_octree_sizes(const stk_octree *t, long long *out);
+/* per node: level, parent (-1 root), first child (-1 leaf, children contiguous), integer coords (3) */
+int stk_octree_nodes(const stk_octree *t, int *level, int *parent, int *first_child, int *ixyz);
+/* which: 0 U, 1 V, 2 W, 3 X; off has nodes + 1 entries */
+int stk_octree_list(const stk_octree *t, int which, int *off, int *ent);
+/* set: 0 SL, 1 DL, 2 targets; perm (sorted position -> caller index), per-node ranges */
+int stk_octree_set(const stk_octree *t, int set, int *perm, int *node_begin, int *node_end);
+
+/* ---- ker_poten-signature shims (pvfmm::Kernel<double>::Ker_t) -----------------
+ * void (*)(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg,
+ *          int trg_cnt, double *k_out, mem::MemoryManager *mem_mgr)
+ * k_out += scaled kernel sum, FP64 on the GPU.  dof must be 1 (the only value
+ * STKFMM passes, FMMData.cpp:280-281); mem_mgr is ignored. */
+void stk_ker_laplace_p(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                       double *k_out, void *mem_mgr);
+void stk_ker_laplace_pgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                           double *k_out, void *mem_mgr);
+void stk_ker_laplace_dipolep(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                             double *k_out, void *mem_mgr);
+void stk_ker_laplace_dipolepgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                 double *k_out, void *mem_mgr);
+void stk_ker_stokes_vel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                        double *k_out, void *mem_mgr);
+void stk_ker_rpy_u(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt, double *k_out,
+                   void *mem_mgr);
+void stk_ker_rpy_ulapu(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                       double *k_out, void *mem_mgr);
+void stk_ker_stk_ulapu(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                       double *k_out, void *mem_mgr);
+void stk_ker_stokes_regvel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                           double *k_out, void *mem_mgr);
+void stk_ker_stokes_pvel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                         double *k_out, void *mem_mgr);
+void stk_ker_stokes_doublepvel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                               double *k_out, void *mem_mgr);
+/* status of the last ker_poten shim call on this thread (they return void) */
+int stk_ker_last_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STKFMM_B200_H_ */

@@ -1,0 +1,198 @@
+"""CPU FP64 oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes access to ``oracle/liboracle.so`` (the C restatement in stk_oracle.c) and,
+where it was built, ``oracle/_ref/libstk_ref.so`` (the reference's own
+Test/SimpleKernel.cpp).  Only tests/, ``__graft_entry__.smoke()`` and bench.py's
+CPU-baseline legs import this module; the product package never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(HERE, "liboracle.so")
+_REF = os.path.join(HERE, "_ref", "libstk_ref.so")
+
+# micro-kernel ids (same numbering as include/stkfmm_b200.h, enum stk_ukernel)
+UK_LAPLACE_P = 0
+UK_LAPLACE_PGRAD = 1
+UK_LAPLACE_DIPOLEP = 2
+UK_LAPLACE_DIPOLEPGRAD = 3
+UK_STOKES_VEL = 4
+UK_RPY_U = 5
+UK_RPY_ULAPU = 6
+UK_STK_ULAPU = 7
+UK_STOKES_REGVEL = 8
+UK_STOKES_PVEL = 9
+UK_STOKES_DOUBLEPVEL = 10
+UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel",
+            "rpy_u", "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel"]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4]
+
+# reference SimpleKernel selectors (oracle/ref_driver.cpp)
+REF_STOKES_SL, REF_LAP_SL_PGRAD, REF_LAP_DL_PGRAD, REF_STOKES_SL_RPY, REF_STOKES_REG_SL_VEL, \
+    REF_STOKES_SL_PVEL, REF_STOKES_DL_PVEL = range(7)
+REF_DIMS = {REF_STOKES_SL: (3, 6), REF_LAP_SL_PGRAD: (1, 4), REF_LAP_DL_PGRAD: (3, 4),
+            REF_STOKES_SL_RPY: (4, 6), REF_STOKES_REG_SL_VEL: (4, 3), REF_STOKES_SL_PVEL: (4, 4),
+            REF_STOKES_DL_PVEL: (9, 4)}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference tree is present)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(HERE, "stk_oracle.c")):
+            build()
+        _lib = ctypes.CDLL(_LIB)
+        _lib.oracle_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        _lib.oracle_lists.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _dp, _dp, _dp,
+                                      _dp, ctypes.c_double, ctypes.c_int]
+        _lib.oracle_surface.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int, _dp]
+        _lib.oracle_uk_scale.restype = ctypes.c_double
+        _lib.oracle_uk_pair.argtypes = [ctypes.c_int, _dp, _dp, _dp]
+        _lib.oracle_regvel_adjoint.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp,
+                                               ctypes.c_int]
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(_REF):
+            raise FileNotFoundError("oracle/_ref/libstk_ref.so not built (needs the reference tree)")
+        _ref = ctypes.CDLL(_REF)
+        _ref.ref_simple_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp,
+                                           _dp, ctypes.c_int, ctypes.c_int]
+        _ref.ref_simple_lists.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip, _ip, _ip, _dp, _dp,
+                                          ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int]
+    return _ref
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_ip)
+
+
+def uk_scale(uk: int) -> float:
+    return lib().oracle_uk_scale(uk)
+
+
+def direct(uk: int, src, sval, trg, out=None, nthreads: int = 0):
+    """out += scale * sum_s K_uk(trg - src) sval   (FMMData::evaluateKernel semantics)."""
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), UK_SDIM[uk]) if len(src) else np.zeros((0, UK_SDIM[uk])))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), UK_TDIM[uk]))
+    assert out.dtype == np.float64 and out.flags.c_contiguous
+    rc = lib().oracle_direct(uk, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return out
+
+
+def lists(uk: int, trg_begin, trg_end, list_off, list_src, list_shift, src_begin, src_end, src, sval, trg,
+          out=None, period: float = 1.0, nthreads: int = 0):
+    """out += sum over an explicit target-box / source-box list (see stk_oracle.c:oracle_lists)."""
+    tb, ptb = _i(trg_begin)
+    te, pte = _i(trg_end)
+    lo, plo = _i(list_off)
+    ls, pls = _i(list_src)
+    if list_shift is None:
+        psh = None
+    else:
+        lsh, psh = _i(list_shift)
+    sb, psb = _i(src_begin)
+    se, pse = _i(src_end)
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), UK_TDIM[uk]))
+    rc = lib().oracle_lists(uk, len(tb), ptb, pte, plo, pls, psh, psb, pse, ps, pv, pt, out.ctypes.data_as(_dp),
+                            period, nthreads)
+    assert rc == 0
+    return out
+
+
+def surface(p: int, c, alpha: float, depth: int):
+    n = 6 * (p - 1) ** 2 + 2
+    c, pc = _d(np.asarray(c, dtype=np.float64).reshape(3))
+    out = np.zeros((n, 3))
+    rc = lib().oracle_surface(p, pc, alpha, depth, out.ctypes.data_as(_dp))
+    assert rc == 0
+    return out
+
+
+def regvel_adjoint(src, sval, trg, w, nthreads: int = 0):
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1, 4))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    w, pw = _d(np.asarray(w).reshape(-1, 3))
+    gf = np.zeros((len(src), 3))
+    gx = np.zeros((len(src), 3))
+    rc = lib().oracle_regvel_adjoint(len(src), ps, pv, len(trg), pt, pw, gf.ctypes.data_as(_dp),
+                                     gx.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return gf, gx
+
+
+def ref_direct(which: int, src, sval, trg, out=None, nthreads: int = 0):
+    """Run the reference's own SimpleKernel over all pairs (runSimpleKernel protocol)."""
+    sd, td = REF_DIMS[which]
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1, sd))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    rc = ref().ref_simple_direct(which, len(src), ps, pv, sd, len(trg), pt, out.ctypes.data_as(_dp), td, nthreads)
+    assert rc == 0
+    return out
+
+
+def ref_lists(which: int, trg_begin, trg_end, list_off, list_src, src_begin, src_end, src, sval, trg, out=None,
+              nthreads: int = 0):
+    sd, td = REF_DIMS[which]
+    tb, ptb = _i(trg_begin)
+    te, pte = _i(trg_end)
+    lo, plo = _i(list_off)
+    ls, pls = _i(list_src)
+    sb, psb = _i(src_begin)
+    se, pse = _i(src_end)
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    rc = ref().ref_simple_lists(which, len(tb), ptb, pte, plo, pls, psb, pse, ps, pv, sd, pt,
+                                out.ctypes.data_as(_dp), td, nthreads)
+    assert rc == 0
+    return out

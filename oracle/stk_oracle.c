@@ -1,0 +1,366 @@
+/*
+ * stk_oracle.c -- CPU FP64 oracle for the STKFMM direct kernel-evaluation path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is
+ * compared against; it is never linked into, called by, or shipped with the
+ * product library (stkfmm_b200/).  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py load it.
+ *
+ * What it restates (plain C, exact 1/sqrt, FP64):
+ *   - every in-scope STKFMM micro-kernel ("uKerEval" body), one function each,
+ *     with the reference's r^2 > 0 self-interaction mask;
+ *   - the per-kernel scale factor that PVFMM's GenericKernel applies;
+ *   - the dense direct sum of FMMData::evaluateKernel (Lib/src/FMMData.cpp:252-283);
+ *   - a sum over an explicit target-box / source-box interaction list (the U/W/X
+ *     list loops that PVFMM runs inside PtFMM_Evaluate), so the GPU list kernels
+ *     can be checked on the very same lists;
+ *   - the KIFMM cube-surface point generator (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85);
+ *   - the adjoint of the regularized Stokeslet sum (no reference counterpart;
+ *     derived by hand from the forward formula and checked by finite differences).
+ *
+ * Parity pin: tests/golden/ holds outputs of the reference's own FP64 test
+ * kernels (Test/SimpleKernel.cpp, compiled by oracle/Makefile into oracle/_ref/)
+ * on seeded inputs; tests/test_oracle.py checks this file against them.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Micro-kernel ids.  Must match stkfmm_b200/csrc/stk_kernels.cuh and
+ * include/stkfmm_b200.h (enum stk_ukernel). */
+enum {
+    UK_LAPLACE_P = 0,           /* q(1)      -> p(1)              LaplaceLayerKernel.hpp:41-65   */
+    UK_LAPLACE_PGRAD = 1,       /* q(1)      -> p,grad p(4)       LaplaceLayerKernel.hpp:67-96   */
+    UK_LAPLACE_DIPOLEP = 2,     /* d(3)      -> p(1)              LaplaceLayerKernel.hpp:98-113  */
+    UK_LAPLACE_DIPOLEPGRAD = 3, /* d(3)      -> p,grad p(4)       LaplaceLayerKernel.hpp:115-136 */
+    UK_STOKES_VEL = 4,          /* f(3)      -> u(3)              PVFMM stokes_vel (StokesLayerKernel.hpp:39-42) */
+    UK_RPY_U = 5,               /* f,a(4)    -> u(3)              RPYKernel.hpp:17-45            */
+    UK_RPY_ULAPU = 6,           /* f,a(4)    -> u,lap u(6)        RPYKernel.hpp:52-90            */
+    UK_STK_ULAPU = 7,           /* f(3)      -> u,lap u(6)        RPYKernel.hpp:97-129           */
+    UK_STOKES_REGVEL = 8,       /* f,eps(4)  -> u(3)              StokesRegSingleLayerKernel.hpp:17-41 */
+    UK_STOKES_PVEL = 9,         /* f,trD(4)  -> p,u(4)            StokesSingleLayerKernel.hpp:27-47 */
+    UK_STOKES_DOUBLEPVEL = 10,  /* D(9)      -> p,u(4)            StokesDoubleLayerKernel.hpp:25-57 */
+    UK_COUNT = 11
+};
+
+static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9};
+static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4};
+
+static const double PI_ = 3.14159265358979323846264338327950288;
+
+int oracle_uk_dims(int uk, int *sdim, int *tdim) {
+    if (uk < 0 || uk >= UK_COUNT) return 1;
+    *sdim = uk_sdim[uk];
+    *tdim = uk_tdim[uk];
+    return 0;
+}
+
+/* ScaleFactor() of each micro-kernel: 1/(4 pi) for Laplace, 1/(8 pi) for the
+ * Stokes family (e.g. LaplaceLayerKernel.hpp:44-46, RPYKernel.hpp:20-22). */
+double oracle_uk_scale(int uk) {
+    return (uk <= UK_LAPLACE_DIPOLEPGRAD) ? 1.0 / (4.0 * PI_) : 1.0 / (8.0 * PI_);
+}
+
+/* Exact masked 1/sqrt: the reference's approx_rsqrt<digits>(r2, r2 > 0) returns
+ * 0 where the mask is false and ~1/sqrt(r2) elsewhere. */
+static inline double rsqrt_mask(double r2) { return r2 > 0.0 ? 1.0 / sqrt(r2) : 0.0; }
+
+/* One (target, source) pair, unscaled, accumulated into u.  r = x_trg - x_src. */
+static void uk_pair(int uk, const double r[3], const double *f, double *u) {
+    const double dx = r[0], dy = r[1], dz = r[2];
+    switch (uk) {
+    case UK_LAPLACE_P: { /* LaplaceLayerKernel.hpp:59-64 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        u[0] += f[0] * rinv;
+    } break;
+    case UK_LAPLACE_PGRAD: { /* LaplaceLayerKernel.hpp:85-95 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double sv = f[0] * rinv * rinv * rinv;
+        u[0] += sv * r2;
+        u[1] -= sv * dx;
+        u[2] -= sv * dy;
+        u[3] -= sv * dz;
+    } break;
+    case UK_LAPLACE_DIPOLEP: { /* LaplaceLayerKernel.hpp:105-112 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rdotn = f[0] * dx + f[1] * dy + f[2] * dz;
+        u[0] += rinv3 * rdotn;
+    } break;
+    case UK_LAPLACE_DIPOLEPGRAD: { /* LaplaceLayerKernel.hpp:122-135 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double rinv3 = rinv2 * rinv;
+        double rinv5 = rinv3 * rinv2;
+        double rdotn = f[0] * dx + f[1] * dy + f[2] * dz;
+        u[0] += rdotn * rinv3;
+        u[1] += (f[0] * r2 - 3.0 * rdotn * dx) * rinv5;
+        u[2] += (f[1] * r2 - 3.0 * rdotn * dy) * rinv5;
+        u[3] += (f[2] * r2 - 3.0 * rdotn * dz) * rinv5;
+    } break;
+    case UK_STOKES_VEL: {
+        /* Stokeslet u = f/r + r (f.r)/r^3 (times 1/8pi).  The body lives in PVFMM
+         * (not vendored); restated from the Stokeslet formula and pinned by the
+         * reference test kernel StokesSL (Test/SimpleKernel.cpp:986-1023, a = 0). */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
+        u[0] += f[0] * rinv + dx * fdotr * rinv3;
+        u[1] += f[1] * rinv + dy * fdotr * rinv3;
+        u[2] += f[2] * rinv + dz * fdotr * rinv3;
+    } break;
+    case UK_RPY_U: { /* RPYKernel.hpp:24-44; note the truncated 1/3 constant */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        double fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
+        double three_fdotr_rinv5 = 3.0 * fdotr * rinv5;
+        double a2_over_three = 0.3333333333333 * f[3] * f[3];
+        u[0] += (r2 * f[0] + dx * fdotr) * rinv3 + a2_over_three * (f[0] * rinv3 - three_fdotr_rinv5 * dx);
+        u[1] += (r2 * f[1] + dy * fdotr) * rinv3 + a2_over_three * (f[1] * rinv3 - three_fdotr_rinv5 * dy);
+        u[2] += (r2 * f[2] + dz * fdotr) * rinv3 + a2_over_three * (f[2] * rinv3 - three_fdotr_rinv5 * dz);
+    } break;
+    case UK_RPY_ULAPU: { /* RPYKernel.hpp:59-89 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        double fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
+        double fdotr_rinv3 = fdotr * rinv3;
+        double three_fdotr_rinv5 = 3.0 * fdotr * rinv5;
+        double a2_over_three = 0.3333333333333 * f[3] * f[3];
+        double cx = f[0] * rinv3 - three_fdotr_rinv5 * dx;
+        double cy = f[1] * rinv3 - three_fdotr_rinv5 * dy;
+        double cz = f[2] * rinv3 - three_fdotr_rinv5 * dz;
+        u[0] += f[0] * rinv + dx * fdotr_rinv3 + a2_over_three * cx;
+        u[1] += f[1] * rinv + dy * fdotr_rinv3 + a2_over_three * cy;
+        u[2] += f[2] * rinv + dz * fdotr_rinv3 + a2_over_three * cz;
+        u[3] += 2.0 * cx;
+        u[4] += 2.0 * cy;
+        u[5] += 2.0 * cz;
+    } break;
+    case UK_STK_ULAPU: { /* RPYKernel.hpp:104-128 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        double fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
+        double fdotr_rinv3 = fdotr * rinv3;
+        double three_fdotr_rinv5 = 3.0 * fdotr * rinv5;
+        u[0] += f[0] * rinv + dx * fdotr_rinv3;
+        u[1] += f[1] * rinv + dy * fdotr_rinv3;
+        u[2] += f[2] * rinv + dz * fdotr_rinv3;
+        u[3] += 2.0 * (f[0] * rinv3 - three_fdotr_rinv5 * dx);
+        u[4] += 2.0 * (f[1] * rinv3 - three_fdotr_rinv5 * dy);
+        u[5] += 2.0 * (f[2] * rinv3 - three_fdotr_rinv5 * dz);
+    } break;
+    case UK_STOKES_REGVEL: { /* StokesRegSingleLayerKernel.hpp:24-40; the self term is kept */
+        double reg = f[3];
+        double r2 = dx * dx + dy * dy + dz * dz + reg * reg;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double r2reg2 = r2 + reg * reg;
+        double cc = f[0] * dx + f[1] * dy + f[2] * dz;
+        u[0] += rinv3 * (r2reg2 * f[0] + dx * cc);
+        u[1] += rinv3 * (r2reg2 * f[1] + dy * cc);
+        u[2] += rinv3 * (r2reg2 * f[2] + dz * cc);
+    } break;
+    case UK_STOKES_PVEL: { /* StokesSingleLayerKernel.hpp:34-46 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double cc = f[0] * dx + f[1] * dy + f[2] * dz;
+        u[0] += 2.0 * cc * rinv3;
+        cc -= f[3];
+        u[1] += rinv3 * (r2 * f[0] + dx * cc);
+        u[2] += rinv3 * (r2 * f[1] + dy * cc);
+        u[3] += rinv3 * (r2 * f[2] + dz * cc);
+    } break;
+    case UK_STOKES_DOUBLEPVEL: { /* StokesDoubleLayerKernel.hpp:32-56; D row-major */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        double cc = f[0] * dx * dx + f[4] * dy * dy + f[8] * dz * dz;
+        cc += (f[1] + f[3]) * dx * dy;
+        cc += (f[2] + f[6]) * dx * dz;
+        cc += (f[5] + f[7]) * dy * dz;
+        cc *= -3.0 * rinv5;
+        double trace = f[0] + f[4] + f[8];
+        u[0] += 2.0 * (cc + r2 * rinv5 * trace);
+        u[1] += dx * cc;
+        u[2] += dy * cc;
+        u[3] += dz * cc;
+    } break;
+    default:
+        break;
+    }
+}
+
+/* Public single-pair entry (unscaled, accumulating), used by the tests. */
+void oracle_uk_pair(int uk, const double *r, const double *f, double *u) { uk_pair(uk, r, f, u); }
+
+static int clamp_threads(int nthreads) {
+#ifdef _OPENMP
+    if (nthreads < 1 || nthreads > omp_get_max_threads()) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    return nthreads;
+}
+
+/* Dense direct sum, trg_val += scale * sum_s K(x_t - x_s) f_s.
+ * Follows FMMData::evaluateKernel (Lib/src/FMMData.cpp:252-283): raw (unscaled)
+ * coordinates, accumulate into the caller's output, targets split across threads. */
+int oracle_direct(int uk, int nsrc, const double *src_xyz, const double *src_val, int ntrg,
+                  const double *trg_xyz, double *trg_val, int nthreads) {
+    if (uk < 0 || uk >= UK_COUNT || nsrc < 0 || ntrg < 0) return 1;
+    const int sd = uk_sdim[uk], td = uk_tdim[uk];
+    const double sc = oracle_uk_scale(uk);
+    nthreads = clamp_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+    for (int t = 0; t < ntrg; t++) {
+        double acc[16] = {0};
+        const double *xt = trg_xyz + 3 * (size_t)t;
+        for (int s = 0; s < nsrc; s++) {
+            const double *xs = src_xyz + 3 * (size_t)s;
+            double r[3] = {xt[0] - xs[0], xt[1] - xs[1], xt[2] - xs[2]};
+            uk_pair(uk, r, src_val + (size_t)sd * s, acc);
+        }
+        for (int k = 0; k < td; k++) trg_val[(size_t)td * t + k] += sc * acc[k];
+    }
+    return 0;
+}
+
+/* Sum over an explicit interaction list.
+ *   target box b owns targets [trg_begin[b], trg_end[b]) of trg_xyz / trg_val;
+ *   source box s owns sources [src_begin[s], src_end[s]) of src_xyz / src_val;
+ *   target box b interacts with entries list_off[b] .. list_off[b+1]-1, each a
+ *   source box list_src[e] seen through periodic image shift list_shift[e]
+ *   (code = (sx+1) + 3(sy+1) + 9(sz+1), image coordinate x_s + (sx,sy,sz)*period).
+ * This is the U-list S2T loop of PVFMM's PtFMM_Evaluate restated over the same
+ * lists that the GPU kernels receive. */
+int oracle_lists(int uk, int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
+                 const int *list_src, const int *list_shift, const int *src_begin, const int *src_end,
+                 const double *src_xyz, const double *src_val, const double *trg_xyz, double *trg_val,
+                 double period, int nthreads) {
+    if (uk < 0 || uk >= UK_COUNT) return 1;
+    const int sd = uk_sdim[uk], td = uk_tdim[uk];
+    const double sc = oracle_uk_scale(uk);
+    nthreads = clamp_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int b = 0; b < n_trg_box; b++) {
+        for (int t = trg_begin[b]; t < trg_end[b]; t++) {
+            double acc[16] = {0};
+            const double *xt = trg_xyz + 3 * (size_t)t;
+            for (int e = list_off[b]; e < list_off[b + 1]; e++) {
+                const int sb = list_src[e];
+                const int code = list_shift ? list_shift[e] : 13;
+                const double sh[3] = {(code % 3 - 1) * period, ((code / 3) % 3 - 1) * period,
+                                      (code / 9 - 1) * period};
+                for (int s = src_begin[sb]; s < src_end[sb]; s++) {
+                    const double *xs = src_xyz + 3 * (size_t)s;
+                    double r[3] = {xt[0] - (xs[0] + sh[0]), xt[1] - (xs[1] + sh[1]), xt[2] - (xs[2] + sh[2])};
+                    uk_pair(uk, r, src_val + (size_t)sd * s, acc);
+                }
+            }
+            for (int k = 0; k < td; k++) trg_val[(size_t)td * t + k] += sc * acc[k];
+        }
+    }
+    return 0;
+}
+
+/* KIFMM cube surface: n = 6(p-1)^2+2 points on the surface of the cube
+ * [-1,1]^3, mapped to (u+1)*alpha*r + c with r = 0.5*0.5^depth.
+ * Restates stkfmm::surface (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85). */
+int oracle_surface(int p, const double *c, double alpha, int depth, double *coord) {
+    if (p < 2) return 1;
+    const int n = 6 * (p - 1) * (p - 1) + 2;
+    int cnt = 0;
+    coord[0] = coord[1] = coord[2] = -1.0;
+    cnt = 1;
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            coord[3 * cnt + 0] = -1.0;
+            coord[3 * cnt + 1] = (2.0 * (i + 1) - p + 1) / (p - 1);
+            coord[3 * cnt + 2] = (2.0 * j - p + 1) / (p - 1);
+        }
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            coord[3 * cnt + 0] = (2.0 * i - p + 1) / (p - 1);
+            coord[3 * cnt + 1] = -1.0;
+            coord[3 * cnt + 2] = (2.0 * (j + 1) - p + 1) / (p - 1);
+        }
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            coord[3 * cnt + 0] = (2.0 * (i + 1) - p + 1) / (p - 1);
+            coord[3 * cnt + 1] = (2.0 * j - p + 1) / (p - 1);
+            coord[3 * cnt + 2] = -1.0;
+        }
+    /* second half is the point reflection of the first half */
+    for (int i = 0; i < (n / 2) * 3; i++) coord[3 * cnt + i] = -coord[i];
+    const double r = 0.5 * pow(0.5, depth);
+    const double b = alpha * r;
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) coord[3 * i + k] = (coord[3 * i + k] + 1.0) * b + c[k];
+    return 0;
+}
+
+/* Adjoint of the regularized-Stokeslet direct sum (no reference counterpart).
+ * Forward: u_t = 1/(8 pi) sum_s G_eps_s(x_t - x_s) f_s with
+ *   G_eps(r) = ((|r|^2 + 2 eps^2) I + r r^T) / (|r|^2 + eps^2)^{3/2}.
+ * For loss L = sum_t w_t . u_t:
+ *   dL/df_s = 1/(8 pi) sum_t G_eps_s(x_t - x_s) w_t            (G symmetric, even)
+ *   dL/dx_s = -1/(8 pi) sum_t grad_r [w_t . G_eps_s(r) f_s] at r = x_t - x_s
+ *   grad_r [w.G.f] = (2 r (w.f) + w (f.r) + f (w.r)) / R^3
+ *                    - 3 r ((|r|^2 + 2 eps^2)(w.f) + (w.r)(f.r)) / R^5,  R^2 = |r|^2 + eps^2.
+ * src_val holds (f, eps) per source; grads are accumulated. */
+int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val, int ntrg,
+                          const double *trg_xyz, const double *trg_w, double *grad_f, double *grad_x,
+                          int nthreads) {
+    const double sc = 1.0 / (8.0 * PI_);
+    nthreads = clamp_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+    for (int s = 0; s < nsrc; s++) {
+        const double *xs = src_xyz + 3 * (size_t)s;
+        const double *f = src_val + 4 * (size_t)s;
+        const double eps2 = f[3] * f[3];
+        double gf[3] = {0, 0, 0}, gx[3] = {0, 0, 0};
+        for (int t = 0; t < ntrg; t++) {
+            const double *xt = trg_xyz + 3 * (size_t)t;
+            const double *w = trg_w + 3 * (size_t)t;
+            const double r[3] = {xt[0] - xs[0], xt[1] - xs[1], xt[2] - xs[2]};
+            const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            const double R2 = rr + eps2;
+            if (!(R2 > 0.0)) continue;
+            const double Rinv = 1.0 / sqrt(R2);
+            const double Rinv3 = Rinv * Rinv * Rinv;
+            const double Rinv5 = Rinv3 * Rinv * Rinv;
+            const double wr = w[0] * r[0] + w[1] * r[1] + w[2] * r[2];
+            const double fr = f[0] * r[0] + f[1] * r[1] + f[2] * r[2];
+            const double wf = w[0] * f[0] + w[1] * f[1] + w[2] * f[2];
+            const double a = rr + 2.0 * eps2;
+            for (int k = 0; k < 3; k++) {
+                gf[k] += Rinv3 * (a * w[k] + r[k] * wr);
+                double g = (2.0 * r[k] * wf + w[k] * fr + f[k] * wr) * Rinv3 -
+                           3.0 * r[k] * (a * wf + wr * fr) * Rinv5;
+                gx[k] -= g;
+            }
+        }
+        for (int k = 0; k < 3; k++) {
+            grad_f[3 * (size_t)s + k] += sc * gf[k];
+            grad_x[3 * (size_t)s + k] += sc * gx[k];
+        }
+    }
+    return 0;
+}

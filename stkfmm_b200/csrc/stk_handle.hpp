@@ -1,0 +1,63 @@
+// stk_handle.hpp -- state behind the opaque Stk3DFMM handle.
+#pragma once
+#include <map>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "stk_kernel_table.hpp"
+#include "stk_tree.hpp"
+
+namespace stk {
+
+// Owned device allocation (grow-only).
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release();
+    int reserve(size_t n);
+    int upload(const void *src, size_t n, cudaStream_t s);
+};
+
+// One activated kernel: the reference's impl::FMMData (STKFMM_impl.hpp:19-174).
+struct KernelData {
+    const KernelInfo *info = nullptr;
+    Octree tree;
+    bool tree_ready = false;
+    bool fused = false;            // SL and DL at the same points: one fused U-list pass
+    long long u_pairs[2] = {0, 0}; // exact U-list (target, source point) pairs, SL and DL
+    int n_items[2] = {0, 0};
+    DevBuf d_xyz[3], d_perm[3], d_beg[3], d_end[3];  // per point set: sorted coords, perm, node ranges
+    DevBuf d_centre, d_uent, d_items[2], d_counter;
+    DevBuf d_val[2], d_rec[2], d_out_sorted, d_out_user, d_alpha;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the P2P launches of the last evaluation
+    bool timed = false;
+    ~KernelData();
+};
+
+}  // namespace stk
+
+struct Stk3DFMM {
+    int mult_order = 10, max_pts = 2000, pbc = 0;
+    unsigned kernel_comb = 0;
+    double origin[3] = {0, 0, 0};
+    double len = 1.0, scale_factor = 1.0;
+    int precision = 0;
+    int device = 0, sms = 1;
+    cudaStream_t stream = nullptr;
+    bool points_set = false, sl_dl_same = false;
+    int nsl = 0, ndl = 0, ntrg = 0;
+    std::vector<double> sl, dl, trg;  // scaled, wrapped coordinates (caller's order)
+    std::map<unsigned, std::unique_ptr<stk::KernelData>> pool;
+    ~Stk3DFMM();
+};
+
+namespace stk {
+int near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *d_out_user,
+                cudaStream_t s);
+}

@@ -1,0 +1,165 @@
+// stk_work.cpp -- per-thread device workspace and work-list builders.
+#include "stk_work.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "../../include/stkfmm_b200.h"
+#include "stk_tree.hpp"
+
+namespace stk {
+
+Workspace &Workspace::thread_local_ws() {
+    static thread_local Workspace ws;
+    return ws;
+}
+
+Workspace::~Workspace() {
+    for (auto &kv : devs_) {
+        int prev = -1;
+        if (cudaGetDevice(&prev) != cudaSuccess) break;  // runtime already torn down
+        cudaSetDevice(kv.first);
+        for (int s = 0; s < kNumSlots; s++)
+            if (kv.second.ptr[s]) cudaFree(kv.second.ptr[s]);
+        if (kv.second.counter) cudaFree(kv.second.counter);
+        if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
+        cudaSetDevice(prev);
+    }
+}
+
+int Workspace::ensure_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return STK_ERR_NO_DEVICE;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return STK_ERR_CUDA;
+    Dev &d = devs_[dev];
+    cur_ = &d;
+    if (!d.stream) {
+        if (cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking) != cudaSuccess) return STK_ERR_CUDA;
+        if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return STK_ERR_CUDA;
+        if (cudaMalloc(&d.counter, 64) != cudaSuccess) return STK_ERR_CUDA;
+    }
+    return STK_OK;
+}
+
+void *Workspace::raw(int slot, size_t bytes) {
+    if (!cur_ || slot < 0 || slot >= kNumSlots) return nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cur_->cap[slot] < bytes) {
+        const size_t want = std::max(bytes, cur_->cap[slot] * 3 / 2);
+        if (cur_->ptr[slot]) {
+            // the previous contents may still be read by work queued on any stream
+            cudaDeviceSynchronize();
+            cudaFree(cur_->ptr[slot]);
+        }
+        cur_->ptr[slot] = nullptr;
+        cur_->cap[slot] = 0;
+        if (cudaMalloc(&cur_->ptr[slot], want) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        cur_->cap[slot] = want;
+    }
+    return cur_->ptr[slot];
+}
+
+unsigned int *Workspace::counter() { return cur_ ? cur_->counter : nullptr; }
+int Workspace::num_sms() { return cur_ ? cur_->sms : 1; }
+cudaStream_t Workspace::stream() { return cur_ ? cur_->stream : nullptr; }
+
+static inline int lanes_log2(int m) {
+    // largest g = 2^glog with m * g <= 32
+    int glog = 0;
+    while (glog < 5 && (m << (glog + 1)) <= 32) glog++;
+    return glog;
+}
+
+void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &items, std::vector<int> &src_begin,
+                        std::vector<int> &src_end, std::vector<int> &ent) {
+    const int nchunk = (ntrg + 31) / 32;
+    // enough items to fill every warp slot several times over, but source
+    // chunks of at least 256 points
+    const long long want_items = (long long)std::max(num_sms, 1) * 64;
+    int nsc = (int)std::max(1LL, (want_items + nchunk - 1) / nchunk);
+    nsc = std::min(nsc, std::max(1, nsrc / 256));
+    int sc = (nsrc + nsc - 1) / nsc;
+    sc = (sc + 31) / 32 * 32;
+    nsc = (nsrc + sc - 1) / sc;
+    src_begin.resize(nsc);
+    src_end.resize(nsc);
+    ent.resize(nsc);
+    for (int k = 0; k < nsc; k++) {
+        src_begin[k] = k * sc;
+        src_end[k] = std::min(nsrc, (k + 1) * sc);
+        ent[k] = (k << 5) | kShiftNone;
+    }
+    items.clear();
+    items.reserve((size_t)nchunk * nsc);
+    // full chunks first (largest cost), the ragged last chunk at the end
+    for (int c = 0; c < nchunk; c++) {
+        const int t0 = 32 * c;
+        const int m = std::min(32, ntrg - t0);
+        for (int k = 0; k < nsc; k++) items.push_back({c, t0, m, lanes_log2(m), k, k + 1});
+    }
+}
+
+void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
+                      const int *list_ent, const int *src_begin, const int *src_end, std::vector<WorkItem> &items,
+                      long long &pairs) {
+    items.clear();
+    pairs = 0;
+    std::vector<double> cost;
+    for (int b = 0; b < n_trg_box; b++) {
+        const int nt = trg_end[b] - trg_begin[b];
+        if (nt <= 0) continue;
+        long long ns = 0;
+        for (int e = list_off[b]; e < list_off[b + 1]; e++) {
+            const int sb = list_ent[e] >> 5;
+            ns += src_end[sb] - src_begin[sb];
+        }
+        if (ns == 0) continue;
+        pairs += (long long)nt * ns;
+        for (int t0 = trg_begin[b]; t0 < trg_end[b]; t0 += 32) {
+            const int m = std::min(32, trg_end[b] - t0);
+            const int glog = lanes_log2(m);
+            items.push_back({b, t0, m, glog, list_off[b], list_off[b + 1]});
+            cost.push_back((double)ns / (1 << glog) + 64.0 * (list_off[b + 1] - list_off[b]));
+        }
+    }
+    std::vector<int> idx(items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<WorkItem> sorted(items.size());
+    for (size_t i = 0; i < idx.size(); i++) sorted[i] = items[idx[i]];
+    items.swap(sorted);
+}
+
+void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], xyz[3 * (size_t)i + k]);
+            hi[k] = std::max(hi[k], xyz[3 * (size_t)i + k]);
+        }
+    double span = 0;
+    for (int k = 0; k < 3; k++) span = std::max(span, hi[k] - lo[k]);
+    const double inv = span > 0 ? 1.0 / (span * (1.0 + 1e-12)) : 0.0;
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; i++) {
+        double u[3];
+        for (int k = 0; k < 3; k++) u[k] = std::min(std::max((xyz[3 * (size_t)i + k] - lo[k]) * inv, 0.0), 0.999999999);
+        key[i] = morton_key(u[0], u[1], u[2]);
+    }
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+    sorted.resize(3 * (size_t)n);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) sorted[3 * (size_t)i + k] = xyz[3 * (size_t)order[i] + k];
+}
+
+}  // namespace stk

@@ -1,0 +1,291 @@
+"""Python interface mirroring the reference's ctypes binding (Python/PySTKFMM.py).
+
+Same class, method and argument names as ``PySTKFMM.Stk3DFMM``
+(Python/PySTKFMM.py:34-79): ``set_box``, ``get_kernel_dimension``,
+``set_points``, ``setup_tree``, ``evaluate_fmm``, ``clear_fmm``,
+``show_active_kernels``; arrays are C-contiguous float64 numpy arrays of shape
+(n, 3) for coordinates and (n, kdim) for values, and ``evaluate_fmm`` /
+``evaluate_kernel`` add into the target array as the reference does.  Where the
+reference printed a message and called exit(1), these methods raise StkError.
+
+Additions: ``evaluate_kernel`` (STKFMM::evaluateKernel, Lib/src/STKFMM.cpp:88-99),
+``set_precision`` (FP64 / MIXED P2P arithmetic), ``evaluate_near`` (U-list part
+only), ``tree_stats`` and ``ulist``.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from ._lib import P_d, P_f, P_i, P_ll, StkError, check, lib
+
+
+class PAXIS(enum.IntEnum):
+    """Lib/include/STKFMM/STKFMM_common.hpp:29-34"""
+    NONE = 0
+    PX = 1
+    PXY = 2
+    PXYZ = 3
+
+
+class PPKERNEL(enum.IntEnum):
+    """Lib/include/STKFMM/STKFMM_common.hpp:40-44"""
+    SLS2T = 1
+    DLS2T = 2
+    L2T = 4
+
+
+class KERNEL(enum.IntFlag):
+    """Lib/include/STKFMM/STKFMM_common.hpp:46-62"""
+    LapPGrad = 1
+    LapPGradGrad = 2
+    LapQPGradGrad = 4
+    Stokes = 8
+    RPY = 16
+    StokesRegVel = 32
+    StokesRegVelOmega = 64
+    PVel = 128
+    PVelGrad = 256
+    PVelLaplacian = 512
+    Traction = 1024
+
+
+class PRECISION(enum.IntEnum):
+    FP64 = 0
+    MIXED = 1
+
+
+class UKERNEL(enum.IntEnum):
+    """Micro-kernels (one STKFMM uKerEval body each); see include/stkfmm_b200.h."""
+    LAPLACE_P = 0
+    LAPLACE_PGRAD = 1
+    LAPLACE_DIPOLEP = 2
+    LAPLACE_DIPOLEPGRAD = 3
+    STOKES_VEL = 4
+    RPY_U = 5
+    RPY_ULAPU = 6
+    STK_ULAPU = 7
+    STOKES_REGVEL = 8
+    STOKES_PVEL = 9
+    STOKES_DOUBLEPVEL = 10
+    LAPLACE_SLDL_PGRAD = 11
+    STOKES_SLDL_PVEL = 12
+
+
+SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.Stokes, KERNEL.RPY, KERNEL.StokesRegVel, KERNEL.PVel)
+
+
+def _arr(a, cols=None, name="array"):
+    """Return a C-contiguous float64 array (a copy only if needed)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if cols is not None and a.size:
+        a = a.reshape(-1, cols)
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(P_d) if a is not None and a.size else None
+
+
+def get_kernel_dimension(kernel) -> np.ndarray:
+    dims = np.zeros(3, dtype=np.int32)
+    check(lib().stk_get_kernel_dimension(int(kernel), dims.ctypes.data_as(P_i)), "get_kernel_dimension")
+    return dims
+
+
+def get_kernel_name(kernel) -> str:
+    n = lib().stk_get_kernel_name(int(kernel))
+    if n is None:
+        raise StkError(2, "get_kernel_name")
+    return n.decode()
+
+
+def kernel_slot(kernel, slot: int) -> int:
+    return lib().stk_kernel_slot(int(kernel), int(slot))
+
+
+def ukernel_dims(uk) -> tuple:
+    s, t = ctypes.c_int(), ctypes.c_int()
+    check(lib().stk_ukernel_dims(int(uk), ctypes.byref(s), ctypes.byref(t)), "ukernel_dims")
+    return s.value, t.value
+
+
+def device_count() -> int:
+    return lib().stk_device_count()
+
+
+def evaluate_kernel(kernel, p2p, src_coord, src_value, trg_coord, trg_value, precision=PRECISION.FP64):
+    """trg_value += direct sum (STKFMM::evaluateKernel semantics), host arrays, accumulate in place."""
+    sd, dd, td = get_kernel_dimension(kernel)
+    sdim = {PPKERNEL.SLS2T: sd, PPKERNEL.DLS2T: dd, PPKERNEL.L2T: None}[PPKERNEL(p2p)]
+    if sdim is None:
+        uk = kernel_slot(kernel, 6)
+        if uk < 0:
+            raise StkError(2, "evaluate_kernel")
+        sdim = ukernel_dims(uk)[0]
+    src = _arr(src_coord, 3)
+    val = _arr(src_value, sdim)
+    trg = _arr(trg_coord, 3)
+    if not (isinstance(trg_value, np.ndarray) and trg_value.dtype == np.float64 and trg_value.flags.c_contiguous):
+        raise TypeError("trg_value must be a C-contiguous float64 numpy array (accumulated in place)")
+    if len(val) != len(src) or trg_value.size != len(trg) * td:
+        raise StkError(4, "evaluate_kernel")
+    check(lib().stk_evaluate_kernel(int(kernel), int(p2p), len(src), _ptr(src), _ptr(val), len(trg), _ptr(trg),
+                                    _ptr(trg_value), int(precision)), "evaluate_kernel")
+    return trg_value
+
+
+class Stk3DFMM:
+    """B200 counterpart of PySTKFMM.Stk3DFMM (Python/PySTKFMM.py:34-79)."""
+
+    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64):
+        self.mult_order = int(mult_order)
+        self.max_pts = int(max_pts)
+        self.pbc = int(pbc)
+        self.kernels = int(kernels)
+        L = lib()
+        self.fmm = L.Stk3DFMM_create(self.mult_order, self.max_pts, self.pbc, self.kernels)
+        if not self.fmm:
+            status = 6 if L.stk_device_count() <= 0 else 1
+            raise StkError(status, "Stk3DFMM_create")
+        self.set_precision(precision)
+        self._n = (0, 0, 0)
+
+    def __del__(self):
+        f = getattr(self, "fmm", None)
+        if f:
+            lib().Stk3DFMM_destroy(f)
+            self.fmm = None
+
+    def set_precision(self, precision):
+        check(lib().Stk3DFMM_set_precision(self.fmm, int(precision)), "set_precision")
+        self.precision = PRECISION(precision)
+
+    def set_box(self, origin, length):
+        origin = _arr(origin).reshape(3)
+        check(lib().Stk3DFMM_set_box(self.fmm, origin.ctypes.data_as(P_d), float(length)), "set_box")
+
+    def get_kernel_dimension(self, kernel):
+        return get_kernel_dimension(kernel)
+
+    def set_points(self, src_SL_coord, trg_coord, src_DL_coord):
+        sl = _arr(src_SL_coord, 3)
+        trg = _arr(trg_coord, 3)
+        dl = _arr(src_DL_coord, 3) if src_DL_coord is not None else np.zeros((0, 3))
+        check(lib().Stk3DFMM_set_points(self.fmm, len(sl), _ptr(sl), len(trg), _ptr(trg), len(dl), _ptr(dl)),
+              "set_points")
+        self._n = (len(sl), len(dl), len(trg))
+
+    def setup_tree(self, kernel):
+        check(lib().Stk3DFMM_setup_tree(self.fmm, int(kernel)), "setup_tree")
+
+    def clear_fmm(self, kernel):
+        check(lib().Stk3DFMM_clear_fmm(self.fmm, int(kernel)), "clear_fmm")
+
+    def show_active_kernels(self):
+        check(lib().Stk3DFMM_show_active_kernels(self.fmm), "show_active_kernels")
+
+    def _eval(self, fn, name, kernel, src_SL_value, trg_value, src_DL_value):
+        sd, dd, td = get_kernel_dimension(kernel)
+        slv = _arr(src_SL_value, sd)
+        dlv = _arr(src_DL_value, dd) if src_DL_value is not None else np.zeros((0, dd))
+        if not (isinstance(trg_value, np.ndarray) and trg_value.dtype == np.float64 and trg_value.flags.c_contiguous):
+            raise TypeError("trg_value must be a C-contiguous float64 numpy array (accumulated in place)")
+        ntrg = trg_value.size // td if td else 0
+        check(fn(self.fmm, int(kernel), len(slv), _ptr(slv), ntrg, _ptr(trg_value), len(dlv), _ptr(dlv)), name)
+        return trg_value
+
+    def evaluate_fmm(self, kernel, src_SL_value, trg_value, src_DL_value):
+        return self._eval(lib().Stk3DFMM_evaluate_fmm, "evaluate_fmm", kernel, src_SL_value, trg_value, src_DL_value)
+
+    def evaluate_near(self, kernel, src_SL_value, trg_value, src_DL_value):
+        return self._eval(lib().Stk3DFMM_evaluate_near, "evaluate_near", kernel, src_SL_value, trg_value,
+                          src_DL_value)
+
+    def evaluate_near_device(self, kernel, d_sl, d_trg, d_dl=None, stream=None):
+        """Device pointers (ints) in the caller's order; queued on `stream` (a cudaStream_t int or None)."""
+        check(lib().Stk3DFMM_evaluate_near_device(self.fmm, int(kernel), d_sl, d_trg, d_dl, stream),
+              "evaluate_near_device")
+
+    def last_kernel_ms(self, kernel) -> float:
+        ms = ctypes.c_float()
+        check(lib().Stk3DFMM_last_kernel_ms(self.fmm, int(kernel), ctypes.byref(ms)), "last_kernel_ms")
+        return ms.value
+
+    def evaluate_kernel(self, kernel, nThreads, p2p, src_coord, src_value, trg_coord, trg_value):
+        """STKFMM::evaluateKernel through the handle (uses the handle's precision)."""
+        if not (int(kernel) & self.kernels):
+            raise StkError(2, "evaluate_kernel")
+        return evaluate_kernel(kernel, p2p, src_coord, src_value, trg_coord, trg_value, self.precision)
+
+    def tree_stats(self, kernel) -> dict:
+        out = np.zeros(9, dtype=np.int64)
+        check(lib().Stk3DFMM_get_tree_stats(self.fmm, int(kernel), out.ctypes.data_as(P_ll)), "tree_stats")
+        keys = ["nodes", "leaves", "depth", "u_entries", "u_pairs_sl", "u_pairs_dl", "v_entries", "w_entries",
+                "x_entries"]
+        return dict(zip(keys, (int(v) for v in out)))
+
+    def ulist(self, kernel) -> dict:
+        """The U-list of the last setup_tree, in leaf-sorted indices (stk_p2p_lists layout)."""
+        sizes = np.zeros(5, dtype=np.int32)
+        L = lib()
+        nulls = [None] * 11
+        check(L.Stk3DFMM_get_ulist(self.fmm, int(kernel), sizes.ctypes.data_as(P_i), *nulls), "ulist")
+        nn, ne, nsl, ndl, ntrg = (int(v) for v in sizes)
+        arrs = dict(trg_begin=nn, trg_end=nn, list_off=nn + 1, list_ent=ne, sl_begin=nn, sl_end=nn, dl_begin=nn,
+                    dl_end=nn, sl_perm=nsl, dl_perm=ndl, trg_perm=ntrg)
+        out = {k: np.zeros(max(v, 1), dtype=np.int32) for k, v in arrs.items()}
+        check(L.Stk3DFMM_get_ulist(self.fmm, int(kernel), sizes.ctypes.data_as(P_i),
+                                   *[out[k].ctypes.data_as(P_i) for k in arrs]), "ulist")
+        return {k: out[k][:v] for k, v in arrs.items()}
+
+
+class Octree:
+    """Host-only octree + KIFMM lists (no GPU needed); coordinates in [0,1)^3."""
+
+    def __init__(self, tree_pts, max_pts, pbc=0, sl=None, dl=None, trg=None):
+        L = lib()
+        tp = _arr(tree_pts, 3)
+        sl = _arr(sl if sl is not None else np.zeros((0, 3)), 3)
+        dl = _arr(dl if dl is not None else np.zeros((0, 3)), 3)
+        trg = _arr(trg if trg is not None else np.zeros((0, 3)), 3)
+        self.t = L.stk_octree_build(_ptr(tp), len(tp), int(max_pts), int(pbc), _ptr(sl), len(sl), _ptr(dl), len(dl),
+                                    _ptr(trg), len(trg))
+        if not self.t:
+            raise StkError(7, "stk_octree_build")
+        sizes = np.zeros(7, dtype=np.int64)
+        check(L.stk_octree_sizes(self.t, sizes.ctypes.data_as(P_ll)))
+        self.num_nodes, self.num_leaves, self.depth = int(sizes[0]), int(sizes[1]), int(sizes[2])
+        self.list_sizes = dict(U=int(sizes[3]), V=int(sizes[4]), W=int(sizes[5]), X=int(sizes[6]))
+        nn = self.num_nodes
+        self.level = np.zeros(nn, np.int32)
+        self.parent = np.zeros(nn, np.int32)
+        self.first_child = np.zeros(nn, np.int32)
+        self.ixyz = np.zeros((nn, 3), np.int32)
+        check(L.stk_octree_nodes(self.t, self.level.ctypes.data_as(P_i), self.parent.ctypes.data_as(P_i),
+                                 self.first_child.ctypes.data_as(P_i), self.ixyz.ctypes.data_as(P_i)))
+        self.n = (len(sl), len(dl), len(trg))
+
+    def __del__(self):
+        t = getattr(self, "t", None)
+        if t:
+            lib().stk_octree_free(t)
+            self.t = None
+
+    def list(self, which: str):
+        w = "UVWX".index(which)
+        off = np.zeros(self.num_nodes + 1, np.int32)
+        ent = np.zeros(max(self.list_sizes[which], 1), np.int32)
+        check(lib().stk_octree_list(self.t, w, off.ctypes.data_as(P_i), ent.ctypes.data_as(P_i)))
+        return off, ent[:self.list_sizes[which]]
+
+    def point_set(self, k: int):
+        n = self.n[k]
+        perm = np.zeros(max(n, 1), np.int32)
+        b = np.zeros(self.num_nodes, np.int32)
+        e = np.zeros(self.num_nodes, np.int32)
+        check(lib().stk_octree_set(self.t, k, perm.ctypes.data_as(P_i), b.ctypes.data_as(P_i),
+                                   e.ctypes.data_as(P_i)))
+        return perm[:n], b, e

@@ -1,0 +1,111 @@
+"""The CPU oracle pinned against the reference's own kernels (no GPU needed)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from helpers import GOLDEN_MAP, load_golden
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_MAP))
+def test_oracle_matches_golden(name):
+    """The C restatement of each uKerEval reproduces the reference SimpleKernel fixtures."""
+    g = load_golden(name)
+    for uk, osl, vsl in GOLDEN_MAP[name]:
+        for pre in ("", "fixed_"):
+            out = O.direct(uk, g[pre + "src"], g[pre + "val"][:, vsl], g[pre + (
+                "trg")])
+            err = rel_l2(out, g[pre + "out"][:, osl])
+            assert err < 1e-13, (name, O.UK_NAMES[uk], pre, err)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+@pytest.mark.parametrize("which,uk,osl", [
+    (O.REF_STOKES_SL, O.UK_STOKES_VEL, slice(0, 3)),
+    (O.REF_LAP_SL_PGRAD, O.UK_LAPLACE_PGRAD, slice(0, 4)),
+    (O.REF_LAP_DL_PGRAD, O.UK_LAPLACE_DIPOLEPGRAD, slice(0, 4)),
+    (O.REF_STOKES_SL_RPY, O.UK_RPY_ULAPU, slice(0, 6)),
+    (O.REF_STOKES_REG_SL_VEL, O.UK_STOKES_REGVEL, slice(0, 3)),
+    (O.REF_STOKES_SL_PVEL, O.UK_STOKES_PVEL, slice(0, 4)),
+    (O.REF_STOKES_DL_PVEL, O.UK_STOKES_DOUBLEPVEL, slice(0, 4)),
+])
+def test_oracle_matches_live_reference(which, uk, osl, rng):
+    """Fresh random inputs (clustered, with coincident points) through the compiled reference."""
+    src = rng.random((400, 3)) * 0.1 + 0.45
+    trg = np.concatenate([src[:100], rng.random((80, 3))])
+    v = rng.uniform(-1, 1, size=(400, O.REF_DIMS[which][0]))
+    if which in (O.REF_STOKES_SL_RPY, O.REF_STOKES_REG_SL_VEL):
+        v[:, 3] = np.abs(v[:, 3]) * 1e-3
+    ref = O.ref_direct(which, src, v, trg)[:, osl]
+    out = O.direct(uk, src, v[:, :O.UK_SDIM[uk]], trg)
+    assert rel_l2(out, ref) < 1e-13
+
+
+def test_oracle_lists_equals_direct_on_full_list(rng):
+    """A list covering every (target box, source box) pair equals the dense sum."""
+    src = rng.random((300, 3))
+    trg = rng.random((200, 3))
+    v = rng.uniform(-1, 1, (300, 3))
+    sb = np.array([0, 100, 250], np.int32)
+    se = np.array([100, 250, 300], np.int32)
+    tb = np.array([0, 77], np.int32)
+    te = np.array([77, 200], np.int32)
+    off = np.array([0, 3, 6], np.int32)
+    ent = np.array([(s << 5) | 13 for _ in range(2) for s in range(3)], np.int32)
+    out = O.lists(O.UK_STOKES_VEL, tb, te, off, ent >> 5, ent & 31, sb, se, src, v, trg)
+    ref = O.direct(O.UK_STOKES_VEL, src, v, trg)
+    assert rel_l2(out, ref) < 1e-14
+
+
+def test_oracle_periodic_shift(rng):
+    """Shift code s adds s*period to the source coordinate."""
+    src = rng.random((50, 3))
+    trg = rng.random((40, 3))
+    v = rng.uniform(-1, 1, (50, 1))
+    code = (1 + 1) + 3 * (0 + 1) + 9 * (-1 + 1)  # (sx, sy, sz) = (+1, 0, -1)
+    out = O.lists(O.UK_LAPLACE_PGRAD, [0], [40], [0, 1], [0], [code], [0], [50], src, v, trg, period=2.0)
+    ref = O.direct(O.UK_LAPLACE_PGRAD, src + np.array([2.0, 0.0, -2.0]), v, trg)
+    assert rel_l2(out, ref) < 1e-14
+
+
+def test_surface_points():
+    """Cube surface: 6(p-1)^2+2 distinct points, all on the cube boundary, centred on c+alpha*r."""
+    for p in (4, 6, 8, 10, 12):
+        c = np.array([0.25, 0.5, 0.125])
+        pts = O.surface(p, c, 2.95, 2)
+        n = 6 * (p - 1) ** 2 + 2
+        assert pts.shape == (n, 3)
+        r = 0.5 * 0.5 ** 2
+        u = (pts - c) / (2.95 * r) - 1.0  # back to [-1,1]^3
+        assert np.allclose(np.abs(u).max(axis=1), 1.0)
+        assert len(np.unique(np.round(u, 12), axis=0)) == n
+        assert np.allclose(u.mean(axis=0), 0.0, atol=1e-14)
+
+
+def test_regvel_adjoint_finite_difference(rng):
+    """The hand-derived adjoint of the regularized Stokeslet sum against central differences."""
+    ns, nt = 30, 25
+    src = rng.random((ns, 3))
+    trg = np.concatenate([src[:10], rng.random((nt - 10, 3))])
+    sv = rng.uniform(-1, 1, (ns, 4))
+    sv[:, 3] = np.abs(sv[:, 3]) * 0.05 + 0.01
+    w = rng.normal(size=(nt, 3))
+    gf, gx = O.regvel_adjoint(src, sv, trg, w)
+
+    def loss(s, v):
+        return float(np.sum(w * O.direct(O.UK_STOKES_REGVEL, s, v, trg)))
+
+    h = 1e-6
+    for i in (0, 3, 17):
+        for k in range(3):
+            vp, vm = sv.copy(), sv.copy()
+            vp[i, k] += h
+            vm[i, k] -= h
+            fd = (loss(src, vp) - loss(src, vm)) / (2 * h)
+            assert abs(fd - gf[i, k]) <= 1e-6 * max(1.0, abs(fd))
+            sp, sm = src.copy(), src.copy()
+            sp[i, k] += h
+            sm[i, k] -= h
+            # the target copies of points 0..9 stay fixed: this is the source-position gradient
+            fd = (loss(sp, sv) - loss(sm, sv)) / (2 * h)
+            assert abs(fd - gx[i, k]) <= 1e-5 * max(1.0, abs(fd))
