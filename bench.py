@@ -41,11 +41,14 @@ SIGMA = 0.02
 MAX_PTS = 256
 MULT_ORDER = 10
 KERNEL_LAPPGRAD = 1
-# FP32 flops per (target, source point) pair of the fused laplace_pgrad +
-# laplace_dipolepgrad micro-kernel (FMA = 2), counted from stk_ukernels.cuh:
-# displacement 3, r^2 5, Newton step on rsqrt 5, inverse powers 3, r.d 5,
-# q/r^3 1, radial coefficient 3, potential 4, gradient 15.  Plus 1 MUFU rsqrt.
+# Flops per (target, source point) pair of the fused laplace_pgrad +
+# laplace_dipolepgrad micro-kernel (FMA = 2), counted from stk_ukernels.cuh
+# (Uk<UK_LAPLACE_SLDL_PGRAD>::eval): r^2 5, 1/r^2 1, r.d 5, w 2, potential 2,
+# radial coefficient 2, 1/r^3 1, gradient 12 = 30; mixed path adds the hi/lo
+# displacement 9 and the Newton step on the MUFU rsqrt 5 (= 44); the FP64 path
+# adds the plain displacement 3 (= 33) plus one double-precision rsqrt.
 FLOPS_PER_POINT_PAIR_FUSED = 44
+FLOPS_PER_POINT_PAIR_FP64 = 33
 WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clusters (sigma 0.02, centres "
             "U[0.1,0.9]^3), max 256 pts/leaf, p=10, SL=DL=targets")
 
@@ -368,7 +371,7 @@ def b200_arm(args):
     parity64 = float(np.linalg.norm(gpu64 - ref_sorted[sel]) / np.linalg.norm(ref_sorted[sel]))
 
     # ---- roofline of the dominant kernel (the fused mixed P2P kernel) ----
-    peaks = np.zeros(5)
+    peaks = np.zeros(6)
     lib().stk_measure_peaks(peaks.ctypes.data_as(__import__("stkfmm_b200._lib", fromlist=["P_d"]).P_d))
     achieved = point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (kmx * 1e-3) / 1e12
     traffic = None
@@ -401,10 +404,11 @@ def b200_arm(args):
                      "flops_per_point_pair": FLOPS_PER_POINT_PAIR_FUSED,
                      "peak_source": "measured FP32 FMA probe (stk_measure_peaks) on this GPU",
                      "probe": {"fp32_tflops": float(peaks[0]), "fp64_tflops": float(peaks[1]),
-                               "mufu_rsqrt_gops": float(peaks[2]), "probe_sm_mhz": float(peaks[3])},
-                     "fp64_path": {"achieved": point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (k64 * 1e-3) / 1e12,
+                               "mufu_rsqrt_gops": float(peaks[2]), "probe_sm_mhz": float(peaks[3]),
+                               "fp32x2_tflops": float(peaks[5])},
+                     "fp64_path": {"achieved": point_pairs * FLOPS_PER_POINT_PAIR_FP64 / (k64 * 1e-3) / 1e12,
                                    "peak": float(peaks[1]),
-                                   "frac": (point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (k64 * 1e-3) / 1e12)
+                                   "frac": (point_pairs * FLOPS_PER_POINT_PAIR_FP64 / (k64 * 1e-3) / 1e12)
                                    / float(peaks[1]) if peaks[1] > 0 else None}},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes),

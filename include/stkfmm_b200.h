@@ -99,7 +99,7 @@ int stk_device_count(void);
 /* Throughput probes of the running GPU (no reference counterpart; roofline
  * denominators of the P2P kernels): out[0] FP32 TFLOP/s (FMA = 2 flops),
  * out[1] FP64 TFLOP/s, out[2] MUFU rsqrt Gop/s, out[3] SM clock MHz seen by the
- * probe, out[4] SM count. */
+ * probe, out[4] SM count, out[5] packed FP32 (fma.rn.f32x2) TFLOP/s. */
 int stk_measure_peaks(double *out);
 
 /* ---- direct sum (STKFMM::evaluateKernel) --------------------------------- */

@@ -260,6 +260,11 @@ int oracle_lists(int uk, int n_trg_box, const int *trg_begin, const int *trg_end
     nthreads = clamp_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
     for (int b = 0; b < n_trg_box; b++) {
+        /* Boxes without list entries contribute nothing and are skipped: in a
+         * tree, internal nodes (empty lists) overlap their leaves' target
+         * ranges, and touching their targets here would race with the thread
+         * that owns the leaf.  Boxes with entries must be disjoint. */
+        if (list_off[b] == list_off[b + 1]) continue;
         for (int t = trg_begin[b]; t < trg_end[b]; t++) {
             double acc[16] = {0};
             const double *xt = trg_xyz + 3 * (size_t)t;

@@ -12,7 +12,8 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libstkfmm_b200.so")
+# STKFMM_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("STKFMM_B200_LIB") or os.path.join(HERE, "libstkfmm_b200.so")
 
 c_int, c_uint, c_double, c_void_p, c_char_p, c_float, c_longlong = (
     ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_float,
@@ -72,6 +73,8 @@ _lock = threading.Lock()
 
 
 def _stale() -> bool:
+    if os.environ.get("STKFMM_B200_LIB"):
+        return False  # an explicitly chosen build is used as is
     if not os.path.exists(LIB_PATH):
         return True
     import glob

@@ -110,7 +110,7 @@ static int direct_device(int uk, int nsrc, const double *d_src, const double *d_
     double *rec = ws.buf<double>(Workspace::kRec, (size_t)nsrc * rs);
     if (!rec) return STK_ERR_CUDA;
     STK_CUDA(launch_pack_records(nsrc, nullptr, d_src, d_val, sd, nullptr, 0, rs, rec, stream));
-    // work list: 32-target chunks x source chunks
+    // work list: 64-target chunks x source chunks
     std::vector<WorkItem> items;
     std::vector<int> sbeg, send, ent;
     build_direct_items(ntrg, nsrc, ws.num_sms(), items, sbeg, send, ent);
@@ -173,7 +173,7 @@ extern "C" int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, in
 }
 
 // Host-array direct sum for micro-kernel uk (accumulate).  Targets are sorted in
-// Morton order before upload so that 32-target items are compact (tight local
+// Morton order before upload so that 64-target items are compact (tight local
 // origins for the mixed path); results are scattered back to the caller's order.
 static int direct_host(int uk, int nsrc, const double *src, const double *val, int ntrg, const double *trg,
                        double *out, int prec) {

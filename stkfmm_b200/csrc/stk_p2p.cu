@@ -5,23 +5,30 @@
 // FMMData::evaluateKernel (Lib/src/FMMData.cpp:252-283).
 //
 // Design (one warp = one work item, persistent warps):
-//  * A work item is <= 32 targets of one target box plus a range of its
-//    interaction-list entries.  Items are sorted by cost (targets x sources) on
-//    the host, largest first, and persistent warps take them from a global
-//    counter, so uneven adaptive trees balance themselves.
-//  * The warp streams the sources of its list entries through a 32-record
-//    shared-memory tile: lane i loads record i with 16-byte vector loads, the
-//    next tile is prefetched into registers while the current one is consumed.
-//  * Every lane owns one target (or, with fewer than 32 targets, a group of
-//    2^glog lanes owns one target and splits the tile); the group is reduced with
-//    warp shuffles at the end.
-//  * FP64 path: everything in double, r = x_t - (x_s + image shift) exactly as
-//    the oracle forms it.
-//  * Mixed path: when a source record is staged its coordinates are shifted to
-//    the target box's centre in FP64 and rounded to FP32 once; per pair the
-//    displacement is an FP32 difference of two centre-relative coordinates, the
-//    kernel tensor is FP32 with MUFU rsqrt + one Newton step, and each tile's
-//    FP32 partial sum is added into a Kahan-compensated FP32 accumulator.
+//  * A work item is <= 64 targets of one target box plus a range of its
+//    interaction-list entries.  Items are sorted by cost on the host, largest
+//    first; persistent warps take them from a global counter, so uneven
+//    adaptive trees balance themselves.
+//  * Each lane owns two target slots (lane and lane + 32).  With fewer than 64
+//    targets, 2^glog consecutive lanes share a target and split the source
+//    tile; they are reduced with warp shuffles at the end.
+//  * The warp streams the sources of its list entries through a 32-source
+//    shared-memory tile in structure-of-arrays layout: lane i loads source
+//    record i with 16-byte vector loads (the next tile is prefetched into
+//    registers while the current one is consumed), applies the periodic image
+//    shift, computes the per-source staged values (Uk<>::stage) and stores one
+//    row per component.
+//  * FP64 path: one source and two targets per step; r = x_t - (x_s + shift)
+//    formed in double exactly as the oracle forms it.
+//  * Mixed path: at staging each source coordinate, shifted to the target
+//    box's centre c in FP64, is split into FP32 hi + lo parts
+//    (x - c = hi + lo to ~2^-48 relative); targets likewise.  Per pair the
+//    displacement (t_hi - s_hi) + (t_lo - s_lo) is then accurate to FP32
+//    relative precision even for nearly coincident points (t_hi - s_hi is exact
+//    by Sterbenz' lemma when the points are close).  The kernel tensor runs in
+//    Blackwell packed FP32 (fma.rn.f32x2: two sources per instruction) with
+//    MUFU rsqrt + one Newton step; each tile's FP32 partial sums are added into
+//    Kahan-compensated FP32 accumulators.
 #include <algorithm>
 #include <type_traits>
 
@@ -35,11 +42,11 @@ namespace {
 constexpr int kWarpsPerCta = 4;
 constexpr int kThreads = 32 * kWarpsPerCta;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr double kPadCoord = 1.0e4;  // offset of zero-strength padding sources
 
 template <int UK> struct Rec {
     static constexpr int SDIM = Uk<UK>::SDIM;
-    static constexpr int RS = (3 + SDIM + 1) & ~1;   // doubles per global/FP64 record (16-byte multiple)
-    static constexpr int RSF = (3 + SDIM + 3) & ~3;  // floats per FP32 shared-memory record
+    static constexpr int RS = (3 + SDIM + 1) & ~1;  // doubles per global record (16-byte multiple)
 };
 
 // Load N doubles (N even) from 16-byte aligned global memory with double2 loads.
@@ -54,40 +61,49 @@ __device__ __forceinline__ void load_rec_global(double (&r)[N], const double *p)
     }
 }
 
-template <int N>
-__device__ __forceinline__ void load_rec_shared(double (&r)[N], const double *p) {
-#pragma unroll
-    for (int q = 0; q < N / 2; q++) {
-        double2 v = reinterpret_cast<const double2 *>(p)[q];
-        r[2 * q] = v.x;
-        r[2 * q + 1] = v.y;
-    }
-}
+// Resident CTAs per SM requested from the register allocator (1: no
+// constraint; forcing 5 measured slower for the FP64 path and neutral for the
+// mixed path).  STK_MINB_OVERRIDE builds tuning variants.
+template <int UK, bool MIXED> struct MinBlocks {
+#ifdef STK_MINB_OVERRIDE
+    static constexpr int value = STK_MINB_OVERRIDE;
+#else
+    static constexpr int value = 1;
+#endif
+};
 
-template <int N>
-__device__ __forceinline__ void load_rec_shared(float (&r)[N], const float *p) {
-#pragma unroll
-    for (int q = 0; q < N / 4; q++) {
-        float4 v = reinterpret_cast<const float4 *>(p)[q];
-        r[4 * q] = v.x;
-        r[4 * q + 1] = v.y;
-        r[4 * q + 2] = v.z;
-        r[4 * q + 3] = v.w;
-    }
-}
+// How the mixed path forms the displacement (STK_MIXED_DISP selects at build time):
+//   kDispHiLo: FP32 hi + lo parts of the centre-relative coordinates, 3 FP32
+//              operations per coordinate and pair on the FP32 pipe;
+//   kDispF64:  centre-relative coordinates kept in FP64 in shared memory, one
+//              FP64 subtraction and one FP64->FP32 rounding per coordinate and
+//              pair, on the otherwise idle FP64 pipe.
+constexpr int kDispHiLo = 0, kDispF64 = 1;
+#ifdef STK_MIXED_DISP
+constexpr int kMixedDisp = STK_MIXED_DISP;
+#else
+constexpr int kMixedDisp = kDispHiLo;
+#endif
+static_assert(kMixedDisp == kDispHiLo || kMixedDisp == kDispF64, "STK_MIXED_DISP must be 0 or 1");
 
 template <int UK, bool MIXED>
-__global__ void __launch_bounds__(kThreads) list_p2p_kernel(const ListP2PArgs a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2p_kernel(const ListP2PArgs a) {
     using K = Uk<UK>;
-    constexpr int SDIM = K::SDIM;
     constexpr int TDIM = K::TDIM;
+    constexpr int NV = K::NV;
     constexpr int RS = Rec<UK>::RS;
-    using R = typename std::conditional<MIXED, float, double>::type;
-    constexpr int SREC = MIXED ? Rec<UK>::RSF : RS;
+    constexpr bool HILO = MIXED && kMixedDisp == kDispHiLo;
+    // shared tile, one row per component: coordinates (FP64, or FP32 hi x3 + lo x3)
+    // and staged values (FP64 path: double, mixed path: float)
+    constexpr int NCC = HILO ? 6 : 3;
+    using CT = typename std::conditional<HILO, float, double>::type;
+    using S = typename std::conditional<MIXED, float, double>::type;
 
-    __shared__ __align__(16) R tile[kWarpsPerCta][32 * SREC];
+    __shared__ __align__(16) CT tcoord[kWarpsPerCta][NCC][32];
+    __shared__ __align__(16) S tval[kWarpsPerCta][NV][32];
     const int lane = threadIdx.x & 31;
-    R *my = tile[threadIdx.x >> 5];
+    CT(*mc)[32] = tcoord[threadIdx.x >> 5];
+    S(*mv)[32] = tval[threadIdx.x >> 5];
 
     for (;;) {
         int it = 0;
@@ -97,27 +113,47 @@ __global__ void __launch_bounds__(kThreads) list_p2p_kernel(const ListP2PArgs a)
         const WorkItem w = a.items[it];
         const int glog = w.glog;
         const int g = 1 << glog;
-        const int ti = lane >> glog;
         const int sub = lane & (g - 1);
-        const bool active = ti < w.nt;
-        const int t = w.t0 + (active ? ti : 0);
+        const int ti0 = lane >> glog, ti1 = (lane + 32) >> glog;
+        const bool act0 = ti0 < w.nt, act1 = ti1 < w.nt;
+        const int t0 = w.t0 + (act0 ? ti0 : 0), t1 = w.t0 + (act1 ? ti1 : 0);
 
-        const double xt = a.trg_xyz[3 * (size_t)t + 0];
-        const double yt = a.trg_xyz[3 * (size_t)t + 1];
-        const double zt = a.trg_xyz[3 * (size_t)t + 2];
-        double cx = 0.0, cy = 0.0, cz = 0.0;
+        double c[3] = {0.0, 0.0, 0.0};
         if constexpr (MIXED) {
             // local origin: the target box centre, or the item's first target
             const double *o = a.box_centre ? a.box_centre + 3 * (size_t)w.trg_box : a.trg_xyz + 3 * (size_t)w.t0;
-            cx = o[0];
-            cy = o[1];
-            cz = o[2];
+            c[0] = o[0];
+            c[1] = o[1];
+            c[2] = o[2];
         }
-        const R tx = R(xt - cx), ty = R(yt - cy), tz = R(zt - cz);
-
-        R acc[TDIM], comp[TDIM];
+        double xt0[3], xt1[3];
 #pragma unroll
-        for (int k = 0; k < TDIM; k++) acc[k] = comp[k] = R(0);
+        for (int k = 0; k < 3; k++) {
+            xt0[k] = a.trg_xyz[3 * (size_t)t0 + k];
+            xt1[k] = a.trg_xyz[3 * (size_t)t1 + k];
+        }
+
+        // accumulators: FP64 path sums directly; mixed path keeps Kahan sum + compensation
+        S acc0[TDIM], acc1[TDIM], cmp0[TDIM], cmp1[TDIM];
+#pragma unroll
+        for (int k = 0; k < TDIM; k++) acc0[k] = acc1[k] = cmp0[k] = cmp1[k] = S(0);
+        F2 th0[3], tl0[3], th1[3], tl1[3];  // hi/lo targets (HILO)
+        double tr0[3], tr1[3];               // centre-relative targets (FP64 displacement)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            tr0[k] = xt0[k] - c[k];
+            tr1[k] = xt1[k] - c[k];
+        }
+        if constexpr (HILO) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float h0 = (float)tr0[k], h1 = (float)tr1[k];
+                th0[k] = splat(h0);
+                tl0[k] = splat((float)(tr0[k] - (double)h0));
+                th1[k] = splat(h1);
+                tl1[k] = splat((float)(tr1[k] - (double)h1));
+            }
+        }
 
         // ---- tile iterator over the source records of entries [e0, e1) ----
         int e = w.e0, base = 0, end = 0;
@@ -143,35 +179,37 @@ __global__ void __launch_bounds__(kThreads) list_p2p_kernel(const ListP2PArgs a)
 
         while (have) {
             const int n = min(32, end - base);
-            // stage this lane's record of the current tile
-            if (lane < n) {
-                const double sx = rn[0] + shx, sy = rn[1] + shy, sz = rn[2] + shz;
-                R *d = my + lane * SREC;
-                if constexpr (MIXED) {
-                    float4 *d4 = reinterpret_cast<float4 *>(d);
-                    float v[SREC];
-                    v[0] = float(sx - cx);
-                    v[1] = float(sy - cy);
-                    v[2] = float(sz - cz);
-#pragma unroll
-                    for (int q = 0; q < SDIM; q++) v[3 + q] = float(rn[3 + q]);
-#pragma unroll
-                    for (int q = 3 + SDIM; q < SREC; q++) v[q] = 0.0f;
-#pragma unroll
-                    for (int q = 0; q < SREC / 4; q++) d4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            // ---- stage: lane i writes source i of the tile (or zero-strength padding) ----
+            {
+                double v[NV];
+                double x[3];
+                if (lane < n) {
+                    x[0] = rn[0] + shx;
+                    x[1] = rn[1] + shy;
+                    x[2] = rn[2] + shz;
+                    K::stage(rn + 3, v);
                 } else {
-                    double2 *d2 = reinterpret_cast<double2 *>(d);
-                    double v[RS];
-                    v[0] = sx;
-                    v[1] = sy;
-                    v[2] = sz;
 #pragma unroll
-                    for (int q = 3; q < RS; q++) v[q] = rn[q];
+                    for (int k = 0; k < 3; k++) x[k] = c[k] + kPadCoord;
 #pragma unroll
-                    for (int q = 0; q < RS / 2; q++) d2[q] = make_double2(v[2 * q], v[2 * q + 1]);
+                    for (int q = 0; q < NV; q++) v[q] = 0.0;
                 }
+                if constexpr (HILO) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        const double d = x[k] - c[k];
+                        const float h = (float)d;
+                        mc[k][lane] = h;
+                        mc[3 + k][lane] = (float)(d - (double)h);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) mc[k][lane] = x[k] - c[k];  // c = 0 on the FP64 path
+                }
+#pragma unroll
+                for (int q = 0; q < NV; q++) mv[q][lane] = (S)v[q];
             }
-            // advance to the next tile and prefetch it
+            // ---- advance to the next tile and prefetch it ----
             base += 32;
             if (base >= end) {
                 e++;
@@ -185,57 +223,99 @@ __global__ void __launch_bounds__(kThreads) list_p2p_kernel(const ListP2PArgs a)
             if (have && lane < end - base) load_rec_global(rn, a.src_rec + (size_t)(base + lane) * RS);
             __syncwarp();
 
-            if (active) {
-                if constexpr (MIXED) {
-                    R part[TDIM];
+            // ---- consume the tile ----
+            if constexpr (MIXED) {
+                F2 p0[TDIM], p1[TDIM];
 #pragma unroll
-                    for (int k = 0; k < TDIM; k++) part[k] = R(0);
-#pragma unroll 4
-                    for (int j = sub; j < n; j += g) {
-                        R s[SREC];
-                        load_rec_shared(s, my + j * SREC);
-                        K::eval(part, tx - s[0], ty - s[1], tz - s[2], s + 3);
-                    }
-                    // Kahan-compensated accumulation of the tile's partial sum
+                for (int k = 0; k < TDIM; k++) p0[k] = p1[k] = splat(0.0f);
+                // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
+#pragma unroll 2
+                for (int j = 2 * sub; j < n; j += 2 * g) {
+                    F2 s[NV];
 #pragma unroll
-                    for (int k = 0; k < TDIM; k++) {
-                        const R y = part[k] - comp[k];
-                        const R tt = acc[k] + y;
-                        comp[k] = (tt - acc[k]) - y;
-                        acc[k] = tt;
+                    for (int q = 0; q < NV; q++) s[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
+                    if constexpr (HILO) {
+                        F2 sh[3], sl[3];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
+                            sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
+                        }
+                        K::eval(p0, (th0[0] - sh[0]) + (tl0[0] - sl[0]), (th0[1] - sh[1]) + (tl0[1] - sl[1]),
+                                (th0[2] - sh[2]) + (tl0[2] - sl[2]), s);
+                        K::eval(p1, (th1[0] - sh[0]) + (tl1[0] - sl[0]), (th1[1] - sh[1]) + (tl1[1] - sl[1]),
+                                (th1[2] - sh[2]) + (tl1[2] - sl[2]), s);
+                    } else {
+                        double2 sx[3];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
+                        K::eval(p0, mk((float)(tr0[0] - sx[0].x), (float)(tr0[0] - sx[0].y)),
+                                mk((float)(tr0[1] - sx[1].x), (float)(tr0[1] - sx[1].y)),
+                                mk((float)(tr0[2] - sx[2].x), (float)(tr0[2] - sx[2].y)), s);
+                        K::eval(p1, mk((float)(tr1[0] - sx[0].x), (float)(tr1[0] - sx[0].y)),
+                                mk((float)(tr1[1] - sx[1].x), (float)(tr1[1] - sx[1].y)),
+                                mk((float)(tr1[2] - sx[2].x), (float)(tr1[2] - sx[2].y)), s);
                     }
-                } else {
-#pragma unroll 4
-                    for (int j = sub; j < n; j += g) {
-                        R s[SREC];
-                        load_rec_shared(s, my + j * SREC);
-                        K::eval(acc, tx - s[0], ty - s[1], tz - s[2], s + 3);
-                    }
+                }
+                // Kahan-compensated accumulation of the tile's partial sums
+#pragma unroll
+                for (int k = 0; k < TDIM; k++) {
+                    float y = (p0[k].v.x + p0[k].v.y) - cmp0[k];
+                    float tt = acc0[k] + y;
+                    cmp0[k] = (tt - acc0[k]) - y;
+                    acc0[k] = tt;
+                    y = (p1[k].v.x + p1[k].v.y) - cmp1[k];
+                    tt = acc1[k] + y;
+                    cmp1[k] = (tt - acc1[k]) - y;
+                    acc1[k] = tt;
+                }
+            } else {
+#pragma unroll 2
+                for (int j = sub; j < n; j += g) {
+                    double s[NV];
+#pragma unroll
+                    for (int q = 0; q < NV; q++) s[q] = mv[q][j];
+                    const double sx = mc[0][j], sy = mc[1][j], sz = mc[2][j];
+                    K::eval(acc0, xt0[0] - sx, xt0[1] - sy, xt0[2] - sz, s);
+                    K::eval(acc1, xt1[0] - sx, xt1[1] - sy, xt1[2] - sz, s);
                 }
             }
             __syncwarp();
         }
 
         // ---- reduce the lanes that share a target, then accumulate ----
-        double out[TDIM];
+        double o0[TDIM], o1[TDIM];
 #pragma unroll
         for (int k = 0; k < TDIM; k++) {
-            if constexpr (MIXED) out[k] = double(acc[k]) - double(comp[k]);
-            else out[k] = acc[k];
+            if constexpr (MIXED) {
+                o0[k] = double(acc0[k]) - double(cmp0[k]);
+                o1[k] = double(acc1[k]) - double(cmp1[k]);
+            } else {
+                o0[k] = acc0[k];
+                o1[k] = acc1[k];
+            }
         }
         for (int o = 1; o < g; o <<= 1) {
 #pragma unroll
-            for (int k = 0; k < TDIM; k++) out[k] += __shfl_xor_sync(kFull, out[k], o);
-        }
-        if (active && sub == 0) {
-            double *dst = a.trg_out + (size_t)t * TDIM;
-#pragma unroll
             for (int k = 0; k < TDIM; k++) {
-                const double v = K::SCALE * out[k];
-                if (a.atomic_out)
-                    atomicAdd(dst + k, v);
-                else
-                    dst[k] += v;
+                o0[k] += __shfl_xor_sync(kFull, o0[k], o);
+                o1[k] += __shfl_xor_sync(kFull, o1[k], o);
+            }
+        }
+        if (sub == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const bool act = h ? act1 : act0;
+                if (!act) continue;
+                double *dst = a.trg_out + (size_t)(h ? t1 : t0) * TDIM;
+#pragma unroll
+                for (int k = 0; k < TDIM; k++) {
+                    const double val = K::SCALE * K::comp_scale(k) * (h ? o1[k] : o0[k]);
+                    if (a.atomic_out)
+                        atomicAdd(dst + k, val);
+                    else
+                        dst[k] += val;
+                }
             }
         }
     }

@@ -7,13 +7,14 @@ namespace stk {
 
 enum Precision : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
-// One unit of P2P work: up to 32 targets of one target box against source-list
-// entries [e0, e1).  glog = log2(lanes per target): the lanes that share a
-// target split the source tile and are reduced with warp shuffles.
+// One unit of P2P work: up to 64 targets of one target box against source-list
+// entries [e0, e1).  A warp has 64 target slots (two per lane); glog =
+// log2(slots per target) <= 5: the lanes that share a target split the source
+// tile and are reduced with warp shuffles.
 struct WorkItem {
     int trg_box;
     int t0;   // first target (leaf-sorted index)
-    int nt;   // number of targets (1..32)
+    int nt;   // number of targets (1..64)
     int glog; // lanes per target = 1 << glog
     int e0;   // first list entry
     int e1;   // one past the last list entry

@@ -41,6 +41,21 @@ __global__ void fp64_fma_kernel(double *out, int iters, double a, double b) {
     if (s == 1234.5) out[threadIdx.x] = s;
 }
 
+__global__ void fp32x2_fma_kernel(float *out, int iters, float a, float b) {
+    float2 x[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; c++) x[c] = make_float2(threadIdx.x * 1e-7f + c, c + 0.5f);
+    const float2 av = make_float2(a, a), bv = make_float2(b, b);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int c = 0; c < kChains; c++) x[c] = __ffma2_rn(x[c], av, bv);
+    }
+    float s = 0;
+#pragma unroll
+    for (int c = 0; c < kChains; c++) s += x[c].x + x[c].y;
+    if (s == 1234.5f) out[threadIdx.x] = s;
+}
+
 __global__ void mufu_rsqrt_kernel(float *out, int iters) {
     float x[kChains];
 #pragma unroll
@@ -91,7 +106,8 @@ float time_ms(F launch, cudaStream_t s) {
 }  // namespace
 
 // out[0] FP32 TFLOP/s (FMA = 2), out[1] FP64 TFLOP/s, out[2] MUFU rsqrt Gop/s,
-// out[3] SM clock in MHz measured by clock64 / globaltimer, out[4] SM count.
+// out[3] SM clock in MHz measured by clock64 / globaltimer, out[4] SM count,
+// out[5] packed FP32 (fma.rn.f32x2) TFLOP/s.
 extern "C" int stk_measure_peaks(double *out) {
     if (!out) return STK_ERR_INVALID_ARG;
     int dev = 0, sms = 0;
@@ -114,6 +130,8 @@ extern "C" int stk_measure_peaks(double *out) {
     out[1] = nthr * it64 * kChains * 2.0 / (ms * 1e-3) / 1e12;
     ms = time_ms([&] { mufu_rsqrt_kernel<<<blocks, threads, 0, s>>>(fbuf, itmu); }, s);
     out[2] = nthr * itmu * kChains / (ms * 1e-3) / 1e9;
+    ms = time_ms([&] { fp32x2_fma_kernel<<<blocks, threads, 0, s>>>(fbuf, it32 / 2, 0.999f, 1e-3f); }, s);
+    out[5] = nthr * (it32 / 2) * kChains * 4.0 / (ms * 1e-3) / 1e12;
     clock_kernel<<<1, 1, 0, s>>>(cbuf, 20000000LL);
     long long h[2] = {0, 1};
     cudaMemcpy(h, cbuf, sizeof(h), cudaMemcpyDeviceToHost);

@@ -1,9 +1,22 @@
 // stk_ukernels.cuh -- STKFMM pair micro-kernels as sm_100a device functions.
 //
-// Each struct restates one STKFMM "uKerEval" body (one (target, source) pair,
-// unscaled, accumulated) for a real type R (double for the FP64 path, float for
-// the mixed path).  r = x_trg - x_src.  The self-interaction mask of the
-// reference (approx_rsqrt<digits>(r2, r2 > 0)) becomes a select on r2 > 0.
+// Each struct restates one STKFMM "uKerEval" body: the contribution of one
+// source to one target, r = x_trg - x_src, unscaled, accumulated.  The bodies are
+// written once for a value type V and instantiated twice:
+//   V = double : the plain FP64 path (one source, one target);
+//   V = F2     : the mixed path, Blackwell packed FP32 (fma.rn.f32x2 & co.),
+//                two sources against one target per instruction.
+// The algebra is regrouped to use fewer operations than the reference's
+// expressions (e.g. u = rinv (f + r (f.r)/r^2) for the Stokeslet); both
+// precision paths share it, and the FP64 path still matches the reference
+// bodies to ~1e-15 (checked by the parity tests against the oracle, which
+// keeps the reference's own operation order).
+//
+// Source values are "staged" once per source before the pair loop
+// (Uk<ID>::stage): derived per-source quantities (2q, symmetric parts of the
+// double-layer tensor, a^2/3, eps^2 ...) are computed there, not per pair.
+// Target components may carry a constant factor applied after the sum
+// (Uk<ID>::comp_scale), e.g. the pressure's factor 2.
 //
 // Reference bodies:
 //   laplace_p            Lib/include/STKFMM/LaplaceLayerKernel.hpp:41-65
@@ -17,34 +30,54 @@
 //   stokes_regvel        Lib/include/STKFMM/StokesRegSingleLayerKernel.hpp:17-41
 //   stokes_pvel          Lib/include/STKFMM/StokesSingleLayerKernel.hpp:27-47
 //   stokes_doublepvel    Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:25-57
-// Two fused variants (no reference counterpart as one function) evaluate a
-// single-layer and a double-layer source that sit at the same point in one pass,
-// sharing r^2 and 1/r:  laplace_pgrad + laplace_dipolepgrad, and
-// stokes_pvel + stokes_doublepvel.
+// Two fused variants (no single reference function) evaluate a single-layer
+// and a double-layer source at the same point in one pass:
+//   laplace_pgrad + laplace_dipolepgrad, stokes_pvel + stokes_doublepvel.
 #pragma once
 #include <cuda_runtime.h>
 
 namespace stk {
 
-// ---- masked reciprocal square root -----------------------------------------
-template <class R> struct RSqrt;
-
-template <> struct RSqrt<double> {
-    // FP64 path: CUDA's double-precision rsqrt, masked at r2 == 0.
-    static __device__ __forceinline__ double eval(double r2) { return r2 > 0.0 ? rsqrt(r2) : 0.0; }
+// ---------------------------------------------------------------------------
+// packed FP32 pair (two sources in one register pair)
+// ---------------------------------------------------------------------------
+struct F2 {
+    float2 v;
 };
+__device__ __forceinline__ F2 splat(float a) { return {make_float2(a, a)}; }
+__device__ __forceinline__ F2 mk(float a, float b) { return {make_float2(a, b)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return {__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return {__fmul2_rn(a.v, b.v)}; }
+// a - b as one exactly rounded fma(b, -1, a)
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return {__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ F2 fmav(F2 a, F2 b, F2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ double fmav(double a, double b, double c) { return fma(a, b, c); }
 
-template <> struct RSqrt<float> {
-    // Mixed path: hardware approximate rsqrt (MUFU) plus one Newton-Raphson step
-    // y <- y (3 - r2 y^2) / 2, masked at r2 == 0 (select, so inf never leaks).
-    static __device__ __forceinline__ float eval(float r2) {
-        float y;
-        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r2));
-        float h = r2 * y;
-        y = y * fmaf(-0.5f * h, y, 1.5f);
-        return r2 > 0.0f ? y : 0.0f;
-    }
-};
+template <class V> __device__ __forceinline__ V cst(double c);
+template <> __device__ __forceinline__ double cst<double>(double c) { return c; }
+template <> __device__ __forceinline__ F2 cst<F2>(double c) { return splat((float)c); }
+
+// masked reciprocal square root: 0 where r2 == 0 (the reference's
+// approx_rsqrt<digits>(r2, r2 > 0))
+__device__ __forceinline__ double rsq(double r2) { return r2 > 0.0 ? rsqrt(r2) : 0.0; }
+
+// Mixed path: hardware approximate rsqrt (MUFU, one per lane half) plus one
+// Newton-Raphson step y <- y (3 - r2 y^2) / 2 in packed FP32.  Pairs closer
+// than the smallest normal FP32 r^2 (|r| < 1.1e-19) count as coincident.
+__device__ __forceinline__ F2 rsq(F2 r2) {
+    float y0, y1;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(r2.v.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(r2.v.y));
+    F2 y = mk(y0, y1);
+    F2 h = r2 * splat(-0.5f);
+    F2 t = fmav(h, y * y, splat(1.5f));
+    y = y * t;
+    y.v.x = r2.v.x >= 1.17549435e-38f ? y.v.x : 0.0f;
+    y.v.y = r2.v.y >= 1.17549435e-38f ? y.v.y : 0.0f;
+    return y;
+}
+
+template <class V> __device__ __forceinline__ V norm2(V dx, V dy, V dz) { return fmav(dx, dx, fmav(dy, dy, dz * dz)); }
 
 // micro-kernel ids, identical to enum stk_ukernel in include/stkfmm_b200.h
 enum UkId : int {
@@ -59,257 +92,329 @@ enum UkId : int {
     UK_STOKES_REGVEL = 8,
     UK_STOKES_PVEL = 9,
     UK_STOKES_DOUBLEPVEL = 10,
-    UK_LAPLACE_SLDL_PGRAD = 11,  // fused laplace_pgrad (q) + laplace_dipolepgrad (d), values (q, d)
-    UK_STOKES_SLDL_PVEL = 12,    // fused stokes_pvel (f, trD) + stokes_doublepvel (D), values (f, trD, D)
+    UK_LAPLACE_SLDL_PGRAD = 11,  // values (q, d0, d1, d2)
+    UK_STOKES_SLDL_PVEL = 12,    // values (f0, f1, f2, trD, D00 .. D22)
     UK_COUNT = 13
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
 constexpr double kInv8Pi = 0.039788735772973833942220940843128591;  // 1/(8 pi)
+// the reference's truncated 1/3 of rpy_u / rpy_ulapu (RPYKernel.hpp:30,66)
+constexpr double kRpyThird = 0.3333333333333;
 
 template <int ID> struct Uk;
 
+// laplace_p: u0 += q / r
 template <> struct Uk<UK_LAPLACE_P> {
-    static constexpr int SDIM = 1, TDIM = 1;
+    static constexpr int SDIM = 1, TDIM = 1, NV = 1;
     static constexpr double SCALE = kInv4Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        u[0] += f[0] * rinv;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { v[0] = f[0]; }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        u[0] = fmav(v[0], rinv, u[0]);
     }
 };
 
+// laplace_pgrad: p = q/r, grad p = -q r / r^3.  staged (q, -q)
 template <> struct Uk<UK_LAPLACE_PGRAD> {
-    static constexpr int SDIM = 1, TDIM = 4;
+    static constexpr int SDIM = 1, TDIM = 4, NV = 2;
     static constexpr double SCALE = kInv4Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R sv = f[0] * rinv * rinv * rinv;
-        u[0] += sv * r2;
-        u[1] -= sv * dx;
-        u[2] -= sv * dy;
-        u[3] -= sv * dz;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = -f[0];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        u[0] = fmav(v[0], rinv, u[0]);
+        V w = (v[1] * (rinv * rinv)) * rinv;
+        u[1] = fmav(w, dx, u[1]);
+        u[2] = fmav(w, dy, u[2]);
+        u[3] = fmav(w, dz, u[3]);
     }
 };
 
+// laplace_dipolep: p = (d.r) / r^3
 template <> struct Uk<UK_LAPLACE_DIPOLEP> {
-    static constexpr int SDIM = 3, TDIM = 1;
+    static constexpr int SDIM = 3, TDIM = 1, NV = 3;
     static constexpr double SCALE = kInv4Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R rdotn = f[0] * dx + f[1] * dy + f[2] * dz;
-        u[0] += rinv3 * rdotn;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rdn = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        u[0] = fmav(rdn, (rinv * rinv) * rinv, u[0]);
     }
 };
 
+// laplace_dipolepgrad: p = (d.r)/r^3, grad p = (d - 3 (d.r) r / r^2) / r^3
 template <> struct Uk<UK_LAPLACE_DIPOLEPGRAD> {
-    static constexpr int SDIM = 3, TDIM = 4;
+    static constexpr int SDIM = 3, TDIM = 4, NV = 3;
     static constexpr double SCALE = kInv4Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv2 = rinv * rinv;
-        R rinv3 = rinv2 * rinv;
-        R rinv5 = rinv3 * rinv2;
-        R rdotn = f[0] * dx + f[1] * dy + f[2] * dz;
-        R three = R(3);
-        u[0] += rdotn * rinv3;
-        u[1] += (f[0] * r2 - three * rdotn * dx) * rinv5;
-        u[2] += (f[1] * r2 - three * rdotn * dy) * rinv5;
-        u[3] += (f[2] * r2 - three * rdotn * dz) * rinv5;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rdn = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        u[0] = fmav(rdn, rinv3, u[0]);
+        V nA = (rdn * rinv2) * cst<V>(-3.0);
+        u[1] = fmav(fmav(nA, dx, v[0]), rinv3, u[1]);
+        u[2] = fmav(fmav(nA, dy, v[1]), rinv3, u[2]);
+        u[3] = fmav(fmav(nA, dz, v[2]), rinv3, u[3]);
     }
 };
 
+// stokes_vel (Stokeslet): u = (f + r (f.r)/r^2) / r
 template <> struct Uk<UK_STOKES_VEL> {
-    static constexpr int SDIM = 3, TDIM = 3;
+    static constexpr int SDIM = 3, TDIM = 3, NV = 3;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R fdotr_rinv3 = (f[0] * dx + f[1] * dy + f[2] * dz) * rinv3;
-        u[0] += f[0] * rinv + dx * fdotr_rinv3;
-        u[1] += f[1] * rinv + dy * fdotr_rinv3;
-        u[2] += f[2] * rinv + dz * fdotr_rinv3;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V c = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * (rinv * rinv);
+        u[0] = fmav(fmav(c, dx, v[0]), rinv, u[0]);
+        u[1] = fmav(fmav(c, dy, v[1]), rinv, u[1]);
+        u[2] = fmav(fmav(c, dz, v[2]), rinv, u[2]);
     }
 };
 
+// rpy_u: u = f (1/r + a^2/3 / r^3) + r (f.r)/r^2 (1/r - a^2 / r^3).
+// staged (f, a^2/3, -a^2) with the reference's truncated 1/3
 template <> struct Uk<UK_RPY_U> {
-    static constexpr int SDIM = 4, TDIM = 3;
+    static constexpr int SDIM = 4, TDIM = 3, NV = 5;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R rinv5 = rinv3 * rinv * rinv;
-        R fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
-        R three_fdotr_rinv5 = R(3) * fdotr * rinv5;
-        R a2_over_three = R(0.3333333333333) * f[3] * f[3];  // the reference's truncated 1/3
-        u[0] += (r2 * f[0] + dx * fdotr) * rinv3 + a2_over_three * (f[0] * rinv3 - three_fdotr_rinv5 * dx);
-        u[1] += (r2 * f[1] + dy * fdotr) * rinv3 + a2_over_three * (f[1] * rinv3 - three_fdotr_rinv5 * dy);
-        u[2] += (r2 * f[2] + dz * fdotr) * rinv3 + a2_over_three * (f[2] * rinv3 - three_fdotr_rinv5 * dz);
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = kRpyThird * f[3] * f[3];
+        v[4] = -3.0 * v[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * rinv2;
+        V P = fmav(v[3], rinv3, rinv);
+        V Q = c * fmav(v[4], rinv3, rinv);
+        u[0] = fmav(Q, dx, fmav(v[0], P, u[0]));
+        u[1] = fmav(Q, dy, fmav(v[1], P, u[1]));
+        u[2] = fmav(Q, dz, fmav(v[2], P, u[2]));
     }
 };
 
+// rpy_ulapu: C = (f - 3 r (f.r)/r^2) / r^3, u = (f + r (f.r)/r^2)/r + a^2/3 C,
+// lap u = 2 C (the factor 2 applied after the sum).  staged (f, a^2/3)
 template <> struct Uk<UK_RPY_ULAPU> {
-    static constexpr int SDIM = 4, TDIM = 6;
+    static constexpr int SDIM = 4, TDIM = 6, NV = 4;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R rinv5 = rinv3 * rinv * rinv;
-        R fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
-        R fdotr_rinv3 = fdotr * rinv3;
-        R three_fdotr_rinv5 = R(3) * fdotr * rinv5;
-        R a2_over_three = R(0.3333333333333) * f[3] * f[3];
-        R cx = f[0] * rinv3 - three_fdotr_rinv5 * dx;
-        R cy = f[1] * rinv3 - three_fdotr_rinv5 * dy;
-        R cz = f[2] * rinv3 - three_fdotr_rinv5 * dz;
-        u[0] += f[0] * rinv + dx * fdotr_rinv3 + a2_over_three * cx;
-        u[1] += f[1] * rinv + dy * fdotr_rinv3 + a2_over_three * cy;
-        u[2] += f[2] * rinv + dz * fdotr_rinv3 + a2_over_three * cz;
-        u[3] += R(2) * cx;
-        u[4] += R(2) * cy;
-        u[5] += R(2) * cz;
+    static __host__ __device__ constexpr double comp_scale(int k) { return k >= 3 ? 2.0 : 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = kRpyThird * f[3] * f[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * rinv2;
+        V nc3 = c * cst<V>(-3.0);
+        V Cx = fmav(nc3, dx, v[0]) * rinv3;
+        V Cy = fmav(nc3, dy, v[1]) * rinv3;
+        V Cz = fmav(nc3, dz, v[2]) * rinv3;
+        u[0] = fmav(v[3], Cx, fmav(fmav(c, dx, v[0]), rinv, u[0]));
+        u[1] = fmav(v[3], Cy, fmav(fmav(c, dy, v[1]), rinv, u[1]));
+        u[2] = fmav(v[3], Cz, fmav(fmav(c, dz, v[2]), rinv, u[2]));
+        u[3] = u[3] + Cx;
+        u[4] = u[4] + Cy;
+        u[5] = u[5] + Cz;
     }
 };
 
+// stk_ulapu: u = (f + r (f.r)/r^2)/r, lap u = 2 (f - 3 r (f.r)/r^2)/r^3
 template <> struct Uk<UK_STK_ULAPU> {
-    static constexpr int SDIM = 3, TDIM = 6;
+    static constexpr int SDIM = 3, TDIM = 6, NV = 3;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R rinv5 = rinv3 * rinv * rinv;
-        R fdotr = f[0] * dx + f[1] * dy + f[2] * dz;
-        R fdotr_rinv3 = fdotr * rinv3;
-        R three_fdotr_rinv5 = R(3) * fdotr * rinv5;
-        u[0] += f[0] * rinv + dx * fdotr_rinv3;
-        u[1] += f[1] * rinv + dy * fdotr_rinv3;
-        u[2] += f[2] * rinv + dz * fdotr_rinv3;
-        u[3] += R(2) * (f[0] * rinv3 - three_fdotr_rinv5 * dx);
-        u[4] += R(2) * (f[1] * rinv3 - three_fdotr_rinv5 * dy);
-        u[5] += R(2) * (f[2] * rinv3 - three_fdotr_rinv5 * dz);
+    static __host__ __device__ constexpr double comp_scale(int k) { return k >= 3 ? 2.0 : 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * rinv2;
+        V nc3 = c * cst<V>(-3.0);
+        u[0] = fmav(fmav(c, dx, v[0]), rinv, u[0]);
+        u[1] = fmav(fmav(c, dy, v[1]), rinv, u[1]);
+        u[2] = fmav(fmav(c, dz, v[2]), rinv, u[2]);
+        u[3] = fmav(fmav(nc3, dx, v[0]), rinv3, u[3]);
+        u[4] = fmav(fmav(nc3, dy, v[1]), rinv3, u[4]);
+        u[5] = fmav(fmav(nc3, dz, v[2]), rinv3, u[5]);
     }
 };
 
+// stokes_regvel: R^2 = r^2 + eps^2, u = ((R^2 + eps^2) f + r (f.r)) / R^3; the
+// self term is kept (mask on R^2).  staged (f, eps^2)
 template <> struct Uk<UK_STOKES_REGVEL> {
-    static constexpr int SDIM = 4, TDIM = 3;
+    static constexpr int SDIM = 4, TDIM = 3, NV = 4;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R reg2 = f[3] * f[3];
-        R r2 = dx * dx + dy * dy + dz * dz + reg2;  // self term kept (mask on r^2 + eps^2)
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R r2reg2 = r2 + reg2;
-        R cc = f[0] * dx + f[1] * dy + f[2] * dz;
-        u[0] += rinv3 * (r2reg2 * f[0] + dx * cc);
-        u[1] += rinv3 * (r2reg2 * f[1] + dy * cc);
-        u[2] += rinv3 * (r2reg2 * f[2] + dz * cc);
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = f[3] * f[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V R2 = fmav(dx, dx, fmav(dy, dy, fmav(dz, dz, v[3])));
+        V rinv = rsq(R2);
+        V rinv3 = (rinv * rinv) * rinv;
+        V al = (R2 + v[3]) * rinv3;
+        V be = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * rinv3;
+        u[0] = fmav(be, dx, fmav(al, v[0], u[0]));
+        u[1] = fmav(be, dy, fmav(al, v[1], u[1]));
+        u[2] = fmav(be, dz, fmav(al, v[2], u[2]));
     }
 };
 
+// stokes_pvel: p = 2 (f.r)/r^3 (factor 2 after the sum),
+// u = f / r + r ((f.r) - trD) / r^3.  values (f, trD)
 template <> struct Uk<UK_STOKES_PVEL> {
-    static constexpr int SDIM = 4, TDIM = 4;
+    static constexpr int SDIM = 4, TDIM = 4, NV = 4;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv3 = rinv * rinv * rinv;
-        R cc = f[0] * dx + f[1] * dy + f[2] * dz;
-        u[0] += R(2) * cc * rinv3;
-        cc -= f[3];
-        u[1] += rinv3 * (r2 * f[0] + dx * cc);
-        u[2] += rinv3 * (r2 * f[1] + dy * cc);
-        u[3] += rinv3 * (r2 * f[2] + dz * cc);
+    static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = f[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv3 = (rinv * rinv) * rinv;
+        V fdr = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        u[0] = fmav(fdr, rinv3, u[0]);
+        V c = (fdr - v[3]) * rinv3;
+        u[1] = fmav(c, dx, fmav(v[0], rinv, u[1]));
+        u[2] = fmav(c, dy, fmav(v[1], rinv, u[2]));
+        u[3] = fmav(c, dz, fmav(v[2], rinv, u[3]));
     }
 };
 
+// stokes_doublepvel: m = r^T D r / r^2, p = 2 (tr D - 3 m) / r^3 (factor 2
+// after the sum), u = -3 m r / r^3.  staged symmetric parts
+// (D00, D11, D22, D01+D10, D02+D20, D12+D21, tr D)
 template <> struct Uk<UK_STOKES_DOUBLEPVEL> {
-    static constexpr int SDIM = 9, TDIM = 4;
+    static constexpr int SDIM = 9, TDIM = 4, NV = 7;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv2 = rinv * rinv;
-        R rinv5 = rinv2 * rinv2 * rinv;
-        R cc = f[0] * dx * dx + f[4] * dy * dy + f[8] * dz * dz;
-        cc += (f[1] + f[3]) * dx * dy;
-        cc += (f[2] + f[6]) * dx * dz;
-        cc += (f[5] + f[7]) * dy * dz;
-        cc *= R(-3) * rinv5;
-        R trace = f[0] + f[4] + f[8];
-        u[0] += R(2) * (cc + r2 * rinv5 * trace);
-        u[1] += dx * cc;
-        u[2] += dy * cc;
-        u[3] += dz * cc;
+    static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[4];
+        v[2] = f[8];
+        v[3] = f[1] + f[3];
+        v[4] = f[2] + f[6];
+        v[5] = f[5] + f[7];
+        v[6] = f[0] + f[4] + f[8];
+    }
+    template <class V> static __device__ __forceinline__ V rdr(V dx, V dy, V dz, const V *s) {
+        V a = fmav(s[4], dz, fmav(s[3], dy, s[0] * dx));
+        V b = fmav(s[5], dz, s[1] * dy);
+        return fmav(dx, a, fmav(dy, b, dz * (s[2] * dz)));
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V nm3 = (rdr(dx, dy, dz, v) * rinv2) * cst<V>(-3.0);
+        u[0] = fmav(v[6] + nm3, rinv3, u[0]);
+        V w = nm3 * rinv3;
+        u[1] = fmav(w, dx, u[1]);
+        u[2] = fmav(w, dy, u[2]);
+        u[3] = fmav(w, dz, u[3]);
     }
 };
 
+// laplace_pgrad + laplace_dipolepgrad at one point, values (q, d):
+// w = q + (d.r)/r^2, p = w / r, grad p = (d - r (q + 3 (d.r)/r^2)) / r^3.
+// staged (q, 2q, d)
 template <> struct Uk<UK_LAPLACE_SLDL_PGRAD> {
-    static constexpr int SDIM = 4, TDIM = 4;  // values (q, dx, dy, dz)
+    static constexpr int SDIM = 4, TDIM = 4, NV = 5;
     static constexpr double SCALE = kInv4Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv2 = rinv * rinv;
-        R rinv3 = rinv2 * rinv;
-        R rinv5 = rinv3 * rinv2;
-        R rdotn = f[1] * dx + f[2] * dy + f[3] * dz;
-        R qr3 = f[0] * rinv3;
-        R c = R(3) * rdotn * rinv5 + qr3;  // single-layer gradient and dipole radial part together
-        u[0] += qr3 * r2 + rdotn * rinv3;
-        u[1] += f[1] * r2 * rinv5 - c * dx;
-        u[2] += f[2] * r2 * rinv5 - c * dy;
-        u[3] += f[3] * r2 * rinv5 - c * dz;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = 2.0 * f[0];
+        v[2] = f[1];
+        v[3] = f[2];
+        v[4] = f[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rdn = fmav(v[2], dx, fmav(v[3], dy, v[4] * dz));
+        V w = fmav(rdn, rinv2, v[0]);
+        u[0] = fmav(w, rinv, u[0]);
+        V nA = fmav(w, cst<V>(-3.0), v[1]);  // -(q + 3 (d.r)/r^2)
+        V rinv3 = rinv2 * rinv;
+        u[1] = fmav(fmav(nA, dx, v[2]), rinv3, u[1]);
+        u[2] = fmav(fmav(nA, dy, v[3]), rinv3, u[2]);
+        u[3] = fmav(fmav(nA, dz, v[4]), rinv3, u[3]);
     }
 };
 
+// stokes_pvel + stokes_doublepvel at one point, values (f, trD, D):
+// m = r^T D r / r^2, p = 2 ((f.r) + tr D - 3 m) / r^3,
+// u = f / r + r ((f.r) - trD - 3 m) / r^3.  staged (f, trD, D symmetric parts, tr D)
 template <> struct Uk<UK_STOKES_SLDL_PVEL> {
-    static constexpr int SDIM = 13, TDIM = 4;  // values (fx, fy, fz, trD, D00..D22)
+    static constexpr int SDIM = 13, TDIM = 4, NV = 11;
     static constexpr double SCALE = kInv8Pi;
-    template <class R>
-    static __device__ __forceinline__ void eval(R (&u)[TDIM], R dx, R dy, R dz, const R *f) {
-        R r2 = dx * dx + dy * dy + dz * dz;
-        R rinv = RSqrt<R>::eval(r2);
-        R rinv2 = rinv * rinv;
-        R rinv3 = rinv2 * rinv;
-        R rinv5 = rinv3 * rinv2;
-        const R *D = f + 4;
-        R cc = f[0] * dx + f[1] * dy + f[2] * dz;
-        R dd = D[0] * dx * dx + D[4] * dy * dy + D[8] * dz * dz;
-        dd += (D[1] + D[3]) * dx * dy;
-        dd += (D[2] + D[6]) * dx * dz;
-        dd += (D[5] + D[7]) * dy * dz;
-        dd *= R(-3) * rinv5;
-        R trace = D[0] + D[4] + D[8];
-        u[0] += R(2) * (cc * rinv3 + dd + r2 * rinv5 * trace);
-        R c2 = (cc - f[3]) * rinv3 + dd;
-        R r2rinv3 = r2 * rinv3;
-        u[1] += r2rinv3 * f[0] + dx * c2;
-        u[2] += r2rinv3 * f[1] + dy * c2;
-        u[3] += r2rinv3 * f[2] + dz * c2;
+    static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = f[3];
+        Uk<UK_STOKES_DOUBLEPVEL>::stage(f + 4, v + 4);
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V fdr = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        V nm3 = (Uk<UK_STOKES_DOUBLEPVEL>::rdr(dx, dy, dz, v + 4) * rinv2) * cst<V>(-3.0);
+        V fm = fdr + nm3;
+        u[0] = fmav(fm + v[10], rinv3, u[0]);
+        V c = (fm - v[3]) * rinv3;
+        u[1] = fmav(c, dx, fmav(v[0], rinv, u[1]));
+        u[2] = fmav(c, dy, fmav(v[1], rinv, u[2]));
+        u[3] = fmav(c, dz, fmav(v[2], rinv, u[3]));
     }
 };
 
-// Host/device table of dimensions, for launch-time checks.
+// Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
          : id == UK_LAPLACE_DIPOLEPGRAD ? 3 : id == UK_STOKES_VEL ? 3 : id == UK_RPY_U ? 4

@@ -71,16 +71,19 @@ unsigned int *Workspace::counter() { return cur_ ? cur_->counter : nullptr; }
 int Workspace::num_sms() { return cur_ ? cur_->sms : 1; }
 cudaStream_t Workspace::stream() { return cur_ ? cur_->stream : nullptr; }
 
+// A warp has 64 target slots (two per lane); items hold at most kItemTargets targets.
+constexpr int kItemTargets = 64;
+
 static inline int lanes_log2(int m) {
-    // largest g = 2^glog with m * g <= 32
+    // largest g = 2^glog <= 32 with m * g <= 64 slots
     int glog = 0;
-    while (glog < 5 && (m << (glog + 1)) <= 32) glog++;
+    while (glog < 5 && (m << (glog + 1)) <= kItemTargets) glog++;
     return glog;
 }
 
 void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &items, std::vector<int> &src_begin,
                         std::vector<int> &src_end, std::vector<int> &ent) {
-    const int nchunk = (ntrg + 31) / 32;
+    const int nchunk = (ntrg + kItemTargets - 1) / kItemTargets;
     // enough items to fill every warp slot several times over, but source
     // chunks of at least 256 points
     const long long want_items = (long long)std::max(num_sms, 1) * 64;
@@ -101,8 +104,8 @@ void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &
     items.reserve((size_t)nchunk * nsc);
     // full chunks first (largest cost), the ragged last chunk at the end
     for (int c = 0; c < nchunk; c++) {
-        const int t0 = 32 * c;
-        const int m = std::min(32, ntrg - t0);
+        const int t0 = kItemTargets * c;
+        const int m = std::min(kItemTargets, ntrg - t0);
         for (int k = 0; k < nsc; k++) items.push_back({c, t0, m, lanes_log2(m), k, k + 1});
     }
 }
@@ -123,11 +126,25 @@ void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, c
         }
         if (ns == 0) continue;
         pairs += (long long)nt * ns;
-        for (int t0 = trg_begin[b]; t0 < trg_end[b]; t0 += 32) {
-            const int m = std::min(32, trg_end[b] - t0);
+        // Split the box into full 64-target items, then power-of-two chunks of
+        // the remainder (32, 16, 8 targets; the last < 8 targets together): a
+        // chunk of m = 2^k targets fills all 64 slots with 64/m lanes per target,
+        // so the box costs ~nt/64 warp passes over its sources instead of
+        // ceil(nt/64).  Chunks below 8 targets would mostly re-stage sources.
+        int t0 = trg_begin[b];
+        int left = nt;
+        while (left > 0) {
+            int m = kItemTargets;
+            if (left < kItemTargets) {
+                m = 1;
+                while (m * 2 <= left) m *= 2;
+                if (m < 8) m = left;
+            }
             const int glog = lanes_log2(m);
             items.push_back({b, t0, m, glog, list_off[b], list_off[b + 1]});
             cost.push_back((double)ns / (1 << glog) + 64.0 * (list_off[b + 1] - list_off[b]));
+            t0 += m;
+            left -= m;
         }
     }
     std::vector<int> idx(items.size());

@@ -39,7 +39,7 @@ class Workspace {
     void *raw(int slot, size_t bytes);
 };
 
-// Direct sum as a list problem: 32-target chunks x source chunks.
+// Direct sum as a list problem: 64-target chunks x source chunks.
 void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &items, std::vector<int> &src_begin,
                         std::vector<int> &src_end, std::vector<int> &ent);
 

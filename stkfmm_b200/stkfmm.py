@@ -119,12 +119,11 @@ def device_count() -> int:
 def evaluate_kernel(kernel, p2p, src_coord, src_value, trg_coord, trg_value, precision=PRECISION.FP64):
     """trg_value += direct sum (STKFMM::evaluateKernel semantics), host arrays, accumulate in place."""
     sd, dd, td = get_kernel_dimension(kernel)
-    sdim = {PPKERNEL.SLS2T: sd, PPKERNEL.DLS2T: dd, PPKERNEL.L2T: None}[PPKERNEL(p2p)]
-    if sdim is None:
-        uk = kernel_slot(kernel, 6)
-        if uk < 0:
-            raise StkError(2, "evaluate_kernel")
-        sdim = ukernel_dims(uk)[0]
+    # the sub-kernel must exist before the value layout can be checked (FMMData.cpp:261-273)
+    uk = kernel_slot(kernel, {PPKERNEL.SLS2T: 0, PPKERNEL.DLS2T: 1, PPKERNEL.L2T: 6}[PPKERNEL(p2p)])
+    if uk < 0:
+        raise StkError(2, "evaluate_kernel")
+    sdim = {PPKERNEL.SLS2T: sd, PPKERNEL.DLS2T: dd, PPKERNEL.L2T: ukernel_dims(uk)[0]}[PPKERNEL(p2p)]
     src = _arr(src_coord, 3)
     val = _arr(src_value, sdim)
     trg = _arr(trg_coord, 3)

@@ -57,6 +57,30 @@ def test_oracle_lists_equals_direct_on_full_list(rng):
     assert rel_l2(out, ref) < 1e-14
 
 
+def test_oracle_lists_on_tree_repeatable():
+    """Tree lists include internal nodes whose (empty-list) target ranges overlap
+    their leaves: the threaded oracle must give the same result every time, equal
+    to a plain numpy sum over the leaves."""
+    from helpers import clustered_points
+    from stkfmm_b200 import Octree
+    rng = np.random.default_rng(4)
+    pts = clustered_points(rng, 3000, nclusters=4, sigma=0.05)
+    t = Octree(pts, 24, 0, sl=pts, trg=pts)
+    sp, sb, se = t.point_set(0)
+    tp, tb, te = t.point_set(2)
+    off, ent = t.list("U")
+    src, trg = pts[sp], pts[tp]
+    q = rng.uniform(-1, 1, (len(pts), 1))
+    ref = np.zeros((len(pts), 4))
+    for b in range(t.num_nodes):
+        for e in ent[off[b]:off[b + 1]]:
+            s = e >> 5
+            ref[tb[b]:te[b]] += O.direct(O.UK_LAPLACE_PGRAD, src[sb[s]:se[s]], q[sb[s]:se[s]], trg[tb[b]:te[b]])
+    for _ in range(8):
+        out = O.lists(O.UK_LAPLACE_PGRAD, tb, te, off, ent >> 5, ent & 31, sb, se, src, q, trg, nthreads=8)
+        assert rel_l2(out, ref) < 1e-14
+
+
 def test_oracle_periodic_shift(rng):
     """Shift code s adds s*period to the source coordinate."""
     src = rng.random((50, 3))
