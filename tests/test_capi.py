@@ -1,0 +1,77 @@
+"""The C ABI library on a machine without a GPU: it loads, exports every symbol
+include/stkfmm_b200.h declares, describes the kernels as the reference does, and
+refuses to compute without a device (there is no CPU path)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import stkfmm_b200 as S
+from conftest import cuda_available
+from stkfmm_b200._lib import LIB_PATH, SIGNATURES, lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "stkfmm_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
+    return sorted(set(n for n in names if n.startswith(("stk_", "Stk3DFMM_"))))
+
+
+def test_header_symbols_exported():
+    names = declared_functions()
+    assert len(names) >= 40
+    so = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in names if not hasattr(so, n)]
+    assert not missing, missing
+    # every declared function has a Python signature, and vice versa
+    bound = {n for n, _, _ in SIGNATURES}
+    assert set(names) <= bound, sorted(set(names) - bound)
+
+
+def test_kernel_descriptors_match_reference():
+    # (kdimSL, kdimDL, kdimTrg) from getKernelDimension (Lib/src/STKFMM.cpp:33-40)
+    expect = {1: (1, 3, 4), 8: (3, 6, 3), 16: (4, 7, 6), 32: (4, 7, 3), 128: (4, 9, 4), 256: (4, 9, 16),
+              512: (4, 9, 7), 1024: (4, 9, 9), 2: (1, 3, 10), 4: (9, 12, 10), 64: (7, 10, 6)}
+    for k, d in expect.items():
+        assert tuple(S.get_kernel_dimension(k)) == d
+    assert S.get_kernel_name(S.KERNEL.LapPGrad) == "laplace_PGrad"
+    assert S.get_kernel_name(S.KERNEL.Stokes) == "stokes_vel"
+    assert S.get_kernel_name(S.KERNEL.RPY) == "rpy_ulapu"
+    assert S.get_kernel_name(S.KERNEL.StokesRegVel) == "stokes_regvel"
+    assert S.get_kernel_name(S.KERNEL.PVel) == "stokes_PVel"
+    with pytest.raises(S.StkError):
+        S.get_kernel_dimension(3)
+    # slot compositions (RPYKernel.hpp:137-154): s2t rpy_ulapu, s2m rpy_u, m2x stokes_vel, m2t/l2t stk_ulapu
+    assert [S.kernel_slot(16, s) for s in range(9)] == [6, -1, 5, -1, 4, 7, 7, 5, -1]
+    # LapPGrad (LaplaceLayerKernel.hpp:314-326)
+    assert [S.kernel_slot(1, s) for s in range(9)] == [1, 3, 0, 2, 0, 1, 1, 0, 2]
+    # StokesRegVel (StokesRegSingleLayerKernel.hpp:211-218)
+    assert [S.kernel_slot(32, s) for s in range(9)] == [8, -1, 8, -1, 4, 4, 4, 8, -1]
+    assert S.ukernel_dims(S.UKERNEL.STOKES_SLDL_PVEL) == (13, 4)
+
+
+def test_status_strings():
+    L = lib()
+    for st in range(9):
+        assert L.stk_status_string(st)
+    assert L.stk_status_string(6).decode().startswith("no CUDA device")
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-device behaviour")
+def test_no_cpu_fallback():
+    L = lib()
+    assert L.stk_device_count() == 0
+    src = np.random.default_rng(0).random((10, 3))
+    out = np.zeros((10, 3))
+    with pytest.raises(S.StkError) as e:
+        S.evaluate_kernel(S.KERNEL.Stokes, S.PPKERNEL.SLS2T, src, src, src, out)
+    assert e.value.status == 6
+    assert np.all(out == 0)
+    with pytest.raises(S.StkError):
+        S.Stk3DFMM(8, 64, 0, S.KERNEL.Stokes)
+    assert not L.Stk3DFMM_create(8, 64, 0, 8)
