@@ -117,6 +117,20 @@ int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, int nsrc, con
 int stk_ukernel_direct_device(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
                               int ntrg, const double *d_trg_coord, double *d_trg_value, int precision,
                               void *stream);
+/* The same direct sum for callers that cannot allocate device memory while they
+ * run: code being captured into a CUDA graph (cudaMalloc/cudaFree are not
+ * capturable and synchronise the device), frameworks whose own allocator owns
+ * the device, hosts that forbid run-time allocation.  No reference counterpart.
+ * It calls no cudaMalloc/cudaFree: all scratch lives in one fixed 8 MiB array
+ * that the library reserves on every GPU where it is loaded.  Sizes whose
+ * scratch (work list + nsrc packed source records) exceeds 8 MiB are refused
+ * with STK_ERR_SIZE (about 130k sources for 8-double records).  The first call
+ * on a device looks the array up (cudaGetSymbolAddress) and should come before
+ * any stream capture.  Work is queued on `stream` without a host wait.  All
+ * calls share the array: calls that overlap on the GPU race; outputs accumulate. */
+int stk_ukernel_direct_device_noalloc(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
+                                      int ntrg, const double *d_trg_coord, double *d_trg_value, int precision,
+                                      void *stream);
 
 /* ---- list-level P2P ---------------------------------------------------------
  * One micro-kernel over an explicit interaction list (device pointers):

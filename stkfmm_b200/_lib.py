@@ -37,6 +37,8 @@ SIGNATURES = [
                                            c_int, c_void_p]),
     ("stk_ukernel_direct_device", c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
                                           c_void_p]),
+    ("stk_ukernel_direct_device_noalloc", c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                                  c_int, c_void_p]),
     ("stk_p2p_lists", c_int, [c_int, c_int, c_int, P_i, P_i, P_i, P_i, c_int, P_i, P_i, c_int, c_void_p, c_void_p,
                               c_int, c_void_p, c_void_p, c_double, c_void_p]),
     ("Stk3DFMM_create", c_void_p, [c_int, c_int, c_int, c_uint]),
