@@ -80,7 +80,16 @@ enum stk_ukernel {
     STK_UK_STOKES_PVEL = 9,         /* 4 -> 4   StokesSingleLayerKernel.hpp:27-47           */
     STK_UK_STOKES_DOUBLEPVEL = 10,  /* 9 -> 4   StokesDoubleLayerKernel.hpp:25-57           */
     STK_UK_LAPLACE_SLDL_PGRAD = 11, /* 1+3 -> 4 laplace_pgrad + laplace_dipolepgrad at one point */
-    STK_UK_STOKES_SLDL_PVEL = 12    /* 4+9 -> 4 stokes_pvel + stokes_doublepvel at one point     */
+    STK_UK_STOKES_SLDL_PVEL = 12,   /* 4+9 -> 4 stokes_pvel + stokes_doublepvel at one point     */
+    /* Adjoint of stokes_regvel (no reference counterpart).  Both read 3 or 4
+     * values per OUTPUT point (stk_ukernel_aux_dim) and evaluate at the
+     * displacement (output point - input point):
+     *   ADJ_SRC: outputs = forward sources with values (f, eps), inputs = forward
+     *            targets with values w = dL/du  ->  (dL/df 3, dL/deps 1, dL/dx_src 3)
+     *   ADJ_TRG: outputs = forward targets with values w, inputs = forward sources
+     *            with values (f, eps)  ->  dL/dx_trg 3 */
+    STK_UK_REGVEL_ADJ_SRC = 13,     /* 3 -> 7, 4 values per output point */
+    STK_UK_REGVEL_ADJ_TRG = 14      /* 4 -> 3, 3 values per output point */
 };
 
 /* ---- kernel descriptors --------------------------------------------------- */
@@ -95,6 +104,8 @@ const char *stk_get_kernel_name(unsigned kernel);
  * RPYKernel.hpp:137-154, LaplaceLayerKernel.hpp:314-326. */
 int stk_kernel_slot(unsigned kernel, int slot);
 int stk_ukernel_dims(int ukernel, int *sdim, int *tdim);
+/* values per output point a micro-kernel reads (0 for all but the adjoint kernels) */
+int stk_ukernel_aux_dim(int ukernel);
 int stk_device_count(void);
 /* Throughput probes of the running GPU (no reference counterpart; roofline
  * denominators of the P2P kernels): out[0] FP32 TFLOP/s (FMA = 2 flops),
@@ -117,6 +128,11 @@ int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, int nsrc, con
 int stk_ukernel_direct_device(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
                               int ntrg, const double *d_trg_coord, double *d_trg_value, int precision,
                               void *stream);
+/* Direct sum of a micro-kernel that reads values per output point (the adjoint
+ * kernels): d_trg_aux holds stk_ukernel_aux_dim(ukernel) doubles per target. */
+int stk_ukernel_direct_aux_device(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
+                                  int ntrg, const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value,
+                                  int precision, void *stream);
 /* The same direct sum for callers that cannot allocate device memory while they
  * run: code being captured into a CUDA graph (cudaMalloc/cudaFree are not
  * capturable and synchronise the device), frameworks whose own allocator owns
@@ -144,6 +160,12 @@ int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begi
                   const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
                   const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value, int ntrg,
                   const double *d_trg_coord, double *d_trg_value, double period, void *stream);
+/* The same for micro-kernels with per-output-point values (the adjoint kernels). */
+int stk_p2p_lists_aux(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
+                      const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
+                      const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value, int ntrg,
+                      const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value, double period,
+                      void *stream);
 
 /* ---- Stk3DFMM handle (Lib/include/STKFMM/STKFMM.h, Lib/src/Stk3DFMM-c.cpp) -- */
 typedef struct Stk3DFMM Stk3DFMM;

@@ -30,6 +30,7 @@ SIGNATURES = [
     ("stk_get_kernel_name", c_char_p, [c_uint]),
     ("stk_kernel_slot", c_int, [c_uint, c_int]),
     ("stk_ukernel_dims", c_int, [c_int, P_i, P_i]),
+    ("stk_ukernel_aux_dim", c_int, [c_int]),
     ("stk_device_count", c_int, []),
     ("stk_measure_peaks", c_int, [P_d]),
     ("stk_evaluate_kernel", c_int, [c_uint, c_uint, c_int, P_d, P_d, c_int, P_d, P_d, c_int]),
@@ -41,6 +42,10 @@ SIGNATURES = [
                                                   c_int, c_void_p]),
     ("stk_p2p_lists", c_int, [c_int, c_int, c_int, P_i, P_i, P_i, P_i, c_int, P_i, P_i, c_int, c_void_p, c_void_p,
                               c_int, c_void_p, c_void_p, c_double, c_void_p]),
+    ("stk_p2p_lists_aux", c_int, [c_int, c_int, c_int, P_i, P_i, P_i, P_i, c_int, P_i, P_i, c_int, c_void_p,
+                                  c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
+    ("stk_ukernel_direct_aux_device", c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                              c_void_p, c_int, c_void_p]),
     ("Stk3DFMM_create", c_void_p, [c_int, c_int, c_int, c_uint]),
     ("Stk3DFMM_destroy", None, [c_void_p]),
     ("Stk3DFMM_set_points", c_int, [c_void_p, c_int, P_d, c_int, P_d, c_int, P_d]),

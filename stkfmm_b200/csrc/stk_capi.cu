@@ -84,6 +84,8 @@ extern "C" int stk_ukernel_dims(int uk, int *sdim, int *tdim) {
     return STK_OK;
 }
 
+extern "C" int stk_ukernel_aux_dim(int uk) { return (uk < 0 || uk >= UK_COUNT) ? -1 : uk_tvdim_host(uk); }
+
 #define STK_CUDA(call)                                                                                     \
     do {                                                                                                   \
         cudaError_t e_ = (call);                                                                           \
@@ -97,11 +99,13 @@ extern "C" int stk_ukernel_dims(int uk, int *sdim, int *tdim) {
 // direct sum on device pointers
 // ---------------------------------------------------------------------------
 static int direct_device(int uk, int nsrc, const double *d_src, const double *d_val, int ntrg, const double *d_trg,
-                         double *d_out, int prec, cudaStream_t stream, Workspace &ws) {
+                         double *d_out, int prec, cudaStream_t stream, Workspace &ws,
+                         const double *d_trg_aux = nullptr) {
     if (uk < 0 || uk >= UK_COUNT || nsrc < 0 || ntrg < 0) return STK_ERR_INVALID_ARG;
     if (prec != PREC_FP64 && prec != PREC_MIXED) return STK_ERR_INVALID_ARG;
     if (nsrc == 0 || ntrg == 0) return STK_OK;
     if (!d_src || !d_val || !d_trg || !d_out) return STK_ERR_INVALID_ARG;
+    if ((uk_tvdim_host(uk) > 0) != (d_trg_aux != nullptr)) return STK_ERR_INVALID_ARG;
     int rc = ws.ensure_device();
     if (rc) return rc;
     const int sd = uk_sdim_host(uk);
@@ -136,6 +140,7 @@ static int direct_device(int uk, int nsrc, const double *d_src, const double *d_
     a.box_centre = nullptr;  // per-item origin: the item's first target
     a.period = 1.0;
     a.atomic_out = sbeg.size() > 1 ? 1 : 0;
+    a.trg_aux = d_trg_aux;
     STK_CUDA(launch_list_p2p(uk, prec, a, ws.num_sms(), stream));
     // the host staging vectors die at return: make the async copies complete first
     STK_CUDA(cudaStreamSynchronize(stream));
@@ -147,6 +152,14 @@ extern "C" int stk_ukernel_direct_device(int ukernel, int nsrc, const double *d_
                                          void *stream) {
     return direct_device(ukernel, nsrc, d_src_coord, d_src_value, ntrg, d_trg_coord, d_trg_value, precision,
                          (cudaStream_t)stream, Workspace::thread_local_ws());
+}
+
+extern "C" int stk_ukernel_direct_aux_device(int ukernel, int nsrc, const double *d_src_coord,
+                                             const double *d_src_value, int ntrg, const double *d_trg_coord,
+                                             const double *d_trg_aux, double *d_trg_value, int precision,
+                                             void *stream) {
+    return direct_device(ukernel, nsrc, d_src_coord, d_src_value, ntrg, d_trg_coord, d_trg_value, precision,
+                         (cudaStream_t)stream, Workspace::thread_local_ws(), d_trg_aux);
 }
 
 static int pick_ppkernel(unsigned kernel, unsigned ppkernel, int &uk) {
@@ -177,7 +190,7 @@ extern "C" int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, in
 // origins for the mixed path); results are scattered back to the caller's order.
 static int direct_host(int uk, int nsrc, const double *src, const double *val, int ntrg, const double *trg,
                        double *out, int prec) {
-    if (uk < 0 || uk >= UK_COUNT || nsrc < 0 || ntrg < 0) return STK_ERR_INVALID_ARG;
+    if (uk < 0 || uk >= UK_COUNT || nsrc < 0 || ntrg < 0 || uk_tvdim_host(uk) > 0) return STK_ERR_INVALID_ARG;
     if (prec != PREC_FP64 && prec != PREC_MIXED) return STK_ERR_INVALID_ARG;
     if (nsrc == 0 || ntrg == 0) return STK_OK;
     if (!src || !val || !trg || !out) return STK_ERR_INVALID_ARG;
@@ -220,10 +233,11 @@ extern "C" int stk_evaluate_kernel(unsigned kernel, unsigned ppkernel, int nsrc,
 // ---------------------------------------------------------------------------
 // list-level P2P
 // ---------------------------------------------------------------------------
-extern "C" int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
-                             const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
-                             const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value,
-                             int ntrg, const double *d_trg_coord, double *d_trg_value, double period, void *stream) {
+static int p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
+                     const int *list_off, const int *list_ent, int n_src_box, const int *src_begin, const int *src_end,
+                     int nsrc, const double *d_src_coord, const double *d_src_value, int ntrg,
+                     const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value, double period,
+                     void *stream) {
     if (ukernel < 0 || ukernel >= UK_COUNT || n_trg_box < 0 || n_src_box < 0 || nsrc < 0 || ntrg < 0)
         return STK_ERR_INVALID_ARG;
     if (precision != PREC_FP64 && precision != PREC_MIXED) return STK_ERR_INVALID_ARG;
@@ -245,6 +259,7 @@ extern "C" int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const in
     }
     if (nsrc > 0 && (!d_src_coord || !d_src_value)) return STK_ERR_INVALID_ARG;
     if (!d_trg_coord || !d_trg_value) return STK_ERR_INVALID_ARG;
+    if ((uk_tvdim_host(ukernel) > 0) != (d_trg_aux != nullptr)) return STK_ERR_INVALID_ARG;
     Workspace &ws = Workspace::thread_local_ws();
     int rc = ws.ensure_device();
     if (rc) return rc;
@@ -278,9 +293,28 @@ extern "C" int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const in
     a.box_centre = nullptr;
     a.period = period;
     a.atomic_out = 0;
+    a.trg_aux = d_trg_aux;
     STK_CUDA(launch_list_p2p(ukernel, precision, a, ws.num_sms(), s));
     STK_CUDA(cudaStreamSynchronize(s));
     return STK_OK;
+}
+
+extern "C" int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
+                             const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
+                             const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value,
+                             int ntrg, const double *d_trg_coord, double *d_trg_value, double period, void *stream) {
+    return p2p_lists(ukernel, precision, n_trg_box, trg_begin, trg_end, list_off, list_ent, n_src_box, src_begin,
+                     src_end, nsrc, d_src_coord, d_src_value, ntrg, d_trg_coord, nullptr, d_trg_value, period, stream);
+}
+
+extern "C" int stk_p2p_lists_aux(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,
+                                 const int *list_off, const int *list_ent, int n_src_box, const int *src_begin,
+                                 const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value,
+                                 int ntrg, const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value,
+                                 double period, void *stream) {
+    return p2p_lists(ukernel, precision, n_trg_box, trg_begin, trg_end, list_off, list_ent, n_src_box, src_begin,
+                     src_end, nsrc, d_src_coord, d_src_value, ntrg, d_trg_coord, d_trg_aux, d_trg_value, period,
+                     stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -44,6 +44,15 @@ constexpr int kThreads = 32 * kWarpsPerCta;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kPadCoord = 1.0e4;  // offset of zero-strength padding sources
 
+// Number of staged per-output-point values of a micro-kernel (1 as a dummy
+// array size when it has none).
+template <class K, class = void> struct NtvOf {
+    static constexpr int value = 1;
+};
+template <class K> struct NtvOf<K, std::void_t<decltype(K::NTV)>> {
+    static constexpr int value = K::NTV;
+};
+
 template <int UK> struct Rec {
     static constexpr int SDIM = Uk<UK>::SDIM;
     static constexpr int RS = (3 + SDIM + 1) & ~1;  // doubles per global record (16-byte multiple)
@@ -91,6 +100,8 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
     using K = Uk<UK>;
     constexpr int TDIM = K::TDIM;
     constexpr int NV = K::NV;
+    constexpr int TV = K::TV;  // per-output-point values (adjoint kernels)
+    constexpr int NTV = NtvOf<K>::value;
     constexpr int RS = Rec<UK>::RS;
     constexpr bool HILO = MIXED && kMixedDisp == kDispHiLo;
     // shared tile, one row per component: coordinates (FP64, or FP32 hi x3 + lo x3)
@@ -132,6 +143,36 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
             xt0[k] = a.trg_xyz[3 * (size_t)t0 + k];
             xt1[k] = a.trg_xyz[3 * (size_t)t1 + k];
         }
+
+        // per-output-point values, staged once per item
+        using V = typename std::conditional<MIXED, F2, double>::type;
+        V ta0[NTV], ta1[NTV];
+        if constexpr (TV > 0) {
+            double r0[TV], r1[TV], s0[NTV], s1[NTV];
+#pragma unroll
+            for (int q = 0; q < TV; q++) {
+                r0[q] = a.trg_aux[(size_t)t0 * TV + q];
+                r1[q] = a.trg_aux[(size_t)t1 * TV + q];
+            }
+            K::stage_aux(r0, s0);
+            K::stage_aux(r1, s1);
+#pragma unroll
+            for (int q = 0; q < NTV; q++) {
+                if constexpr (MIXED) {
+                    ta0[q] = splat((float)s0[q]);
+                    ta1[q] = splat((float)s1[q]);
+                } else {
+                    ta0[q] = s0[q];
+                    ta1[q] = s1[q];
+                }
+            }
+        }
+        auto eval = [&](auto &u, V dx, V dy, V dz, const V *sv, const V *ta) {
+            if constexpr (TV > 0)
+                K::eval(u, dx, dy, dz, sv, ta);
+            else
+                K::eval(u, dx, dy, dz, sv);
+        };
 
         // accumulators: FP64 path sums directly; mixed path keeps Kahan sum + compensation
         S acc0[TDIM], acc1[TDIM], cmp0[TDIM], cmp1[TDIM];
@@ -241,20 +282,20 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                             sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
                             sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
                         }
-                        K::eval(p0, (th0[0] - sh[0]) + (tl0[0] - sl[0]), (th0[1] - sh[1]) + (tl0[1] - sl[1]),
-                                (th0[2] - sh[2]) + (tl0[2] - sl[2]), s);
-                        K::eval(p1, (th1[0] - sh[0]) + (tl1[0] - sl[0]), (th1[1] - sh[1]) + (tl1[1] - sl[1]),
-                                (th1[2] - sh[2]) + (tl1[2] - sl[2]), s);
+                        eval(p0, (th0[0] - sh[0]) + (tl0[0] - sl[0]), (th0[1] - sh[1]) + (tl0[1] - sl[1]),
+                             (th0[2] - sh[2]) + (tl0[2] - sl[2]), s, ta0);
+                        eval(p1, (th1[0] - sh[0]) + (tl1[0] - sl[0]), (th1[1] - sh[1]) + (tl1[1] - sl[1]),
+                             (th1[2] - sh[2]) + (tl1[2] - sl[2]), s, ta1);
                     } else {
                         double2 sx[3];
 #pragma unroll
                         for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
-                        K::eval(p0, mk((float)(tr0[0] - sx[0].x), (float)(tr0[0] - sx[0].y)),
-                                mk((float)(tr0[1] - sx[1].x), (float)(tr0[1] - sx[1].y)),
-                                mk((float)(tr0[2] - sx[2].x), (float)(tr0[2] - sx[2].y)), s);
-                        K::eval(p1, mk((float)(tr1[0] - sx[0].x), (float)(tr1[0] - sx[0].y)),
-                                mk((float)(tr1[1] - sx[1].x), (float)(tr1[1] - sx[1].y)),
-                                mk((float)(tr1[2] - sx[2].x), (float)(tr1[2] - sx[2].y)), s);
+                        eval(p0, mk((float)(tr0[0] - sx[0].x), (float)(tr0[0] - sx[0].y)),
+                             mk((float)(tr0[1] - sx[1].x), (float)(tr0[1] - sx[1].y)),
+                             mk((float)(tr0[2] - sx[2].x), (float)(tr0[2] - sx[2].y)), s, ta0);
+                        eval(p1, mk((float)(tr1[0] - sx[0].x), (float)(tr1[0] - sx[0].y)),
+                             mk((float)(tr1[1] - sx[1].x), (float)(tr1[1] - sx[1].y)),
+                             mk((float)(tr1[2] - sx[2].x), (float)(tr1[2] - sx[2].y)), s, ta1);
                     }
                 }
                 // Kahan-compensated accumulation of the tile's partial sums
@@ -276,8 +317,8 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 #pragma unroll
                     for (int q = 0; q < NV; q++) s[q] = mv[q][j];
                     const double sx = mc[0][j], sy = mc[1][j], sz = mc[2][j];
-                    K::eval(acc0, xt0[0] - sx, xt0[1] - sy, xt0[2] - sz, s);
-                    K::eval(acc1, xt1[0] - sx, xt1[1] - sy, xt1[2] - sz, s);
+                    eval(acc0, xt0[0] - sx, xt0[1] - sy, xt0[2] - sz, s, ta0);
+                    eval(acc1, xt1[0] - sx, xt1[1] - sy, xt1[2] - sz, s, ta1);
                 }
             }
             __syncwarp();
@@ -375,6 +416,7 @@ __global__ void scatter_add_kernel(int n, int d, const int *__restrict__ perm, c
 
 int uk_sdim_host(int uk) { return uk_sdim(uk); }
 int uk_tdim_host(int uk) { return uk_tdim(uk); }
+int uk_tvdim_host(int uk) { return uk_tvdim(uk); }
 double uk_scale_host(int uk) { return uk_scale(uk); }
 int uk_record_stride(int uk) { return (3 + uk_sdim(uk) + 1) & ~1; }
 
@@ -394,6 +436,12 @@ cudaError_t launch_list_p2p(int uk, int prec, const ListP2PArgs &a, int num_sms,
     case UK_STOKES_DOUBLEPVEL: return launch_prec<UK_STOKES_DOUBLEPVEL>(prec, a, num_sms, stream);
     case UK_LAPLACE_SLDL_PGRAD: return launch_prec<UK_LAPLACE_SLDL_PGRAD>(prec, a, num_sms, stream);
     case UK_STOKES_SLDL_PVEL: return launch_prec<UK_STOKES_SLDL_PVEL>(prec, a, num_sms, stream);
+    case UK_REGVEL_ADJ_SRC:
+        if (!a.trg_aux) return cudaErrorInvalidValue;
+        return launch_prec<UK_REGVEL_ADJ_SRC>(prec, a, num_sms, stream);
+    case UK_REGVEL_ADJ_TRG:
+        if (!a.trg_aux) return cudaErrorInvalidValue;
+        return launch_prec<UK_REGVEL_ADJ_TRG>(prec, a, num_sms, stream);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -34,6 +34,7 @@ struct ListP2PArgs {
     const double *box_centre;  // per target box: local origin for the mixed path (3 doubles)
     double period;             // periodic image length (1 for the unit box)
     int atomic_out;            // 1 when several items may write the same target
+    const double *trg_aux;     // per-target values (TV doubles each) of the adjoint kernels, else null
 };
 
 // Record stride (doubles) for a micro-kernel: 3 coordinates + SDIM values,
@@ -41,6 +42,7 @@ struct ListP2PArgs {
 int uk_record_stride(int uk);
 int uk_sdim_host(int uk);
 int uk_tdim_host(int uk);
+int uk_tvdim_host(int uk);  // per-target values read by a micro-kernel (adjoint kernels)
 double uk_scale_host(int uk);
 
 // Launch the list kernel for micro-kernel `uk` with the given precision.

@@ -94,7 +94,9 @@ enum UkId : int {
     UK_STOKES_DOUBLEPVEL = 10,
     UK_LAPLACE_SLDL_PGRAD = 11,  // values (q, d0, d1, d2)
     UK_STOKES_SLDL_PVEL = 12,    // values (f0, f1, f2, trD, D00 .. D22)
-    UK_COUNT = 13
+    UK_REGVEL_ADJ_SRC = 13,      // adjoint of stokes_regvel, source side (see below)
+    UK_REGVEL_ADJ_TRG = 14,      // adjoint of stokes_regvel, target positions
+    UK_COUNT = 15
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
@@ -108,6 +110,7 @@ template <int ID> struct Uk;
 template <> struct Uk<UK_LAPLACE_P> {
     static constexpr int SDIM = 1, TDIM = 1, NV = 1;
     static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) { v[0] = f[0]; }
     template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
@@ -120,6 +123,7 @@ template <> struct Uk<UK_LAPLACE_P> {
 template <> struct Uk<UK_LAPLACE_PGRAD> {
     static constexpr int SDIM = 1, TDIM = 4, NV = 2;
     static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -139,6 +143,7 @@ template <> struct Uk<UK_LAPLACE_PGRAD> {
 template <> struct Uk<UK_LAPLACE_DIPOLEP> {
     static constexpr int SDIM = 3, TDIM = 1, NV = 3;
     static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -156,6 +161,7 @@ template <> struct Uk<UK_LAPLACE_DIPOLEP> {
 template <> struct Uk<UK_LAPLACE_DIPOLEPGRAD> {
     static constexpr int SDIM = 3, TDIM = 4, NV = 3;
     static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -179,6 +185,7 @@ template <> struct Uk<UK_LAPLACE_DIPOLEPGRAD> {
 template <> struct Uk<UK_STOKES_VEL> {
     static constexpr int SDIM = 3, TDIM = 3, NV = 3;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -199,6 +206,7 @@ template <> struct Uk<UK_STOKES_VEL> {
 template <> struct Uk<UK_RPY_U> {
     static constexpr int SDIM = 4, TDIM = 3, NV = 5;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -225,6 +233,7 @@ template <> struct Uk<UK_RPY_U> {
 template <> struct Uk<UK_RPY_ULAPU> {
     static constexpr int SDIM = 4, TDIM = 6, NV = 4;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int k) { return k >= 3 ? 2.0 : 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -254,6 +263,7 @@ template <> struct Uk<UK_RPY_ULAPU> {
 template <> struct Uk<UK_STK_ULAPU> {
     static constexpr int SDIM = 3, TDIM = 6, NV = 3;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int k) { return k >= 3 ? 2.0 : 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -280,6 +290,7 @@ template <> struct Uk<UK_STK_ULAPU> {
 template <> struct Uk<UK_STOKES_REGVEL> {
     static constexpr int SDIM = 4, TDIM = 3, NV = 4;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -304,6 +315,7 @@ template <> struct Uk<UK_STOKES_REGVEL> {
 template <> struct Uk<UK_STOKES_PVEL> {
     static constexpr int SDIM = 4, TDIM = 4, NV = 4;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -329,6 +341,7 @@ template <> struct Uk<UK_STOKES_PVEL> {
 template <> struct Uk<UK_STOKES_DOUBLEPVEL> {
     static constexpr int SDIM = 9, TDIM = 4, NV = 7;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -363,6 +376,7 @@ template <> struct Uk<UK_STOKES_DOUBLEPVEL> {
 template <> struct Uk<UK_LAPLACE_SLDL_PGRAD> {
     static constexpr int SDIM = 4, TDIM = 4, NV = 5;
     static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -391,6 +405,7 @@ template <> struct Uk<UK_LAPLACE_SLDL_PGRAD> {
 template <> struct Uk<UK_STOKES_SLDL_PVEL> {
     static constexpr int SDIM = 13, TDIM = 4, NV = 11;
     static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
     static __host__ __device__ constexpr double comp_scale(int k) { return k == 0 ? 2.0 : 1.0; }
     static __device__ void stage(const double *f, double *v) {
         v[0] = f[0];
@@ -414,20 +429,116 @@ template <> struct Uk<UK_STOKES_SLDL_PVEL> {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Adjoint of the regularized Stokeslet sum (no reference counterpart).
+// Forward: u_t = 1/(8 pi) sum_s G_{eps_s}(x_t - x_s) f_s with
+//   G_eps(r) = ((|r|^2 + 2 eps^2) I + r r^T) / R^3,  R^2 = |r|^2 + eps^2.
+// For a loss L = sum_t w_t . u_t, with F(r) = w . G_eps(r) f (F is even in r):
+//   dL/df_s   = 1/(8 pi) sum_t G_{eps_s}(x_t - x_s) w_t
+//   dL/deps_s = 1/(8 pi) sum_t eps_s (4 (w.f) - 3 m) / R^3,  m = ((|r|^2+2eps^2)(w.f) + (w.r)(f.r)) / R^2
+//   dL/dx_s   = 1/(8 pi) sum_t grad F (x_s - x_t)
+//   dL/dx_t   = 1/(8 pi) sum_s grad F (x_t - x_s)
+//   grad F(d) = (d (2 (w.f) - 3 m) + w (f.d) + f (w.d)) / R^3.
+// Both gradient sums are P2P sums over the displacement d = (output point) -
+// (input point), so they run on the list kernel with per-output-point values:
+// ---------------------------------------------------------------------------
+
+// Source side: output points are the forward sources with per-point values
+// (f, eps) (TV = 4, staged as f, eps^2, eps); input points are the forward
+// targets with values w.  Outputs (dL/df 3, dL/deps 1, dL/dx_s 3).
+template <> struct Uk<UK_REGVEL_ADJ_SRC> {
+    static constexpr int SDIM = 3, TDIM = 7, NV = 3, TV = 4, NTV = 5;
+    static constexpr double SCALE = kInv8Pi;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+    }
+    static __device__ void stage_aux(const double *a, double *t) {
+        t[0] = a[0];
+        t[1] = a[1];
+        t[2] = a[2];
+        t[3] = a[3] * a[3];
+        t[4] = a[3];
+    }
+    template <class V>
+    static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *w, const V *t) {
+        V R2 = fmav(dx, dx, fmav(dy, dy, fmav(dz, dz, t[3])));
+        V Rinv = rsq(R2);
+        V Rinv2 = Rinv * Rinv;
+        V Rinv3 = Rinv2 * Rinv;
+        V a = R2 + t[3];  // |d|^2 + 2 eps^2
+        V wd = fmav(w[0], dx, fmav(w[1], dy, w[2] * dz));
+        V fd = fmav(t[0], dx, fmav(t[1], dy, t[2] * dz));
+        V wf = fmav(w[0], t[0], fmav(w[1], t[1], w[2] * t[2]));
+        V al = a * Rinv3, be = wd * Rinv3;
+        u[0] = fmav(be, dx, fmav(al, w[0], u[0]));
+        u[1] = fmav(be, dy, fmav(al, w[1], u[1]));
+        u[2] = fmav(be, dz, fmav(al, w[2], u[2]));
+        V m = fmav(a, wf, wd * fd) * Rinv2;
+        u[3] = fmav(fmav(wf, cst<V>(4.0), m * cst<V>(-3.0)), t[4] * Rinv3, u[3]);
+        V c = fmav(m, cst<V>(-3.0), wf + wf);
+        u[4] = fmav(fmav(c, dx, fmav(fd, w[0], wd * t[0])), Rinv3, u[4]);
+        u[5] = fmav(fmav(c, dy, fmav(fd, w[1], wd * t[1])), Rinv3, u[5]);
+        u[6] = fmav(fmav(c, dz, fmav(fd, w[2], wd * t[2])), Rinv3, u[6]);
+    }
+};
+
+// Target positions: output points are the forward targets with per-point
+// values w (TV = 3); input points are the forward sources with values (f, eps)
+// (staged f, eps^2).  Output dL/dx_t (3).
+template <> struct Uk<UK_REGVEL_ADJ_TRG> {
+    static constexpr int SDIM = 4, TDIM = 3, NV = 4, TV = 3, NTV = 3;
+    static constexpr double SCALE = kInv8Pi;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = f[3] * f[3];
+    }
+    static __device__ void stage_aux(const double *a, double *t) {
+        t[0] = a[0];
+        t[1] = a[1];
+        t[2] = a[2];
+    }
+    template <class V>
+    static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *f, const V *w) {
+        V R2 = fmav(dx, dx, fmav(dy, dy, fmav(dz, dz, f[3])));
+        V Rinv = rsq(R2);
+        V Rinv2 = Rinv * Rinv;
+        V Rinv3 = Rinv2 * Rinv;
+        V a = R2 + f[3];
+        V wd = fmav(w[0], dx, fmav(w[1], dy, w[2] * dz));
+        V fd = fmav(f[0], dx, fmav(f[1], dy, f[2] * dz));
+        V wf = fmav(w[0], f[0], fmav(w[1], f[1], w[2] * f[2]));
+        V m = fmav(a, wf, wd * fd) * Rinv2;
+        V c = fmav(m, cst<V>(-3.0), wf + wf);
+        u[0] = fmav(fmav(c, dx, fmav(fd, w[0], wd * f[0])), Rinv3, u[0]);
+        u[1] = fmav(fmav(c, dy, fmav(fd, w[1], wd * f[1])), Rinv3, u[1]);
+        u[2] = fmav(fmav(c, dz, fmav(fd, w[2], wd * f[2])), Rinv3, u[2]);
+    }
+};
+
 // Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
          : id == UK_LAPLACE_DIPOLEPGRAD ? 3 : id == UK_STOKES_VEL ? 3 : id == UK_RPY_U ? 4
          : id == UK_RPY_ULAPU ? 4 : id == UK_STK_ULAPU ? 3 : id == UK_STOKES_REGVEL ? 4
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 9 : id == UK_LAPLACE_SLDL_PGRAD ? 4
-         : id == UK_STOKES_SLDL_PVEL ? 13 : 0;
+         : id == UK_STOKES_SLDL_PVEL ? 13 : id == UK_REGVEL_ADJ_SRC ? 3 : id == UK_REGVEL_ADJ_TRG ? 4 : 0;
 }
 __host__ __device__ constexpr int uk_tdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 4 : id == UK_LAPLACE_DIPOLEP ? 1
          : id == UK_LAPLACE_DIPOLEPGRAD ? 4 : id == UK_STOKES_VEL ? 3 : id == UK_RPY_U ? 3
          : id == UK_RPY_ULAPU ? 6 : id == UK_STK_ULAPU ? 6 : id == UK_STOKES_REGVEL ? 3
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 4 : id == UK_LAPLACE_SLDL_PGRAD ? 4
-         : id == UK_STOKES_SLDL_PVEL ? 4 : 0;
+         : id == UK_STOKES_SLDL_PVEL ? 4 : id == UK_REGVEL_ADJ_SRC ? 7 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
+}
+// per-output-point (target-side) values a micro-kernel reads
+__host__ __device__ constexpr int uk_tvdim(int id) {
+    return id == UK_REGVEL_ADJ_SRC ? 4 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
 }
 __host__ __device__ constexpr double uk_scale(int id) {
     return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD ? kInv4Pi : kInv8Pi;

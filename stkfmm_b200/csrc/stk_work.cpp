@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 
 #include "../../include/stkfmm_b200.h"
@@ -10,23 +11,53 @@
 
 namespace stk {
 
-Workspace &Workspace::thread_local_ws() {
-    static thread_local Workspace ws;
-    return ws;
+namespace {
+
+// Workspaces outlive the threads that used them: when a thread ends (for
+// example torch's autograd worker at interpreter shutdown) its workspace goes
+// back to this free list, with no CUDA call, and the next new thread reuses it.
+// Calling cudaFree from a thread-exit destructor can run after the CUDA runtime
+// has been torn down.  The pool itself is never destroyed; its device memory
+// is released with the CUDA context when the process ends.
+class WorkspacePool {
+  public:
+    Workspace *acquire() {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (!free_.empty()) {
+            Workspace *w = free_.back();
+            free_.pop_back();
+            return w;
+        }
+        return new Workspace();
+    }
+    void release(Workspace *w) {
+        std::lock_guard<std::mutex> lock(mu_);
+        free_.push_back(w);
+    }
+
+  private:
+    std::mutex mu_;
+    std::vector<Workspace *> free_;
+};
+
+WorkspacePool &pool() {
+    static WorkspacePool *p = new WorkspacePool();
+    return *p;
 }
 
-Workspace::~Workspace() {
-    for (auto &kv : devs_) {
-        int prev = -1;
-        if (cudaGetDevice(&prev) != cudaSuccess) break;  // runtime already torn down
-        cudaSetDevice(kv.first);
-        for (int s = 0; s < kNumSlots; s++)
-            if (kv.second.ptr[s]) cudaFree(kv.second.ptr[s]);
-        if (kv.second.counter) cudaFree(kv.second.counter);
-        if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
-        cudaSetDevice(prev);
-    }
+struct WorkspaceHolder {
+    Workspace *ws = pool().acquire();
+    ~WorkspaceHolder() { pool().release(ws); }
+};
+
+}  // namespace
+
+Workspace &Workspace::thread_local_ws() {
+    static thread_local WorkspaceHolder holder;
+    return *holder.ws;
 }
+
+Workspace::~Workspace() = default;
 
 int Workspace::ensure_device() {
     int n = 0;

@@ -14,7 +14,8 @@ namespace stk {
 // non-blocking stream and the persistent-kernel work counter.  The stateless
 // C-ABI calls (direct sums, ker_poten shims, list calls) use it, so they are
 // re-entrant across host threads (the reference calls ker_poten from OpenMP
-// threads concurrently, Lib/src/FMMData.cpp:275-282).
+// threads concurrently, Lib/src/FMMData.cpp:275-282).  A workspace is handed
+// to the next thread when its thread ends and is never freed before exit.
 class Workspace {
   public:
     enum Slot { kRec, kSrcBeg, kSrcEnd, kEnt, kItems, kHostSrc, kHostVal, kHostTrg, kHostOut, kNumSlots };

@@ -72,6 +72,8 @@ class UKERNEL(enum.IntEnum):
     STOKES_DOUBLEPVEL = 10
     LAPLACE_SLDL_PGRAD = 11
     STOKES_SLDL_PVEL = 12
+    REGVEL_ADJ_SRC = 13  # adjoint of stokes_regvel: (dL/df, dL/deps, dL/dx) at the sources
+    REGVEL_ADJ_TRG = 14  # adjoint of stokes_regvel: dL/dx at the targets
 
 
 SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.Stokes, KERNEL.RPY, KERNEL.StokesRegVel, KERNEL.PVel)
