@@ -183,7 +183,10 @@ int Stk3DFMM_set_box(Stk3DFMM *fmm, double *origin, double len);
 int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:26 (not declared in the reference header) */
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
-/* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources); see stk_fmm_far_field_available */
+/* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
+ * KIFMM far field.  The far field is built for free space (pbc = 0) and for the
+ * kernels whose translations use laplace_p or stokes_vel (LapPGrad, Stokes, RPY,
+ * StokesRegVel); other cases return STK_ERR_NOT_SUPPORTED. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
                           double *trg_value, const int nDL, double *src_DL_value);
 /* Stk3DFMM-c.cpp:33-35 */
@@ -204,8 +207,14 @@ int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double
  * the handle's stream) without a host synchronisation. */
 int Stk3DFMM_evaluate_near_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value, double *d_trg_value,
                                   const double *d_src_DL_value, void *stream);
-/* Device time (ms, CUDA events on the launching stream) of the P2P kernel
- * launches of the last near-field evaluation of `kernel`. */
+/* evaluate_fmm on device buffers in the caller's order (values as given, unit
+ * box only: STK_ERR_NOT_SUPPORTED otherwise), queued on `stream` without a host
+ * synchronisation: d_trg_value += near field + KIFMM far field.  The first call
+ * after setup_tree builds the far-field operators and synchronises. */
+int Stk3DFMM_evaluate_fmm_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value, double *d_trg_value,
+                                 const double *d_src_DL_value, void *stream);
+/* Device time (ms, CUDA events on the launching stream) of the kernel launches
+ * of the last near-field or FMM evaluation of `kernel`. */
 int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms);
 /* Tree / list statistics of the last setup_tree for `kernel`:
  * out[0] nodes, [1] leaves, [2] depth, [3] U-list entries, [4] U-list SL point pairs,

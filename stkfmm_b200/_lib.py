@@ -59,6 +59,7 @@ SIGNATURES = [
     ("Stk3DFMM_set_precision", c_int, [c_void_p, c_int]),
     ("Stk3DFMM_evaluate_near", c_int, [c_void_p, c_uint, c_int, P_d, c_int, P_d, c_int, P_d]),
     ("Stk3DFMM_evaluate_near_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("Stk3DFMM_evaluate_fmm_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("Stk3DFMM_last_kernel_ms", c_int, [c_void_p, c_uint, P_f]),
     ("Stk3DFMM_get_tree_stats", c_int, [c_void_p, c_uint, P_ll]),
     ("Stk3DFMM_get_ulist", c_int, [c_void_p, c_uint, P_i] + [P_i] * 11),

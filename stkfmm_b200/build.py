@@ -2,7 +2,9 @@
 
 Every CUDA / C++ source under stkfmm_b200/csrc is compiled by nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` and linked into
-``stkfmm_b200/libstkfmm_b200.so`` with a static CUDA runtime.  Objects go to
+``stkfmm_b200/libstkfmm_b200.so`` with a static CUDA runtime; the far field's
+dense translations and operator pseudo-inverses link cuBLAS and cuSOLVER from
+the CUDA toolkit (an rpath points there).  Objects go to
 ``stkfmm_b200/_build`` and are rebuilt only when a source or header changed.
 """
 from __future__ import annotations
@@ -38,6 +40,11 @@ def host_compiler() -> list:
         if os.path.exists(cand):
             return ["-ccbin", cand]
     return []
+
+
+def _cuda_libs() -> list:
+    libdir = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc()))), "lib64")
+    return ["-L" + libdir, "-Xlinker", "-rpath=" + libdir, "-lcublas", "-lcusolver"]
 
 
 def _sources():
@@ -81,7 +88,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             list(ex.map(lambda so: _compile(so[0], so[1], verbose), todo))
     if force or todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
         tmp = LIB + ".tmp"
-        cmd = [nvcc()] + host_compiler() + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+        cmd = ([nvcc()] + host_compiler() + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+               + _cuda_libs())
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc link failed:\n%s%s" % (r.stdout, r.stderr))

@@ -1,0 +1,687 @@
+// stk_farfield.cu -- KIFMM far field on the GPU (see stk_farfield.hpp).
+//
+// Operators.  The translation kernels handled here (laplace_p, stokes_vel) are
+// homogeneous of degree -1: K(s x) = K(x) / s.  With check and equivalent
+// surfaces scaled with the box, the pseudo-inverses scale as 2^-l at level l
+// and the kernel matrices as 2^l, so M2M, L2L and M2L (which includes the
+// downward check-to-equivalent solve) are the same at every level.  They are
+// built once per (kernel, p) from a reference box of side 1:
+//   UC2UE = pinv(K(UC, UE)),  DC2DE = pinv(K(DC, DE))           (FP64 SVD)
+//   M2M_o = UC2UE K(UC, UE_child o)        8 child octants
+//   L2L_o = DC2DE_child K(DC_child o, DE)  8 child octants
+//   M2L_d = DC2DE K(DC, UE shifted by d)   316 well-separated offsets d
+// S2M and S2L produce check potentials directly (P2P), solved with 2^-l UC2UE /
+// 2^-l DC2DE.  M2M, L2L and M2L run as cuBLAS DGEMMs; S2M, S2L, M2T (W-list)
+// and L2T run on the list P2P kernel with the surface points as sources or
+// targets.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/stkfmm_b200.h"
+#include "stk_farfield.hpp"
+#include "stk_ukernels.cuh"
+#include "stk_work.hpp"
+
+namespace stk {
+
+namespace {
+
+#define FCUDA(call)                                    \
+    do {                                               \
+        if ((call) != cudaSuccess) return STK_ERR_CUDA; \
+    } while (0)
+#define FBLAS(call)                                               \
+    do {                                                          \
+        if ((call) != CUBLAS_STATUS_SUCCESS) return STK_ERR_CUDA; \
+    } while (0)
+
+constexpr int kNumOffsets = 343;  // (dx, dy, dz) in [-3, 3]^3
+
+// Points of the KIFMM cube surface on [-1, 1]^3, in the order of stkfmm::surface
+// (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85) before its affine map.
+std::vector<double> unit_surface(int p) {
+    const int n = 6 * (p - 1) * (p - 1) + 2;
+    std::vector<double> c(3 * (size_t)n);
+    c[0] = c[1] = c[2] = -1.0;
+    int cnt = 1;
+    const double q = p - 1;
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            c[3 * cnt + 0] = -1.0;
+            c[3 * cnt + 1] = (2.0 * (i + 1) - p + 1) / q;
+            c[3 * cnt + 2] = (2.0 * j - p + 1) / q;
+        }
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            c[3 * cnt + 0] = (2.0 * i - p + 1) / q;
+            c[3 * cnt + 1] = -1.0;
+            c[3 * cnt + 2] = (2.0 * (j + 1) - p + 1) / q;
+        }
+    for (int i = 0; i < p - 1; i++)
+        for (int j = 0; j < p - 1; j++, cnt++) {
+            c[3 * cnt + 0] = (2.0 * (i + 1) - p + 1) / q;
+            c[3 * cnt + 1] = (2.0 * j - p + 1) / q;
+            c[3 * cnt + 2] = -1.0;
+        }
+    for (int i = 0; i < (n / 2) * 3; i++) c[3 * (size_t)cnt + i] = -c[i];
+    return c;
+}
+
+// out[(i n + k) 3 + d] = centre(node_i) + alpha r(node_i) unit[k]; node_i = nodes[i]
+// (or i when nodes is null), r = 0.5 * 2^-level.
+__global__ void surface_points_kernel(const int *__restrict__ nodes, int m, const double *__restrict__ centre,
+                                      const int *__restrict__ level, double alpha, const double *__restrict__ unit,
+                                      int n, double *__restrict__ out) {
+    const long long total = (long long)m * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / n), k = (int)(idx - (long long)i * n);
+        const int b = nodes ? nodes[i] : i;
+        const double r = alpha * ldexp(0.5, -level[b]);
+#pragma unroll
+        for (int d = 0; d < 3; d++) out[3 * idx + d] = centre[3 * (size_t)b + d] + r * unit[3 * k + d];
+    }
+}
+
+// M[(i TDIM + a) + ld (j SDIM + c)] = SCALE comp_scale(a) K_ac(X_i - Y_j): the
+// kernel matrix from unit source densities.
+template <int UK>
+__global__ void kernel_matrix_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
+                                     double *__restrict__ M, int ld) {
+    using K = Uk<UK>;
+    const long long total = (long long)ni * nj;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % ni), j = (int)(idx / ni);
+        const double dx = X[3 * i] - Y[3 * j], dy = X[3 * i + 1] - Y[3 * j + 1], dz = X[3 * i + 2] - Y[3 * j + 2];
+        for (int c = 0; c < K::SDIM; c++) {
+            double f[K::SDIM], v[K::NV], u[K::TDIM];
+            for (int q = 0; q < K::SDIM; q++) f[q] = q == c ? 1.0 : 0.0;
+            for (int a = 0; a < K::TDIM; a++) u[a] = 0.0;
+            K::stage(f, v);
+            K::eval(u, dx, dy, dz, v);
+            for (int a = 0; a < K::TDIM; a++)
+                M[(size_t)(i * K::TDIM + a) + (size_t)ld * (j * K::SDIM + c)] = K::SCALE * K::comp_scale(a) * u[a];
+        }
+    }
+}
+
+int kernel_matrix(int uk, const double *X, int ni, const double *Y, int nj, double *M, int ld, cudaStream_t s) {
+    const long long total = (long long)ni * nj;
+    const int threads = 256;
+    const int grid = (int)std::min<long long>((total + threads - 1) / threads, 148 * 32);
+    if (uk == UK_LAPLACE_P)
+        kernel_matrix_kernel<UK_LAPLACE_P><<<grid, threads, 0, s>>>(X, ni, Y, nj, M, ld);
+    else if (uk == UK_STOKES_VEL)
+        kernel_matrix_kernel<UK_STOKES_VEL><<<grid, threads, 0, s>>>(X, ni, Y, nj, M, ld);
+    else
+        return STK_ERR_NOT_SUPPORTED;
+    return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+// W[i + m j] = U[j + m i] / S_i for S_i above the cut, else 0  (W = S^+ U^T)
+__global__ void pinv_scale_kernel(const double *__restrict__ U, const double *__restrict__ S, int m, double rtol,
+                                  double *__restrict__ W) {
+    const double cut = rtol * S[0];
+    const long long total = (long long)m * m;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % m), j = (int)(idx / m);
+        const double si = S[i];
+        W[idx] = si > cut ? U[j + (size_t)m * i] / si : 0.0;
+    }
+}
+
+// dst[:, j] (= or +=) src[:, col(j)] for N-row column blocks; col = null -> j
+__global__ void gather_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int m, int N,
+                                   double *__restrict__ dst) {
+    const long long total = (long long)m * N;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / N), r = (int)(idx - (long long)j * N);
+        dst[idx] = src[(size_t)cols[j] * N + r];
+    }
+}
+
+__global__ void scatter_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int m, int N,
+                                    double alpha, int add, double *__restrict__ dst) {
+    const long long total = (long long)m * N;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / N), r = (int)(idx - (long long)j * N);
+        double *d = dst + (size_t)cols[j] * N + r;
+        *d = add ? *d + alpha * src[idx] : alpha * src[idx];
+    }
+}
+
+inline int grid_for(long long total) { return (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 32)); }
+
+int gather_cols(const double *src, const int *cols, int m, int N, double *dst, cudaStream_t s) {
+    if (m <= 0) return STK_OK;
+    gather_cols_kernel<<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, dst);
+    return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+int scatter_cols(const double *src, const int *cols, int m, int N, double alpha, int add, double *dst,
+                 cudaStream_t s) {
+    if (m <= 0) return STK_OK;
+    scatter_cols_kernel<<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, alpha, add, dst);
+    return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+// A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
+// at rtol * sigma_max.  A is overwritten.
+int pinv(FarField &F, double *A, int m, double *A_inv, double rtol, cudaStream_t s) {
+    cusolverDnSetStream(F.solver, s);
+    int lwork = 0;
+    if (cusolverDnDgesvd_bufferSize(F.solver, m, m, &lwork) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    DevBuf work, S, U, VT, W, info, rwork;
+    int rc = work.reserve(sizeof(double) * (size_t)std::max(lwork, 1));
+    if (!rc) rc = S.reserve(sizeof(double) * m);
+    if (!rc) rc = U.reserve(sizeof(double) * (size_t)m * m);
+    if (!rc) rc = VT.reserve(sizeof(double) * (size_t)m * m);
+    if (!rc) rc = W.reserve(sizeof(double) * (size_t)m * m);
+    if (!rc) rc = info.reserve(sizeof(int));
+    if (!rc) rc = rwork.reserve(sizeof(double) * m);
+    if (rc) return rc;
+    if (cusolverDnDgesvd(F.solver, 'A', 'A', m, m, A, m, (double *)S.ptr, (double *)U.ptr, m, (double *)VT.ptr, m,
+                         (double *)work.ptr, lwork, (double *)rwork.ptr, (int *)info.ptr) != CUSOLVER_STATUS_SUCCESS)
+        return STK_ERR_CUDA;
+    pinv_scale_kernel<<<grid_for((long long)m * m), 256, 0, s>>>((const double *)U.ptr, (const double *)S.ptr, m, rtol,
+                                                               (double *)W.ptr);
+    FCUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    cublasSetStream(F.blas, s);
+    // A_inv = V W = VT^T W
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, &one, (const double *)VT.ptr, m,
+                      (const double *)W.ptr, m, &zero, A_inv, m));
+    int h_info = 0;
+    FCUDA(cudaMemcpyAsync(&h_info, info.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaStreamSynchronize(s));
+    return h_info == 0 ? STK_OK : STK_ERR_CUDA;
+}
+
+int upload_points(DevBuf &b, const std::vector<double> &v, cudaStream_t s) {
+    return b.upload(v.data(), v.size() * sizeof(double), s);
+}
+
+std::vector<double> scaled_surface(const std::vector<double> &unit, double cx, double cy, double cz, double r) {
+    std::vector<double> o(unit.size());
+    for (size_t i = 0; i < unit.size(); i += 3) {
+        o[i] = cx + r * unit[i];
+        o[i + 1] = cy + r * unit[i + 1];
+        o[i + 2] = cz + r * unit[i + 2];
+    }
+    return o;
+}
+
+// Build the level-independent operators for (m2x, p).
+int build_operators(FarField &F, cudaStream_t s) {
+    const int n = F.n, N = F.n * F.ke;
+    if (F.kc != F.ke) return STK_ERR_NOT_SUPPORTED;
+    std::vector<double> unit = unit_surface(F.p);
+    const double r0 = 0.5;  // reference box: side 1, centred at 0
+    DevBuf X, Y, K, T;
+    int rc = K.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = T.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = F.uc2ue.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = F.dc2de.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = F.m2m.reserve(sizeof(double) * (size_t)N * N * 8);
+    if (!rc) rc = F.l2l.reserve(sizeof(double) * (size_t)N * N * 8);
+    if (rc) return rc;
+    // relative SVD cut: sqrt of the unit roundoff 2^-53, as in the reference's
+    // pinv (M2L/SVD_pvfmm.hpp:599-604)
+    const double rtol = std::sqrt(std::ldexp(1.0, -53));
+    auto kmat = [&](const std::vector<double> &trg, const std::vector<double> &src, double *M) {
+        int r = upload_points(X, trg, s);
+        if (!r) r = upload_points(Y, src, s);
+        if (!r) r = kernel_matrix(F.m2x, (const double *)X.ptr, n, (const double *)Y.ptr, n, M, N, s);
+        return r;
+    };
+    const double one = 1.0, zero = 0.0, half = 0.5;
+    cublasSetStream(F.blas, s);
+    // UC2UE and DC2DE
+    rc = kmat(scaled_surface(unit, 0, 0, 0, kRad1 * r0), scaled_surface(unit, 0, 0, 0, kRad0 * r0), (double *)K.ptr);
+    if (!rc) rc = pinv(F, (double *)K.ptr, N, (double *)F.uc2ue.ptr, rtol, s);
+    if (!rc) rc = kmat(scaled_surface(unit, 0, 0, 0, kRad0 * r0), scaled_surface(unit, 0, 0, 0, kRad1 * r0), (double *)K.ptr);
+    if (!rc) rc = pinv(F, (double *)K.ptr, N, (double *)F.dc2de.ptr, rtol, s);
+    if (rc) return rc;
+    // M2M and L2L per child octant (child centre at +-r0/2, half-width r0/2)
+    for (int o = 0; o < 8; o++) {
+        const double cx = (o & 1) ? r0 / 2 : -r0 / 2, cy = (o & 2) ? r0 / 2 : -r0 / 2, cz = (o & 4) ? r0 / 2 : -r0 / 2;
+        rc = kmat(scaled_surface(unit, 0, 0, 0, kRad1 * r0), scaled_surface(unit, cx, cy, cz, kRad0 * r0 / 2),
+                  (double *)K.ptr);
+        if (rc) return rc;
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &one, (const double *)F.uc2ue.ptr, N,
+                          (const double *)K.ptr, N, &zero, (double *)F.m2m.ptr + (size_t)o * N * N, N));
+        rc = kmat(scaled_surface(unit, cx, cy, cz, kRad0 * r0 / 2), scaled_surface(unit, 0, 0, 0, kRad1 * r0),
+                  (double *)K.ptr);
+        if (rc) return rc;
+        // the child's DC2DE is half the parent's (degree -1 kernels); rows o N .. of the 8N x N stack
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &half, (const double *)F.dc2de.ptr, N,
+                          (const double *)K.ptr, N, &zero, (double *)F.l2l.ptr + (size_t)o * N, 8 * N));
+    }
+    // M2L for every well-separated offset of a same-level source box
+    F.m2l_slot.assign(kNumOffsets, -1);
+    int nslot = 0;
+    for (int code = 0; code < kNumOffsets; code++) {
+        const int dx = code % 7 - 3, dy = (code / 7) % 7 - 3, dz = code / 49 - 3;
+        if (std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz))) >= 2) F.m2l_slot[code] = nslot++;
+    }
+    rc = F.m2l.reserve(sizeof(double) * (size_t)N * N * nslot);
+    if (rc) return rc;
+    for (int code = 0; code < kNumOffsets; code++) {
+        const int sl = F.m2l_slot[code];
+        if (sl < 0) continue;
+        const double dx = code % 7 - 3, dy = (code / 7) % 7 - 3, dz = code / 49 - 3;
+        rc = kmat(scaled_surface(unit, 0, 0, 0, kRad0 * r0), scaled_surface(unit, dx, dy, dz, kRad0 * r0),
+                  (double *)K.ptr);
+        if (rc) return rc;
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &one, (const double *)F.dc2de.ptr, N,
+                          (const double *)K.ptr, N, &zero, (double *)F.m2l.ptr + (size_t)sl * N * N, N));
+    }
+    FCUDA(cudaStreamSynchronize(s));
+    return STK_OK;
+}
+
+// Set up one list pass: target boxes with contiguous target ranges, list entries
+// over source boxes.  src_beg / src_end are device arrays owned elsewhere when
+// own_src is false.
+int setup_pass(ListPass &P, int uk, const std::vector<int> &tb, const std::vector<int> &te,
+               const std::vector<int> &off, const std::vector<int> &ent, const int *h_src_beg, const int *h_src_end,
+               int n_src_box, bool own_src, const std::vector<double> &centres, cudaStream_t s) {
+    P.uk = uk;
+    std::vector<WorkItem> items;
+    build_list_items((int)tb.size(), tb.data(), te.data(), off.data(), ent.data(), h_src_beg, h_src_end, items,
+                     P.pairs);
+    P.n_items = (int)items.size();
+    int rc = P.items.upload(items.data(), items.size() * sizeof(WorkItem), s);
+    if (!rc) rc = P.ent.upload(ent.data(), ent.size() * sizeof(int), s);
+    if (!rc && own_src) rc = P.src_beg.upload(h_src_beg, sizeof(int) * n_src_box, s);
+    if (!rc && own_src) rc = P.src_end.upload(h_src_end, sizeof(int) * n_src_box, s);
+    if (!rc) rc = P.trg_box_centre.upload(centres.data(), centres.size() * sizeof(double), s);
+    return rc;
+}
+
+int run_pass(const ListPass &P, int prec, const double *rec, const int *src_beg, const int *src_end,
+             const double *trg_xyz, double *out, unsigned int *counter, int sms, cudaStream_t s) {
+    if (P.n_items == 0) return STK_OK;
+    ListP2PArgs a{};
+    a.src_rec = rec;
+    a.src_box_begin = src_beg;
+    a.src_box_end = src_end;
+    a.list_ent = (const int *)P.ent.ptr;
+    a.items = (const WorkItem *)P.items.ptr;
+    a.n_items = P.n_items;
+    a.counter = counter;
+    a.trg_xyz = trg_xyz;
+    a.trg_out = out;
+    a.box_centre = (const double *)P.trg_box_centre.ptr;
+    a.period = 1.0;
+    a.atomic_out = 0;
+    a.trg_aux = nullptr;
+    return launch_list_p2p(P.uk, prec, a, sms, s) == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+}  // namespace
+
+FarField::~FarField() {
+    if (blas) cublasDestroy(blas);
+    if (solver) cusolverDnDestroy(solver);
+}
+
+int farfield_setup(Stk3DFMM *f, KernelData *kd) {
+    const KernelInfo *ki = kd->info;
+    if (f->pbc != 0) return STK_ERR_NOT_SUPPORTED;  // periodic far field (M2C) is not built
+    const int m2x = ki->slot[SLOT_M2X];
+    if (m2x != UK_LAPLACE_P && m2x != UK_STOKES_VEL) return STK_ERR_NOT_SUPPORTED;
+    if (!kd->far) kd->far.reset(new FarField());
+    FarField &F = *kd->far;
+    cudaStream_t s = f->stream;
+    F.ready = false;
+    if (!F.blas && cublasCreate(&F.blas) != CUBLAS_STATUS_SUCCESS) return STK_ERR_CUDA;
+    if (!F.solver && cusolverDnCreate(&F.solver) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    const int p = f->mult_order;
+    const int ke = uk_sdim_host(m2x), kc = uk_tdim_host(m2x);
+    int rc = STK_OK;
+    if (F.p != p || F.m2x != m2x) {
+        F.p = p;
+        F.n = 6 * (p - 1) * (p - 1) + 2;
+        F.ke = ke;
+        F.kc = kc;
+        F.m2x = m2x;
+        rc = build_operators(F, s);
+        if (rc) {
+            F.p = 0;
+            return rc;
+        }
+    }
+    const Octree &T = kd->tree;
+    const int nn = T.num_nodes(), n = F.n, N = n * ke;
+    std::vector<double> unit = unit_surface(p);
+    rc = upload_points(F.unit_surf, unit, s);
+    // node levels and centres on the device
+    std::vector<int> lev(T.level.begin(), T.level.end());
+    DevBuf d_level;
+    if (!rc) rc = d_level.upload(lev.data(), lev.size() * sizeof(int), s);
+    const double *centre = (const double *)kd->d_centre.ptr;
+    // every node's upward-equivalent and downward-equivalent surface
+    if (!rc) rc = F.ue_xyz.reserve(sizeof(double) * 3 * (size_t)nn * n);
+    if (!rc) rc = F.de_xyz.reserve(sizeof(double) * 3 * (size_t)nn * n);
+    if (rc) return rc;
+    surface_points_kernel<<<grid_for((long long)nn * n), 256, 0, s>>>(nullptr, nn, centre, (const int *)d_level.ptr,
+                                                                      kRad0, (const double *)F.unit_surf.ptr, n,
+                                                                      (double *)F.ue_xyz.ptr);
+    surface_points_kernel<<<grid_for((long long)nn * n), 256, 0, s>>>(nullptr, nn, centre, (const int *)d_level.ptr,
+                                                                      kRad1, (const double *)F.unit_surf.ptr, n,
+                                                                      (double *)F.de_xyz.ptr);
+    FCUDA(cudaGetLastError());
+    rc = F.phi.reserve(sizeof(double) * (size_t)nn * N);
+    if (!rc) rc = F.psi.reserve(sizeof(double) * (size_t)nn * N);
+    if (rc) return rc;
+
+    auto by_level = [&](std::vector<int> &nodes, std::vector<int> &off) {
+        std::stable_sort(nodes.begin(), nodes.end(), [&](int a, int b) { return T.level[a] < T.level[b]; });
+        off.assign(T.depth() + 2, 0);
+        for (int b : nodes) off[T.level[b] + 1]++;
+        for (int l = 0; l <= T.depth(); l++) off[l + 1] += off[l];
+    };
+    std::vector<double> ctr(3 * (size_t)nn);
+    for (int i = 0; i < nn; i++) T.centre(i, &ctr[3 * (size_t)i]);
+
+    // ---- S2M: leaves with sources; targets = their upward check surfaces ----
+    F.s2m_nodes.clear();
+    for (int b : T.leaves)
+        if (T.src_count(b) > 0) F.s2m_nodes.push_back(b);
+    by_level(F.s2m_nodes, F.s2m_level_off);
+    const int ms = (int)F.s2m_nodes.size();
+    rc = F.d_s2m_nodes.upload(F.s2m_nodes.data(), sizeof(int) * std::max(ms, 1), s);
+    if (!rc) rc = F.uc_xyz.reserve(sizeof(double) * 3 * (size_t)std::max(ms, 1) * n);
+    if (!rc) rc = F.check.reserve(sizeof(double) * (size_t)std::max(ms, 1) * n * kc);
+    if (rc) return rc;
+    if (ms)
+        surface_points_kernel<<<grid_for((long long)ms * n), 256, 0, s>>>(
+            (const int *)F.d_s2m_nodes.ptr, ms, centre, (const int *)d_level.ptr, kRad1,
+            (const double *)F.unit_surf.ptr, n, (double *)F.uc_xyz.ptr);
+    {
+        std::vector<int> tb(ms), te(ms), off(ms + 1), ent(ms);
+        std::vector<double> cc(3 * (size_t)std::max(ms, 1));
+        for (int i = 0; i < ms; i++) {
+            tb[i] = i * n;
+            te[i] = (i + 1) * n;
+            off[i] = i;
+            ent[i] = (F.s2m_nodes[i] << 5) | kShiftNone;
+            for (int d = 0; d < 3; d++) cc[3 * i + d] = ctr[3 * (size_t)F.s2m_nodes[i] + d];
+        }
+        off[ms] = ms;
+        for (int k = 0; k < 2; k++) {
+            const int uk = ki->slot[k == 0 ? SLOT_S2M_SL : SLOT_S2M_DL];
+            F.s2m[k].reset();
+            if (uk < 0 || T.sets[k].n == 0) continue;
+            rc = setup_pass(F.s2m[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
+                            nn, false, cc, s);
+            if (rc) return rc;
+        }
+    }
+
+    // ---- S2L: nodes with X lists; targets = their downward check surfaces ----
+    F.s2l_nodes.clear();
+    for (int b = 0; b < nn; b++)
+        if (T.X.off[b + 1] > T.X.off[b]) F.s2l_nodes.push_back(b);
+    by_level(F.s2l_nodes, F.s2l_level_off);
+    const int mx = (int)F.s2l_nodes.size();
+    rc = F.d_s2l_nodes.upload(F.s2l_nodes.data(), sizeof(int) * std::max(mx, 1), s);
+    if (!rc) rc = F.dc_xyz.reserve(sizeof(double) * 3 * (size_t)std::max(mx, 1) * n);
+    if (!rc) rc = F.dcheck.reserve(sizeof(double) * (size_t)std::max(mx, 1) * n * kc);
+    if (rc) return rc;
+    if (mx)
+        surface_points_kernel<<<grid_for((long long)mx * n), 256, 0, s>>>(
+            (const int *)F.d_s2l_nodes.ptr, mx, centre, (const int *)d_level.ptr, kRad0,
+            (const double *)F.unit_surf.ptr, n, (double *)F.dc_xyz.ptr);
+    {
+        std::vector<int> tb(mx), te(mx), off(mx + 1, 0), ent;
+        std::vector<double> cc(3 * (size_t)std::max(mx, 1));
+        for (int i = 0; i < mx; i++) {
+            const int b = F.s2l_nodes[i];
+            tb[i] = i * n;
+            te[i] = (i + 1) * n;
+            off[i] = (int)ent.size();
+            for (int e = T.X.off[b]; e < T.X.off[b + 1]; e++) ent.push_back(T.X.ent[e]);
+            for (int d = 0; d < 3; d++) cc[3 * i + d] = ctr[3 * (size_t)b + d];
+        }
+        off[mx] = (int)ent.size();
+        for (int k = 0; k < 2; k++) {
+            const int uk = ki->slot[k == 0 ? SLOT_S2L_SL : SLOT_S2L_DL];
+            F.s2l[k].reset();
+            if (uk < 0 || T.sets[k].n == 0) continue;
+            rc = setup_pass(F.s2l[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
+                            nn, false, cc, s);
+            if (rc) return rc;
+        }
+    }
+
+    // ---- M2T (W list) and L2T: targets = leaf targets; sources = node surfaces ----
+    {
+        std::vector<int> sb(nn), se(nn);
+        for (int b = 0; b < nn; b++) {
+            sb[b] = b * n;
+            se[b] = (b + 1) * n;
+        }
+        const PointSet &tg = T.sets[2];
+        std::vector<int> loff(nn + 1, 0), lent;
+        for (int b = 0; b < nn; b++) {
+            loff[b] = (int)lent.size();
+            if (T.is_leaf(b) && tg.count(b) > 0) lent.push_back((b << 5) | kShiftNone);
+        }
+        loff[nn] = (int)lent.size();
+        F.m2t.reset();
+        F.l2t.reset();
+        rc = setup_pass(F.m2t, ki->slot[SLOT_M2T], tg.node_begin, tg.node_end, T.W.off, T.W.ent, sb.data(),
+                        se.data(), nn, true, ctr, s);
+        if (!rc)
+            rc = setup_pass(F.l2t, ki->slot[SLOT_L2T], tg.node_begin, tg.node_end, loff, lent, sb.data(), se.data(),
+                            nn, true, ctr, s);
+        if (rc) return rc;
+    }
+
+    // ---- M2M / L2L: non-leaf nodes per level ----
+    F.parents.clear();
+    F.parent_off.assign(T.depth() + 2, 0);
+    for (int l = 0; l <= T.depth(); l++) {
+        F.parent_off[l] = (int)F.parents.size();
+        int j = 0;
+        for (int b = T.level_begin[l]; b < T.level_begin[l + 1]; b++) {
+            if (T.is_leaf(b)) continue;
+            // children of the level-l parents fill level l+1 in parent order
+            if (T.first_child[b] != T.level_begin[l + 1] + 8 * j) return STK_ERR_STATE;
+            F.parents.push_back(b);
+            j++;
+        }
+    }
+    F.parent_off[T.depth() + 1] = (int)F.parents.size();
+    rc = F.d_parents.upload(F.parents.data(), sizeof(int) * std::max<size_t>(F.parents.size(), 1), s);
+    if (rc) return rc;
+
+    // ---- M2L: V-list pairs grouped by offset ----
+    {
+        const int nslot = (int)std::count_if(F.m2l_slot.begin(), F.m2l_slot.end(), [](int v) { return v >= 0; });
+        std::vector<std::vector<int>> srcs(nslot), trgs(nslot);
+        for (int b = 0; b < nn; b++)
+            for (int e = T.V.off[b]; e < T.V.off[b + 1]; e++) {
+                const int a = T.V.ent[e] >> 5, code = T.V.ent[e] & 31;
+                const int sx = code % 3 - 1, sy = (code / 3) % 3 - 1, sz = code / 9 - 1;
+                const int64_t L = 1LL << T.level[b];
+                const int dx = (int)((int64_t)T.ix[a] + sx * L - T.ix[b]);
+                const int dy = (int)((int64_t)T.iy[a] + sy * L - T.iy[b]);
+                const int dz = (int)((int64_t)T.iz[a] + sz * L - T.iz[b]);
+                if (std::abs(dx) > 3 || std::abs(dy) > 3 || std::abs(dz) > 3) return STK_ERR_STATE;
+                const int sl = F.m2l_slot[(dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)];
+                if (sl < 0) return STK_ERR_STATE;
+                srcs[sl].push_back(a);
+                trgs[sl].push_back(b);
+            }
+        F.m2l_off.assign(nslot + 1, 0);
+        std::vector<int> hs, ht;
+        for (int sl = 0; sl < nslot; sl++) {
+            F.m2l_off[sl] = (int)hs.size();
+            hs.insert(hs.end(), srcs[sl].begin(), srcs[sl].end());
+            ht.insert(ht.end(), trgs[sl].begin(), trgs[sl].end());
+        }
+        F.m2l_off[nslot] = (int)hs.size();
+        F.m2l_pairs = (long long)hs.size();
+        rc = F.d_m2l_src.upload(hs.data(), sizeof(int) * std::max<size_t>(hs.size(), 1), s);
+        if (!rc) rc = F.d_m2l_trg.upload(ht.data(), sizeof(int) * std::max<size_t>(ht.size(), 1), s);
+        if (rc) return rc;
+        int maxm = 0;
+        for (int sl = 0; sl < nslot; sl++) maxm = std::max(maxm, F.m2l_off[sl + 1] - F.m2l_off[sl]);
+        for (int l = 0; l <= T.depth(); l++) maxm = std::max(maxm, F.parent_off[l + 1] - F.parent_off[l]);
+        maxm = std::max(maxm, std::max(ms, mx));
+        rc = F.tmp0.reserve(sizeof(double) * (size_t)std::max(maxm, 1) * N);
+        if (!rc) rc = F.tmp1.reserve(sizeof(double) * (size_t)std::max(maxm, 1) * N);
+        if (rc) return rc;
+    }
+    FCUDA(cudaStreamSynchronize(s));
+    F.ready = true;
+    return STK_OK;
+}
+
+int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *trg_sorted,
+                      cudaStream_t s) {
+    FarField &F = *kd->far;
+    const KernelInfo *ki = kd->info;
+    const Octree &T = kd->tree;
+    const int nn = T.num_nodes(), n = F.n, ke = F.ke, kc = F.kc, N = n * ke;
+    const int prec = f->precision;
+    const int sms = f->sms;
+    unsigned int *counter = (unsigned int *)kd->d_counter.ptr;
+    const double one = 1.0, zero = 0.0;
+    cublasSetStream(F.blas, s);
+    double *phi = (double *)F.phi.ptr, *psi = (double *)F.psi.ptr;
+    double *X = (double *)F.tmp0.ptr, *Y = (double *)F.tmp1.ptr;
+    FCUDA(cudaMemsetAsync(phi, 0, sizeof(double) * (size_t)nn * N, s));
+    FCUDA(cudaMemsetAsync(psi, 0, sizeof(double) * (size_t)nn * N, s));
+
+    // source records of the point sets for the S2M / S2L kernels
+    auto pack_points = [&](int k, int uk) -> int {
+        const int rs = uk_record_stride(uk);
+        const PointSet &ps = T.sets[k];
+        int rc = F.rec_pts[k].reserve(sizeof(double) * (size_t)std::max(ps.n, 1) * rs);
+        if (rc) return rc;
+        if (launch_pack_records(ps.n, (const int *)kd->d_perm[k].ptr, (const double *)kd->d_xyz[k].ptr,
+                                k == 0 ? d_sl : d_dl, k == 0 ? ki->kdim_sl : ki->kdim_dl, nullptr, 0, rs,
+                                (double *)F.rec_pts[k].ptr, s) != cudaSuccess)
+            return STK_ERR_CUDA;
+        return STK_OK;
+    };
+
+    // ---- upward pass: S2M, then check -> equivalent per level ----
+    const int ms = (int)F.s2m_nodes.size();
+    if (ms) {
+        FCUDA(cudaMemsetAsync(F.check.ptr, 0, sizeof(double) * (size_t)ms * n * kc, s));
+        for (int k = 0; k < 2; k++) {
+            if (F.s2m[k].uk < 0 || (k == 1 && !d_dl)) continue;
+            int rc = pack_points(k, F.s2m[k].uk);
+            if (!rc)
+                rc = run_pass(F.s2m[k], prec, (const double *)F.rec_pts[k].ptr, (const int *)kd->d_beg[k].ptr,
+                              (const int *)kd->d_end[k].ptr, (const double *)F.uc_xyz.ptr, (double *)F.check.ptr,
+                              counter, sms, s);
+            if (rc) return rc;
+        }
+        for (int l = 0; l + 1 < (int)F.s2m_level_off.size(); l++) {
+            const int a = F.s2m_level_off[l], m = F.s2m_level_off[l + 1] - a;
+            if (m <= 0) continue;
+            const double alpha = std::ldexp(1.0, -l);
+            FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, n * kc, &alpha, (const double *)F.uc2ue.ptr, N,
+                              (const double *)F.check.ptr + (size_t)a * n * kc, n * kc, &zero, Y, N));
+            int rc = scatter_cols(Y, (const int *)F.d_s2m_nodes.ptr + a, m, N, 1.0, 0, phi, s);
+            if (rc) return rc;
+        }
+    }
+    // M2M, bottom up: parents of level l from the contiguous children block at level l+1
+    const int *d_parents = (const int *)F.d_parents.ptr;
+    for (int l = T.depth() - 1; l >= 0; l--) {
+        const int a = F.parent_off[l], m = F.parent_off[l + 1] - a;
+        if (m == 0) continue;
+        const double *Xc = phi + (size_t)T.level_begin[l + 1] * N;
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, 8 * N, &one, (const double *)F.m2m.ptr, N, Xc, 8 * N,
+                          &zero, Y, N));
+        int rc = scatter_cols(Y, d_parents + a, m, N, 1.0, 0, phi, s);
+        if (rc) return rc;
+    }
+
+    // ---- downward pass: M2L per offset ----
+    const int nslot = (int)F.m2l_off.size() - 1;
+    for (int sl = 0; sl < nslot; sl++) {
+        const int a = F.m2l_off[sl], m = F.m2l_off[sl + 1] - a;
+        if (m <= 0) continue;
+        int rc = gather_cols(phi, (const int *)F.d_m2l_src.ptr + a, m, N, X, s);
+        if (rc) return rc;
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, N, &one, (const double *)F.m2l.ptr + (size_t)sl * N * N,
+                          N, X, N, &zero, Y, N));
+        rc = scatter_cols(Y, (const int *)F.d_m2l_trg.ptr + a, m, N, 1.0, 1, psi, s);
+        if (rc) return rc;
+    }
+    // S2L (X list): downward check potentials, solved per level
+    const int mx = (int)F.s2l_nodes.size();
+    if (mx) {
+        FCUDA(cudaMemsetAsync(F.dcheck.ptr, 0, sizeof(double) * (size_t)mx * n * kc, s));
+        bool any = false;
+        for (int k = 0; k < 2; k++) {
+            if (F.s2l[k].uk < 0 || F.s2l[k].n_items == 0 || (k == 1 && !d_dl)) continue;
+            int rc = pack_points(k, F.s2l[k].uk);
+            if (!rc)
+                rc = run_pass(F.s2l[k], prec, (const double *)F.rec_pts[k].ptr, (const int *)kd->d_beg[k].ptr,
+                              (const int *)kd->d_end[k].ptr, (const double *)F.dc_xyz.ptr, (double *)F.dcheck.ptr,
+                              counter, sms, s);
+            if (rc) return rc;
+            any = true;
+        }
+        if (any)
+            for (int l = 0; l + 1 < (int)F.s2l_level_off.size(); l++) {
+                const int a = F.s2l_level_off[l], m = F.s2l_level_off[l + 1] - a;
+                if (m <= 0) continue;
+                const double alpha = std::ldexp(1.0, -l);
+                FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, n * kc, &alpha, (const double *)F.dc2de.ptr,
+                                  N, (const double *)F.dcheck.ptr + (size_t)a * n * kc, n * kc, &zero, Y, N));
+                int rc = scatter_cols(Y, (const int *)F.d_s2l_nodes.ptr + a, m, N, 1.0, 1, psi, s);
+                if (rc) return rc;
+            }
+    }
+    // L2L, top down: the level-l children block of the level-(l-1) parents
+    for (int l = 1; l <= T.depth(); l++) {
+        const int a = F.parent_off[l - 1], m = F.parent_off[l] - a;
+        if (m == 0) continue;
+        int rc = gather_cols(psi, d_parents + a, m, N, X, s);
+        if (rc) return rc;
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, 8 * N, m, N, &one, (const double *)F.l2l.ptr, 8 * N, X, N,
+                          &one, psi + (size_t)T.level_begin[l] * N, 8 * N));
+    }
+
+    // ---- evaluation at the targets: L2T and M2T (W list) ----
+    const long long npts = (long long)nn * n;
+    auto pack_surface = [&](const DevBuf &xyz, const double *dens, int uk) -> int {
+        const int rs = uk_record_stride(uk);
+        int rc = F.rec_surf.reserve(sizeof(double) * (size_t)npts * rs);
+        if (rc) return rc;
+        if (launch_pack_records((int)npts, nullptr, (const double *)xyz.ptr, dens, ke, nullptr, 0, rs,
+                                (double *)F.rec_surf.ptr, s) != cudaSuccess)
+            return STK_ERR_CUDA;
+        return STK_OK;
+    };
+    const double *trg_xyz = (const double *)kd->d_xyz[2].ptr;
+    int rc = pack_surface(F.de_xyz, psi, F.l2t.uk);
+    if (!rc)
+        rc = run_pass(F.l2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.l2t.src_beg.ptr,
+                      (const int *)F.l2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
+    if (!rc && F.m2t.n_items) {
+        rc = pack_surface(F.ue_xyz, phi, F.m2t.uk);
+        if (!rc)
+            rc = run_pass(F.m2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.m2t.src_beg.ptr,
+                          (const int *)F.m2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
+    }
+    return rc;
+}
+
+}  // namespace stk

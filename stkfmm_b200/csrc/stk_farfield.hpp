@@ -1,0 +1,84 @@
+// stk_farfield.hpp -- KIFMM far field (S2M, M2M, M2L, S2L, L2L, L2T, M2T) on the GPU.
+//
+// Stands in for the far-field part of PVFMM's PtFMM_Evaluate
+// (Lib/src/FMMData.cpp:198), which is not part of the reference tree.  Surfaces
+// follow stkfmm::surface (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85) and the
+// radii of the reference's operator generator (M2L/SVD_pvfmm.hpp:37-38):
+// upward equivalent and downward check at 1.05, upward check and downward
+// equivalent at 2.95 times the box half-width, centred on the box.
+#pragma once
+#include <vector>
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include "stk_handle.hpp"
+#include "stk_kernel_table.hpp"
+#include "stk_p2p.cuh"
+#include "stk_tree.hpp"
+
+namespace stk {
+
+constexpr double kRad0 = 1.05;  // upward equivalent, downward check
+constexpr double kRad1 = 2.95;  // upward check, downward equivalent
+
+// One P2P evaluation over a list, with its work items resident on the device.
+struct ListPass {
+    int uk = -1;
+    int n_items = 0;
+    long long pairs = 0;
+    DevBuf items, ent, src_beg, src_end, trg_box_centre;
+    void reset() {
+        uk = -1;
+        n_items = 0;
+        pairs = 0;
+    }
+};
+
+struct FarField {
+    int p = 0, n = 0;      // multipole order, surface points per box
+    int ke = 0, kc = 0;    // equivalent density and check potential dims
+    int m2x = -1;          // micro-kernel of the translations (k_m2m = k_m2l = k_l2l)
+    bool ready = false;
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    // level-independent operators (column-major, FP64)
+    DevBuf uc2ue, dc2de;   // (n ke) x (n kc)
+    DevBuf m2m;            // [M2M_0 .. M2M_7]: (n ke) x (8 n ke)
+    DevBuf l2l;            // [L2L_0; ..; L2L_7]: (8 n ke) x (n ke)
+    DevBuf m2l;            // 316 blocks of (n ke) x (n ke)
+    std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
+    // per-tree data
+    DevBuf unit_surf;          // n x 3 points on [-1,1]^3
+    DevBuf ue_xyz, de_xyz;     // every node's surfaces (nodes x n x 3)
+    DevBuf uc_xyz, dc_xyz;     // S2M targets (leaves with sources), S2L targets (nodes with X lists)
+    DevBuf phi, psi;           // equivalent densities per node (nodes x n x ke)
+    DevBuf check, dcheck;      // S2M / S2L check potentials (compact)
+    DevBuf rec_surf, rec_pts[2], tmp0, tmp1;
+    std::vector<int> s2m_nodes, s2l_nodes;          // compact order (sorted by level)
+    std::vector<int> s2m_level_off, s2l_level_off;  // per level start in the compact order
+    DevBuf d_s2m_nodes, d_s2l_nodes;
+    ListPass s2m[2], s2l[2], m2t, l2t;  // [SL, DL]
+    // M2M / L2L per level: the parents (non-leaf nodes) of level l are
+    // parents[parent_off[l] .. parent_off[l+1]) in node order
+    std::vector<int> parents, parent_off;
+    DevBuf d_parents;
+    // M2L: V-list pairs grouped by offset
+    std::vector<int> m2l_off;               // per block, start in the pair arrays
+    DevBuf d_m2l_src, d_m2l_trg;
+    long long m2l_pairs = 0;
+    ~FarField();
+};
+
+// Precompute the operators for (kernel, p) and the per-tree data; returns a
+// stk_status.  Supported: kernels whose translation kernel is laplace_p or
+// stokes_vel (LapPGrad, Stokes, RPY, StokesRegVel) in free space.
+int farfield_setup(Stk3DFMM *f, KernelData *kd);
+
+// trg_sorted += far field of the sources (values already packed / scaled as the
+// near field uses them: d_sl, d_dl in the caller's order).
+int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *trg_sorted,
+                      cudaStream_t s);
+
+}  // namespace stk

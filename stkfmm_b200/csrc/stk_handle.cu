@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/stkfmm_b200.h"
+#include "stk_farfield.hpp"
 #include "stk_handle.hpp"
 #include "stk_kernel_table.hpp"
 #include "stk_p2p.cuh"
@@ -195,6 +196,7 @@ extern "C" int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel) {
     if (!fmm->points_set) return STK_ERR_STATE;
     cudaSetDevice(fmm->device);
     kd->tree_ready = false;
+    kd->far_ready = false;
     const bool dl = has_dl(kd) && fmm->ndl > 0;
     const int nsl = fmm->nsl, ndl = dl ? fmm->ndl : 0, ntrg = fmm->ntrg;
     // tree points: the largest of SL / DL / targets, ties to targets (FMMData.cpp:123-135)
@@ -282,11 +284,12 @@ extern "C" int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision) {
     return STK_OK;
 }
 
-// Near-field evaluation on device buffers in the caller's order.  d_sl / d_dl
-// hold values already scaled (scaleSrc); d_out_user receives
-// trg += sF^k * result (scaleTrg) in the caller's order.
+// Near-field (and with far = true, the KIFMM far-field) evaluation on device
+// buffers in the caller's order.  d_sl / d_dl hold values already scaled
+// (scaleSrc); d_out_user receives trg += sF^k * result (scaleTrg) in the
+// caller's order.
 int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *d_out_user,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool far) {
     const KernelInfo *ki = kd->info;
     Octree &T = kd->tree;
     const int nn = T.num_nodes();
@@ -328,6 +331,10 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
         a.period = 1.0;
         a.atomic_out = 0;
         HCUDA(launch_list_p2p(uk, f->precision, a, f->sms, s));
+    }
+    if (far) {
+        rc = farfield_evaluate(f, kd, d_sl, dl ? d_dl : nullptr, out, s);
+        if (rc) return rc;
     }
     HCUDA(cudaEventRecord(kd->ev1, s));
     // caller order + scaleTrg factors
@@ -384,7 +391,7 @@ extern "C" int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int 
     if (rc) return rc;
     HCUDA(cudaMemsetAsync(kd->d_out_user.ptr, 0, sizeof(double) * nTrg * ki->kdim_trg, s));
     rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
-                     (double *)kd->d_out_user.ptr, s);
+                     (double *)kd->d_out_user.ptr, s, false);
     if (rc) return rc;
     std::vector<double> res((size_t)nTrg * ki->kdim_trg);
     HCUDA(cudaMemcpyAsync(res.data(), kd->d_out_user.ptr, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -406,7 +413,7 @@ extern "C" int Stk3DFMM_evaluate_near_device(Stk3DFMM *fmm, unsigned kernel, con
         return STK_ERR_INVALID_ARG;
     cudaSetDevice(fmm->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : fmm->stream;
-    return near_device(fmm, kd, d_src_SL_value, dl ? d_src_DL_value : nullptr, d_trg_value, s);
+    return near_device(fmm, kd, d_src_SL_value, dl ? d_src_DL_value : nullptr, d_trg_value, s, false);
 }
 
 extern "C" int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms) {
@@ -468,13 +475,62 @@ extern "C" int Stk3DFMM_get_ulist(Stk3DFMM *fmm, unsigned kernel, int *sizes, in
     return STK_OK;
 }
 
+// The KIFMM operators and per-tree far-field data are built at the first
+// evaluation after setupTree (the reference builds them in setupTree,
+// FMMData.cpp:107-167); evaluate_near never needs them.
+static int ensure_far(Stk3DFMM *fmm, KernelData *kd) {
+    if (kd->far_ready) return STK_OK;
+    const int rc = farfield_setup(fmm, kd);
+    if (rc) return rc;
+    kd->far_ready = true;
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value,
                                      const int nTrg, double *trg_value, const int nDL, double *src_DL_value) {
     KernelData *kd = nullptr;
     int rc = check_eval_args(fmm, kernel, nSL, src_SL_value, nTrg, trg_value, nDL, src_DL_value, kd);
     if (rc) return rc;
-    // the KIFMM far field (S2M, M2M, M2L, L2L, L2T, W/X lists) is not built yet
-    return STK_ERR_NOT_SUPPORTED;
+    cudaSetDevice(fmm->device);
+    rc = ensure_far(fmm, kd);
+    if (rc) return rc;
+    const KernelInfo *ki = kd->info;
+    const bool dl = has_dl(kd) && fmm->ndl > 0;
+    cudaStream_t s = fmm->stream;
+    std::vector<double> slv(src_SL_value, src_SL_value + (size_t)nSL * ki->kdim_sl);
+    std::vector<double> dlv;
+    if (dl) dlv.assign(src_DL_value, src_DL_value + (size_t)nDL * ki->kdim_dl);
+    scale_src(fmm, kd, slv, dlv);
+    rc = kd->d_val[0].upload(slv.data(), slv.size() * sizeof(double), s);
+    if (!rc && dl) rc = kd->d_val[1].upload(dlv.data(), dlv.size() * sizeof(double), s);
+    if (!rc) rc = kd->d_out_user.reserve(sizeof(double) * std::max(1, nTrg) * ki->kdim_trg);
+    if (rc) return rc;
+    HCUDA(cudaMemsetAsync(kd->d_out_user.ptr, 0, sizeof(double) * nTrg * ki->kdim_trg, s));
+    rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
+                     (double *)kd->d_out_user.ptr, s, true);
+    if (rc) return rc;
+    std::vector<double> res((size_t)nTrg * ki->kdim_trg);
+    HCUDA(cudaMemcpyAsync(res.data(), kd->d_out_user.ptr, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    HCUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < res.size(); i++) trg_value[i] += res[i];
+    return STK_OK;
+}
+
+extern "C" int Stk3DFMM_evaluate_fmm_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value,
+                                            double *d_trg_value, const double *d_src_DL_value, void *stream) {
+    if (!fmm) return STK_ERR_INVALID_ARG;
+    KernelData *kd = get_kd(fmm, kernel);
+    if (!kd) return STK_ERR_KERNEL;
+    if (!kd->tree_ready) return STK_ERR_STATE;
+    if (fmm->scale_factor != 1.0) return STK_ERR_NOT_SUPPORTED;
+    const bool dl = has_dl(kd) && fmm->ndl > 0;
+    if ((fmm->nsl > 0 && !d_src_SL_value) || (dl && !d_src_DL_value) || (fmm->ntrg > 0 && !d_trg_value))
+        return STK_ERR_INVALID_ARG;
+    cudaSetDevice(fmm->device);
+    const int rc = ensure_far(fmm, kd);
+    if (rc) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : fmm->stream;
+    return near_device(fmm, kd, d_src_SL_value, dl ? d_src_DL_value : nullptr, d_trg_value, s, true);
 }
 
 extern "C" int Stk3DFMM_evaluate_kernel(Stk3DFMM *fmm, unsigned kernel, int nThreads, unsigned p2p, int nSrc,

@@ -24,6 +24,8 @@ struct DevBuf {
     int upload(const void *src, size_t n, cudaStream_t s);
 };
 
+struct FarField;
+
 // One activated kernel: the reference's impl::FMMData (STKFMM_impl.hpp:19-174).
 struct KernelData {
     const KernelInfo *info = nullptr;
@@ -37,6 +39,8 @@ struct KernelData {
     DevBuf d_val[2], d_rec[2], d_out_sorted, d_out_user, d_alpha;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the P2P launches of the last evaluation
     bool timed = false;
+    std::unique_ptr<FarField> far;  // KIFMM operators and per-tree far-field data
+    bool far_ready = false;
     ~KernelData();
 };
 
@@ -59,5 +63,5 @@ struct Stk3DFMM {
 
 namespace stk {
 int near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *d_out_user,
-                cudaStream_t s);
+                cudaStream_t s, bool far);
 }

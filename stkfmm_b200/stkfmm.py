@@ -210,6 +210,11 @@ class Stk3DFMM:
         check(lib().Stk3DFMM_evaluate_near_device(self.fmm, int(kernel), d_sl, d_trg, d_dl, stream),
               "evaluate_near_device")
 
+    def evaluate_fmm_device(self, kernel, d_sl, d_trg, d_dl=None, stream=None):
+        """evaluate_fmm on device pointers (ints) in the caller's order, unit box only."""
+        check(lib().Stk3DFMM_evaluate_fmm_device(self.fmm, int(kernel), d_sl, d_trg, d_dl, stream),
+              "evaluate_fmm_device")
+
     def last_kernel_ms(self, kernel) -> float:
         ms = ctypes.c_float()
         check(lib().Stk3DFMM_last_kernel_ms(self.fmm, int(kernel), ctypes.byref(ms)), "last_kernel_ms")
