@@ -61,6 +61,8 @@ SIGNATURES = [
     ("Stk3DFMM_evaluate_near_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("Stk3DFMM_evaluate_fmm_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("Stk3DFMM_last_kernel_ms", c_int, [c_void_p, c_uint, P_f]),
+    ("Stk3DFMM_last_phase_ms", c_int, [c_void_p, c_uint, P_f]),
+    ("Stk3DFMM_get_fmm_stats", c_int, [c_void_p, c_uint, P_ll]),
     ("Stk3DFMM_get_tree_stats", c_int, [c_void_p, c_uint, P_ll]),
     ("Stk3DFMM_get_ulist", c_int, [c_void_p, c_uint, P_i] + [P_i] * 11),
     ("stk_octree_build", c_void_p, [P_d, c_int, c_int, c_int, P_d, c_int, P_d, c_int, P_d, c_int]),

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/stkfmm_b200.h"
@@ -134,41 +135,90 @@ __global__ void pinv_scale_kernel(const double *__restrict__ U, const double *__
     }
 }
 
-// dst[:, j] (= or +=) src[:, col(j)] for N-row column blocks; col = null -> j
-__global__ void gather_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int m, int N,
-                                   double *__restrict__ dst) {
+// dst[:, j] = src[:, cols[j]] for N-row columns (converted to the type of dst)
+template <class TS, class TD>
+__global__ void gather_cols_kernel(const TS *__restrict__ src, const int *__restrict__ cols, int m, int N,
+                                   TD *__restrict__ dst) {
     const long long total = (long long)m * N;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(idx / N), r = (int)(idx - (long long)j * N);
-        dst[idx] = src[(size_t)cols[j] * N + r];
+        dst[idx] = (TD)src[(size_t)cols[j] * N + r];
     }
 }
 
-__global__ void scatter_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int m, int N,
+// dst[:, cols[j]] (= or +=) alpha src[:, j]; no two j may share a column
+template <class TS>
+__global__ void scatter_cols_kernel(const TS *__restrict__ src, const int *__restrict__ cols, int m, int N,
                                     double alpha, int add, double *__restrict__ dst) {
     const long long total = (long long)m * N;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(idx / N), r = (int)(idx - (long long)j * N);
         double *d = dst + (size_t)cols[j] * N + r;
-        *d = add ? *d + alpha * src[idx] : alpha * src[idx];
+        *d = add ? *d + alpha * (double)src[idx] : alpha * (double)src[idx];
     }
 }
 
 inline int grid_for(long long total) { return (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 32)); }
 
-int gather_cols(const double *src, const int *cols, int m, int N, double *dst, cudaStream_t s) {
+template <class TS, class TD>
+int gather_cols(const TS *src, const int *cols, int m, int N, TD *dst, cudaStream_t s) {
     if (m <= 0) return STK_OK;
-    gather_cols_kernel<<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, dst);
+    gather_cols_kernel<TS, TD><<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, dst);
     return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
 }
 
-int scatter_cols(const double *src, const int *cols, int m, int N, double alpha, int add, double *dst,
-                 cudaStream_t s) {
+template <class TS>
+int scatter_cols(const TS *src, const int *cols, int m, int N, double alpha, int add, double *dst, cudaStream_t s) {
     if (m <= 0) return STK_OK;
-    scatter_cols_kernel<<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, alpha, add, dst);
+    scatter_cols_kernel<TS><<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, alpha, add, dst);
     return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+// R[i + N j] = A[i + m j] for i <= j (the R factor of a QR factorisation)
+__global__ void upper_copy_kernel(const double *__restrict__ A, long long m, int N, double *__restrict__ R) {
+    const long long total = (long long)N * N;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % N), j = (int)(idx / N);
+        if (i <= j) R[idx] = A[(size_t)i + (size_t)m * j];
+    }
+}
+
+constexpr int kM2LChunk = 256;  // pairs (columns) per batched-GEMM problem of the M2L
+
+// X[r + k j] = phi_hat[r + k gsrc[j]], or 0 for a padding column (gsrc[j] < 0)
+template <class T>
+__global__ void m2l_gather_kernel(const double *__restrict__ phi_hat, const int *__restrict__ gsrc, int k,
+                                  long long ncol, T *__restrict__ X) {
+    const long long total = ncol * k;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long j = idx / k;
+        const int r = (int)(idx - j * k);
+        const int a = gsrc[j];
+        X[idx] = a >= 0 ? (T)phi_hat[(size_t)a * k + r] : (T)0;
+    }
+}
+
+// psi_hat[r + k t] = sum over the columns of target t (in order) of Y[r + k col]
+template <class T>
+__global__ void m2l_reduce_kernel(const T *__restrict__ Y, const int *__restrict__ off, const int *__restrict__ col,
+                                  int nn, int k, double *__restrict__ psi_hat) {
+    const long long total = (long long)nn * k;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(idx / k), r = (int)(idx - (long long)t * k);
+        double acc = 0.0;
+        for (int e = off[t]; e < off[t + 1]; e++) acc += (double)Y[(size_t)col[e] * k + r];
+        psi_hat[idx] = acc;
+    }
+}
+
+__global__ void to_float_kernel(const double *__restrict__ a, long long n, float *__restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
 }
 
 // A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
@@ -201,6 +251,38 @@ int pinv(FarField &F, double *A, int m, double *A_inv, double rtol, cudaStream_t
     FCUDA(cudaMemcpyAsync(&h_info, info.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
     FCUDA(cudaStreamSynchronize(s));
     return h_info == 0 ? STK_OK : STK_ERR_CUDA;
+}
+
+// Singular values S and right singular vectors VT (N x N, rows v_i^T) of a tall
+// m x N matrix A (m >= N, column-major, overwritten): Householder QR A = Q R,
+// then the SVD of the N x N factor R, which has the same S and V.
+int tall_svd(FarField &F, double *A, long long m, int N, double *S, double *VT, cudaStream_t s) {
+    if (m > 0x7fffffffLL) return STK_ERR_SIZE;
+    cusolverDnSetStream(F.solver, s);
+    int lq = 0, ls = 0;
+    if (cusolverDnDgeqrf_bufferSize(F.solver, (int)m, N, A, (int)m, &lq) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    if (cusolverDnDgesvd_bufferSize(F.solver, N, N, &ls) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    DevBuf work, tau, R, info, rwork;
+    int rc = work.reserve(sizeof(double) * (size_t)std::max(std::max(lq, ls), 1));
+    if (!rc) rc = tau.reserve(sizeof(double) * N);
+    if (!rc) rc = R.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = info.reserve(2 * sizeof(int));
+    if (!rc) rc = rwork.reserve(sizeof(double) * N);
+    if (rc) return rc;
+    if (cusolverDnDgeqrf(F.solver, (int)m, N, A, (int)m, (double *)tau.ptr, (double *)work.ptr, lq, (int *)info.ptr) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return STK_ERR_CUDA;
+    // R: the upper triangle of the first N rows
+    FCUDA(cudaMemsetAsync(R.ptr, 0, sizeof(double) * (size_t)N * N, s));
+    upper_copy_kernel<<<grid_for((long long)N * N), 256, 0, s>>>(A, m, N, (double *)R.ptr);
+    FCUDA(cudaGetLastError());
+    if (cusolverDnDgesvd(F.solver, 'N', 'A', N, N, (double *)R.ptr, N, S, nullptr, N, VT, N, (double *)work.ptr, ls,
+                         (double *)rwork.ptr, (int *)info.ptr + 1) != CUSOLVER_STATUS_SUCCESS)
+        return STK_ERR_CUDA;
+    int h_info[2] = {0, 0};
+    FCUDA(cudaMemcpyAsync(h_info, info.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaStreamSynchronize(s));
+    return h_info[0] == 0 && h_info[1] == 0 ? STK_OK : STK_ERR_CUDA;
 }
 
 int upload_points(DevBuf &b, const std::vector<double> &v, cudaStream_t s) {
@@ -263,25 +345,81 @@ int build_operators(FarField &F, cudaStream_t s) {
         FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &half, (const double *)F.dc2de.ptr, N,
                           (const double *)K.ptr, N, &zero, (double *)F.l2l.ptr + (size_t)o * N, 8 * N));
     }
-    // M2L for every well-separated offset of a same-level source box
+    // M2L for every well-separated offset d of a same-level source box, in the
+    // compressed form  M2L_d = DC2DE U C_d V^T,  C_d = U^T A_d V,  A_d = K(DC, UE + d).
+    // U spans the columns of [A_d ...] and V the rows of [A_d; ...], both cut at
+    // the relative singular value m2l_rtol, so one M2L costs 2 k^2 flops per pair
+    // instead of 2 N^2.
     F.m2l_slot.assign(kNumOffsets, -1);
     int nslot = 0;
     for (int code = 0; code < kNumOffsets; code++) {
         const int dx = code % 7 - 3, dy = (code / 7) % 7 - 3, dz = code / 49 - 3;
         if (std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz))) >= 2) F.m2l_slot[code] = nslot++;
     }
-    rc = F.m2l.reserve(sizeof(double) * (size_t)N * N * nslot);
+    auto offset_matrix = [&](int code, double *M, int ld) {
+        const double dx = code % 7 - 3, dy = (code / 7) % 7 - 3, dz = code / 49 - 3;
+        int r = upload_points(X, scaled_surface(unit, 0, 0, 0, kRad0 * r0), s);
+        if (!r) r = upload_points(Y, scaled_surface(unit, dx, dy, dz, kRad0 * r0), s);
+        if (!r) r = kernel_matrix(F.m2x, (const double *)X.ptr, n, (const double *)Y.ptr, n, M, ld, s);
+        return r;
+    };
+    const long long m = (long long)nslot * N;
+    DevBuf stack, VTv, VTu, Sv, Su;
+    rc = stack.reserve(sizeof(double) * (size_t)m * N);
+    if (!rc) rc = VTv.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = VTu.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = Sv.reserve(sizeof(double) * N);
+    if (!rc) rc = Su.reserve(sizeof(double) * N);
     if (rc) return rc;
+    double *A = (double *)stack.ptr;
+    // rows of [A_d; ...] -> V
+    for (int code = 0; code < kNumOffsets; code++)
+        if (F.m2l_slot[code] >= 0 && (rc = offset_matrix(code, A + (size_t)F.m2l_slot[code] * N, (int)m))) return rc;
+    rc = tall_svd(F, A, m, N, (double *)Sv.ptr, (double *)VTv.ptr, s);
+    if (rc) return rc;
+    // columns of [A_d ...] = rows of [A_d^T; ...] -> U
     for (int code = 0; code < kNumOffsets; code++) {
         const int sl = F.m2l_slot[code];
         if (sl < 0) continue;
-        const double dx = code % 7 - 3, dy = (code / 7) % 7 - 3, dz = code / 49 - 3;
-        rc = kmat(scaled_surface(unit, 0, 0, 0, kRad0 * r0), scaled_surface(unit, dx, dy, dz, kRad0 * r0),
-                  (double *)K.ptr);
-        if (rc) return rc;
-        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &one, (const double *)F.dc2de.ptr, N,
-                          (const double *)K.ptr, N, &zero, (double *)F.m2l.ptr + (size_t)sl * N * N, N));
+        if ((rc = offset_matrix(code, (double *)K.ptr, N))) return rc;
+        FBLAS(cublasDgeam(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, &one, (const double *)K.ptr, N, &zero,
+                          (const double *)K.ptr, N, A + (size_t)sl * N, (int)m));
     }
+    rc = tall_svd(F, A, m, N, (double *)Su.ptr, (double *)VTu.ptr, s);
+    if (rc) return rc;
+    std::vector<double> sv(N), su(N);
+    FCUDA(cudaMemcpyAsync(sv.data(), Sv.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaMemcpyAsync(su.data(), Su.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaStreamSynchronize(s));
+    int k = 1;
+    for (int i = 0; i < N; i++)
+        if (sv[i] > F.m2l_rtol * sv[0] || su[i] > F.m2l_rtol * su[0]) k = std::max(k, i + 1);
+    F.m2l_rank = k;
+    rc = F.m2l_c.reserve(sizeof(double) * (size_t)nslot * k * k);
+    if (!rc) rc = F.m2l_vt.reserve(sizeof(double) * (size_t)k * N);
+    if (!rc) rc = F.m2l_e.reserve(sizeof(double) * (size_t)N * k);
+    if (rc) return rc;
+    // V^T: the first k rows of VTv;  E = DC2DE U,  U^T = the first k rows of VTu
+    FBLAS(cublasDgeam(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, N, &one, (const double *)VTv.ptr, N, &zero,
+                      (const double *)VTv.ptr, N, (double *)F.m2l_vt.ptr, k));
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_T, N, k, N, &one, (const double *)F.dc2de.ptr, N,
+                      (const double *)VTu.ptr, N, &zero, (double *)F.m2l_e.ptr, N));
+    for (int code = 0; code < kNumOffsets; code++) {
+        const int sl = F.m2l_slot[code];
+        if (sl < 0) continue;
+        if ((rc = offset_matrix(code, (double *)K.ptr, N))) return rc;
+        // T = A_d V (N x k), C_d = U^T T (k x k)
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_T, N, k, N, &one, (const double *)K.ptr, N,
+                          (const double *)VTv.ptr, N, &zero, (double *)T.ptr, N));
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, k, N, &one, (const double *)VTu.ptr, N,
+                          (const double *)T.ptr, N, &zero, (double *)F.m2l_c.ptr + (size_t)sl * k * k, k));
+    }
+    // FP32 copy for the mixed-precision path (C_d holds no pseudo-inverse)
+    rc = F.m2l_c32.reserve(sizeof(float) * (size_t)nslot * k * k);
+    if (rc) return rc;
+    to_float_kernel<<<grid_for((long long)nslot * k * k), 256, 0, s>>>((const double *)F.m2l_c.ptr,
+                                                                      (long long)nslot * k * k, (float *)F.m2l_c32.ptr);
+    FCUDA(cudaGetLastError());
     FCUDA(cudaStreamSynchronize(s));
     return STK_OK;
 }
@@ -346,7 +484,12 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     const int p = f->mult_order;
     const int ke = uk_sdim_host(m2x), kc = uk_tdim_host(m2x);
     int rc = STK_OK;
-    if (F.p != p || F.m2x != m2x) {
+    // relative singular-value cut of the compressed M2L (environment override for studies)
+    const char *env_rtol = getenv("STKFMM_M2L_RTOL");
+    // (1e-8 changes the FMM error by under 15% up to p = 10; higher orders keep more rank)
+    const double m2l_rtol = env_rtol ? atof(env_rtol) : (p <= 10 ? 1e-8 : 1e-10);
+    if (F.p != p || F.m2x != m2x || F.m2l_rtol != m2l_rtol) {
+        F.m2l_rtol = m2l_rtol;
         F.p = p;
         F.n = 6 * (p - 1) * (p - 1) + 2;
         F.ke = ke;
@@ -380,6 +523,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     FCUDA(cudaGetLastError());
     rc = F.phi.reserve(sizeof(double) * (size_t)nn * N);
     if (!rc) rc = F.psi.reserve(sizeof(double) * (size_t)nn * N);
+    if (!rc) rc = F.phi_hat.reserve(sizeof(double) * (size_t)nn * F.m2l_rank);
+    if (!rc) rc = F.psi_hat.reserve(sizeof(double) * (size_t)nn * F.m2l_rank);
     if (rc) return rc;
 
     auto by_level = [&](std::vector<int> &nodes, std::vector<int> &off) {
@@ -397,7 +542,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         if (T.src_count(b) > 0) F.s2m_nodes.push_back(b);
     by_level(F.s2m_nodes, F.s2m_level_off);
     const int ms = (int)F.s2m_nodes.size();
-    rc = F.d_s2m_nodes.upload(F.s2m_nodes.data(), sizeof(int) * std::max(ms, 1), s);
+    rc = F.d_s2m_nodes.upload(F.s2m_nodes.data(), sizeof(int) * ms, s);
     if (!rc) rc = F.uc_xyz.reserve(sizeof(double) * 3 * (size_t)std::max(ms, 1) * n);
     if (!rc) rc = F.check.reserve(sizeof(double) * (size_t)std::max(ms, 1) * n * kc);
     if (rc) return rc;
@@ -426,13 +571,48 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
     }
 
+    // W- and X-list interactions whose point count is at most the surface size
+    // are cheaper, and exact, as direct source-to-target pairs: a W-list source
+    // node with few sources, an X-list target node with few targets.  They join
+    // the U list in the near-field pass of the FMM.
+    // (with SL and DL at the same points one fused pass covers both sets)
+    auto w_direct = [&](int a) {
+        const int c0 = T.sets[0].count(a), c1 = T.sets[1].count(a);
+        return (kd->fused ? std::max(c0, c1) : c0 + c1) <= n;
+    };
+    auto x_direct = [&](int c) { return T.trg_count(c) <= n; };
+
+    // ---- near field of the FMM: U list + direct W / X entries, per target leaf ----
+    {
+        const PointSet &tg = T.sets[2];
+        std::vector<int> noff(nn + 1, 0), nent;
+        for (int b = 0; b < nn; b++) {
+            noff[b] = (int)nent.size();
+            if (!T.is_leaf(b) || tg.count(b) == 0) continue;
+            for (int e = T.U.off[b]; e < T.U.off[b + 1]; e++) nent.push_back(T.U.ent[e]);
+            for (int e = T.W.off[b]; e < T.W.off[b + 1]; e++)
+                if (w_direct(T.W.ent[e] >> 5)) nent.push_back(T.W.ent[e]);
+            for (int c = b; c >= 0; c = T.parent[c])
+                if (x_direct(c))
+                    for (int e = T.X.off[c]; e < T.X.off[c + 1]; e++) nent.push_back(T.X.ent[e]);
+        }
+        noff[nn] = (int)nent.size();
+        for (int k = 0; k < 2; k++) {
+            F.near[k].reset();
+            if (T.sets[k].n == 0 || ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL] < 0) continue;
+            rc = setup_pass(F.near[k], ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL], tg.node_begin, tg.node_end, noff,
+                            nent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(), nn, false, ctr, s);
+            if (rc) return rc;
+        }
+    }
+
     // ---- S2L: nodes with X lists; targets = their downward check surfaces ----
     F.s2l_nodes.clear();
     for (int b = 0; b < nn; b++)
-        if (T.X.off[b + 1] > T.X.off[b]) F.s2l_nodes.push_back(b);
+        if (T.X.off[b + 1] > T.X.off[b] && !x_direct(b)) F.s2l_nodes.push_back(b);
     by_level(F.s2l_nodes, F.s2l_level_off);
     const int mx = (int)F.s2l_nodes.size();
-    rc = F.d_s2l_nodes.upload(F.s2l_nodes.data(), sizeof(int) * std::max(mx, 1), s);
+    rc = F.d_s2l_nodes.upload(F.s2l_nodes.data(), sizeof(int) * mx, s);
     if (!rc) rc = F.dc_xyz.reserve(sizeof(double) * 3 * (size_t)std::max(mx, 1) * n);
     if (!rc) rc = F.dcheck.reserve(sizeof(double) * (size_t)std::max(mx, 1) * n * kc);
     if (rc) return rc;
@@ -476,10 +656,17 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             if (T.is_leaf(b) && tg.count(b) > 0) lent.push_back((b << 5) | kShiftNone);
         }
         loff[nn] = (int)lent.size();
+        std::vector<int> woff(nn + 1, 0), went;
+        for (int b = 0; b < nn; b++) {
+            woff[b] = (int)went.size();
+            for (int e = T.W.off[b]; e < T.W.off[b + 1]; e++)
+                if (!w_direct(T.W.ent[e] >> 5)) went.push_back(T.W.ent[e]);
+        }
+        woff[nn] = (int)went.size();
         F.m2t.reset();
         F.l2t.reset();
-        rc = setup_pass(F.m2t, ki->slot[SLOT_M2T], tg.node_begin, tg.node_end, T.W.off, T.W.ent, sb.data(),
-                        se.data(), nn, true, ctr, s);
+        rc = setup_pass(F.m2t, ki->slot[SLOT_M2T], tg.node_begin, tg.node_end, woff, went, sb.data(), se.data(), nn,
+                        true, ctr, s);
         if (!rc)
             rc = setup_pass(F.l2t, ki->slot[SLOT_L2T], tg.node_begin, tg.node_end, loff, lent, sb.data(), se.data(),
                             nn, true, ctr, s);
@@ -501,7 +688,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
     }
     F.parent_off[T.depth() + 1] = (int)F.parents.size();
-    rc = F.d_parents.upload(F.parents.data(), sizeof(int) * std::max<size_t>(F.parents.size(), 1), s);
+    rc = F.d_parents.upload(F.parents.data(), sizeof(int) * F.parents.size(), s);
     if (rc) return rc;
 
     // ---- M2L: V-list pairs grouped by offset ----
@@ -522,20 +709,64 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
                 srcs[sl].push_back(a);
                 trgs[sl].push_back(b);
             }
-        F.m2l_off.assign(nslot + 1, 0);
-        std::vector<int> hs, ht;
+        // column chunks of kM2LChunk pairs of one offset; padded columns gather zeros
+        std::vector<int> gsrc, chunk_slot;
+        std::vector<std::vector<int>> cols_of(nn);  // per target node: its columns, by offset
+        long long pairs = 0;
         for (int sl = 0; sl < nslot; sl++) {
-            F.m2l_off[sl] = (int)hs.size();
-            hs.insert(hs.end(), srcs[sl].begin(), srcs[sl].end());
-            ht.insert(ht.end(), trgs[sl].begin(), trgs[sl].end());
+            const int m = (int)srcs[sl].size();
+            for (int c0 = 0; c0 < m; c0 += kM2LChunk) {
+                const int base = (int)gsrc.size();
+                chunk_slot.push_back(sl);
+                for (int i = 0; i < kM2LChunk; i++) {
+                    const bool real = c0 + i < m;
+                    gsrc.push_back(real ? srcs[sl][c0 + i] : -1);
+                    if (real) cols_of[trgs[sl][c0 + i]].push_back(base + i);
+                }
+            }
+            pairs += m;
         }
-        F.m2l_off[nslot] = (int)hs.size();
-        F.m2l_pairs = (long long)hs.size();
-        rc = F.d_m2l_src.upload(hs.data(), sizeof(int) * std::max<size_t>(hs.size(), 1), s);
-        if (!rc) rc = F.d_m2l_trg.upload(ht.data(), sizeof(int) * std::max<size_t>(ht.size(), 1), s);
+        F.m2l_pairs = pairs;
+        F.m2l_chunks = (int)chunk_slot.size();
+        F.m2l_cols = (long long)gsrc.size();
+        std::vector<int> red_off(nn + 1, 0), red_col;
+        red_col.reserve(pairs);
+        for (int b = 0; b < nn; b++) {
+            red_off[b] = (int)red_col.size();
+            red_col.insert(red_col.end(), cols_of[b].begin(), cols_of[b].end());
+        }
+        red_off[nn] = (int)red_col.size();
+        const int k = F.m2l_rank;
+        rc = F.d_m2l_gsrc.upload(gsrc.data(), sizeof(int) * gsrc.size(), s);
+        if (!rc) rc = F.d_m2l_red_off.upload(red_off.data(), sizeof(int) * red_off.size(), s);
+        if (!rc) rc = F.d_m2l_red_col.upload(red_col.data(), sizeof(int) * red_col.size(), s);
+        if (!rc) rc = F.m2l_x.reserve(sizeof(double) * (size_t)k * std::max<long long>(F.m2l_cols, 1));
+        if (!rc) rc = F.m2l_y.reserve(sizeof(double) * (size_t)k * std::max<long long>(F.m2l_cols, 1));
         if (rc) return rc;
+        // pointer arrays of the batched GEMMs (FP64 and FP32 views of the same buffers)
+        const int nc = F.m2l_chunks;
+        std::vector<const double *> pa(nc), pb(nc);
+        std::vector<double *> pc(nc);
+        std::vector<const float *> qa(nc), qb(nc);
+        std::vector<float *> qc(nc);
+        const size_t step = (size_t)kM2LChunk * k;
+        for (int c = 0; c < nc; c++) {
+            pa[c] = (const double *)F.m2l_c.ptr + (size_t)chunk_slot[c] * k * k;
+            pb[c] = (const double *)F.m2l_x.ptr + c * step;
+            pc[c] = (double *)F.m2l_y.ptr + c * step;
+            qa[c] = (const float *)F.m2l_c32.ptr + (size_t)chunk_slot[c] * k * k;
+            qb[c] = (const float *)F.m2l_x.ptr + c * step;
+            qc[c] = (float *)F.m2l_y.ptr + c * step;
+        }
+        rc = F.d_ptr64[0].upload(pa.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_ptr64[1].upload(pb.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_ptr64[2].upload(pc.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_ptr32[0].upload(qa.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_ptr32[1].upload(qb.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_ptr32[2].upload(qc.data(), sizeof(void *) * nc, s);
+        if (rc) return rc;
+        // host vectors above are pageable: their copies complete before upload returns
         int maxm = 0;
-        for (int sl = 0; sl < nslot; sl++) maxm = std::max(maxm, F.m2l_off[sl + 1] - F.m2l_off[sl]);
         for (int l = 0; l <= T.depth(); l++) maxm = std::max(maxm, F.parent_off[l + 1] - F.parent_off[l]);
         maxm = std::max(maxm, std::max(ms, mx));
         rc = F.tmp0.reserve(sizeof(double) * (size_t)std::max(maxm, 1) * N);
@@ -599,6 +830,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
             if (rc) return rc;
         }
     }
+    FCUDA(cudaEventRecord(kd->ph[1], s));
     // M2M, bottom up: parents of level l from the contiguous children block at level l+1
     const int *d_parents = (const int *)F.d_parents.ptr;
     for (int l = T.depth() - 1; l >= 0; l--) {
@@ -611,18 +843,48 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         if (rc) return rc;
     }
 
-    // ---- downward pass: M2L per offset ----
-    const int nslot = (int)F.m2l_off.size() - 1;
-    for (int sl = 0; sl < nslot; sl++) {
-        const int a = F.m2l_off[sl], m = F.m2l_off[sl + 1] - a;
-        if (m <= 0) continue;
-        int rc = gather_cols(phi, (const int *)F.d_m2l_src.ptr + a, m, N, X, s);
-        if (rc) return rc;
-        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, N, &one, (const double *)F.m2l.ptr + (size_t)sl * N * N,
-                          N, X, N, &zero, Y, N));
-        rc = scatter_cols(Y, (const int *)F.d_m2l_trg.ptr + a, m, N, 1.0, 1, psi, s);
-        if (rc) return rc;
+    FCUDA(cudaEventRecord(kd->ph[2], s));
+    // ---- downward pass: compressed M2L per offset ----
+    const int k = F.m2l_rank;
+    double *phi_hat = (double *)F.phi_hat.ptr, *psi_hat = (double *)F.psi_hat.ptr;
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, nn, N, &one, (const double *)F.m2l_vt.ptr, k, phi, N, &zero,
+                      phi_hat, k));
+    // gather the sources of every (offset, chunk) column, one batched GEMM over the
+    // chunks, then each target sums its columns in offset order (deterministic)
+    const long long ncol = F.m2l_cols;
+    if (ncol > 0) {
+        const int gg = grid_for(ncol * k);
+        if (prec == PREC_MIXED) {
+            // the translation C_d carries no pseudo-inverse: FP32 operands, FP32 accumulation
+            m2l_gather_kernel<float><<<gg, 256, 0, s>>>(phi_hat, (const int *)F.d_m2l_gsrc.ptr, k, ncol,
+                                                        (float *)F.m2l_x.ptr);
+            FCUDA(cudaGetLastError());
+            const float onef = 1.0f, zerof = 0.0f;
+            FBLAS(cublasSgemmBatched(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &onef,
+                                     (const float *const *)F.d_ptr32[0].ptr, k, (const float *const *)F.d_ptr32[1].ptr,
+                                     k, &zerof, (float *const *)F.d_ptr32[2].ptr, k, F.m2l_chunks));
+            m2l_reduce_kernel<float><<<grid_for((long long)nn * k), 256, 0, s>>>(
+                (const float *)F.m2l_y.ptr, (const int *)F.d_m2l_red_off.ptr, (const int *)F.d_m2l_red_col.ptr, nn, k,
+                psi_hat);
+        } else {
+            m2l_gather_kernel<double><<<gg, 256, 0, s>>>(phi_hat, (const int *)F.d_m2l_gsrc.ptr, k, ncol,
+                                                         (double *)F.m2l_x.ptr);
+            FCUDA(cudaGetLastError());
+            FBLAS(cublasDgemmBatched(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &one,
+                                     (const double *const *)F.d_ptr64[0].ptr, k,
+                                     (const double *const *)F.d_ptr64[1].ptr, k, &zero,
+                                     (double *const *)F.d_ptr64[2].ptr, k, F.m2l_chunks));
+            m2l_reduce_kernel<double><<<grid_for((long long)nn * k), 256, 0, s>>>(
+                (const double *)F.m2l_y.ptr, (const int *)F.d_m2l_red_off.ptr, (const int *)F.d_m2l_red_col.ptr, nn,
+                k, psi_hat);
+        }
+        FCUDA(cudaGetLastError());
+    } else {
+        FCUDA(cudaMemsetAsync(psi_hat, 0, sizeof(double) * (size_t)nn * k, s));
     }
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,
+                      psi, N));
+    FCUDA(cudaEventRecord(kd->ph[3], s));
     // S2L (X list): downward check potentials, solved per level
     const int mx = (int)F.s2l_nodes.size();
     if (mx) {
@@ -649,6 +911,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
                 if (rc) return rc;
             }
     }
+    FCUDA(cudaEventRecord(kd->ph[4], s));
     // L2L, top down: the level-l children block of the level-(l-1) parents
     for (int l = 1; l <= T.depth(); l++) {
         const int a = F.parent_off[l - 1], m = F.parent_off[l] - a;
@@ -670,18 +933,23 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
             return STK_ERR_CUDA;
         return STK_OK;
     };
+    FCUDA(cudaEventRecord(kd->ph[5], s));
     const double *trg_xyz = (const double *)kd->d_xyz[2].ptr;
     int rc = pack_surface(F.de_xyz, psi, F.l2t.uk);
     if (!rc)
         rc = run_pass(F.l2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.l2t.src_beg.ptr,
                       (const int *)F.l2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
-    if (!rc && F.m2t.n_items) {
+    if (rc) return rc;
+    FCUDA(cudaEventRecord(kd->ph[6], s));
+    if (F.m2t.n_items) {
         rc = pack_surface(F.ue_xyz, phi, F.m2t.uk);
         if (!rc)
             rc = run_pass(F.m2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.m2t.src_beg.ptr,
                           (const int *)F.m2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
+        if (rc) return rc;
     }
-    return rc;
+    FCUDA(cudaEventRecord(kd->ph[7], s));
+    return STK_OK;
 }
 
 }  // namespace stk

@@ -47,27 +47,37 @@ struct FarField {
     DevBuf uc2ue, dc2de;   // (n ke) x (n kc)
     DevBuf m2m;            // [M2M_0 .. M2M_7]: (n ke) x (8 n ke)
     DevBuf l2l;            // [L2L_0; ..; L2L_7]: (8 n ke) x (n ke)
-    DevBuf m2l;            // 316 blocks of (n ke) x (n ke)
+    // compressed M2L: M2L_d = m2l_e C_d m2l_vt
+    double m2l_rtol = 0;        // relative singular-value cut of the M2L bases
+    int m2l_rank = 0;           // k
+    DevBuf m2l_c, m2l_c32;      // 316 blocks of k x k (FP64, FP32 copy for the mixed path)
+    DevBuf m2l_vt;              // V^T: k x (n ke)
+    DevBuf m2l_e;               // DC2DE U: (n ke) x k
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
     // per-tree data
     DevBuf unit_surf;          // n x 3 points on [-1,1]^3
     DevBuf ue_xyz, de_xyz;     // every node's surfaces (nodes x n x 3)
     DevBuf uc_xyz, dc_xyz;     // S2M targets (leaves with sources), S2L targets (nodes with X lists)
     DevBuf phi, psi;           // equivalent densities per node (nodes x n x ke)
+    DevBuf phi_hat, psi_hat;   // compressed M2L sources / targets (nodes x k)
     DevBuf check, dcheck;      // S2M / S2L check potentials (compact)
     DevBuf rec_surf, rec_pts[2], tmp0, tmp1;
     std::vector<int> s2m_nodes, s2l_nodes;          // compact order (sorted by level)
     std::vector<int> s2m_level_off, s2l_level_off;  // per level start in the compact order
     DevBuf d_s2m_nodes, d_s2l_nodes;
     ListPass s2m[2], s2l[2], m2t, l2t;  // [SL, DL]
+    ListPass near[2];  // FMM near field per source set: U list + direct W / X entries
     // M2M / L2L per level: the parents (non-leaf nodes) of level l are
     // parents[parent_off[l] .. parent_off[l+1]) in node order
     std::vector<int> parents, parent_off;
     DevBuf d_parents;
-    // M2L: V-list pairs grouped by offset
-    std::vector<int> m2l_off;               // per block, start in the pair arrays
-    DevBuf d_m2l_src, d_m2l_trg;
-    long long m2l_pairs = 0;
+    // M2L: V-list pairs grouped by offset in chunks of columns (one batched GEMM)
+    long long m2l_pairs = 0, m2l_cols = 0;  // pairs; columns including chunk padding
+    int m2l_chunks = 0;
+    DevBuf d_m2l_gsrc;                      // per column: source node, -1 = padding
+    DevBuf d_m2l_red_off, d_m2l_red_col;    // per target node: its columns (CSR, offset order)
+    DevBuf m2l_x, m2l_y;                    // k x columns (FP64, or FP32 in the mixed path)
+    DevBuf d_ptr64[3], d_ptr32[3];          // batched-GEMM pointer arrays (C_d, X chunk, Y chunk)
     ~FarField();
 };
 

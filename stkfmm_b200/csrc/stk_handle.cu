@@ -76,6 +76,8 @@ int DevBuf::upload(const void *src, size_t n, cudaStream_t s) {
 KernelData::~KernelData() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : ph)
+        if (e) cudaEventDestroy(e);
 }
 
 }  // namespace stk
@@ -254,6 +256,8 @@ extern "C" int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel) {
     if (!rc) rc = kd->d_counter.reserve(64);
     if (!rc && !kd->ev0) {
         if (cudaEventCreate(&kd->ev0) != cudaSuccess || cudaEventCreate(&kd->ev1) != cudaSuccess) rc = STK_ERR_CUDA;
+        for (int i = 0; i < KernelData::kPhases && !rc; i++)
+            if (cudaEventCreate(&kd->ph[i]) != cudaSuccess) rc = STK_ERR_CUDA;
     }
     if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = STK_ERR_CUDA;
     if (rc) return rc;
@@ -303,7 +307,10 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
     HCUDA(cudaEventRecord(kd->ev0, s));
     for (int k = 0; k < 2; k++) {
         if (k == 1 && (!dl || kd->fused)) continue;
-        if (kd->n_items[k] == 0) continue;
+        // the FMM's near field: U list plus the W / X interactions evaluated directly
+        const ListPass *fp = far ? &kd->far->near[k] : nullptr;
+        const int n_items = far ? fp->n_items : kd->n_items[k];
+        if (n_items == 0) continue;
         const int uk = kd->fused ? fused_uk(kd) : ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL];
         const int rs = uk_record_stride(uk);
         const PointSet &sp = T.sets[k];
@@ -321,9 +328,9 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
         a.src_rec = rec;
         a.src_box_begin = (const int *)kd->d_beg[k].ptr;
         a.src_box_end = (const int *)kd->d_end[k].ptr;
-        a.list_ent = (const int *)kd->d_uent.ptr;
-        a.items = (const WorkItem *)kd->d_items[k].ptr;
-        a.n_items = kd->n_items[k];
+        a.list_ent = far ? (const int *)fp->ent.ptr : (const int *)kd->d_uent.ptr;
+        a.items = far ? (const WorkItem *)fp->items.ptr : (const WorkItem *)kd->d_items[k].ptr;
+        a.n_items = n_items;
         a.counter = (unsigned int *)kd->d_counter.ptr;
         a.trg_xyz = (const double *)kd->d_xyz[2].ptr;
         a.trg_out = out;
@@ -332,6 +339,8 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
         a.atomic_out = 0;
         HCUDA(launch_list_p2p(uk, f->precision, a, f->sms, s));
     }
+    HCUDA(cudaEventRecord(kd->ph[0], s));
+    kd->last_far = far;
     if (far) {
         rc = farfield_evaluate(f, kd, d_sl, dl ? d_dl : nullptr, out, s);
         if (rc) return rc;
@@ -426,6 +435,23 @@ extern "C" int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms
     return STK_OK;
 }
 
+extern "C" int Stk3DFMM_last_phase_ms(Stk3DFMM *fmm, unsigned kernel, float *ms) {
+    if (!fmm || !ms) return STK_ERR_INVALID_ARG;
+    KernelData *kd = get_kd(fmm, kernel);
+    if (!kd) return STK_ERR_KERNEL;
+    if (!kd->timed) return STK_ERR_STATE;
+    if (cudaEventSynchronize(kd->ev1) != cudaSuccess) return STK_ERR_CUDA;
+    const int np = kd->last_far ? KernelData::kPhases : 1;
+    cudaEvent_t prev = kd->ev0;
+    for (int i = 0; i < KernelData::kPhases; i++) {
+        ms[i] = 0.0f;
+        if (i >= np) continue;
+        if (cudaEventElapsedTime(&ms[i], prev, kd->ph[i]) != cudaSuccess) return STK_ERR_CUDA;
+        prev = kd->ph[i];
+    }
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long *out) {
     if (!fmm || !out) return STK_ERR_INVALID_ARG;
     KernelData *kd = get_kd(fmm, kernel);
@@ -441,6 +467,24 @@ extern "C" int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long
     out[6] = (long long)T.V.size();
     out[7] = (long long)T.W.size();
     out[8] = (long long)T.X.size();
+    return STK_OK;
+}
+
+extern "C" int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long *out) {
+    if (!fmm || !out) return STK_ERR_INVALID_ARG;
+    KernelData *kd = get_kd(fmm, kernel);
+    if (!kd) return STK_ERR_KERNEL;
+    if (!kd->tree_ready || !kd->far_ready) return STK_ERR_STATE;
+    const FarField &F = *kd->far;
+    out[0] = F.near[0].pairs;
+    out[1] = kd->fused ? F.near[0].pairs : F.near[1].pairs;
+    out[2] = F.s2m[0].pairs + F.s2m[1].pairs;
+    out[3] = F.s2l[0].pairs + F.s2l[1].pairs;
+    out[4] = F.m2t.pairs;
+    out[5] = F.l2t.pairs;
+    out[6] = F.m2l_pairs;
+    out[7] = F.n;
+    out[8] = F.m2l_rank;
     return STK_OK;
 }
 

@@ -37,8 +37,13 @@ struct KernelData {
     DevBuf d_xyz[3], d_perm[3], d_beg[3], d_end[3];  // per point set: sorted coords, perm, node ranges
     DevBuf d_centre, d_uent, d_items[2], d_counter;
     DevBuf d_val[2], d_rec[2], d_out_sorted, d_out_user, d_alpha;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the P2P launches of the last evaluation
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the kernel launches of the last evaluation
     bool timed = false;
+    // end of each phase of the last evaluation: 0 U-list P2P, 1 S2M (+ solve),
+    // 2 M2M, 3 M2L, 4 S2L (+ solve), 5 L2L, 6 L2T, 7 M2T
+    static constexpr int kPhases = 8;
+    cudaEvent_t ph[kPhases] = {};
+    bool last_far = false;
     std::unique_ptr<FarField> far;  // KIFMM operators and per-tree far-field data
     bool far_ready = false;
     ~KernelData();

@@ -267,14 +267,34 @@ void Octree::build_lists() {
         std::sort(Vl[b].begin(), Vl[b].end());
     }
 
-    // X: transpose of W (target box gains the larger leaf, with the inverse shift)
-    for (int a = 0; a < nn; a++)
-        for (int e : Wl[a]) {
-            const int b = e >> 5, code = e & 31;
-            if (trg_count(b) == 0 || src_count(a) == 0) continue;
-            Xl[b].push_back((a << 5) | shift_negate(code));
-        }
-    for (auto &x : Xl) std::sort(x.begin(), x.end());
+    // X: the W relation seen from the source side.  For every leaf a with
+    // sources, the nodes with targets that are descendants of a's colleagues,
+    // not adjacent to a, with a parent adjacent to a, gain a (with the inverse
+    // shift).  Walking from the source leaves also covers source leaves that hold
+    // no targets, which have no W list of their own.
+    for (int a : leaves) {
+        if (src_count(a) == 0) continue;
+        neighbours(a, [&](int node, int code, const int64_t *, int) {
+            if (node < 0 || is_leaf(node)) return;
+            std::vector<int> stack(1, node);
+            while (!stack.empty()) {
+                const int m = stack.back();
+                stack.pop_back();
+                for (int c = first_child[m]; c < first_child[m] + 8; c++) {
+                    if (trg_count(c) == 0) continue;
+                    if (adjacent(c, code, a)) {
+                        if (!is_leaf(c)) stack.push_back(c);
+                    } else {
+                        Xl[c].push_back((a << 5) | shift_negate(code));
+                    }
+                }
+            }
+        });
+    }
+    for (auto &x : Xl) {
+        std::sort(x.begin(), x.end());
+        x.erase(std::unique(x.begin(), x.end()), x.end());
+    }
 
     U = to_csr(Ul);
     V = to_csr(Vl);

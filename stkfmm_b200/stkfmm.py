@@ -226,6 +226,22 @@ class Stk3DFMM:
             raise StkError(2, "evaluate_kernel")
         return evaluate_kernel(kernel, p2p, src_coord, src_value, trg_coord, trg_value, self.precision)
 
+    PHASES = ("near", "s2m", "m2m", "m2l", "s2l", "l2l", "l2t", "m2t")
+
+    def last_phase_ms(self, kernel) -> dict:
+        """Device time (ms) per phase of the last evaluation (near-field-only calls: far phases 0)."""
+        ms = np.zeros(8, dtype=np.float32)
+        check(lib().Stk3DFMM_last_phase_ms(self.fmm, int(kernel), ms.ctypes.data_as(P_f)), "last_phase_ms")
+        return dict(zip(self.PHASES, (float(v) for v in ms)))
+
+    def fmm_stats(self, kernel) -> dict:
+        """Pair counts of one evaluate_fmm (available after the first call)."""
+        out = np.zeros(9, dtype=np.int64)
+        check(lib().Stk3DFMM_get_fmm_stats(self.fmm, int(kernel), out.ctypes.data_as(P_ll)), "fmm_stats")
+        keys = ["near_pairs_sl", "near_pairs_dl", "s2m_pairs", "s2l_pairs", "m2t_pairs", "l2t_pairs", "m2l_pairs",
+                "surface_points", "m2l_rank"]
+        return dict(zip(keys, (int(v) for v in out)))
+
     def tree_stats(self, kernel) -> dict:
         out = np.zeros(9, dtype=np.int64)
         check(lib().Stk3DFMM_get_tree_stats(self.fmm, int(kernel), out.ctypes.data_as(P_ll)), "tree_stats")

@@ -57,17 +57,15 @@ def brute_lists(t, src_count, trg_count, pbc):
                 if leaf[b] and leaf[a] and adj:
                     U[b].add((a << 5) | code(s))
                 pa = t.parent[a]
+                pb = t.parent[b]
                 if pa >= 0 and not adj:
                     if leaf[b] and t.level[a] > t.level[b] and adjacent(lo, hi, pa, s, b):
                         W[b].add((a << 5) | code(s))
-                    pb = t.parent[b]
                     if pb >= 0 and t.level[a] == t.level[b] and adjacent(lo, hi, pa, s, pb):
                         V[b].add((a << 5) | code(s))
-    for a in range(nn):
-        for e in W[a]:
-            b, c = e >> 5, e & 31
-            if trg_count[b] and src_count[a]:
-                X[b].add((a << 5) | (26 - c))
+                # X: b is in the W relation of the source leaf a (a need not hold targets)
+                if pb >= 0 and not adj and leaf[a] and t.level[b] > t.level[a] and adjacent(lo, hi, a, s, pb):
+                    X[b].add((a << 5) | code(s))
     return U, V, W, X
 
 
@@ -77,6 +75,8 @@ CASES = [
     ("uniform", 3, 16),
     ("clustered", 2, 10),
     ("clustered", 1, 10),
+    ("clustered-apart", 0, 12),  # targets apart from the sources: leaves with sources only
+    ("clustered-apart", 3, 12),
 ]
 
 
@@ -85,7 +85,7 @@ def test_lists_match_kifmm_definitions(dist, pbc, max_pts):
     rng = np.random.default_rng(7 + pbc)
     n = 700
     pts = rng.random((n, 3)) if dist == "uniform" else clustered_points(rng, n, nclusters=4, sigma=0.05)
-    trg = pts[: n // 2]
+    trg = rng.random((n // 2, 3)) if dist == "clustered-apart" else pts[: n // 2]
     t = Octree(pts, max_pts, pbc, sl=pts, trg=trg)
     _, sb, se = t.point_set(0)
     _, tb, te = t.point_set(2)
