@@ -51,6 +51,9 @@ FLOPS_PER_POINT_PAIR_FUSED = 44
 FLOPS_PER_POINT_PAIR_FP64 = 33
 WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clusters (sigma 0.02, centres "
             "U[0.1,0.9]^3), max 256 pts/leaf, p=10, SL=DL=targets")
+WORKLOAD_FMM = ("LapPGrad free-space FMM (evaluate_fmm: U/W/X near field + KIFMM far field), same points and "
+                "values, p=10, max 256 pts/leaf")
+FMM_SAMPLE = 2000
 
 
 def make_points(seed: int):
@@ -297,6 +300,7 @@ def b200_arm(args):
         barrier()
         torch.cuda.synchronize()
         tw0 = time.perf_counter()
+        torch.cuda.profiler.start()  # a profiler started with --profile-from-start off sees only timed steps
         with torch.cuda.stream(stream):
             for i in range(steps):
                 flush.zero_()  # L2 flush (256 MB write) between timed steps, outside the step events
@@ -306,6 +310,7 @@ def b200_arm(args):
                 evs[i][1].record(stream)
                 stream.synchronize()
                 kern.append(fmm.last_kernel_ms(K))
+        torch.cuda.profiler.stop()
         torch.cuda.synchronize()
         barrier()
         wall = time.perf_counter() - tw0
@@ -319,11 +324,49 @@ def b200_arm(args):
         outs[prec] = out
         return ms, kms, wall
 
+    def run_fmm(prec, steps, warmup):
+        """Whole evaluate_fmm (near field + KIFMM far field) on device-resident values."""
+        fmm.set_precision(prec)
+        out = torch.zeros((N_POINTS, 4), dtype=torch.float64, device="cuda")
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+        stream.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        phases = []
+        barrier()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush.zero_()
+                out.zero_()
+                evs[i][0].record(stream)
+                fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+                evs[i][1].record(stream)
+                stream.synchronize()
+                phases.append(fmm.last_phase_ms(K))
+        torch.cuda.profiler.stop()
+        torch.cuda.synchronize()
+        barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        if ws > 1:
+            tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt[0])
+        ph = {k: sum(p[k] for p in phases) / steps for k in phases[0]}
+        return ms, ph, out
+
     clocks = ClockSampler(dev) if rank == 0 else None
     if clocks:
         clocks.start()
     ms64, k64, _ = run(S.PRECISION.FP64, args.steps, args.warmup)
+    near_launches = fmm.last_launch_count(K)
     msmx, kmx, _ = run(S.PRECISION.MIXED, args.steps, args.warmup)
+    fms64, fph64, fout64 = run_fmm(S.PRECISION.FP64, args.steps, args.warmup)
+    fmsmx, fphmx, foutmx = run_fmm(S.PRECISION.MIXED, args.steps, args.warmup)
+    fmm_launches = fmm.last_launch_count(K)
+    fst = fmm.fmm_stats(K)
     clk = clocks.stop() if clocks else None
 
     value = ws * pairs / (msmx * 1e-3)
@@ -353,6 +396,23 @@ def b200_arm(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt[0])
     e2e_val = ws * pairs / e2e_s
+
+    # ---- FMM e2e: Stk3DFMM_evaluate_fmm with pinned host arrays (mixed) ----
+    fmm.set_precision(S.PRECISION.MIXED)
+    for _ in range(args.warmup):
+        fmm.evaluate_fmm(K, qh, oh, dh)
+    barrier()
+    fe2e_t = []
+    for _ in range(args.steps):
+        oh[:] = 0.0
+        t0 = time.perf_counter()
+        fmm.evaluate_fmm(K, qh, oh, dh)
+        fe2e_t.append(time.perf_counter() - t0)
+    fe2e_s = sum(fe2e_t) / len(fe2e_t)
+    if ws > 1:
+        tt = torch.tensor([fe2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        fe2e_s = float(tt[0])
 
     if rank != 0:
         if ws > 1:
@@ -384,6 +444,34 @@ def b200_arm(args):
 
     cpu = cpu_baseline(ul, pts, q, d) if ws == 1 else None
 
+    # ---- FMM accuracy: both precisions against the oracle's direct sum on a target sample ----
+    samp = np.random.default_rng(11).choice(N_POINTS, FMM_SAMPLE, replace=False)
+    t0 = time.perf_counter()
+    ref = O.direct(O.UK_LAPLACE_PGRAD, pts, q, pts[samp]) + O.direct(O.UK_LAPLACE_DIPOLEPGRAD, pts, d, pts[samp])
+    oracle_s = time.perf_counter() - t0
+    fmm_err = {}
+    for name, o in (("fp64", fout64), ("mixed", foutmx)):
+        got = o.cpu().numpy()[samp]
+        fmm_err[name] = {"all": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                         "per_component": [float(np.linalg.norm(got[:, c] - ref[:, c]) / np.linalg.norm(ref[:, c]))
+                                           for c in range(4)]}
+    fmm_block = {
+        "workload": WORKLOAD_FMM,
+        "fp64": {"evals_per_s": ws * 1e3 / fms64, "ms_per_eval": fms64, "phases_ms": fph64},
+        "mixed": {"evals_per_s": ws * 1e3 / fmsmx, "ms_per_eval": fmsmx, "phases_ms": fphmx},
+        "mixed_over_fp64": fms64 / fmsmx,
+        "rel_l2_vs_direct_sum_sample": fmm_err,
+        "sample": "%d targets drawn with seed 11; oracle direct sum over all %d sources (%.1f s on the host)"
+                  % (FMM_SAMPLE, N_POINTS, oracle_s),
+        "work_per_eval": fst,
+        "e2e": {"evals_per_s": ws / fe2e_s, "ms_per_eval": fe2e_s * 1e3,
+                "api": "Stk3DFMM_evaluate_fmm (C ABI, pinned host arrays, mixed)",
+                "h2d_bytes_per_eval": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
+                "d2h_bytes_per_eval": int(N_POINTS * 4 * 8)},
+        "gpu_launches_per_eval": fmm_launches,
+        "timing": "CUDA events on the launching stream around each evaluate_fmm_device, 256 MB L2 flush between",
+    }
+
     line = {
         "metric": "P2P pair-interactions/s (U-list S2T, mixed precision; FP64 path beside it)",
         "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -397,7 +485,8 @@ def b200_arm(args):
         "mixed_over_fp64": value / value64,
         "rel_l2_mixed_vs_fp64": err_mx, "rel_l2_mixed_vs_fp64_per_component": err_cols,
         "rel_l2_fp64_vs_oracle_sample": parity64,
-        "fmm_evals_per_s": None,
+        "fmm_evals_per_s": ws * 1e3 / fmsmx,
+        "fmm": fmm_block,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peaks[0]), "unit": "TFLOP/s",
                      "frac": achieved / float(peaks[0]) if peaks[0] > 0 else None, "traffic": traffic,
                      "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, mixed>", "kernel_ms": kmx,
@@ -411,10 +500,10 @@ def b200_arm(args):
                                    "frac": (point_pairs * FLOPS_PER_POINT_PAIR_FP64 / (k64 * 1e-3) / 1e12)
                                    / float(peaks[1]) if peaks[1] > 0 else None}},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes),
+        "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
                 "d2h_bytes_per_step": int(N_POINTS * 4 * 8), "ms_per_step": e2e_s * 1e3,
                 "api": "Stk3DFMM_evaluate_near (C ABI, pinned host arrays)"},
-        "gpu_launches": 3 * args.steps * 2,
+        "gpu_launches": args.steps * (2 * near_launches + 2 * fmm_launches),
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -220,6 +220,9 @@ int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms);
  * P2P, [1] S2M + check-to-equivalent solve, [2] M2M, [3] M2L, [4] S2L + solve,
  * [5] L2L, [6] L2T, [7] M2T (W list); [1..7] are 0 after a near-field-only call. */
 int Stk3DFMM_last_phase_ms(Stk3DFMM *fmm, unsigned kernel, float *ms);
+/* Number of this library's kernels launched by the last evaluation of `kernel`
+ * (near-field or FMM; cuBLAS calls of the far field excluded). */
+int Stk3DFMM_last_launch_count(Stk3DFMM *fmm, unsigned kernel, int *count);
 /* Tree / list statistics of the last setup_tree for `kernel`:
  * out[0] nodes, [1] leaves, [2] depth, [3] U-list entries, [4] U-list SL point pairs,
  * [5] U-list DL point pairs, [6] V entries, [7] W entries, [8] X entries. */
@@ -227,7 +230,8 @@ int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
 /* Work of one evaluate_fmm of `kernel` (after its first call): out[0] near-field
  * (U list + direct W / X) SL point pairs, [1] DL point pairs, [2] S2M, [3] S2L,
  * [4] M2T, [5] L2T point pairs (sources x check / surface points), [6] M2L node
- * pairs, [7] points per check / equivalent surface, [8] rank of the compressed M2L. */
+ * pairs, [7] points per check / equivalent surface, [8] rank of the compressed M2L,
+ * [9] kernels of this library launched by the last evaluation (cuBLAS calls excluded). */
 int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
 /* Copy the U-list of the last setup_tree (leaf-sorted indices, same layout as
  * stk_p2p_lists).  Pass null arrays to query sizes: sizes = {n_leaf_boxes, n_entries, nSL, nDL, nTrg}. */

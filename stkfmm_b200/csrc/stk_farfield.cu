@@ -40,6 +40,9 @@ namespace {
 
 constexpr int kNumOffsets = 343;  // (dx, dy, dz) in [-3, 3]^3
 
+// kernels of this file launched by the current evaluation on this host thread
+thread_local int t_launches = 0;
+
 // Points of the KIFMM cube surface on [-1, 1]^3, in the order of stkfmm::surface
 // (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85) before its affine map.
 std::vector<double> unit_surface(int p) {
@@ -165,6 +168,7 @@ inline int grid_for(long long total) { return (int)std::max<long long>(1, std::m
 template <class TS, class TD>
 int gather_cols(const TS *src, const int *cols, int m, int N, TD *dst, cudaStream_t s) {
     if (m <= 0) return STK_OK;
+    t_launches++;
     gather_cols_kernel<TS, TD><<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, dst);
     return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
 }
@@ -172,6 +176,7 @@ int gather_cols(const TS *src, const int *cols, int m, int N, TD *dst, cudaStrea
 template <class TS>
 int scatter_cols(const TS *src, const int *cols, int m, int N, double alpha, int add, double *dst, cudaStream_t s) {
     if (m <= 0) return STK_OK;
+    t_launches++;
     scatter_cols_kernel<TS><<<grid_for((long long)m * N), 256, 0, s>>>(src, cols, m, N, alpha, add, dst);
     return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
 }
@@ -429,11 +434,11 @@ int build_operators(FarField &F, cudaStream_t s) {
 // own_src is false.
 int setup_pass(ListPass &P, int uk, const std::vector<int> &tb, const std::vector<int> &te,
                const std::vector<int> &off, const std::vector<int> &ent, const int *h_src_beg, const int *h_src_end,
-               int n_src_box, bool own_src, const std::vector<double> &centres, cudaStream_t s) {
+               int n_src_box, bool own_src, const std::vector<double> &centres, int balance_warps, cudaStream_t s) {
     P.uk = uk;
     std::vector<WorkItem> items;
     build_list_items((int)tb.size(), tb.data(), te.data(), off.data(), ent.data(), h_src_beg, h_src_end, items,
-                     P.pairs);
+                     P.pairs, balance_warps);
     P.n_items = (int)items.size();
     int rc = P.items.upload(items.data(), items.size() * sizeof(WorkItem), s);
     if (!rc) rc = P.ent.upload(ent.data(), ent.size() * sizeof(int), s);
@@ -446,6 +451,7 @@ int setup_pass(ListPass &P, int uk, const std::vector<int> &tb, const std::vecto
 int run_pass(const ListPass &P, int prec, const double *rec, const int *src_beg, const int *src_end,
              const double *trg_xyz, double *out, unsigned int *counter, int sms, cudaStream_t s) {
     if (P.n_items == 0) return STK_OK;
+    t_launches++;
     ListP2PArgs a{};
     a.src_rec = rec;
     a.src_box_begin = src_beg;
@@ -535,6 +541,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     };
     std::vector<double> ctr(3 * (size_t)nn);
     for (int i = 0; i < nn; i++) T.centre(i, &ctr[3 * (size_t)i]);
+    const int bw = f->sms * 12;  // resident warps of the list kernel, roughly
 
     // ---- S2M: leaves with sources; targets = their upward check surfaces ----
     F.s2m_nodes.clear();
@@ -566,7 +573,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             F.s2m[k].reset();
             if (uk < 0 || T.sets[k].n == 0) continue;
             rc = setup_pass(F.s2m[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
-                            nn, false, cc, s);
+                            nn, false, cc, bw, s);
             if (rc) return rc;
         }
     }
@@ -601,7 +608,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             F.near[k].reset();
             if (T.sets[k].n == 0 || ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL] < 0) continue;
             rc = setup_pass(F.near[k], ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL], tg.node_begin, tg.node_end, noff,
-                            nent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(), nn, false, ctr, s);
+                            nent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(), nn, false, ctr, bw, s);
             if (rc) return rc;
         }
     }
@@ -637,7 +644,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             F.s2l[k].reset();
             if (uk < 0 || T.sets[k].n == 0) continue;
             rc = setup_pass(F.s2l[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
-                            nn, false, cc, s);
+                            nn, false, cc, bw, s);
             if (rc) return rc;
         }
     }
@@ -666,10 +673,10 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         F.m2t.reset();
         F.l2t.reset();
         rc = setup_pass(F.m2t, ki->slot[SLOT_M2T], tg.node_begin, tg.node_end, woff, went, sb.data(), se.data(), nn,
-                        true, ctr, s);
+                        true, ctr, bw, s);
         if (!rc)
             rc = setup_pass(F.l2t, ki->slot[SLOT_L2T], tg.node_begin, tg.node_end, loff, lent, sb.data(), se.data(),
-                            nn, true, ctr, s);
+                            nn, true, ctr, bw, s);
         if (rc) return rc;
     }
 
@@ -791,6 +798,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     cublasSetStream(F.blas, s);
     double *phi = (double *)F.phi.ptr, *psi = (double *)F.psi.ptr;
     double *X = (double *)F.tmp0.ptr, *Y = (double *)F.tmp1.ptr;
+    t_launches = 0;
     FCUDA(cudaMemsetAsync(phi, 0, sizeof(double) * (size_t)nn * N, s));
     FCUDA(cudaMemsetAsync(psi, 0, sizeof(double) * (size_t)nn * N, s));
 
@@ -800,6 +808,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         const PointSet &ps = T.sets[k];
         int rc = F.rec_pts[k].reserve(sizeof(double) * (size_t)std::max(ps.n, 1) * rs);
         if (rc) return rc;
+        t_launches++;
         if (launch_pack_records(ps.n, (const int *)kd->d_perm[k].ptr, (const double *)kd->d_xyz[k].ptr,
                                 k == 0 ? d_sl : d_dl, k == 0 ? ki->kdim_sl : ki->kdim_dl, nullptr, 0, rs,
                                 (double *)F.rec_pts[k].ptr, s) != cudaSuccess)
@@ -854,6 +863,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     const long long ncol = F.m2l_cols;
     if (ncol > 0) {
         const int gg = grid_for(ncol * k);
+        t_launches += 2;
         if (prec == PREC_MIXED) {
             // the translation C_d carries no pseudo-inverse: FP32 operands, FP32 accumulation
             m2l_gather_kernel<float><<<gg, 256, 0, s>>>(phi_hat, (const int *)F.d_m2l_gsrc.ptr, k, ncol,
@@ -928,6 +938,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         const int rs = uk_record_stride(uk);
         int rc = F.rec_surf.reserve(sizeof(double) * (size_t)npts * rs);
         if (rc) return rc;
+        t_launches++;
         if (launch_pack_records((int)npts, nullptr, (const double *)xyz.ptr, dens, ke, nullptr, 0, rs,
                                 (double *)F.rec_surf.ptr, s) != cudaSuccess)
             return STK_ERR_CUDA;
@@ -949,6 +960,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         if (rc) return rc;
     }
     FCUDA(cudaEventRecord(kd->ph[7], s));
+    F.launches = t_launches;
     return STK_OK;
 }
 

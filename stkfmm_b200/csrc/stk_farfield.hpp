@@ -72,6 +72,7 @@ struct FarField {
     std::vector<int> parents, parent_off;
     DevBuf d_parents;
     // M2L: V-list pairs grouped by offset in chunks of columns (one batched GEMM)
+    int launches = 0;                       // own kernels of the last evaluation (cuBLAS excluded)
     long long m2l_pairs = 0, m2l_cols = 0;  // pairs; columns including chunk padding
     int m2l_chunks = 0;
     DevBuf d_m2l_gsrc;                      // per column: source node, -1 = padding

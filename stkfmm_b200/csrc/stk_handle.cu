@@ -247,7 +247,7 @@ extern "C" int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel) {
         std::vector<WorkItem> items;
         long long pairs = 0;
         build_list_items(nn, tg.node_begin.data(), tg.node_end.data(), T.U.off.data(), T.U.ent.data(),
-                         sp.node_begin.data(), sp.node_end.data(), items, pairs);
+                         sp.node_begin.data(), sp.node_end.data(), items, pairs, fmm->sms * 12);
         kd->u_pairs[k] = pairs;
         kd->n_items[k] = (int)items.size();
         up(kd->d_items[k], items.data(), items.size() * sizeof(WorkItem));
@@ -305,6 +305,7 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
     double *out = (double *)kd->d_out_sorted.ptr;
     HCUDA(cudaMemsetAsync(out, 0, sizeof(double) * ntrg * td, s));
     HCUDA(cudaEventRecord(kd->ev0, s));
+    int launches = 0;
     for (int k = 0; k < 2; k++) {
         if (k == 1 && (!dl || kd->fused)) continue;
         // the FMM's near field: U list plus the W / X interactions evaluated directly
@@ -338,6 +339,7 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
         a.period = 1.0;
         a.atomic_out = 0;
         HCUDA(launch_list_p2p(uk, f->precision, a, f->sms, s));
+        launches += 2;  // record packing + list kernel
     }
     HCUDA(cudaEventRecord(kd->ph[0], s));
     kd->last_far = far;
@@ -354,18 +356,9 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
     (void)nn;
     HCUDA(launch_scatter_add(ntrg, td, (const int *)kd->d_perm[2].ptr, out, (const double *)kd->d_alpha.ptr,
                              d_out_user, s));
+    kd->launches = launches + (ntrg > 0 ? 1 : 0) + (far ? kd->far->launches : 0);
     kd->timed = true;
     return STK_OK;
-}
-
-// scaleSrc (FMMData.cpp:285-317) on host copies
-static void scale_src(const Stk3DFMM *f, const KernelData *kd, std::vector<double> &sl, std::vector<double> &dl) {
-    const double sf = f->scale_factor;
-    for (double &v : dl) v *= sf;
-    if (kd->info->sl_last_scales) {
-        const int d = kd->info->kdim_sl;
-        for (size_t i = d - 1; i < sl.size(); i += d) sl[i] *= sf;
-    }
 }
 
 static int check_eval_args(Stk3DFMM *fmm, unsigned kernel, int nSL, const double *slv, int nTrg, double *trgv,
@@ -381,32 +374,56 @@ static int check_eval_args(Stk3DFMM *fmm, unsigned kernel, int nSL, const double
     return STK_OK;
 }
 
-extern "C" int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value,
-                                      const int nTrg, double *trg_value, const int nDL, double *src_DL_value) {
+// v[i stride + offset] *= a for i < n
+__global__ void scale_strided_kernel(double *__restrict__ v, long long n, int stride, int offset, double a) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[i * stride + offset] *= a;
+}
+
+static cudaError_t scale_strided(double *v, long long n, int stride, int offset, double a, cudaStream_t s) {
+    if (n <= 0 || a == 1.0) return cudaSuccess;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    scale_strided_kernel<<<grid, 256, 0, s>>>(v, n, stride, offset, a);
+    return cudaGetLastError();
+}
+
+static int ensure_far(Stk3DFMM *fmm, KernelData *kd);
+
+// Host-array evaluation (evaluate_near / evaluate_fmm): the caller's arrays are
+// copied straight to the device (DMA when they are pinned), scaleSrc runs on
+// the device, the caller's target array is accumulated on the device and copied
+// back in place: trg_value += result.
+static int eval_host(Stk3DFMM *fmm, unsigned kernel, const int nSL, const double *src_SL_value, const int nTrg,
+                     double *trg_value, const int nDL, const double *src_DL_value, bool far) {
     KernelData *kd = nullptr;
     int rc = check_eval_args(fmm, kernel, nSL, src_SL_value, nTrg, trg_value, nDL, src_DL_value, kd);
     if (rc) return rc;
     cudaSetDevice(fmm->device);
+    if (far && (rc = ensure_far(fmm, kd))) return rc;
     const KernelInfo *ki = kd->info;
     const bool dl = has_dl(kd) && fmm->ndl > 0;
     cudaStream_t s = fmm->stream;
-    std::vector<double> slv(src_SL_value, src_SL_value + (size_t)nSL * ki->kdim_sl);
-    std::vector<double> dlv;
-    if (dl) dlv.assign(src_DL_value, src_DL_value + (size_t)nDL * ki->kdim_dl);
-    scale_src(fmm, kd, slv, dlv);
-    rc = kd->d_val[0].upload(slv.data(), slv.size() * sizeof(double), s);
-    if (!rc && dl) rc = kd->d_val[1].upload(dlv.data(), dlv.size() * sizeof(double), s);
-    if (!rc) rc = kd->d_out_user.reserve(sizeof(double) * std::max(1, nTrg) * ki->kdim_trg);
+    const size_t nsl_v = (size_t)nSL * ki->kdim_sl, ndl_v = dl ? (size_t)nDL * ki->kdim_dl : 0;
+    const size_t ntrg_v = (size_t)nTrg * ki->kdim_trg;
+    rc = kd->d_val[0].upload(src_SL_value, nsl_v * sizeof(double), s);
+    if (!rc && dl) rc = kd->d_val[1].upload(src_DL_value, ndl_v * sizeof(double), s);
+    if (!rc) rc = kd->d_out_user.upload(trg_value, ntrg_v * sizeof(double), s);
     if (rc) return rc;
-    HCUDA(cudaMemsetAsync(kd->d_out_user.ptr, 0, sizeof(double) * nTrg * ki->kdim_trg, s));
+    // scaleSrc (FMMData.cpp:285-317): DL values and a scaling last SL component times sF
+    const double sf = fmm->scale_factor;
+    if (dl) HCUDA(scale_strided((double *)kd->d_val[1].ptr, (long long)ndl_v, 1, 0, sf, s));
+    if (ki->sl_last_scales) HCUDA(scale_strided((double *)kd->d_val[0].ptr, nSL, ki->kdim_sl, ki->kdim_sl - 1, sf, s));
     rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
-                     (double *)kd->d_out_user.ptr, s, false);
+                     (double *)kd->d_out_user.ptr, s, far);
     if (rc) return rc;
-    std::vector<double> res((size_t)nTrg * ki->kdim_trg);
-    HCUDA(cudaMemcpyAsync(res.data(), kd->d_out_user.ptr, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (ntrg_v) HCUDA(cudaMemcpyAsync(trg_value, kd->d_out_user.ptr, ntrg_v * sizeof(double), cudaMemcpyDeviceToHost, s));
     HCUDA(cudaStreamSynchronize(s));
-    for (size_t i = 0; i < res.size(); i++) trg_value[i] += res[i];
     return STK_OK;
+}
+
+extern "C" int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value,
+                                      const int nTrg, double *trg_value, const int nDL, double *src_DL_value) {
+    return eval_host(fmm, kernel, nSL, src_SL_value, nTrg, trg_value, nDL, src_DL_value, false);
 }
 
 extern "C" int Stk3DFMM_evaluate_near_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value,
@@ -452,6 +469,15 @@ extern "C" int Stk3DFMM_last_phase_ms(Stk3DFMM *fmm, unsigned kernel, float *ms)
     return STK_OK;
 }
 
+extern "C" int Stk3DFMM_last_launch_count(Stk3DFMM *fmm, unsigned kernel, int *count) {
+    if (!fmm || !count) return STK_ERR_INVALID_ARG;
+    KernelData *kd = get_kd(fmm, kernel);
+    if (!kd) return STK_ERR_KERNEL;
+    if (!kd->timed) return STK_ERR_STATE;
+    *count = kd->launches;
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long *out) {
     if (!fmm || !out) return STK_ERR_INVALID_ARG;
     KernelData *kd = get_kd(fmm, kernel);
@@ -485,6 +511,7 @@ extern "C" int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long 
     out[6] = F.m2l_pairs;
     out[7] = F.n;
     out[8] = F.m2l_rank;
+    out[9] = kd->launches;
     return STK_OK;
 }
 
@@ -532,32 +559,7 @@ static int ensure_far(Stk3DFMM *fmm, KernelData *kd) {
 
 extern "C" int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value,
                                      const int nTrg, double *trg_value, const int nDL, double *src_DL_value) {
-    KernelData *kd = nullptr;
-    int rc = check_eval_args(fmm, kernel, nSL, src_SL_value, nTrg, trg_value, nDL, src_DL_value, kd);
-    if (rc) return rc;
-    cudaSetDevice(fmm->device);
-    rc = ensure_far(fmm, kd);
-    if (rc) return rc;
-    const KernelInfo *ki = kd->info;
-    const bool dl = has_dl(kd) && fmm->ndl > 0;
-    cudaStream_t s = fmm->stream;
-    std::vector<double> slv(src_SL_value, src_SL_value + (size_t)nSL * ki->kdim_sl);
-    std::vector<double> dlv;
-    if (dl) dlv.assign(src_DL_value, src_DL_value + (size_t)nDL * ki->kdim_dl);
-    scale_src(fmm, kd, slv, dlv);
-    rc = kd->d_val[0].upload(slv.data(), slv.size() * sizeof(double), s);
-    if (!rc && dl) rc = kd->d_val[1].upload(dlv.data(), dlv.size() * sizeof(double), s);
-    if (!rc) rc = kd->d_out_user.reserve(sizeof(double) * std::max(1, nTrg) * ki->kdim_trg);
-    if (rc) return rc;
-    HCUDA(cudaMemsetAsync(kd->d_out_user.ptr, 0, sizeof(double) * nTrg * ki->kdim_trg, s));
-    rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
-                     (double *)kd->d_out_user.ptr, s, true);
-    if (rc) return rc;
-    std::vector<double> res((size_t)nTrg * ki->kdim_trg);
-    HCUDA(cudaMemcpyAsync(res.data(), kd->d_out_user.ptr, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    HCUDA(cudaStreamSynchronize(s));
-    for (size_t i = 0; i < res.size(); i++) trg_value[i] += res[i];
-    return STK_OK;
+    return eval_host(fmm, kernel, nSL, src_SL_value, nTrg, trg_value, nDL, src_DL_value, true);
 }
 
 extern "C" int Stk3DFMM_evaluate_fmm_device(Stk3DFMM *fmm, unsigned kernel, const double *d_src_SL_value,

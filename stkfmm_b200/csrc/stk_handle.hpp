@@ -44,6 +44,7 @@ struct KernelData {
     static constexpr int kPhases = 8;
     cudaEvent_t ph[kPhases] = {};
     bool last_far = false;
+    int launches = 0;  // own kernels launched by the last evaluation (cuBLAS calls excluded)
     std::unique_ptr<FarField> far;  // KIFMM operators and per-tree far-field data
     bool far_ready = false;
     ~KernelData();

@@ -143,10 +143,10 @@ void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &
 
 void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
                       const int *list_ent, const int *src_begin, const int *src_end, std::vector<WorkItem> &items,
-                      long long &pairs) {
+                      long long &pairs, int balance_warps) {
     items.clear();
     pairs = 0;
-    std::vector<double> cost;
+    std::vector<long long> box_ns(n_trg_box, 0);
     for (int b = 0; b < n_trg_box; b++) {
         const int nt = trg_end[b] - trg_begin[b];
         if (nt <= 0) continue;
@@ -155,9 +155,22 @@ void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, c
             const int sb = list_ent[e] >> 5;
             ns += src_end[sb] - src_begin[sb];
         }
-        if (ns == 0) continue;
+        box_ns[b] = ns;
         pairs += (long long)nt * ns;
-        // Split the box into full 64-target items, then power-of-two chunks of
+    }
+    // Load balance: no item above ~half of one warp's share of the pairs, so a
+    // box with very many sources (a long W list) is not a single long item that
+    // finishes after every other warp.  Items keep at least 8 targets (64 slots
+    // filled with 8 lanes per target).
+    const long long cap = balance_warps > 0 ? std::max(pairs / (2LL * balance_warps), 1LL) : 0;
+    std::vector<double> cost;
+    for (int b = 0; b < n_trg_box; b++) {
+        const int nt = trg_end[b] - trg_begin[b];
+        const long long ns = box_ns[b];
+        if (nt <= 0 || ns == 0) continue;
+        int mmax = kItemTargets;
+        while (cap > 0 && mmax > 8 && (long long)mmax * ns > cap) mmax /= 2;
+        // Split the box into full mmax-target items, then power-of-two chunks of
         // the remainder (32, 16, 8 targets; the last < 8 targets together): a
         // chunk of m = 2^k targets fills all 64 slots with 64/m lanes per target,
         // so the box costs ~nt/64 warp passes over its sources instead of
@@ -165,8 +178,8 @@ void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, c
         int t0 = trg_begin[b];
         int left = nt;
         while (left > 0) {
-            int m = kItemTargets;
-            if (left < kItemTargets) {
+            int m = mmax;
+            if (left < mmax) {
                 m = 1;
                 while (m * 2 <= left) m *= 2;
                 if (m < 8) m = left;

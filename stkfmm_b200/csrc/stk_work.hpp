@@ -45,9 +45,11 @@ void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &
                         std::vector<int> &src_end, std::vector<int> &ent);
 
 // Cost-sorted work items for an explicit list; pairs = exact (target, source point) pair count.
+// balance_warps > 0: boxes with many sources get smaller target chunks, so that no
+// item holds more than ~pairs / (2 balance_warps) pairs.
 void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
                       const int *list_ent, const int *src_begin, const int *src_end, std::vector<WorkItem> &items,
-                      long long &pairs);
+                      long long &pairs, int balance_warps = 0);
 
 // Morton order of points inside their own bounding box.
 void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted);

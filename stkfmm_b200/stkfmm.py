@@ -234,12 +234,18 @@ class Stk3DFMM:
         check(lib().Stk3DFMM_last_phase_ms(self.fmm, int(kernel), ms.ctypes.data_as(P_f)), "last_phase_ms")
         return dict(zip(self.PHASES, (float(v) for v in ms)))
 
+    def last_launch_count(self, kernel) -> int:
+        n = ctypes.c_int()
+        check(lib().Stk3DFMM_last_launch_count(self.fmm, int(kernel), ctypes.byref(n)), "last_launch_count")
+        return int(n.value)
+
     def fmm_stats(self, kernel) -> dict:
         """Pair counts of one evaluate_fmm (available after the first call)."""
-        out = np.zeros(9, dtype=np.int64)
+        out = np.zeros(10, dtype=np.int64)
         check(lib().Stk3DFMM_get_fmm_stats(self.fmm, int(kernel), out.ctypes.data_as(P_ll)), "fmm_stats")
         keys = ["near_pairs_sl", "near_pairs_dl", "s2m_pairs", "s2l_pairs", "m2t_pairs", "l2t_pairs", "m2l_pairs",
-                "surface_points", "m2l_rank"]
+                "surface_points", "m2l_rank",
+                "launches"]
         return dict(zip(keys, (int(v) for v in out)))
 
     def tree_stats(self, kernel) -> dict:
