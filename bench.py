@@ -54,6 +54,7 @@ WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clust
 WORKLOAD_FMM = ("LapPGrad free-space FMM (evaluate_fmm: U/W/X near field + KIFMM far field), same points and "
                 "values, p=10, max 256 pts/leaf")
 FMM_SAMPLE = 2000
+METRIC = "P2P pair-interactions/s (U-list S2T SL+DL; mixed path, FP64 beside it; FMM evals/s in fmm)"
 
 
 def make_points(seed: int):
@@ -72,6 +73,22 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def max_over_ranks(vals, ws, device="cuda"):
+    """Element-wise max of per-rank timings over the process group (identity for one rank)."""
+    if ws <= 1:
+        return [float(v) for v in vals]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_rate(units_per_rank, ws, seconds):
+    """Whole-job throughput: every rank processes units_per_rank in (max over ranks) seconds."""
+    return ws * units_per_rank / seconds
 
 
 # ---------------------------------------------------------------- clocks ----
@@ -236,7 +253,7 @@ def reference_arm(args):
     value = pairs / dt
     cores = os.cpu_count() or 1
     kind = "reference" if use_ref else "port"
-    line = {"impl": "reference", "metric": "P2P pair-interactions/s", "value": value, "unit": "pairs/s",
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "step": "bounded sample: U-lists of %d target leaves (%.3g pairs)"
@@ -317,10 +334,7 @@ def b200_arm(args):
         step_ms = [a.elapsed_time(b) for a, b in evs]
         ms = sum(step_ms) / len(step_ms)
         kms = sum(kern) / len(kern)
-        if ws > 1:
-            tt = torch.tensor([ms, kms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms, kms = float(tt[0]), float(tt[1])
+        ms, kms = max_over_ranks([ms, kms], ws)
         outs[prec] = out
         return ms, kms, wall
 
@@ -349,11 +363,7 @@ def b200_arm(args):
         torch.cuda.profiler.stop()
         torch.cuda.synchronize()
         barrier()
-        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
-        if ws > 1:
-            tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt[0])
+        ms = max_over_ranks([sum(a.elapsed_time(b) for a, b in evs) / steps], ws)[0]
         ph = {k: sum(p[k] for p in phases) / steps for k in phases[0]}
         return ms, ph, out
 
@@ -369,8 +379,8 @@ def b200_arm(args):
     fst = fmm.fmm_stats(K)
     clk = clocks.stop() if clocks else None
 
-    value = ws * pairs / (msmx * 1e-3)
-    value64 = ws * pairs / (ms64 * 1e-3)
+    value = job_rate(pairs, ws, msmx * 1e-3)
+    value64 = job_rate(pairs, ws, ms64 * 1e-3)
     o64 = outs[S.PRECISION.FP64].double()
     omx = outs[S.PRECISION.MIXED].double()
     err_mx = float(torch.linalg.norm(omx - o64) / torch.linalg.norm(o64))
@@ -390,12 +400,8 @@ def b200_arm(args):
         t0 = time.perf_counter()
         fmm.evaluate_near(K, qh, oh, dh)
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_t) / len(e2e_t)
-    if ws > 1:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt[0])
-    e2e_val = ws * pairs / e2e_s
+    e2e_s = max_over_ranks([sum(e2e_t) / len(e2e_t)], ws)[0]
+    e2e_val = job_rate(pairs, ws, e2e_s)
 
     # ---- FMM e2e: Stk3DFMM_evaluate_fmm with pinned host arrays (mixed) ----
     fmm.set_precision(S.PRECISION.MIXED)
@@ -408,11 +414,7 @@ def b200_arm(args):
         t0 = time.perf_counter()
         fmm.evaluate_fmm(K, qh, oh, dh)
         fe2e_t.append(time.perf_counter() - t0)
-    fe2e_s = sum(fe2e_t) / len(fe2e_t)
-    if ws > 1:
-        tt = torch.tensor([fe2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        fe2e_s = float(tt[0])
+    fe2e_s = max_over_ranks([sum(fe2e_t) / len(fe2e_t)], ws)[0]
 
     if rank != 0:
         if ws > 1:
@@ -457,14 +459,14 @@ def b200_arm(args):
                                            for c in range(4)]}
     fmm_block = {
         "workload": WORKLOAD_FMM,
-        "fp64": {"evals_per_s": ws * 1e3 / fms64, "ms_per_eval": fms64, "phases_ms": fph64},
-        "mixed": {"evals_per_s": ws * 1e3 / fmsmx, "ms_per_eval": fmsmx, "phases_ms": fphmx},
+        "fp64": {"evals_per_s": job_rate(1, ws, fms64 * 1e-3), "ms_per_eval": fms64, "phases_ms": fph64},
+        "mixed": {"evals_per_s": job_rate(1, ws, fmsmx * 1e-3), "ms_per_eval": fmsmx, "phases_ms": fphmx},
         "mixed_over_fp64": fms64 / fmsmx,
         "rel_l2_vs_direct_sum_sample": fmm_err,
         "sample": "%d targets drawn with seed 11; oracle direct sum over all %d sources (%.1f s on the host)"
                   % (FMM_SAMPLE, N_POINTS, oracle_s),
         "work_per_eval": fst,
-        "e2e": {"evals_per_s": ws / fe2e_s, "ms_per_eval": fe2e_s * 1e3,
+        "e2e": {"evals_per_s": job_rate(1, ws, fe2e_s), "ms_per_eval": fe2e_s * 1e3,
                 "api": "Stk3DFMM_evaluate_fmm (C ABI, pinned host arrays, mixed)",
                 "h2d_bytes_per_eval": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
                 "d2h_bytes_per_eval": int(N_POINTS * 4 * 8)},
@@ -473,7 +475,7 @@ def b200_arm(args):
     }
 
     line = {
-        "metric": "P2P pair-interactions/s (U-list S2T, mixed precision; FP64 path beside it)",
+        "metric": METRIC,
         "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (f64 displacement, Kahan f32 accumulation)", "data": "synthetic",
@@ -485,7 +487,7 @@ def b200_arm(args):
         "mixed_over_fp64": value / value64,
         "rel_l2_mixed_vs_fp64": err_mx, "rel_l2_mixed_vs_fp64_per_component": err_cols,
         "rel_l2_fp64_vs_oracle_sample": parity64,
-        "fmm_evals_per_s": ws * 1e3 / fmsmx,
+        "fmm_evals_per_s": job_rate(1, ws, fmsmx * 1e-3),
         "fmm": fmm_block,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peaks[0]), "unit": "TFLOP/s",
                      "frac": achieved / float(peaks[0]) if peaks[0] > 0 else None, "traffic": traffic,

@@ -59,7 +59,27 @@ template <> __device__ __forceinline__ F2 cst<F2>(double c) { return splat((floa
 
 // masked reciprocal square root: 0 where r2 == 0 (the reference's
 // approx_rsqrt<digits>(r2, r2 > 0))
+#ifndef STK_RSQ64_NEWTON
+#define STK_RSQ64_NEWTON 2  // Newton steps after the hardware approximation; 0 = CUDA's rsqrt
+#endif
+#if STK_RSQ64_NEWTON
+// Hardware approximation (MUFU, rsqrt.approx.ftz.f64) refined by Newton-Raphson
+// steps y <- y + y e / 2 with e = 1 - r2 y^2 (quadratic convergence; e from one
+// rounded product and one fma).  r2 below the smallest normal double counts as
+// coincident (|r| < 1.5e-154).
+__device__ __forceinline__ double rsq(double r2) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r2));
+#pragma unroll
+    for (int it = 0; it < STK_RSQ64_NEWTON; it++) {
+        const double e = fma(-(r2 * y), y, 1.0);
+        y = fma(0.5 * y, e, y);
+    }
+    return r2 >= 2.2250738585072014e-308 ? y : 0.0;
+}
+#else
 __device__ __forceinline__ double rsq(double r2) { return r2 > 0.0 ? rsqrt(r2) : 0.0; }
+#endif
 
 // Mixed path: hardware approximate rsqrt (MUFU, one per lane half) plus one
 // Newton-Raphson step y <- y (3 - r2 y^2) / 2 in packed FP32.  Pairs closer
