@@ -72,6 +72,8 @@ def lib():
         _lib.oracle_uk_pair.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         _lib.oracle_regvel_adjoint.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp,
                                                ctypes.c_int]
+        _lib.oracle_ewald.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                      _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
     return _lib
 
 
@@ -196,3 +198,26 @@ def ref_lists(which: int, trg_begin, trg_end, list_off, list_src, src_begin, src
                                 out.ctypes.data_as(_dp), td, nthreads)
     assert rc == 0
     return out
+
+
+EWALD_LAPLACE, EWALD_STOKES = 0, 1
+
+
+def ewald(kind: int, src, sval, trg, xi: float = 7.0, nreal: int = 1, nwave: int = 14, out=None, nthreads: int = 0):
+    """out += triply periodic (unit cell) sum by Ewald summation (see stk_oracle.c:oracle_ewald).
+
+    kind EWALD_LAPLACE: charges (n, 1) -> potential + gradient (n, 4), zero-mean Green's function;
+    kind EWALD_STOKES: forces (n, 3) -> velocity (n, 3).  Defaults (xi = 7, one real-space image
+    shell, |m| <= 14) converge to ~1e-15 for points in [0, 1)^3.
+    """
+    sd, td = (1, 4) if kind == EWALD_LAPLACE else (3, 3)
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    assert out.dtype == np.float64 and out.flags.c_contiguous
+    rc = lib().oracle_ewald(kind, xi, nreal, nwave, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return out
+

@@ -369,3 +369,134 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Triply periodic sums (unit cell) by Ewald summation.
+ *
+ * Restates the periodic Green's functions of the reference's M2C generator:
+ *   Laplace   M2L/Laplace/Laplace3D3D.cpp:14-84  (freal, frealp, gKernelEwald:
+ *             real terms erfc(xi r)/r, wave terms 4 pi cos(k.r) exp(-k^2/4xi^2)/k^2,
+ *             self term -2 xi/sqrt(pi), constant -pi/xi^2; all / 4 pi), i.e. the
+ *             zero-mean periodic Green's function;
+ *   Stokeslet M2L/Stokeslet/Stokes3D3D.cpp:19-68 (AEW, BEW, GkernelEwald: real
+ *             tensor A(xi, r), wave tensor B(xi, k) cos(k.r), self -4 xi/sqrt(pi) I,
+ *             k = 0 dropped; all / 8 pi).
+ * kind 0: q (1 value)  -> potential and gradient (4 outputs);
+ * kind 1: f (3 values) -> velocity (3 outputs).
+ * Real-space images |s_i| <= nreal around the minimum-image displacement, wave
+ * vectors k = 2 pi m with 0 < max|m_i| <= nwave (structure factors per k).  A
+ * target on a source point gets that source's periodic images but not the source
+ * itself (the self term).  out is accumulated.
+ * ------------------------------------------------------------------------ */
+int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const double *src, const double *val,
+                 int ntrg, const double *trg, double *out, int nthreads) {
+    if ((kind != 0 && kind != 1) || nsrc < 0 || ntrg < 0 || nreal < 0 || nwave < 0 || !(xi > 0)) return 1;
+    const int sd = kind == 0 ? 1 : 3, td = kind == 0 ? 4 : 3;
+    const double sqpi = sqrt(PI_), xi2 = xi * xi;
+    const double eps = 1e-13;
+    nthreads = clamp_threads(nthreads);
+    /* wave vectors and structure factors S_c = sum v cos(k.x), S_s = sum v sin(k.x) */
+    const int nm = 2 * nwave + 1, nk = nm * nm * nm;
+    double *Sc = (double *)calloc((size_t)nk * sd, sizeof(double));
+    double *Ss = (double *)calloc((size_t)nk * sd, sizeof(double));
+    if (!Sc || !Ss) {
+        free(Sc);
+        free(Ss);
+        return 2;
+    }
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int ik = 0; ik < nk; ik++) {
+        const int mx = ik % nm - nwave, my = (ik / nm) % nm - nwave, mz = ik / (nm * nm) - nwave;
+        if (mx == 0 && my == 0 && mz == 0) continue;
+        const double k[3] = {2 * PI_ * mx, 2 * PI_ * my, 2 * PI_ * mz};
+        double c[3] = {0, 0, 0}, sn[3] = {0, 0, 0};
+        for (int j = 0; j < nsrc; j++) {
+            const double ph = k[0] * src[3 * (size_t)j] + k[1] * src[3 * (size_t)j + 1] + k[2] * src[3 * (size_t)j + 2];
+            const double cp = cos(ph), sp = sin(ph);
+            for (int a = 0; a < sd; a++) {
+                c[a] += val[(size_t)sd * j + a] * cp;
+                sn[a] += val[(size_t)sd * j + a] * sp;
+            }
+        }
+        for (int a = 0; a < sd; a++) {
+            Sc[(size_t)sd * ik + a] = c[a];
+            Ss[(size_t)sd * ik + a] = sn[a];
+        }
+    }
+    double qsum = 0;
+    if (kind == 0)
+        for (int j = 0; j < nsrc; j++) qsum += val[j];
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads)
+    for (int t = 0; t < ntrg; t++) {
+        const double *x = trg + 3 * (size_t)t;
+        double acc[4] = {0, 0, 0, 0};
+        /* real space */
+        for (int j = 0; j < nsrc; j++) {
+            double d0[3];
+            for (int a = 0; a < 3; a++) {
+                d0[a] = x[a] - src[3 * (size_t)j + a];
+                d0[a] -= floor(d0[a] + 0.5);
+            }
+            const double *v = val + (size_t)sd * j;
+            for (int i = -nreal; i <= nreal; i++)
+                for (int jj = -nreal; jj <= nreal; jj++)
+                    for (int kk = -nreal; kk <= nreal; kk++) {
+                        const double r[3] = {d0[0] + i, d0[1] + jj, d0[2] + kk};
+                        const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                        if (rr < eps) {
+                            /* the source itself: its self term instead */
+                            if (kind == 0)
+                                acc[0] += -2 * xi / sqpi * v[0];
+                            else
+                                for (int a = 0; a < 3; a++) acc[a] += -4 * xi / sqpi * v[a];
+                            continue;
+                        }
+                        if (xi * rr > 7.0) continue; /* erfc(7) ~ 4e-23 */
+                        const double ex = exp(-xi2 * rr * rr), ec = erfc(xi * rr);
+                        if (kind == 0) {
+                            acc[0] += v[0] * ec / rr;
+                            const double fp = -(2. * ex * xi) / (sqpi * rr) - ec / (rr * rr);
+                            for (int a = 0; a < 3; a++) acc[1 + a] += v[0] * fp / rr * r[a];
+                        } else {
+                            const double c1 = 2 * (xi * ex / (sqpi * rr * rr) + ec / (2 * rr * rr * rr));
+                            const double c2 = 4 * xi / sqpi * ex;
+                            const double rf = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
+                            for (int a = 0; a < 3; a++) acc[a] += c1 * (rr * rr * v[a] + r[a] * rf) - c2 * v[a];
+                        }
+                    }
+        }
+        /* wave space */
+        for (int ik = 0; ik < nk; ik++) {
+            const int mx = ik % nm - nwave, my = (ik / nm) % nm - nwave, mz = ik / (nm * nm) - nwave;
+            if (mx == 0 && my == 0 && mz == 0) continue;
+            const double k[3] = {2 * PI_ * mx, 2 * PI_ * my, 2 * PI_ * mz};
+            const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+            const double ph = k[0] * x[0] + k[1] * x[1] + k[2] * x[2];
+            const double cp = cos(ph), sp = sin(ph);
+            const double g = exp(-k2 / (4 * xi2));
+            if (kind == 0) {
+                const double w = 4 * PI_ * g / k2;
+                /* sum_j q cos(k.(x - x_j)) and sum_j q sin(k.(x - x_j)) */
+                const double C = cp * Sc[ik] + sp * Ss[ik];
+                const double Sn = sp * Sc[ik] - cp * Ss[ik];
+                acc[0] += w * C;
+                for (int a = 0; a < 3; a++) acc[1 + a] -= w * k[a] * Sn;
+            } else {
+                const double w = 8 * PI_ * (1 + k2 / (4 * xi2)) * g / (k2 * k2);
+                double C[3];
+                for (int a = 0; a < 3; a++) C[a] = cp * Sc[3 * (size_t)ik + a] + sp * Ss[3 * (size_t)ik + a];
+                const double kC = k[0] * C[0] + k[1] * C[1] + k[2] * C[2];
+                for (int a = 0; a < 3; a++) acc[a] += w * (k2 * C[a] - k[a] * kC);
+            }
+        }
+        if (kind == 0) {
+            acc[0] -= PI_ / xi2 * qsum;
+            for (int a = 0; a < 4; a++) out[(size_t)td * t + a] += acc[a] / (4 * PI_);
+        } else {
+            for (int a = 0; a < 3; a++) out[(size_t)td * t + a] += acc[a] / (8 * PI_);
+        }
+    }
+    free(Sc);
+    free(Ss);
+    return 0;
+}

@@ -54,6 +54,10 @@ struct FarField {
     DevBuf m2l_vt;              // V^T: k x (n ke)
     DevBuf m2l_e;               // DC2DE U: (n ke) x k
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
+    // triply periodic: DC2DE M2C of the root (far images, max |s| >= 2)
+    bool periodic = false;
+    int m2c_p = 0, m2c_m2x = -1;
+    DevBuf m2c_op;
     // per-tree data
     DevBuf unit_surf;          // n x 3 points on [-1,1]^3
     DevBuf ue_xyz, de_xyz;     // every node's surfaces (nodes x n x 3)

@@ -1,0 +1,106 @@
+"""GPU: triply periodic (PXYZ) evaluate_fmm against the oracle's Ewald sums.
+
+The oracle (oracle/stk_oracle.c:oracle_ewald) restates the periodic Green's
+functions of the reference's M2C generator (M2L/Laplace/Laplace3D3D.cpp,
+M2L/Stokeslet/Stokes3D3D.cpp) and is itself checked for independence of the
+Ewald split and against lattice sums (tests/test_oracle.py).  Inputs follow the
+reference's periodic tests: net force (charge) removed (Test/Test.cpp:332-351).
+Error measure: relative L2 per output component (Test/Test.cpp:113-151).
+"""
+import numpy as np
+import pytest
+
+from conftest import component_errors
+from helpers import clustered_points
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {8: 2e-5, 10: 2e-6}
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def points(kind, n, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        return rng.random((n, 3)), rng
+    return np.minimum(clustered_points(rng, n, nclusters=5, sigma=0.05), 0.999), rng
+
+
+def periodic_fmm(kernel, p, max_pts, pts, slv):
+    import stkfmm_b200 as S
+    fmm = S.Stk3DFMM(p, max_pts, S.PAXIS.PXYZ, kernel)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    fmm.setup_tree(kernel)
+    out = np.zeros((len(pts), S.get_kernel_dimension(kernel)[2]))
+    fmm.evaluate_fmm(kernel, slv, out, None)
+    return fmm, out
+
+
+@pytest.mark.parametrize("dist", ["uniform", "clustered"])
+@pytest.mark.parametrize("p", [8, 10])
+def test_periodic_stokes(torch_cuda, dist, p):
+    pts, rng = points(dist, 5000, 3)
+    f = rng.normal(size=(len(pts), 3))
+    f -= f.mean(0)
+    fmm, out = periodic_fmm(8, p, 64, pts, f)
+    ref = O.ewald(O.EWALD_STOKES, pts, f, pts)
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[p], errs
+
+
+@pytest.mark.parametrize("p", [8, 10])
+def test_periodic_laplace(torch_cuda, p):
+    pts, rng = points("clustered", 5000, 4)
+    q = rng.uniform(-0.5, 0.5, (len(pts), 1))
+    q -= q.mean()
+    _, out = periodic_fmm(1, p, 64, pts, q)
+    ref = O.ewald(O.EWALD_LAPLACE, pts, q, pts)
+    # the periodic potential is defined up to a constant: compare it with the mean removed
+    out[:, 0] -= out[:, 0].mean()
+    ref[:, 0] -= ref[:, 0].mean()
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[p], errs
+
+
+def test_periodic_rpy_velocity(torch_cuda):
+    """RPY (u, lap u): u against Ewald Stokeslet + the finite-radius terms of the
+    27 nearest images (beyond those, b^2/r^3 terms are below 1e-8)."""
+    pts, rng = points("uniform", 4000, 5)
+    f = rng.normal(size=(len(pts), 3))
+    f -= f.mean(0)
+    b = rng.uniform(1e-4, 5e-4, len(pts))
+    slv = np.concatenate([f, b[:, None]], axis=1)
+    _, out = periodic_fmm(16, 10, 64, pts, slv)
+    ref = O.ewald(O.EWALD_STOKES, pts, f, pts)
+    r = np.arange(-1, 2)
+    shifts = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    imgs = (pts[None] + shifts[:, None]).reshape(-1, 3)
+    corr = O.direct(O.UK_RPY_U, imgs, np.tile(slv, (27, 1)), pts) - O.direct(O.UK_STOKES_VEL, imgs,
+                                                                            np.tile(f, (27, 1)), pts)
+    errs = component_errors(out[:, :3], ref + corr)
+    assert max(errs) < TOL[10], errs
+
+
+def test_periodic_mixed_close_to_fp64(torch_cuda):
+    import stkfmm_b200 as S
+    pts, rng = points("clustered", 5000, 6)
+    f = rng.normal(size=(len(pts), 3))
+    f -= f.mean(0)
+    res = []
+    for prec in (S.PRECISION.FP64, S.PRECISION.MIXED):
+        fmm = S.Stk3DFMM(10, 64, S.PAXIS.PXYZ, 8, precision=prec)
+        fmm.set_box(np.zeros(3), 1.0)
+        fmm.set_points(pts, pts, None)
+        fmm.setup_tree(8)
+        out = np.zeros((len(pts), 3))
+        fmm.evaluate_fmm(8, f, out, None)
+        res.append(out)
+    assert np.linalg.norm(res[1] - res[0]) / np.linalg.norm(res[0]) < 1e-6

@@ -133,3 +133,45 @@ def test_regvel_adjoint_finite_difference(rng):
             # the target copies of points 0..9 stay fixed: this is the source-position gradient
             fd = (loss(sp, sv) - loss(sm, sv)) / (2 * h)
             assert abs(fd - gx[i, k]) <= 1e-5 * max(1.0, abs(fd))
+
+
+# ---- triply periodic Ewald sums (the periodic FMM's oracle) ----------------------
+
+@pytest.mark.parametrize("kind", [O.EWALD_LAPLACE, O.EWALD_STOKES])
+def test_ewald_splitting_independent(kind):
+    """The Ewald split (xi, image counts) must not change the periodic sum."""
+    rng = np.random.default_rng(21 + kind)
+    src = rng.random((200, 3))
+    v = rng.normal(size=(200, 1 if kind == O.EWALD_LAPLACE else 3))
+    v -= v.mean(0)
+    trg = np.concatenate([rng.random((40, 3)), src[:10]])   # includes targets on source points
+    a = O.ewald(kind, src, v, trg)
+    b = O.ewald(kind, src, v, trg, xi=2.0, nreal=4, nwave=5)
+    c = O.ewald(kind, src, v, trg, xi=4.0, nreal=2, nwave=9)
+    assert np.abs(a - b).max() < 1e-13 * np.abs(a).max()
+    assert np.abs(a - c).max() < 1e-13 * np.abs(a).max()
+    # periodic in every axis
+    d = O.ewald(kind, src, v, trg + np.array([1.0, -2.0, 3.0]))
+    assert np.abs(a - d).max() < 1e-13 * np.abs(a).max()
+
+
+def test_ewald_laplace_field_matches_image_sum():
+    """For a cell whose charges have no net charge, dipole or quadrupole moment
+    (alternating charges on the corners of small cubes) the field of the image
+    lattice summed over growing cubes converges to the Ewald field."""
+    import itertools
+    rng = np.random.default_rng(5)
+    c = rng.random((3, 3)) * 0.5 + 0.25
+    sg = np.array(list(itertools.product([-1, 1], [-1, 1], [-1, 1])), dtype=np.float64)
+    src = np.concatenate([ci + 0.04 * sg for ci in c])
+    q = np.tile(sg.prod(1), 3)[:, None]
+    trg = rng.random((5, 3))
+    ew = O.ewald(O.EWALD_LAPLACE, src, q, trg)[:, 1:]
+    errs = []
+    for L in (2, 8):
+        r = np.arange(-L, L + 1)
+        shifts = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+        imgs = (src[None, :, :] + shifts[:, None, :]).reshape(-1, 3)
+        direct = O.direct(O.UK_LAPLACE_PGRAD, imgs, np.tile(q, (len(shifts), 1)), trg)[:, 1:]
+        errs.append(np.abs(direct - ew).max() / np.abs(ew).max())
+    assert errs[1] < 1e-6 and errs[1] < errs[0] / 50, errs
