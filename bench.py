@@ -144,6 +144,83 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------- further FMM workloads ----
+EXTRA_FMM = [
+    {"name": "stokes_32k_uniform", "kernel": 8, "pbc": 0, "p": 8, "max_pts": 128, "n": 32768,
+     "workload": "StokesVel free-space FMM: 32,768 points ~ U[0,1)^3 as sources and targets, f ~ N(0,1)^3, "
+                 "p=8, max 128 pts/leaf, seed 0"},
+    {"name": "rpy_pxyz_2m_uniform", "kernel": 16, "pbc": 3, "p": 8, "max_pts": 256, "n": 2097152,
+     "workload": "RPY triply periodic (PXYZ) FMM: 2,097,152 points ~ U[0,1)^3, f ~ N(0,1)^3 minus its mean, "
+                 "b ~ U(1e-4,5e-4), p=8, max 256 pts/leaf, seed 0"},
+]
+
+
+def extra_fmm_inputs(cfg, seed):
+    rng = np.random.default_rng(seed)
+    n = cfg["n"]
+    pts = rng.random((n, 3))
+    f = rng.normal(size=(n, 3))
+    if cfg["pbc"]:
+        f -= f.mean(0)  # net force removed for the periodic sum (Test/Test.cpp:332-351)
+    if cfg["kernel"] == 16:
+        f = np.concatenate([f, rng.uniform(1e-4, 5e-4, (n, 1))], axis=1)
+    return pts, f
+
+
+def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
+    """evaluate_fmm_device of one further workload, FP64 and mixed, CUDA events per evaluation."""
+    import torch
+    import stkfmm_b200 as S
+    pts, slv = extra_fmm_inputs(cfg, seed)
+    K = cfg["kernel"]
+    td = S.get_kernel_dimension(K)[2]
+    fmm = S.Stk3DFMM(cfg["p"], cfg["max_pts"], cfg["pbc"], K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    fmm.setup_tree(K)
+    d_sl = torch.as_tensor(slv).cuda()
+    res = {"workload": cfg["workload"], "tree": fmm.tree_stats(K)}
+    outs = {}
+    for prec, nm in ((S.PRECISION.FP64, "fp64"), (S.PRECISION.MIXED, "mixed")):
+        fmm.set_precision(prec)
+        out = torch.zeros((len(pts), td), dtype=torch.float64, device="cuda")
+        for _ in range(warmup):
+            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), 0, None)
+        torch.cuda.synchronize()
+        ms, phases = [], []
+        for _ in range(steps):
+            flush.zero_()
+            out.zero_()
+            torch.cuda.synchronize()
+            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), 0, None)
+            torch.cuda.synchronize()
+            ms.append(fmm.last_kernel_ms(K))
+            phases.append(fmm.last_phase_ms(K))
+        m = max_over_ranks([sum(ms) / steps], ws)[0]
+        res[nm] = {"evals_per_s": job_rate(1, ws, m * 1e-3), "ms_per_eval": m,
+                   "phases_ms": {k: sum(p[k] for p in phases) / steps for k in phases[0]}}
+        outs[nm] = out.cpu().numpy()
+    res["mixed_over_fp64"] = res["fp64"]["ms_per_eval"] / res["mixed"]["ms_per_eval"]
+    res["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(outs["mixed"] - outs["fp64"]) / np.linalg.norm(outs["fp64"]))
+    res["work_per_eval"] = fmm.fmm_stats(K)
+    res["gpu_launches_per_eval"] = fmm.last_launch_count(K)
+    res["timing"] = "device time of each evaluate_fmm_device (CUDA events on the handle's stream), L2 flushed between"
+    return res, pts, slv, outs
+
+
+def extra_fmm_accuracy(cfg, pts, slv, outs, nsample=4096):
+    """Free-space workloads: both precisions against the oracle's direct sum on a target sample."""
+    if cfg["pbc"]:
+        return None
+    from oracle import oracle as O
+    O.build()
+    samp = np.random.default_rng(13).choice(len(pts), min(nsample, len(pts)), replace=False)
+    uk = {8: O.UK_STOKES_VEL}[cfg["kernel"]]
+    ref = O.direct(uk, pts, slv, pts[samp])
+    return {nm: [float(np.linalg.norm(o[samp, c] - ref[:, c]) / np.linalg.norm(ref[:, c]))
+                 for c in range(ref.shape[1])] for nm, o in outs.items()}
+
+
 # ---------------------------------------------------------- CPU baseline ----
 def sample_boxes(ul, budget_pairs, seed=1):
     """Random target leaves of the U-list whose SL+DL pairs sum to ~budget_pairs."""
@@ -416,6 +493,12 @@ def b200_arm(args):
         fe2e_t.append(time.perf_counter() - t0)
     fe2e_s = max_over_ranks([sum(fe2e_t) / len(fe2e_t)], ws)[0]
 
+    # ---- the further FMM workloads (configs 1 and 3): every rank runs its own replica ----
+    extra = []
+    for cfg in EXTRA_FMM:
+        r, epts, eslv, eouts = time_extra_fmm(cfg, rank, args.steps, args.warmup, ws, flush)
+        extra.append((cfg, r, epts, eslv, eouts))
+
     if rank != 0:
         if ws > 1:
             dist.barrier()
@@ -457,6 +540,10 @@ def b200_arm(args):
         fmm_err[name] = {"all": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
                          "per_component": [float(np.linalg.norm(got[:, c] - ref[:, c]) / np.linalg.norm(ref[:, c]))
                                            for c in range(4)]}
+    extra_blocks = {}
+    for cfg, r, epts, eslv, eouts in extra:
+        r["rel_l2_vs_direct_sum_sample_per_component"] = extra_fmm_accuracy(cfg, epts, eslv, eouts)
+        extra_blocks[cfg["name"]] = r
     fmm_block = {
         "workload": WORKLOAD_FMM,
         "fp64": {"evals_per_s": job_rate(1, ws, fms64 * 1e-3), "ms_per_eval": fms64, "phases_ms": fph64},
@@ -489,6 +576,7 @@ def b200_arm(args):
         "rel_l2_fp64_vs_oracle_sample": parity64,
         "fmm_evals_per_s": job_rate(1, ws, fmsmx * 1e-3),
         "fmm": fmm_block,
+        "fmm_other_workloads": extra_blocks,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peaks[0]), "unit": "TFLOP/s",
                      "frac": achieved / float(peaks[0]) if peaks[0] > 0 else None, "traffic": traffic,
                      "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, mixed>", "kernel_ms": kmx,
@@ -505,7 +593,8 @@ def b200_arm(args):
         "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
                 "d2h_bytes_per_step": int(N_POINTS * 4 * 8), "ms_per_step": e2e_s * 1e3,
                 "api": "Stk3DFMM_evaluate_near (C ABI, pinned host arrays)"},
-        "gpu_launches": args.steps * (2 * near_launches + 2 * fmm_launches),
+        "gpu_launches": args.steps * (2 * near_launches + 2 * fmm_launches
+                                      + sum(2 * b["gpu_launches_per_eval"] for b in extra_blocks.values())),
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
