@@ -201,9 +201,41 @@ int kernel_matrix(int uk, const double *X, int ni, const double *Y, int nj, doub
         kernel_matrix_kernel<UK_LAPLACE_P><<<grid, threads, 0, s>>>(X, ni, Y, nj, M, ld);
     else if (uk == UK_STOKES_VEL)
         kernel_matrix_kernel<UK_STOKES_VEL><<<grid, threads, 0, s>>>(X, ni, Y, nj, M, ld);
+    else if (uk == UK_STOKES_PVEL)
+        kernel_matrix_kernel<UK_STOKES_PVEL><<<grid, threads, 0, s>>>(X, ni, Y, nj, M, ld);
     else
         return STK_ERR_NOT_SUPPORTED;
     return cudaGetLastError() == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+// Per-component factors (up to 4 components, repeated over surface points).
+struct CompF {
+    double v[4];
+};
+
+// M[i + ld j] *= fr.v[i % dim] * fc.v[j % dim]   (rows x cols)
+__global__ void scale_rc_kernel(double *__restrict__ M, int rows, int cols, int ld, int dim, CompF fr, CompF fc) {
+    const long long total = (long long)rows * cols;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % rows), j = (int)(idx / rows);
+        M[(size_t)i + (size_t)ld * j] *= fr.v[i % dim] * fc.v[j % dim];
+    }
+}
+
+// Column c of buf (rows_per_col values, components interleaved with period dim)
+// is multiplied per row by 2^(-level * e[row % dim]); level = col_level[c], or
+// level_all when col_level is null.
+__global__ void level_scale_kernel(double *__restrict__ buf, long long ncols, int rows_per_col, int dim,
+                                   const int *__restrict__ col_level, int level_all, CompF e) {
+    const long long total = ncols * rows_per_col;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx / rows_per_col;
+        const int r = (int)(idx - c * rows_per_col);
+        const int l = col_level ? col_level[c] : level_all;
+        buf[idx] *= exp2(-(double)l * e.v[r % dim]);
+    }
 }
 
 // W[i + m j] = U[j + m i] / S_i for S_i above the cut, else 0  (W = S^+ U^T)
@@ -422,11 +454,25 @@ int build_operators(FarField &F, cudaStream_t s) {
         rc = kmat(scaled_surface(unit, 0, 0, 0, kRad1 * r0), scaled_surface(unit, cx, cy, cz, kRad0 * r0 / 2),
                   (double *)K.ptr);
         if (rc) return rc;
+        if (F.scaled) {
+            // child densities are normalised one level deeper: component c carries 2^-den_exp[c] more
+            CompF one4 = {{1, 1, 1, 1}}, fc;
+            for (int c = 0; c < 4; c++) fc.v[c] = std::exp2(-F.den_exp[c]);
+            scale_rc_kernel<<<grid_for((long long)N * N), 256, 0, s>>>((double *)K.ptr, N, N, N, F.ke, one4, fc);
+            FCUDA(cudaGetLastError());
+        }
         FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &one, (const double *)F.uc2ue.ptr, N,
                           (const double *)K.ptr, N, &zero, (double *)F.m2m.ptr + (size_t)o * N * N, N));
         rc = kmat(scaled_surface(unit, cx, cy, cz, kRad0 * r0 / 2), scaled_surface(unit, 0, 0, 0, kRad1 * r0),
                   (double *)K.ptr);
         if (rc) return rc;
+        if (F.scaled) {
+            // child check potentials are normalised one level deeper: component a carries 2^-pot_exp[a] more
+            CompF one4 = {{1, 1, 1, 1}}, fr;
+            for (int a = 0; a < 4; a++) fr.v[a] = std::exp2(-F.pot_exp[a]);
+            scale_rc_kernel<<<grid_for((long long)N * N), 256, 0, s>>>((double *)K.ptr, N, N, N, F.kc, fr, one4);
+            FCUDA(cudaGetLastError());
+        }
         // the child's DC2DE is half the parent's (degree -1 kernels); rows o N .. of the 8N x N stack
         FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &half, (const double *)F.dc2de.ptr, N,
                           (const double *)K.ptr, N, &zero, (double *)F.l2l.ptr + (size_t)o * N, 8 * N));
@@ -594,7 +640,10 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     // PX / PXY far fields are not built
     if (f->pbc != 0 && f->pbc != 3) return STK_ERR_NOT_SUPPORTED;
     const int m2x = ki->slot[SLOT_M2X];
-    if (m2x != UK_LAPLACE_P && m2x != UK_STOKES_VEL) return STK_ERR_NOT_SUPPORTED;
+    if (m2x != UK_LAPLACE_P && m2x != UK_STOKES_VEL && m2x != UK_STOKES_PVEL) return STK_ERR_NOT_SUPPORTED;
+    // stokes_pvel mixes homogeneity degrees (PVFMM's per-component source / target
+    // scaling): p from f and u from trD fall off one power faster than u from f
+    if (m2x == UK_STOKES_PVEL && f->pbc != 0) return STK_ERR_NOT_SUPPORTED;
     if (!kd->far) kd->far.reset(new FarField());
     FarField &F = *kd->far;
     cudaStream_t s = f->stream;
@@ -610,6 +659,12 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     const double m2l_rtol = env_rtol ? atof(env_rtol) : (p <= 10 ? 1e-8 : 1e-10);
     if (F.p != p || F.m2x != m2x || F.m2l_rtol != m2l_rtol) {
         F.m2l_rtol = m2l_rtol;
+        for (int c = 0; c < 4; c++) F.pot_exp[c] = F.den_exp[c] = 0.0;
+        F.scaled = m2x == UK_STOKES_PVEL;
+        if (F.scaled) {
+            F.pot_exp[0] = 1.0;  // pressure
+            F.den_exp[3] = 1.0;  // trD
+        }
         F.p = p;
         F.n = 6 * (p - 1) * (p - 1) + 2;
         F.ke = ke;
@@ -632,7 +687,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     rc = upload_points(F.unit_surf, unit, s);
     // node levels and centres on the device
     std::vector<int> lev(T.level.begin(), T.level.end());
-    DevBuf d_level;
+    DevBuf &d_level = F.d_level;
     if (!rc) rc = d_level.upload(lev.data(), lev.size() * sizeof(int), s);
     const double *centre = (const double *)kd->d_centre.ptr;
     // every node's upward-equivalent and downward-equivalent surface
@@ -951,7 +1006,17 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         for (int l = 0; l + 1 < (int)F.s2m_level_off.size(); l++) {
             const int a = F.s2m_level_off[l], m = F.s2m_level_off[l + 1] - a;
             if (m <= 0) continue;
-            const double alpha = std::ldexp(1.0, -l);
+            double alpha = std::ldexp(1.0, -l);
+            if (F.scaled) {
+                // normalised check potential: 2^-l (1 + pot_exp[a]) per component
+                CompF e;
+                for (int c = 0; c < 4; c++) e.v[c] = 1.0 + F.pot_exp[c];
+                level_scale_kernel<<<grid_for((long long)m * n * kc), 256, 0, s>>>(
+                    (double *)F.check.ptr + (size_t)a * n * kc, m, n * kc, kc, nullptr, l, e);
+                FCUDA(cudaGetLastError());
+                t_launches++;
+                alpha = 1.0;
+            }
             FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, n * kc, &alpha, (const double *)F.uc2ue.ptr, N,
                               (const double *)F.check.ptr + (size_t)a * n * kc, n * kc, &zero, Y, N));
             int rc = scatter_cols(Y, (const int *)F.d_s2m_nodes.ptr + a, m, N, 1.0, 0, phi, s);
@@ -1036,7 +1101,16 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
             for (int l = 0; l + 1 < (int)F.s2l_level_off.size(); l++) {
                 const int a = F.s2l_level_off[l], m = F.s2l_level_off[l + 1] - a;
                 if (m <= 0) continue;
-                const double alpha = std::ldexp(1.0, -l);
+                double alpha = std::ldexp(1.0, -l);
+                if (F.scaled) {
+                    CompF e;
+                    for (int c = 0; c < 4; c++) e.v[c] = 1.0 + F.pot_exp[c];
+                    level_scale_kernel<<<grid_for((long long)m * n * kc), 256, 0, s>>>(
+                        (double *)F.dcheck.ptr + (size_t)a * n * kc, m, n * kc, kc, nullptr, l, e);
+                    FCUDA(cudaGetLastError());
+                    t_launches++;
+                    alpha = 1.0;
+                }
                 FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, m, n * kc, &alpha, (const double *)F.dc2de.ptr,
                                   N, (const double *)F.dcheck.ptr + (size_t)a * n * kc, n * kc, &zero, Y, N));
                 int rc = scatter_cols(Y, (const int *)F.d_s2l_nodes.ptr + a, m, N, 1.0, 1, psi, s);
@@ -1068,6 +1142,17 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     };
     FCUDA(cudaEventRecord(kd->ph[5], s));
     const double *trg_xyz = (const double *)kd->d_xyz[2].ptr;
+    if (F.scaled) {
+        // back to physical densities at each node's level: component c times 2^-l den_exp[c]
+        CompF e;
+        for (int c = 0; c < 4; c++) e.v[c] = F.den_exp[c];
+        level_scale_kernel<<<grid_for((long long)nn * N), 256, 0, s>>>(psi, nn, N, ke, (const int *)F.d_level.ptr, 0,
+                                                                      e);
+        level_scale_kernel<<<grid_for((long long)nn * N), 256, 0, s>>>(phi, nn, N, ke, (const int *)F.d_level.ptr, 0,
+                                                                      e);
+        FCUDA(cudaGetLastError());
+        t_launches += 2;
+    }
     int rc = pack_surface(F.de_xyz, psi, F.l2t.uk);
     if (!rc)
         rc = run_pass(F.l2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.l2t.src_beg.ptr,

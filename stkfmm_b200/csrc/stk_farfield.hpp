@@ -40,6 +40,11 @@ struct FarField {
     int p = 0, n = 0;      // multipole order, surface points per box
     int ke = 0, kc = 0;    // equivalent density and check potential dims
     int m2x = -1;          // micro-kernel of the translations (k_m2m = k_m2l = k_l2l)
+    // K(s r) = s^-1 diag(s^-pot_exp) K(r) diag(s^-den_exp): with densities and check
+    // potentials normalised per level and component, the operators of a side-1 box
+    // serve every level (all zero for laplace_p / stokes_vel)
+    bool scaled = false;
+    double pot_exp[4] = {0, 0, 0, 0}, den_exp[4] = {0, 0, 0, 0};
     bool ready = false;
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;
@@ -60,6 +65,7 @@ struct FarField {
     DevBuf m2c_op;
     // per-tree data
     DevBuf unit_surf;          // n x 3 points on [-1,1]^3
+    DevBuf d_level;            // node levels
     DevBuf ue_xyz, de_xyz;     // every node's surfaces (nodes x n x 3)
     DevBuf uc_xyz, dc_xyz;     // S2M targets (leaves with sources), S2L targets (nodes with X lists)
     DevBuf phi, psi;           // equivalent densities per node (nodes x n x ke)
