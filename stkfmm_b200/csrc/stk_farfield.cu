@@ -304,6 +304,51 @@ __global__ void upper_copy_kernel(const double *__restrict__ A, long long m, int
     }
 }
 
+// Optional tensor-core M2L for the mixed path (STK_M2L_TF32_TERMS = 3, 4 or 6;
+// 0 = off, the default): each operand is split into kTf32Pieces TF32 values
+// (cvt.rna.tf32.f32, 10 explicit mantissa bits each) a = a0 + a1 (+ a2), and the
+// product is the sum of the TF32 products listed in kTf32Terms (piece of C_d,
+// piece of the sources), smallest first, accumulated by the tensor cores.
+// Measured on B200: 2-3x faster than the FP32 SIMT GEMM, but the FMM's
+// mixed-vs-FP64 error rises from 4.5e-7 to 1.4e-6 (StokesVel, 32k points, p = 8)
+// and the LapPGrad potential's from 1.5e-7 to 2.4e-6, independent of the number
+// of pieces: the compressed M2L sums terms much larger than its result (the
+// equivalent densities carry the pseudo-inverse's large oscillating parts), and
+// the tensor cores' FP32 accumulation loses more there than FMA-by-FMA FP32.
+#ifndef STK_M2L_TF32_TERMS
+#define STK_M2L_TF32_TERMS 0
+#endif
+#if STK_M2L_TF32_TERMS == 3
+constexpr int kTf32Pieces = 2, kTf32Terms = 3;
+constexpr int kTf32Term[3][2] = {{1, 0}, {0, 1}, {0, 0}};
+#elif STK_M2L_TF32_TERMS == 4
+constexpr int kTf32Pieces = 2, kTf32Terms = 4;
+constexpr int kTf32Term[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};
+#elif STK_M2L_TF32_TERMS == 6
+constexpr int kTf32Pieces = 3, kTf32Terms = 6;
+constexpr int kTf32Term[6][2] = {{2, 0}, {0, 2}, {1, 1}, {1, 0}, {0, 1}, {0, 0}};
+#else
+constexpr int kTf32Pieces = 1, kTf32Terms = 1;  // one FP32 piece: the FP32 SIMT GEMM
+constexpr int kTf32Term[1][2] = {{0, 0}};
+#endif
+constexpr bool kM2LTensor = STK_M2L_TF32_TERMS != 0;
+
+__device__ __forceinline__ float tf32_rna(float x) {
+    unsigned int u;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+    return __uint_as_float(u);
+}
+
+// piece p of a (p < kTf32Pieces): a0 = tf32(a), a1 = tf32(a - a0), a2 = a - a0 - a1
+__device__ __forceinline__ void split_tf32(double a, float *out, size_t stride) {
+    double r = a;
+    for (int p = 0; p < kTf32Pieces; p++) {
+        const float v = p + 1 < kTf32Pieces ? tf32_rna((float)r) : (float)r;
+        out[p * stride] = v;
+        r -= (double)v;
+    }
+}
+
 constexpr int kM2LChunk = 256;  // pairs (columns) per batched-GEMM problem of the M2L
 
 // X[r + k j] = phi_hat[r + k gsrc[j]], or 0 for a padding column (gsrc[j] < 0)
@@ -320,23 +365,41 @@ __global__ void m2l_gather_kernel(const double *__restrict__ phi_hat, const int 
     }
 }
 
-// psi_hat[r + k t] = sum over the columns of target t (in order) of Y[r + k col]
+// the same gather, split into TF32 pieces (piece p at X + p * k * ncol)
+__global__ void m2l_gather_split_kernel(const double *__restrict__ phi_hat, const int *__restrict__ gsrc, int k,
+                                        long long ncol, float *__restrict__ X) {
+    const long long total = ncol * k;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long j = idx / k;
+        const int r = (int)(idx - j * k);
+        const int a = gsrc[j];
+        split_tf32(a >= 0 ? phi_hat[(size_t)a * k + r] : 0.0, X + idx, (size_t)total);
+    }
+}
+
+// psi_hat[r + k t] += sum, in order, of Y[r + k (col[e] - c0)] over target t's
+// entries e in [beg[t], end[t]) -- its columns inside the current group, which
+// starts at column c0 (a target's columns ascend, so they form one run per group)
 template <class T>
-__global__ void m2l_reduce_kernel(const T *__restrict__ Y, const int *__restrict__ off, const int *__restrict__ col,
-                                  int nn, int k, double *__restrict__ psi_hat) {
+__global__ void m2l_reduce_kernel(const T *__restrict__ Y, const int *__restrict__ beg, const int *__restrict__ end,
+                                  const int *__restrict__ col, int nn, int k, long long c0,
+                                  double *__restrict__ psi_hat) {
     const long long total = (long long)nn * k;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const int t = (int)(idx / k), r = (int)(idx - (long long)t * k);
+        const int e0 = beg[t], e1 = end[t];
+        if (e0 == e1) continue;
         double acc = 0.0;
-        for (int e = off[t]; e < off[t + 1]; e++) acc += (double)Y[(size_t)col[e] * k + r];
-        psi_hat[idx] = acc;
+        for (int e = e0; e < e1; e++) acc += (double)Y[(size_t)((long long)col[e] - c0) * k + r];
+        psi_hat[idx] += acc;
     }
 }
 
-__global__ void to_float_kernel(const double *__restrict__ a, long long n, float *__restrict__ b) {
+__global__ void split_tf32_kernel(const double *__restrict__ a, long long n, float *__restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
+        split_tf32(a[i], out + i, (size_t)n);
 }
 
 // A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
@@ -546,11 +609,11 @@ int build_operators(FarField &F, cudaStream_t s) {
         FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, k, N, &one, (const double *)VTu.ptr, N,
                           (const double *)T.ptr, N, &zero, (double *)F.m2l_c.ptr + (size_t)sl * k * k, k));
     }
-    // FP32 copy for the mixed-precision path (C_d holds no pseudo-inverse)
-    rc = F.m2l_c32.reserve(sizeof(float) * (size_t)nslot * k * k);
+    // TF32 pieces for the mixed path's tensor-core M2L (C_d holds no pseudo-inverse)
+    rc = F.m2l_c32.reserve(kTf32Pieces * sizeof(float) * (size_t)nslot * k * k);
     if (rc) return rc;
-    to_float_kernel<<<grid_for((long long)nslot * k * k), 256, 0, s>>>((const double *)F.m2l_c.ptr,
-                                                                      (long long)nslot * k * k, (float *)F.m2l_c32.ptr);
+    split_tf32_kernel<<<grid_for((long long)nslot * k * k), 256, 0, s>>>(
+        (const double *)F.m2l_c.ptr, (long long)nslot * k * k, (float *)F.m2l_c32.ptr);
     FCUDA(cudaGetLastError());
     FCUDA(cudaStreamSynchronize(s));
     return STK_OK;
@@ -921,30 +984,53 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         rc = F.d_m2l_gsrc.upload(gsrc.data(), sizeof(int) * gsrc.size(), s);
         if (!rc) rc = F.d_m2l_red_off.upload(red_off.data(), sizeof(int) * red_off.size(), s);
         if (!rc) rc = F.d_m2l_red_col.upload(red_col.data(), sizeof(int) * red_col.size(), s);
-        if (!rc) rc = F.m2l_x.reserve(sizeof(double) * (size_t)k * std::max<long long>(F.m2l_cols, 1));
-        if (!rc) rc = F.m2l_y.reserve(sizeof(double) * (size_t)k * std::max<long long>(F.m2l_cols, 1));
         if (rc) return rc;
-        // pointer arrays of the batched GEMMs (FP64 and FP32 views of the same buffers)
+        // columns are processed in groups of whole chunks that keep the gathered sources and
+        // the products within ~2 GiB each
         const int nc = F.m2l_chunks;
-        std::vector<const double *> pa(nc), pb(nc);
-        std::vector<double *> pc(nc);
-        std::vector<const float *> qa(nc), qb(nc);
-        std::vector<float *> qc(nc);
+        const size_t per_chunk = (size_t)kM2LChunk * k * sizeof(double);
+        F.m2l_group_chunks = (int)std::max<size_t>(1, std::min<size_t>(nc, (2ull << 30) / per_chunk));
+        const int gc = F.m2l_group_chunks;
+        const size_t gcols = (size_t)gc * kM2LChunk;
+        // per group g and target t: the first of t's entries whose column is in group g or later
+        const int ngroups = (nc + gc - 1) / gc;
+        std::vector<int> gstart((size_t)(ngroups + 1) * nn);
+        for (int b = 0; b < nn; b++) {
+            int e = red_off[b];
+            for (int g = 0; g <= ngroups; g++) {
+                const long long gcol0 = (long long)g * gc * kM2LChunk;
+                while (e < red_off[b + 1] && red_col[e] < gcol0) e++;
+                gstart[(size_t)g * nn + b] = e;
+            }
+        }
+        rc = F.d_m2l_gstart.upload(gstart.data(), sizeof(int) * gstart.size(), s);
+        if (rc) return rc;
+        rc = F.m2l_x.reserve(std::max(sizeof(double), kTf32Pieces * sizeof(float)) * (size_t)k * gcols);
+        if (!rc) rc = F.m2l_y.reserve(sizeof(double) * (size_t)k * gcols);
+        if (rc) return rc;
+        // pointer arrays of the batched GEMMs: C_d per chunk (global); X / Y chunk
+        // positions within one group (FP64 and FP32 views of the same buffers)
+        std::vector<const void *> pa(nc), pb(gc), pc(gc);
+        std::vector<const void *> qa((size_t)kTf32Pieces * nc), qb((size_t)kTf32Pieces * gc), qc(gc);
         const size_t step = (size_t)kM2LChunk * k;
+        const size_t cpiece = (size_t)nslot * k * k, xpiece = (size_t)k * gcols;
         for (int c = 0; c < nc; c++) {
             pa[c] = (const double *)F.m2l_c.ptr + (size_t)chunk_slot[c] * k * k;
+            for (int p = 0; p < kTf32Pieces; p++)
+                qa[(size_t)p * nc + c] = (const float *)F.m2l_c32.ptr + p * cpiece + (size_t)chunk_slot[c] * k * k;
+        }
+        for (int c = 0; c < gc; c++) {
             pb[c] = (const double *)F.m2l_x.ptr + c * step;
             pc[c] = (double *)F.m2l_y.ptr + c * step;
-            qa[c] = (const float *)F.m2l_c32.ptr + (size_t)chunk_slot[c] * k * k;
-            qb[c] = (const float *)F.m2l_x.ptr + c * step;
+            for (int p = 0; p < kTf32Pieces; p++) qb[(size_t)p * gc + c] = (const float *)F.m2l_x.ptr + p * xpiece + c * step;
             qc[c] = (float *)F.m2l_y.ptr + c * step;
         }
-        rc = F.d_ptr64[0].upload(pa.data(), sizeof(void *) * nc, s);
-        if (!rc) rc = F.d_ptr64[1].upload(pb.data(), sizeof(void *) * nc, s);
-        if (!rc) rc = F.d_ptr64[2].upload(pc.data(), sizeof(void *) * nc, s);
-        if (!rc) rc = F.d_ptr32[0].upload(qa.data(), sizeof(void *) * nc, s);
-        if (!rc) rc = F.d_ptr32[1].upload(qb.data(), sizeof(void *) * nc, s);
-        if (!rc) rc = F.d_ptr32[2].upload(qc.data(), sizeof(void *) * nc, s);
+        rc = F.d_ptr64[0].upload(pa.data(), sizeof(void *) * pa.size(), s);
+        if (!rc) rc = F.d_ptr64[1].upload(pb.data(), sizeof(void *) * pb.size(), s);
+        if (!rc) rc = F.d_ptr64[2].upload(pc.data(), sizeof(void *) * pc.size(), s);
+        if (!rc) rc = F.d_ptr32[0].upload(qa.data(), sizeof(void *) * qa.size(), s);
+        if (!rc) rc = F.d_ptr32[1].upload(qb.data(), sizeof(void *) * qb.size(), s);
+        if (!rc) rc = F.d_ptr32[2].upload(qc.data(), sizeof(void *) * qc.size(), s);
         if (rc) return rc;
         // host vectors above are pageable: their copies complete before upload returns
         int maxm = 0;
@@ -1044,37 +1130,43 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
                       phi_hat, k));
     // gather the sources of every (offset, chunk) column, one batched GEMM over the
     // chunks, then each target sums its columns in offset order (deterministic)
-    const long long ncol = F.m2l_cols;
-    if (ncol > 0) {
+    FCUDA(cudaMemsetAsync(psi_hat, 0, sizeof(double) * (size_t)nn * k, s));
+    const int nc = F.m2l_chunks, gc = F.m2l_group_chunks;
+    for (int c0 = 0; c0 < nc; c0 += gc) {
+        const int *gbeg = (const int *)F.d_m2l_gstart.ptr + (size_t)(c0 / gc) * nn, *gend = gbeg + nn;
+        const int ncg = std::min(gc, nc - c0);
+        const long long col0 = (long long)c0 * kM2LChunk, ncol = (long long)ncg * kM2LChunk;
+        const int *gsrc = (const int *)F.d_m2l_gsrc.ptr + col0;
         const int gg = grid_for(ncol * k);
         t_launches += 2;
         if (prec == PREC_MIXED) {
-            // the translation C_d carries no pseudo-inverse: FP32 operands, FP32 accumulation
-            m2l_gather_kernel<float><<<gg, 256, 0, s>>>(phi_hat, (const int *)F.d_m2l_gsrc.ptr, k, ncol,
-                                                        (float *)F.m2l_x.ptr);
+            // The translation C_d carries no pseudo-inverse: FP32 operands and FP32
+            // accumulation (or the optional TF32 piece products, see kTf32Terms)
+            m2l_gather_split_kernel<<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (float *)F.m2l_x.ptr);
             FCUDA(cudaGetLastError());
             const float onef = 1.0f, zerof = 0.0f;
-            FBLAS(cublasSgemmBatched(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &onef,
-                                     (const float *const *)F.d_ptr32[0].ptr, k, (const float *const *)F.d_ptr32[1].ptr,
-                                     k, &zerof, (float *const *)F.d_ptr32[2].ptr, k, F.m2l_chunks));
+            const void *const *qa = (const void *const *)F.d_ptr32[0].ptr;
+            const void *const *qb = (const void *const *)F.d_ptr32[1].ptr;
+            for (int t = 0; t < kTf32Terms; t++)
+                FBLAS(cublasGemmBatchedEx(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &onef,
+                                          qa + (size_t)kTf32Term[t][0] * nc + c0, CUDA_R_32F, k,
+                                          qb + (size_t)kTf32Term[t][1] * gc, CUDA_R_32F, k, t == 0 ? &zerof : &onef,
+                                          (void *const *)F.d_ptr32[2].ptr, CUDA_R_32F, k, ncg,
+                                          kM2LTensor ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F,
+                                          CUBLAS_GEMM_DEFAULT));
             m2l_reduce_kernel<float><<<grid_for((long long)nn * k), 256, 0, s>>>(
-                (const float *)F.m2l_y.ptr, (const int *)F.d_m2l_red_off.ptr, (const int *)F.d_m2l_red_col.ptr, nn, k,
-                psi_hat);
+                (const float *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
         } else {
-            m2l_gather_kernel<double><<<gg, 256, 0, s>>>(phi_hat, (const int *)F.d_m2l_gsrc.ptr, k, ncol,
-                                                         (double *)F.m2l_x.ptr);
+            m2l_gather_kernel<double><<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (double *)F.m2l_x.ptr);
             FCUDA(cudaGetLastError());
             FBLAS(cublasDgemmBatched(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &one,
-                                     (const double *const *)F.d_ptr64[0].ptr, k,
+                                     (const double *const *)F.d_ptr64[0].ptr + c0, k,
                                      (const double *const *)F.d_ptr64[1].ptr, k, &zero,
-                                     (double *const *)F.d_ptr64[2].ptr, k, F.m2l_chunks));
+                                     (double *const *)F.d_ptr64[2].ptr, k, ncg));
             m2l_reduce_kernel<double><<<grid_for((long long)nn * k), 256, 0, s>>>(
-                (const double *)F.m2l_y.ptr, (const int *)F.d_m2l_red_off.ptr, (const int *)F.d_m2l_red_col.ptr, nn,
-                k, psi_hat);
+                (const double *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
         }
         FCUDA(cudaGetLastError());
-    } else {
-        FCUDA(cudaMemsetAsync(psi_hat, 0, sizeof(double) * (size_t)nn * k, s));
     }
     FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,
                       psi, N));

@@ -55,7 +55,7 @@ struct FarField {
     // compressed M2L: M2L_d = m2l_e C_d m2l_vt
     double m2l_rtol = 0;        // relative singular-value cut of the M2L bases
     int m2l_rank = 0;           // k
-    DevBuf m2l_c, m2l_c32;      // 316 blocks of k x k (FP64, FP32 copy for the mixed path)
+    DevBuf m2l_c, m2l_c32;      // 316 blocks of k x k (FP64; TF32 pieces for the mixed path)
     DevBuf m2l_vt;              // V^T: k x (n ke)
     DevBuf m2l_e;               // DC2DE U: (n ke) x k
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
@@ -84,11 +84,12 @@ struct FarField {
     // M2L: V-list pairs grouped by offset in chunks of columns (one batched GEMM)
     int launches = 0;                       // own kernels of the last evaluation (cuBLAS excluded)
     long long m2l_pairs = 0, m2l_cols = 0;  // pairs; columns including chunk padding
-    int m2l_chunks = 0;
+    int m2l_chunks = 0, m2l_group_chunks = 1;  // chunks; chunks per group of columns
     DevBuf d_m2l_gsrc;                      // per column: source node, -1 = padding
     DevBuf d_m2l_red_off, d_m2l_red_col;    // per target node: its columns (CSR, offset order)
-    DevBuf m2l_x, m2l_y;                    // k x columns (FP64, or FP32 in the mixed path)
-    DevBuf d_ptr64[3], d_ptr32[3];          // batched-GEMM pointer arrays (C_d, X chunk, Y chunk)
+    DevBuf d_m2l_gstart;                    // per group and target node: first entry in that group
+    DevBuf m2l_x, m2l_y;                    // one group of columns: k x columns (FP64, or FP32 pieces)
+    DevBuf d_ptr64[3], d_ptr32[3];          // batched-GEMM pointer arrays: C_d (per chunk), X and Y (per group slot)
     ~FarField();
 };
 
