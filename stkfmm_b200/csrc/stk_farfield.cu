@@ -312,9 +312,8 @@ __global__ void upper_copy_kernel(const double *__restrict__ A, long long m, int
 // Measured on B200: 2-3x faster than the FP32 SIMT GEMM, but the FMM's
 // mixed-vs-FP64 error rises from 4.5e-7 to 1.4e-6 (StokesVel, 32k points, p = 8)
 // and the LapPGrad potential's from 1.5e-7 to 2.4e-6, independent of the number
-// of pieces: the compressed M2L sums terms much larger than its result (the
-// equivalent densities carry the pseudo-inverse's large oscillating parts), and
-// the tensor cores' FP32 accumulation loses more there than FMA-by-FMA FP32.
+// of pieces, so the limit is the tensor cores' FP32 accumulation over k = 240-716
+// terms, not the operand split.
 #ifndef STK_M2L_TF32_TERMS
 #define STK_M2L_TF32_TERMS 0
 #endif
