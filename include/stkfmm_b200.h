@@ -198,6 +198,12 @@ int Stk3DFMM_evaluate_kernel(Stk3DFMM *fmm, unsigned kernel, int nThreads, unsig
                              double *srcCoord, double *srcValue, int nTrg, double *trgCoord, double *trgValue);
 /* choose FP64 or MIXED for the P2P kernels of this handle (default FP64) */
 int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision);
+/* Multi-GPU sharding of one problem: this handle evaluates only shard `rank` of
+ * `nranks` of the target-side work (near-field P2P, L2T, M2T), dealt by cost;
+ * the upward pass, S2L and M2L are computed in full on every shard.  The sum of
+ * all shards' evaluate_near / evaluate_fmm outputs (e.g. an all-reduce) is the
+ * unsharded result.  Takes effect at the next setup_tree (default 0 of 1). */
+int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks);
 /* Near-field (U-list S2T) part of evaluate_fmm only, on the tree of setup_tree:
  * trg_value += sum over U-list leaf pairs, in the caller's coordinates/units. */
 int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
@@ -248,6 +254,10 @@ typedef struct stk_octree stk_octree;
 stk_octree *stk_octree_build(const double *tree_pts, int n, int max_pts, int pbc, const double *sl, int nsl,
                              const double *dl, int ndl, const double *trg, int ntrg);
 void stk_octree_free(stk_octree *t);
+/* The shard assignment behind Stk3DFMM_set_shard (host only): n work items in the
+ * given order (largest cost first) are dealt to the least-loaded of nparts parts;
+ * owner[i] receives the part of item i. */
+int stk_partition_lpt(int n, const double *cost, int nparts, int *owner);
 /* out = {nodes, leaves, depth, U entries, V entries, W entries, X entries} */
 int stk_octree_sizes(const stk_octree *t, long long *out);
 /* per node: level, parent (-1 root), first child (-1 leaf, children contiguous), integer coords (3) */

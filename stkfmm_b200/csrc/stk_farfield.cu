@@ -654,11 +654,12 @@ int build_periodic(FarField &F, cudaStream_t s) {
 // own_src is false.
 int setup_pass(ListPass &P, int uk, const std::vector<int> &tb, const std::vector<int> &te,
                const std::vector<int> &off, const std::vector<int> &ent, const int *h_src_beg, const int *h_src_end,
-               int n_src_box, bool own_src, const std::vector<double> &centres, int balance_warps, cudaStream_t s) {
+               int n_src_box, bool own_src, const std::vector<double> &centres, int balance_warps, cudaStream_t s,
+               int shard_rank = 0, int shard_n = 1) {
     P.uk = uk;
     std::vector<WorkItem> items;
     build_list_items((int)tb.size(), tb.data(), te.data(), off.data(), ent.data(), h_src_beg, h_src_end, items,
-                     P.pairs, balance_warps);
+                     P.pairs, balance_warps, shard_rank, shard_n);
     P.n_items = (int)items.size();
     int rc = P.items.upload(items.data(), items.size() * sizeof(WorkItem), s);
     if (!rc) rc = P.ent.upload(ent.data(), ent.size() * sizeof(int), s);
@@ -844,7 +845,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             F.near[k].reset();
             if (T.sets[k].n == 0 || ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL] < 0) continue;
             rc = setup_pass(F.near[k], ki->slot[k == 0 ? SLOT_S2T_SL : SLOT_S2T_DL], tg.node_begin, tg.node_end, noff,
-                            nent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(), nn, false, ctr, bw, s);
+                            nent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(), nn, false, ctr, bw, s,
+                            f->shard_rank, f->shard_n);
             if (rc) return rc;
         }
     }
@@ -908,11 +910,13 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         woff[nn] = (int)went.size();
         F.m2t.reset();
         F.l2t.reset();
+        // target-side passes follow the handle's shard (the upward pass, S2L and the
+        // M2L are computed in full on every shard)
         rc = setup_pass(F.m2t, ki->slot[SLOT_M2T], tg.node_begin, tg.node_end, woff, went, sb.data(), se.data(), nn,
-                        true, ctr, bw, s);
+                        true, ctr, bw, s, f->shard_rank, f->shard_n);
         if (!rc)
             rc = setup_pass(F.l2t, ki->slot[SLOT_L2T], tg.node_begin, tg.node_end, loff, lent, sb.data(), se.data(),
-                            nn, true, ctr, bw, s);
+                            nn, true, ctr, bw, s, f->shard_rank, f->shard_n);
         if (rc) return rc;
     }
 

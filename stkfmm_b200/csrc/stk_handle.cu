@@ -247,7 +247,8 @@ extern "C" int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel) {
         std::vector<WorkItem> items;
         long long pairs = 0;
         build_list_items(nn, tg.node_begin.data(), tg.node_end.data(), T.U.off.data(), T.U.ent.data(),
-                         sp.node_begin.data(), sp.node_end.data(), items, pairs, fmm->sms * 12);
+                         sp.node_begin.data(), sp.node_end.data(), items, pairs, fmm->sms * 12, fmm->shard_rank,
+                         fmm->shard_n);
         kd->u_pairs[k] = pairs;
         kd->n_items[k] = (int)items.size();
         up(kd->d_items[k], items.data(), items.size() * sizeof(WorkItem));
@@ -279,6 +280,18 @@ extern "C" int Stk3DFMM_show_active_kernels(Stk3DFMM *fmm) {
     for (int i = 0; i < kNumKernels; i++)
         if (fmm->kernel_comb & kKernels[i].id) printf("\t%s", kKernels[i].name);
     printf("\n");
+    return STK_OK;
+}
+
+extern "C" int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks) {
+    if (!fmm || nranks < 1 || rank < 0 || rank >= nranks) return STK_ERR_INVALID_ARG;
+    if (fmm->shard_rank != rank || fmm->shard_n != nranks)
+        for (auto &kv : fmm->pool) {
+            kv.second->tree_ready = false;  // work lists are rebuilt by the next setup_tree
+            kv.second->far_ready = false;
+        }
+    fmm->shard_rank = rank;
+    fmm->shard_n = nranks;
     return STK_OK;
 }
 

@@ -59,6 +59,7 @@ struct Stk3DFMM {
     double len = 1.0, scale_factor = 1.0;
     int precision = 0;
     int device = 0, sms = 1;
+    int shard_rank = 0, shard_n = 1;  // target-side work of this handle: shard shard_rank of shard_n
     cudaStream_t stream = nullptr;
     bool points_set = false, sl_dl_same = false;
     int nsl = 0, ndl = 0, ntrg = 0;

@@ -9,6 +9,7 @@
 
 #include "../../include/stkfmm_b200.h"
 #include "stk_tree.hpp"
+#include "stk_work.hpp"
 
 struct stk_octree {
     stk::Octree tree;
@@ -80,5 +81,15 @@ extern "C" int stk_octree_set(const stk_octree *t, int set, int *perm, int *node
     if (perm && P.n) std::memcpy(perm, P.perm.data(), P.perm.size() * sizeof(int));
     if (node_begin) std::memcpy(node_begin, P.node_begin.data(), P.node_begin.size() * sizeof(int));
     if (node_end) std::memcpy(node_end, P.node_end.data(), P.node_end.size() * sizeof(int));
+    return STK_OK;
+}
+
+// The shard assignment used by Stk3DFMM_set_shard: items in the given order
+// (largest cost first) dealt to the least-loaded part.  Host only.
+extern "C" int stk_partition_lpt(int n, const double *cost, int nparts, int *owner) {
+    if (n < 0 || nparts < 1 || (n > 0 && (!cost || !owner))) return STK_ERR_INVALID_ARG;
+    std::vector<int> o;
+    stk::partition_lpt(n, cost, nparts, o);
+    if (n) std::memcpy(owner, o.data(), sizeof(int) * n);
     return STK_OK;
 }

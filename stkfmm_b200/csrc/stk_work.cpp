@@ -143,7 +143,7 @@ void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &
 
 void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
                       const int *list_ent, const int *src_begin, const int *src_end, std::vector<WorkItem> &items,
-                      long long &pairs, int balance_warps) {
+                      long long &pairs, int balance_warps, int shard_rank, int shard_n) {
     items.clear();
     pairs = 0;
     std::vector<long long> box_ns(n_trg_box, 0);
@@ -194,9 +194,48 @@ void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, c
     std::vector<int> idx(items.size());
     std::iota(idx.begin(), idx.end(), 0);
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    std::vector<WorkItem> sorted(items.size());
-    for (size_t i = 0; i < idx.size(); i++) sorted[i] = items[idx[i]];
+    std::vector<WorkItem> sorted;
+    sorted.reserve(items.size());
+    if (shard_n > 1) {
+        // this shard's items: the cost-sorted items dealt to the least-loaded
+        // shard in turn (the same deterministic assignment on every shard)
+        std::vector<int> owner;
+        std::vector<double> sc;
+        for (int i : idx) sc.push_back(cost[i]);
+        partition_lpt((int)sc.size(), sc.data(), shard_n, owner);
+        pairs = 0;
+        for (size_t i = 0; i < idx.size(); i++)
+            if (owner[i] == shard_rank) {
+                const WorkItem &w = items[idx[i]];
+                sorted.push_back(w);
+                pairs += (long long)w.nt * pair_sources(w, list_ent, src_begin, src_end);
+            }
+    } else {
+        for (size_t i = 0; i < idx.size(); i++) sorted.push_back(items[idx[i]]);
+    }
     items.swap(sorted);
+}
+
+long long pair_sources(const WorkItem &w, const int *list_ent, const int *src_begin, const int *src_end) {
+    long long ns = 0;
+    for (int e = w.e0; e < w.e1; e++) {
+        const int sb = list_ent[e] >> 5;
+        ns += src_end[sb] - src_begin[sb];
+    }
+    return ns;
+}
+
+void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner) {
+    owner.assign(n, 0);
+    if (nparts <= 1) return;
+    std::vector<double> load(nparts, 0.0);
+    for (int i = 0; i < n; i++) {
+        int best = 0;
+        for (int r = 1; r < nparts; r++)
+            if (load[r] < load[best]) best = r;
+        owner[i] = best;
+        load[best] += cost[i];
+    }
 }
 
 void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted) {

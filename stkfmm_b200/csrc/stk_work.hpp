@@ -46,10 +46,19 @@ void build_direct_items(int ntrg, int nsrc, int num_sms, std::vector<WorkItem> &
 
 // Cost-sorted work items for an explicit list; pairs = exact (target, source point) pair count.
 // balance_warps > 0: boxes with many sources get smaller target chunks, so that no
-// item holds more than ~pairs / (2 balance_warps) pairs.
+// item holds more than ~pairs / (2 balance_warps) pairs.  shard_n > 1: only the items
+// of shard shard_rank are kept (partition_lpt over the cost-sorted items), and pairs
+// counts those.
 void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
                       const int *list_ent, const int *src_begin, const int *src_end, std::vector<WorkItem> &items,
-                      long long &pairs, int balance_warps = 0);
+                      long long &pairs, int balance_warps = 0, int shard_rank = 0, int shard_n = 1);
+
+// Source points of one work item (the sum over its list entries).
+long long pair_sources(const WorkItem &w, const int *list_ent, const int *src_begin, const int *src_end);
+
+// Longest-processing-time assignment: items (in the given order, largest first)
+// each go to the part with the smallest load so far; ties to the lowest part.
+void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner);
 
 // Morton order of points inside their own bounding box.
 void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted);

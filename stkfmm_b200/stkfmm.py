@@ -234,6 +234,10 @@ class Stk3DFMM:
         check(lib().Stk3DFMM_last_phase_ms(self.fmm, int(kernel), ms.ctypes.data_as(P_f)), "last_phase_ms")
         return dict(zip(self.PHASES, (float(v) for v in ms)))
 
+    def set_shard(self, rank: int, nranks: int):
+        """Evaluate only shard `rank` of `nranks` of the target-side work (sum over shards = full result)."""
+        check(lib().Stk3DFMM_set_shard(self.fmm, int(rank), int(nranks)), "set_shard")
+
     def last_launch_count(self, kernel) -> int:
         n = ctypes.c_int()
         check(lib().Stk3DFMM_last_launch_count(self.fmm, int(kernel), ctypes.byref(n)), "last_launch_count")
