@@ -74,6 +74,7 @@ def lib():
                                                ctypes.c_int]
         _lib.oracle_ewald.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                       _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        _lib.oracle_ewald2d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
     return _lib
 
 
@@ -207,10 +208,11 @@ def ewald(kind: int, src, sval, trg, xi: float = 7.0, nreal: int = 1, nwave: int
     """out += triply periodic (unit cell) sum by Ewald summation (see stk_oracle.c:oracle_ewald).
 
     kind EWALD_LAPLACE: charges (n, 1) -> potential + gradient (n, 4), zero-mean Green's function;
-    kind EWALD_STOKES: forces (n, 3) -> velocity (n, 3).  Defaults (xi = 7, one real-space image
+    kind EWALD_STOKES: forces (n, 3) -> velocity (n, 3); kind EWALD_PVEL: (f, trD) (n, 4) -> pressure and
+    velocity of stokes_pvel (n, 4).  Defaults (xi = 7, one real-space image
     shell, |m| <= 14) converge to ~1e-15 for points in [0, 1)^3.
     """
-    sd, td = (1, 4) if kind == EWALD_LAPLACE else (3, 3)
+    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), 2: (4, 4)}[kind]
     src, ps = _d(np.asarray(src).reshape(-1, 3))
     sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
     trg, pt = _d(np.asarray(trg).reshape(-1, 3))
@@ -218,6 +220,27 @@ def ewald(kind: int, src, sval, trg, xi: float = 7.0, nreal: int = 1, nwave: int
         out = np.zeros((len(trg), td))
     assert out.dtype == np.float64 and out.flags.c_contiguous
     rc = lib().oracle_ewald(kind, xi, nreal, nwave, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return out
+
+
+EWALD_PVEL = 2
+
+
+def ewald2d(kind: int, src, sval, trg, out=None, nthreads: int = 0):
+    """out += doubly periodic (x, y; z free) sum per pair (see stk_oracle.c:oracle_ewald2d).
+
+    kind EWALD_LAPLACE: (n, 1) -> (n, 4) potential + gradient; EWALD_STOKES: (n, 3) -> (n, 3);
+    EWALD_PVEL: (f, trD) (n, 4) -> (pressure, velocity) (n, 4).
+    """
+    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), EWALD_PVEL: (4, 4)}[kind]
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    assert out.dtype == np.float64 and out.flags.c_contiguous
+    rc = lib().oracle_ewald2d(kind, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
     assert rc == 0
     return out
 

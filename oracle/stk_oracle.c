@@ -382,7 +382,10 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
  *             tensor A(xi, r), wave tensor B(xi, k) cos(k.r), self -4 xi/sqrt(pi) I,
  *             k = 0 dropped; all / 8 pi).
  * kind 0: q (1 value)  -> potential and gradient (4 outputs);
- * kind 1: f (3 values) -> velocity (3 outputs).
+ * kind 1: f (3 values) -> velocity (3 outputs);
+ * kind 2: (f, trD) (4 values) -> stokes_pvel's pressure and velocity (4 outputs):
+ *         p = -grad(psi).f / 4 pi, u = G f / 8 pi + grad(psi) trD / 8 pi, with psi the
+ *         Laplace sum above and G the Stokeslet sum.
  * Real-space images |s_i| <= nreal around the minimum-image displacement, wave
  * vectors k = 2 pi m with 0 < max|m_i| <= nwave (structure factors per k).  A
  * target on a source point gets that source's periodic images but not the source
@@ -390,15 +393,17 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
  * ------------------------------------------------------------------------ */
 int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const double *src, const double *val,
                  int ntrg, const double *trg, double *out, int nthreads) {
-    if ((kind != 0 && kind != 1) || nsrc < 0 || ntrg < 0 || nreal < 0 || nwave < 0 || !(xi > 0)) return 1;
-    const int sd = kind == 0 ? 1 : 3, td = kind == 0 ? 4 : 3;
+    if (kind < 0 || kind > 2 || nsrc < 0 || ntrg < 0 || nreal < 0 || nwave < 0 || !(xi > 0)) return 1;
+    const int sd = kind == 0 ? 1 : kind == 1 ? 3 : 4, td = kind == 1 ? 3 : 4;
+    /* structure-factor columns: the values, plus f.k for kind 2 */
+    const int ns = kind == 2 ? 5 : sd;
     const double sqpi = sqrt(PI_), xi2 = xi * xi;
     const double eps = 1e-13;
     nthreads = clamp_threads(nthreads);
     /* wave vectors and structure factors S_c = sum v cos(k.x), S_s = sum v sin(k.x) */
     const int nm = 2 * nwave + 1, nk = nm * nm * nm;
-    double *Sc = (double *)calloc((size_t)nk * sd, sizeof(double));
-    double *Ss = (double *)calloc((size_t)nk * sd, sizeof(double));
+    double *Sc = (double *)calloc((size_t)nk * ns, sizeof(double));
+    double *Ss = (double *)calloc((size_t)nk * ns, sizeof(double));
     if (!Sc || !Ss) {
         free(Sc);
         free(Ss);
@@ -409,18 +414,24 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
         const int mx = ik % nm - nwave, my = (ik / nm) % nm - nwave, mz = ik / (nm * nm) - nwave;
         if (mx == 0 && my == 0 && mz == 0) continue;
         const double k[3] = {2 * PI_ * mx, 2 * PI_ * my, 2 * PI_ * mz};
-        double c[3] = {0, 0, 0}, sn[3] = {0, 0, 0};
+        double c[5] = {0, 0, 0, 0, 0}, sn[5] = {0, 0, 0, 0, 0};
         for (int j = 0; j < nsrc; j++) {
             const double ph = k[0] * src[3 * (size_t)j] + k[1] * src[3 * (size_t)j + 1] + k[2] * src[3 * (size_t)j + 2];
             const double cp = cos(ph), sp = sin(ph);
+            const double *v = val + (size_t)sd * j;
             for (int a = 0; a < sd; a++) {
-                c[a] += val[(size_t)sd * j + a] * cp;
-                sn[a] += val[(size_t)sd * j + a] * sp;
+                c[a] += v[a] * cp;
+                sn[a] += v[a] * sp;
+            }
+            if (kind == 2) {
+                const double fk = v[0] * k[0] + v[1] * k[1] + v[2] * k[2];
+                c[4] += fk * cp;
+                sn[4] += fk * sp;
             }
         }
-        for (int a = 0; a < sd; a++) {
-            Sc[(size_t)sd * ik + a] = c[a];
-            Ss[(size_t)sd * ik + a] = sn[a];
+        for (int a = 0; a < ns; a++) {
+            Sc[(size_t)ns * ik + a] = c[a];
+            Ss[(size_t)ns * ik + a] = sn[a];
         }
     }
     double qsum = 0;
@@ -444,24 +455,33 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
                         const double r[3] = {d0[0] + i, d0[1] + jj, d0[2] + kk};
                         const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
                         if (rr < eps) {
-                            /* the source itself: its self term instead */
+                            /* the source itself: its self term instead (no gradient) */
                             if (kind == 0)
                                 acc[0] += -2 * xi / sqpi * v[0];
-                            else
+                            else if (kind == 1)
                                 for (int a = 0; a < 3; a++) acc[a] += -4 * xi / sqpi * v[a];
+                            else
+                                for (int a = 0; a < 3; a++) acc[1 + a] += -4 * xi / sqpi * v[a];
                             continue;
                         }
                         if (xi * rr > 7.0) continue; /* erfc(7) ~ 4e-23 */
                         const double ex = exp(-xi2 * rr * rr), ec = erfc(xi * rr);
+                        const double fp = -(2. * ex * xi) / (sqpi * rr) - ec / (rr * rr);
                         if (kind == 0) {
                             acc[0] += v[0] * ec / rr;
-                            const double fp = -(2. * ex * xi) / (sqpi * rr) - ec / (rr * rr);
                             for (int a = 0; a < 3; a++) acc[1 + a] += v[0] * fp / rr * r[a];
                         } else {
                             const double c1 = 2 * (xi * ex / (sqpi * rr * rr) + ec / (2 * rr * rr * rr));
                             const double c2 = 4 * xi / sqpi * ex;
                             const double rf = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
-                            for (int a = 0; a < 3; a++) acc[a] += c1 * (rr * rr * v[a] + r[a] * rf) - c2 * v[a];
+                            if (kind == 1) {
+                                for (int a = 0; a < 3; a++) acc[a] += c1 * (rr * rr * v[a] + r[a] * rf) - c2 * v[a];
+                            } else {
+                                /* accumulated in units of 1 / 4 pi; the velocity rows halve at the end */
+                                acc[0] -= fp / rr * rf;
+                                for (int a = 0; a < 3; a++)
+                                    acc[1 + a] += c1 * (rr * rr * v[a] + r[a] * rf) - c2 * v[a] + fp / rr * r[a] * v[3];
+                            }
                         }
                     }
         }
@@ -483,20 +503,174 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
                 for (int a = 0; a < 3; a++) acc[1 + a] -= w * k[a] * Sn;
             } else {
                 const double w = 8 * PI_ * (1 + k2 / (4 * xi2)) * g / (k2 * k2);
+                const int o = kind == 1 ? 0 : 1;
                 double C[3];
-                for (int a = 0; a < 3; a++) C[a] = cp * Sc[3 * (size_t)ik + a] + sp * Ss[3 * (size_t)ik + a];
+                for (int a = 0; a < 3; a++) C[a] = cp * Sc[(size_t)ns * ik + a] + sp * Ss[(size_t)ns * ik + a];
                 const double kC = k[0] * C[0] + k[1] * C[1] + k[2] * C[2];
-                for (int a = 0; a < 3; a++) acc[a] += w * (k2 * C[a] - k[a] * kC);
+                for (int a = 0; a < 3; a++) acc[o + a] += w * (k2 * C[a] - k[a] * kC);
+                if (kind == 2) {
+                    const double wl = 4 * PI_ * g / k2;
+                    /* sum_j (f_j.k) sin(k.(x - x_j)) and sum_j trD_j sin(k.(x - x_j)) */
+                    const double Sfk = sp * Sc[(size_t)ns * ik + 4] - cp * Ss[(size_t)ns * ik + 4];
+                    const double St = sp * Sc[(size_t)ns * ik + 3] - cp * Ss[(size_t)ns * ik + 3];
+                    acc[0] += wl * Sfk;
+                    for (int a = 0; a < 3; a++) acc[1 + a] -= wl * k[a] * St;
+                }
             }
         }
         if (kind == 0) {
             acc[0] -= PI_ / xi2 * qsum;
             for (int a = 0; a < 4; a++) out[(size_t)td * t + a] += acc[a] / (4 * PI_);
-        } else {
+        } else if (kind == 1) {
             for (int a = 0; a < 3; a++) out[(size_t)td * t + a] += acc[a] / (8 * PI_);
+        } else {
+            out[(size_t)td * t] += acc[0] / (4 * PI_);
+            for (int a = 0; a < 3; a++) out[(size_t)td * t + 1 + a] += acc[1 + a] / (8 * PI_);
         }
     }
     free(Sc);
     free(Ss);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Doubly periodic sums (period 1 in x and y, z free), per pair, restating the
+ * reference's generator: Laplace potential M2L/Laplace/Laplace2D3D.cpp:12-83,
+ * Laplace gradient M2L/StokesPVel/StokesPVel2D3D.cpp:167-240, Stokeslet
+ * M2L/Stokeslet/Stokes2D3D.cpp:19-168 (xi = 2; 11 x 11 real images and wave
+ * vectors, as there).  Values without the 1/(4 pi) or 1/(8 pi) factors.
+ * ------------------------------------------------------------------------ */
+static const double XI2D = 2.0;
+static const int NR2D = 5, NW2D = 5;
+
+static void ewald2_laplace(const double r0[3], double *pot, double grad[3]) {
+    const double xi = XI2D, z = r0[2], sp = sqrt(PI_);
+    double p = 0.0, g[3] = {0, 0, 0};
+    for (int a = -NR2D; a <= NR2D; a++)
+        for (int b = -NR2D; b <= NR2D; b++) {
+            const double r[3] = {r0[0] + a, r0[1] + b, z};
+            const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            if (rr < 1e-13) {
+                p += -2 * xi / sp;
+                continue;
+            }
+            p += erfc(xi * rr) / rr;
+            const double fp = -(2. * exp(-rr * rr * xi * xi) * xi) / (sp * rr) - erfc(rr * xi) / (rr * rr);
+            for (int k = 0; k < 3; k++) g[k] += fp / rr * r[k];
+        }
+    for (int a = -NW2D; a <= NW2D; a++)
+        for (int b = -NW2D; b <= NW2D; b++) {
+            if (a == 0 && b == 0) continue;
+            const double kx = 2 * PI_ * a, ky = 2 * PI_ * b, k = sqrt(kx * kx + ky * ky);
+            const double ph = kx * r0[0] + ky * r0[1];
+            const double ep = exp(k * z) * erfc(xi * z + k / (2 * xi));
+            const double em = exp(-k * z) * erfc(-xi * z + k / (2 * xi));
+            const double gz = k * ep - k * em +
+                              (2 * xi / sp) * (exp(-pow(-xi * z + k / (2 * xi), 2) - k * z) -
+                                               exp(-pow(xi * z + k / (2 * xi), 2) + k * z));
+            p += PI_ * cos(ph) * (ep + em) / k;
+            g[0] += -PI_ * sin(ph) * (ep + em) / k * kx;
+            g[1] += -PI_ * sin(ph) * (ep + em) / k * ky;
+            g[2] += PI_ * cos(ph) * gz / k;
+        }
+    p -= 2 * sp * (exp(-xi * xi * z * z) / xi + sp * z * erf(xi * z));
+    g[2] += -2 * PI_ * erf(xi * z);
+    *pot = p;
+    for (int k = 0; k < 3; k++) grad[k] = g[k];
+}
+
+static void ewald2_stokes(const double r0[3], double G[3][3]) {
+    const double xi = XI2D, xi2 = xi * xi, z = r0[2], sp = sqrt(PI_);
+    double A[3][3] = {{0}};
+    for (int a = -NR2D; a <= NR2D; a++)
+        for (int b = -NR2D; b <= NR2D; b++) {
+            const double r[3] = {r0[0] + a, r0[1] + b, z};
+            const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            if (rr < 1e-13) {
+                for (int i = 0; i < 3; i++) A[i][i] += -4 * xi / sp;
+                continue;
+            }
+            const double e2 = exp(-xi2 * rr * rr);
+            const double s1 = 2 * (xi * e2 / (sp * rr * rr) + erfc(xi * rr) / (2 * rr * rr * rr));
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++)
+                    A[i][j] += s1 * ((i == j) * rr * rr + r[i] * r[j]) - (i == j) * 4 * xi / sp * e2;
+        }
+    for (int a = -NW2D; a <= NW2D; a++)
+        for (int b = -NW2D; b <= NW2D; b++) {
+            if (a == 0 && b == 0) continue;
+            const double kk[2] = {2 * PI_ * a, 2 * PI_ * b};
+            const double k = sqrt(kk[0] * kk[0] + kk[1] * kk[1]);
+            const double lam = exp(-k * k / (4 * xi2) - xi2 * z * z);
+            const double thp = exp(k * z) * erfc(k / (2 * xi) + xi * z);
+            const double thm = exp(-k * z) * erfc(k / (2 * xi) - xi * z);
+            const double J00 = sp * lam * xi;
+            const double J10 = PI_ * (thp + thm) / (4 * k);
+            const double J20 = sp * lam / (4 * k * k * xi) +
+                               PI_ * ((thp + thm) / (8 * k * k * k) + (thm - thp) * z / (8 * k * k) -
+                                      (thp + thm) / (16 * k * xi2));
+            const double J12 = PI_ * (-thp - thm) * k / 4 + sp * lam * xi;
+            const double J22 = PI_ * ((thp + thm) * k / (16 * xi2) + (thp + thm) / (8 * k) + (thp - thm) * z / 8) -
+                               sp * lam / (4 * xi);
+            const double K11 = PI_ * (thm - thp) / 4;
+            const double K12 = PI_ * ((thp - thm) / (16 * xi2) + (thm + thp) * z / (8 * k));
+            const double ph = kk[0] * r0[0] + kk[1] * r0[1], c = cos(ph), s = sin(ph);
+            const double fI = 2 * (J00 / (4 * xi2) + J10);
+            const double fR = -2 * (J10 / (4 * xi2) + J20), fZ = -2 * (J12 / (4 * xi2) + J22);
+            const double fM = -2 * (K11 / (4 * xi2) + K12);
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) A[i][j] += 4 * c * ((i == j) * fI + fR * kk[i] * kk[j]);
+            A[2][2] += 4 * c * (fI + fZ);
+            for (int i = 0; i < 2; i++) {
+                A[i][2] -= 4 * s * fM * kk[i];
+                A[2][i] -= 4 * s * fM * kk[i];
+            }
+        }
+    const double k0 = -4 * (PI_ * z * erf(z * xi) + sp / (2 * xi) * exp(-z * z * xi2));
+    A[0][0] += k0;
+    A[1][1] += k0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) G[i][j] = A[i][j];
+}
+
+/* out += doubly periodic sum, per pair (O(ntrg nsrc)).
+ * kind 0: q (1) -> potential, gradient (4); kind 1: f (3) -> velocity (3);
+ * kind 2: (f, trD) (4) -> (pressure, velocity) (4) of stokes_pvel. */
+int oracle_ewald2d(int kind, int nsrc, const double *src, const double *val, int ntrg, const double *trg,
+                   double *out, int nthreads) {
+    if (kind < 0 || kind > 2 || nsrc < 0 || ntrg < 0) return 1;
+    const int sd = kind == 0 ? 1 : kind == 1 ? 3 : 4, td = kind == 1 ? 3 : 4;
+    nthreads = clamp_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int t = 0; t < ntrg; t++) {
+        double acc[4] = {0, 0, 0, 0};
+        for (int j = 0; j < nsrc; j++) {
+            double r[3];
+            for (int k = 0; k < 3; k++) r[k] = trg[3 * (size_t)t + k] - src[3 * (size_t)j + k];
+            r[0] -= floor(r[0] + 0.5);
+            r[1] -= floor(r[1] + 0.5);
+            const double *v = val + (size_t)sd * j;
+            if (kind == 0 || kind == 2) {
+                double pot, g[3];
+                ewald2_laplace(r, &pot, g);
+                if (kind == 0) {
+                    acc[0] += v[0] * pot / (4 * PI_);
+                    for (int k = 0; k < 3; k++) acc[1 + k] += v[0] * g[k] / (4 * PI_);
+                } else {
+                    /* p = -grad(psi) . f / 4pi, u += grad(psi) trD / 8pi */
+                    acc[0] -= (g[0] * v[0] + g[1] * v[1] + g[2] * v[2]) / (4 * PI_);
+                    for (int k = 0; k < 3; k++) acc[1 + k] += g[k] * v[3] / (8 * PI_);
+                }
+            }
+            if (kind == 1 || kind == 2) {
+                double G[3][3];
+                ewald2_stokes(r, G);
+                const int o = kind == 1 ? 0 : 1;
+                for (int a = 0; a < 3; a++)
+                    acc[o + a] += (G[a][0] * v[0] + G[a][1] * v[1] + G[a][2] * v[2]) / (8 * PI_);
+            }
+        }
+        for (int k = 0; k < td; k++) out[(size_t)td * t + k] += acc[k];
+    }
     return 0;
 }

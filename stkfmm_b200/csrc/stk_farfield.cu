@@ -22,6 +22,7 @@
 
 #include "../../include/stkfmm_b200.h"
 #include "stk_farfield.hpp"
+#include "stk_ewald.cuh"
 #include "stk_ukernels.cuh"
 #include "stk_work.hpp"
 
@@ -112,84 +113,65 @@ __global__ void kernel_matrix_kernel(const double *__restrict__ X, int ni, const
     }
 }
 
-// Far-image operator of the triply periodic unit cell: M[(i kc + a) + ld (j ke + c)]
-// = G_far(X_i - Y_j)_ac, the sum of the translation kernel over all periodic
-// images with max |s_k| >= 2 (the 3 x 3 x 3 block of images nearer than that is
-// covered by the tree's periodic lists).  G_far = G_periodic - sum_{|s| <= 1} G(r + s),
-// with G_periodic by Ewald summation as in the reference's M2C generator:
-// Laplace (M2L/Laplace/Laplace3D3D.cpp:14-84): zero-mean periodic Green's
-// function; Stokeslet (M2L/Stokeslet/Stokes3D3D.cpp:19-68): Hasimoto's sum with
-// the k = 0 mode dropped.  xi = 2 with 9^3 real images and 11^3 - 1 wave
-// vectors, as there, converges to machine precision for |r| <= sqrt(3).
-template <int UK>
+// Far-image operator of the periodic unit cell: M[(i kc + a) + ld (j ke + c)] =
+// K_far(X_i - Y_j)_ac, the sum of the translation kernel over every periodic image
+// outside the block the tree's periodic lists cover (images with |s| <= 1 on each
+// periodic axis).  K_far = (Ewald sum over all images) - (that block, summed
+// directly with the micro-kernel itself).  PBC = 3: periodic in x, y, z; PBC = 2:
+// in x and y.  The Ewald sums are those of stk_ewald.cuh; for stokes_pvel the
+// pressure row is -grad(psi).f / 4 pi and the trD column grad(psi) / 8 pi.
+template <int UK, int PBC>
 __global__ void m2c_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
                            double *__restrict__ M, int ld) {
-    constexpr double xi = 2.0, pi = 3.14159265358979323846;
-    constexpr int nreal = 4, nwave = 5;
-    const double sqpi = sqrt(pi), xi2 = xi * xi;
+    using K = Uk<UK>;
+    constexpr double pi = ewald::kPi;
     const long long total = (long long)ni * nj;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(idx % ni), j = (int)(idx / ni);
         const double r0[3] = {X[3 * i] - Y[3 * j], X[3 * i + 1] - Y[3 * j + 1], X[3 * i + 2] - Y[3 * j + 2]};
-        if (UK == UK_LAPLACE_P) {
-            double real = 0.0, wave = 0.0, nearsum = 0.0;
-            for (int a = -nreal; a <= nreal; a++)
-                for (int b = -nreal; b <= nreal; b++)
-                    for (int c = -nreal; c <= nreal; c++) {
-                        const double rx = r0[0] + a, ry = r0[1] + b, rz = r0[2] + c;
-                        const double rr = sqrt(rx * rx + ry * ry + rz * rz);
-                        const bool zero = rr < 1e-13;
-                        real += zero ? -2.0 * xi / sqpi : erfc(xi * rr) / rr;
-                        if (!zero && a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) nearsum += 1.0 / rr;
-                    }
-            for (int a = -nwave; a <= nwave; a++)
-                for (int b = -nwave; b <= nwave; b++)
-                    for (int c = -nwave; c <= nwave; c++) {
-                        if (a == 0 && b == 0 && c == 0) continue;
-                        const double kx = 2 * pi * a, ky = 2 * pi * b, kz = 2 * pi * c;
-                        const double k2 = kx * kx + ky * ky + kz * kz;
-                        wave += 4 * pi * cos(kx * r0[0] + ky * r0[1] + kz * r0[2]) * exp(-k2 / (4 * xi2)) / k2;
-                    }
-            M[(size_t)i + (size_t)ld * j] = (real + wave - pi / xi2 - nearsum) / (4 * pi);
-        } else {
-            double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            for (int a = -nreal; a <= nreal; a++)
-                for (int b = -nreal; b <= nreal; b++)
-                    for (int c = -nreal; c <= nreal; c++) {
-                        const double r[3] = {r0[0] + a, r0[1] + b, r0[2] + c};
-                        const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-                        if (rr < 1e-13) {
-                            for (int p = 0; p < 3; p++) G[p][p] += -4.0 * xi / sqpi;
-                            continue;
-                        }
-                        const double ex = exp(-xi2 * rr * rr), ec = erfc(xi * rr);
-                        const double c1 = 2 * (xi * ex / (sqpi * rr * rr) + ec / (2 * rr * rr * rr));
-                        const double c2 = 4 * xi / sqpi * ex;
-                        const bool nearimg = a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1;
-                        const double ri = 1.0 / rr, ri3 = ri * ri * ri;
-                        for (int p = 0; p < 3; p++)
-                            for (int q = 0; q < 3; q++) {
-                                const double id = p == q ? 1.0 : 0.0;
-                                G[p][q] += c1 * (rr * rr * id + r[p] * r[q]) - c2 * id;
-                                // minus the directly summed near image (Stokeslet I/r + r r^T/r^3, times 8 pi)
-                                if (nearimg) G[p][q] -= id * ri + r[p] * r[q] * ri3;
-                            }
-                    }
-            for (int a = -nwave; a <= nwave; a++)
-                for (int b = -nwave; b <= nwave; b++)
-                    for (int c = -nwave; c <= nwave; c++) {
-                        if (a == 0 && b == 0 && c == 0) continue;
-                        const double k[3] = {2 * pi * a, 2 * pi * b, 2 * pi * c};
-                        const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
-                        const double w = 8 * pi * (1 + k2 / (4 * xi2)) * exp(-k2 / (4 * xi2)) / (k2 * k2) *
-                                         cos(k[0] * r0[0] + k[1] * r0[1] + k[2] * r0[2]);
-                        for (int p = 0; p < 3; p++)
-                            for (int q = 0; q < 3; q++) G[p][q] += w * ((p == q ? k2 : 0.0) - k[p] * k[q]);
-                    }
-            for (int p = 0; p < 3; p++)
-                for (int q = 0; q < 3; q++) M[(size_t)(3 * i + p) + (size_t)ld * (3 * j + q)] = G[p][q] / (8 * pi);
+        double out[K::TDIM][K::SDIM];
+        if (UK == UK_LAPLACE_P || UK == UK_STOKES_PVEL) {
+            double pot, g[3];
+            if (PBC == 3)
+                ewald::lap3(r0, pot, g);
+            else
+                ewald::lap2(r0, pot, g);
+            if constexpr (UK == UK_LAPLACE_P) {
+                out[0][0] = pot / (4 * pi);
+            } else {
+                for (int q = 0; q < 3; q++) out[0][q] = -g[q] / (4 * pi);
+                out[0][3] = 0.0;
+                for (int p = 0; p < 3; p++) out[1 + p][3] = g[p] / (8 * pi);
+            }
         }
+        if (UK == UK_STOKES_VEL || UK == UK_STOKES_PVEL) {
+            double G[3][3];
+            if (PBC == 3)
+                ewald::stk3(r0, G);
+            else
+                ewald::stk2(r0, G);
+            constexpr int o = UK == UK_STOKES_PVEL ? 1 : 0;
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) out[o + p][q] = G[p][q] / (8 * pi);
+        }
+        // minus the directly summed block of images, with the micro-kernel's own normalisation
+        for (int a = -1; a <= 1; a++)
+            for (int b = -1; b <= 1; b++)
+                for (int c = (PBC == 3 ? -1 : 0); c <= (PBC == 3 ? 1 : 0); c++) {
+                    const double dx = r0[0] + a, dy = r0[1] + b, dz = r0[2] + c;
+                    for (int col = 0; col < K::SDIM; col++) {
+                        double f[K::SDIM], v[K::NV], u[K::TDIM];
+                        for (int q = 0; q < K::SDIM; q++) f[q] = q == col ? 1.0 : 0.0;
+                        for (int q = 0; q < K::TDIM; q++) u[q] = 0.0;
+                        K::stage(f, v);
+                        K::eval(u, dx, dy, dz, v);
+                        for (int q = 0; q < K::TDIM; q++) out[q][col] -= K::SCALE * K::comp_scale(q) * u[q];
+                    }
+                }
+        for (int p = 0; p < K::TDIM; p++)
+            for (int q = 0; q < K::SDIM; q++)
+                M[(size_t)(K::TDIM * i + p) + (size_t)ld * (K::SDIM * j + q)] = out[p][q];
     }
 }
 
@@ -620,7 +602,7 @@ int build_operators(FarField &F, cudaStream_t s) {
 
 // Triply periodic far-image operator of the root: m2c_op = DC2DE M2C (FP64),
 // mapping the root's upward equivalent density to its downward one.
-int build_periodic(FarField &F, cudaStream_t s) {
+int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     const int n = F.n, N = F.n * F.ke;
     std::vector<double> unit = unit_surface(F.p);
     // the root: centre (0.5, 0.5, 0.5), half-width 0.5; its UE and DC surfaces coincide (RAD0)
@@ -630,14 +612,24 @@ int build_periodic(FarField &F, cudaStream_t s) {
     if (!rc) rc = F.m2c_op.reserve(sizeof(double) * (size_t)N * N);
     if (rc) return rc;
     const int grid = grid_for((long long)n * n);
-    if (F.m2x == UK_LAPLACE_P)
-        m2c_kernel<UK_LAPLACE_P><<<grid, 128, 0, s>>>((const double *)X.ptr, n, (const double *)X.ptr, n,
-                                                       (double *)M2C.ptr, N);
-    else if (F.m2x == UK_STOKES_VEL)
-        m2c_kernel<UK_STOKES_VEL><<<grid, 128, 0, s>>>((const double *)X.ptr, n, (const double *)X.ptr, n,
-                                                        (double *)M2C.ptr, N);
+    const double *Xp = (const double *)X.ptr;
+    double *Mp = (double *)M2C.ptr;
+#define STK_M2C(UKV, P) m2c_kernel<UKV, P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N)
+    if (pbc == 3 && F.m2x == UK_LAPLACE_P)
+        STK_M2C(UK_LAPLACE_P, 3);
+    else if (pbc == 3 && F.m2x == UK_STOKES_VEL)
+        STK_M2C(UK_STOKES_VEL, 3);
+    else if (pbc == 3 && F.m2x == UK_STOKES_PVEL)
+        STK_M2C(UK_STOKES_PVEL, 3);
+    else if (pbc == 2 && F.m2x == UK_LAPLACE_P)
+        STK_M2C(UK_LAPLACE_P, 2);
+    else if (pbc == 2 && F.m2x == UK_STOKES_VEL)
+        STK_M2C(UK_STOKES_VEL, 2);
+    else if (pbc == 2 && F.m2x == UK_STOKES_PVEL)
+        STK_M2C(UK_STOKES_PVEL, 2);
     else
         return STK_ERR_NOT_SUPPORTED;
+#undef STK_M2C
     FCUDA(cudaGetLastError());
     const double one = 1.0, zero = 0.0;
     cublasSetStream(F.blas, s);
@@ -646,6 +638,7 @@ int build_periodic(FarField &F, cudaStream_t s) {
     FCUDA(cudaStreamSynchronize(s));
     F.m2c_p = F.p;
     F.m2c_m2x = F.m2x;
+    F.m2c_pbc = pbc;
     return STK_OK;
 }
 
@@ -699,14 +692,12 @@ FarField::~FarField() {
 
 int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     const KernelInfo *ki = kd->info;
-    // free space, or triply periodic (the far images through the root's M2C operator);
-    // PX / PXY far fields are not built
-    if (f->pbc != 0 && f->pbc != 3) return STK_ERR_NOT_SUPPORTED;
+    // free space, or periodic in x, y (and z): the far images through the root's M2C
+    // operator; singly periodic (PX) far fields are not built
+    if (f->pbc == 1) return STK_ERR_NOT_SUPPORTED;
     const int m2x = ki->slot[SLOT_M2X];
     if (m2x != UK_LAPLACE_P && m2x != UK_STOKES_VEL && m2x != UK_STOKES_PVEL) return STK_ERR_NOT_SUPPORTED;
-    // stokes_pvel mixes homogeneity degrees (PVFMM's per-component source / target
-    // scaling): p from f and u from trD fall off one power faster than u from f
-    if (m2x == UK_STOKES_PVEL && f->pbc != 0) return STK_ERR_NOT_SUPPORTED;
+
     if (!kd->far) kd->far.reset(new FarField());
     FarField &F = *kd->far;
     cudaStream_t s = f->stream;
@@ -739,9 +730,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             return rc;
         }
     }
-    F.periodic = f->pbc == 3;
-    if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x)) {
-        rc = build_periodic(F, s);
+    F.periodic = f->pbc >= 2;
+    if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x || F.m2c_pbc != f->pbc)) {
+        rc = build_periodic(F, f->pbc, s);
         if (rc) return rc;
     }
     const Octree &T = kd->tree;

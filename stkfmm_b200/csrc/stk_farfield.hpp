@@ -59,9 +59,9 @@ struct FarField {
     DevBuf m2l_vt;              // V^T: k x (n ke)
     DevBuf m2l_e;               // DC2DE U: (n ke) x k
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
-    // triply periodic: DC2DE M2C of the root (far images, max |s| >= 2)
+    // periodic (PXY, PXYZ): DC2DE M2C of the root (far images, max |s| >= 2)
     bool periodic = false;
-    int m2c_p = 0, m2c_m2x = -1;
+    int m2c_p = 0, m2c_m2x = -1, m2c_pbc = 0;
     DevBuf m2c_op;
     // per-tree data
     DevBuf unit_surf;          // n x 3 points on [-1,1]^3

@@ -104,3 +104,69 @@ def test_periodic_mixed_close_to_fp64(torch_cuda):
         fmm.evaluate_fmm(8, f, out, None)
         res.append(out)
     assert np.linalg.norm(res[1] - res[0]) / np.linalg.norm(res[0]) < 1e-6
+
+
+def periodic_fmm_pbc(kernel, pbc, p, max_pts, pts, slv):
+    import stkfmm_b200 as S
+    fmm = S.Stk3DFMM(p, max_pts, pbc, kernel)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    fmm.setup_tree(kernel)
+    out = np.zeros((len(pts), S.get_kernel_dimension(kernel)[2]))
+    fmm.evaluate_fmm(kernel, slv, out, None)
+    return out
+
+
+@pytest.mark.parametrize("dist", ["uniform", "clustered"])
+def test_doubly_periodic_stokes(torch_cuda, dist):
+    pts, rng = points(dist, 2000, 7)
+    f = rng.normal(size=(len(pts), 3))
+    f -= f.mean(0)
+    out = periodic_fmm_pbc(8, 2, 10, 50, pts, f)
+    ref = O.ewald2d(O.EWALD_STOKES, pts, f, pts)
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+
+
+def test_doubly_periodic_laplace(torch_cuda):
+    pts, rng = points("clustered", 2000, 8)
+    q = rng.uniform(-0.5, 0.5, (len(pts), 1))
+    q -= q.mean()
+    out = periodic_fmm_pbc(1, 2, 10, 50, pts, q)
+    ref = O.ewald2d(O.EWALD_LAPLACE, pts, q, pts)
+    out[:, 0] -= out[:, 0].mean()
+    ref[:, 0] -= ref[:, 0].mean()
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+
+
+@pytest.mark.parametrize("pbc", [2, 3])
+def test_periodic_pvel(torch_cuda, pbc):
+    """StokesPVel (pressure and velocity) with f and trD, neutralised as the
+    reference's periodic tests do (Test/Test.cpp:364-402).  Triply periodic
+    pressure and mean velocity are fixed only up to constants; the reference's
+    error measure reports that "drift" (mean difference per component,
+    Test/Test.cpp:143-150) apart from the error, and so does this test: PXY has
+    none, PXYZ is compared with the drift removed."""
+    pts, rng = points("clustered", 2000, 9 + pbc)
+    v = rng.normal(size=(len(pts), 4))
+    v -= v.mean(0)
+    out = periodic_fmm_pbc(128, pbc, 10, 50, pts, v)
+    ref = (O.ewald2d(O.EWALD_PVEL, pts, v, pts) if pbc == 2 else O.ewald(O.EWALD_PVEL, pts, v, pts))
+    if pbc == 3:
+        out = out - (out - ref).mean(0)
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+
+
+def test_periodic_translation(torch_cuda):
+    """Shifting every point by a vector (wrapped into the cell) gives the same
+    values, up to the per-component drift (the reference's translation check,
+    Test/Test.cpp:646-673)."""
+    pts, rng = points("uniform", 3000, 12)
+    f = rng.normal(size=(len(pts), 3))
+    f -= f.mean(0)
+    a = periodic_fmm_pbc(8, 3, 10, 50, pts, f)
+    b = periodic_fmm_pbc(8, 3, 10, 50, np.mod(pts + np.array([0.31, 0.17, 0.73]), 1.0), f)
+    d = (b - a).mean(0)
+    assert max(component_errors(b - d, a)) < TOL[10]

@@ -175,3 +175,58 @@ def test_ewald_laplace_field_matches_image_sum():
         direct = O.direct(O.UK_LAPLACE_PGRAD, imgs, np.tile(q, (len(shifts), 1)), trg)[:, 1:]
         errs.append(np.abs(direct - ew).max() / np.abs(ew).max())
     assert errs[1] < 1e-6 and errs[1] < errs[0] / 50, errs
+
+
+def _zero_moment_cell(rng, ncube=3, h=0.04):
+    """Charges / forces on the corners of small cubes with alternating signs:
+    no net charge, dipole or quadrupole, so lattice sums converge fast."""
+    import itertools
+    c = rng.random((ncube, 3)) * 0.5 + 0.25
+    sg = np.array(list(itertools.product([-1, 1], [-1, 1], [-1, 1])), dtype=np.float64)
+    src = np.concatenate([ci + h * sg for ci in c])
+    s = np.tile(sg.prod(1), ncube)[:, None]
+    return src, s
+
+
+def test_ewald_pvel_splitting_independent():
+    rng = np.random.default_rng(31)
+    src = rng.random((150, 3))
+    v = rng.normal(size=(150, 4))
+    v -= v.mean(0)
+    trg = np.concatenate([rng.random((30, 3)), src[:5]])
+    a = O.ewald(O.EWALD_PVEL, src, v, trg)
+    b = O.ewald(O.EWALD_PVEL, src, v, trg, xi=2.0, nreal=4, nwave=5)
+    assert np.abs(a - b).max() < 1e-13 * np.abs(a).max()
+
+
+def test_ewald_pvel_pressure_matches_image_sum():
+    rng = np.random.default_rng(32)
+    src, s = _zero_moment_cell(rng)
+    pv = np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)
+    trg = rng.random((5, 3))
+    ew = O.ewald(O.EWALD_PVEL, src, pv, trg)
+    r = np.arange(-8, 9)
+    sh = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    imgs = (src[None] + sh[:, None]).reshape(-1, 3)
+    d = O.direct(O.UK_STOKES_PVEL, imgs, np.tile(pv, (len(sh), 1)), trg)
+    assert np.abs(d[:, 0] - ew[:, 0]).max() < 1e-6 * np.abs(ew[:, 0]).max()
+    assert np.abs(d[:, 1:] - ew[:, 1:]).max() < 1e-4 * np.abs(ew[:, 1:]).max()
+
+
+@pytest.mark.parametrize("kind", [O.EWALD_LAPLACE, O.EWALD_STOKES, O.EWALD_PVEL])
+def test_ewald2d_matches_image_sums(kind):
+    """Doubly periodic sums against sums over growing squares of images (x, y)."""
+    rng = np.random.default_rng(33 + kind)
+    src, s = _zero_moment_cell(rng)
+    val = {O.EWALD_LAPLACE: s, O.EWALD_STOKES: s * np.array([[0.3, -0.2, 0.5]]),
+           O.EWALD_PVEL: np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)}[kind]
+    uk = {O.EWALD_LAPLACE: O.UK_LAPLACE_PGRAD, O.EWALD_STOKES: O.UK_STOKES_VEL, O.EWALD_PVEL: O.UK_STOKES_PVEL}[kind]
+    trg = rng.random((5, 3))
+    ew = O.ewald2d(kind, src, val, trg)
+    # periodic in x and y
+    assert np.abs(O.ewald2d(kind, src, val, trg + np.array([2.0, -1.0, 0.0])) - ew).max() < 1e-13 * np.abs(ew).max()
+    r = np.arange(-32, 33)
+    sh = np.stack(np.meshgrid(r, r, [0], indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    imgs = (src[None] + sh[:, None]).reshape(-1, 3)
+    d = O.direct(uk, imgs, np.tile(val, (len(sh), 1)), trg)
+    assert np.abs(d - ew).max() < 1e-6 * np.abs(ew).max()
