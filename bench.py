@@ -152,47 +152,73 @@ EXTRA_FMM = [
     {"name": "rpy_pxyz_2m_uniform", "kernel": 16, "pbc": 3, "p": 8, "max_pts": 256, "n": 2097152,
      "workload": "RPY triply periodic (PXYZ) FMM: 2,097,152 points ~ U[0,1)^3, f ~ N(0,1)^3 minus its mean, "
                  "b ~ U(1e-4,5e-4), p=8, max 256 pts/leaf, seed 0"},
+    {"name": "pvel_pxy_4m_spheres", "kernel": 128, "pbc": 2, "p": 12, "max_pts": 512, "n": 4194304,
+     "workload": "StokesPVel doubly periodic (PXY) FMM, single and double layer: 4,194,304 points on the surfaces "
+                 "of 4,096 spheres (radius 0.01, centres ~ U([0.05,0.95]^2 x [0.05,0.5])), f ~ N(0,1)^3 with "
+                 "trD = 0 and the mean of (f, trD) removed, D ~ N(0,1)^9 with its mean trace removed, p=12, "
+                 "max 512 pts/leaf, seed 0"},
 ]
 
 
 def extra_fmm_inputs(cfg, seed):
+    """Points, SL values and DL values (or None) of a further workload."""
     rng = np.random.default_rng(seed)
     n = cfg["n"]
+    if cfg["kernel"] == 128:
+        # points on sphere surfaces; SL (f, trD = 0) and DL D neutralised as Test/Test.cpp:364-402
+        nsph, per = 4096, n // 4096
+        centres = np.concatenate([rng.uniform(0.05, 0.95, (nsph, 2)), rng.uniform(0.05, 0.5, (nsph, 1))], axis=1)
+        u = rng.normal(size=(nsph, per, 3))
+        u /= np.linalg.norm(u, axis=2, keepdims=True)
+        pts = (centres[:, None, :] + 0.01 * u).reshape(-1, 3)
+        f = np.concatenate([rng.normal(size=(n, 3)), np.zeros((n, 1))], axis=1)
+        f -= f.mean(0)
+        d = rng.normal(size=(n, 9))
+        tr = (d[:, 0] + d[:, 4] + d[:, 8]).mean() / 3
+        d[:, [0, 4, 8]] -= tr
+        return pts, f, d
     pts = rng.random((n, 3))
     f = rng.normal(size=(n, 3))
     if cfg["pbc"]:
         f -= f.mean(0)  # net force removed for the periodic sum (Test/Test.cpp:332-351)
     if cfg["kernel"] == 16:
         f = np.concatenate([f, rng.uniform(1e-4, 5e-4, (n, 1))], axis=1)
-    return pts, f
+    return pts, f, None
 
 
 def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
     """evaluate_fmm_device of one further workload, FP64 and mixed, CUDA events per evaluation."""
     import torch
     import stkfmm_b200 as S
-    pts, slv = extra_fmm_inputs(cfg, seed)
+    pts, slv, dlv = extra_fmm_inputs(cfg, seed)
     K = cfg["kernel"]
     td = S.get_kernel_dimension(K)[2]
     fmm = S.Stk3DFMM(cfg["p"], cfg["max_pts"], cfg["pbc"], K)
     fmm.set_box(np.zeros(3), 1.0)
-    fmm.set_points(pts, pts, None)
+    fmm.set_points(pts, pts, pts if dlv is not None else None)
+    t0 = time.perf_counter()
     fmm.setup_tree(K)
+    tree_s = time.perf_counter() - t0
     d_sl = torch.as_tensor(slv).cuda()
-    res = {"workload": cfg["workload"], "tree": fmm.tree_stats(K)}
+    d_dl = torch.as_tensor(dlv).cuda() if dlv is not None else None
+    dlp = d_dl.data_ptr() if d_dl is not None else 0
+    res = {"workload": cfg["workload"], "tree": fmm.tree_stats(K), "setup_tree_s": tree_s}
     outs = {}
     for prec, nm in ((S.PRECISION.FP64, "fp64"), (S.PRECISION.MIXED, "mixed")):
         fmm.set_precision(prec)
         out = torch.zeros((len(pts), td), dtype=torch.float64, device="cuda")
+        t0 = time.perf_counter()
         for _ in range(warmup):
-            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), 0, None)
+            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), dlp, None)
         torch.cuda.synchronize()
+        if nm == "fp64":
+            res["first_evaluations_s"] = time.perf_counter() - t0  # includes the far-field operator build
         ms, phases = [], []
         for _ in range(steps):
             flush.zero_()
             out.zero_()
             torch.cuda.synchronize()
-            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), 0, None)
+            fmm.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), dlp, None)
             torch.cuda.synchronize()
             ms.append(fmm.last_kernel_ms(K))
             phases.append(fmm.last_phase_ms(K))
@@ -496,7 +522,8 @@ def b200_arm(args):
     # ---- the further FMM workloads (configs 1 and 3): every rank runs its own replica ----
     extra = []
     for cfg in EXTRA_FMM:
-        r, epts, eslv, eouts = time_extra_fmm(cfg, rank, args.steps, args.warmup, ws, flush)
+        # a few timed evaluations each (the largest takes about a second per evaluation)
+        r, epts, eslv, eouts = time_extra_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)
         extra.append((cfg, r, epts, eslv, eouts))
 
     if rank != 0:
