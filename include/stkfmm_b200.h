@@ -184,9 +184,10 @@ int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:26 (not declared in the reference header) */
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
- * KIFMM far field.  The far field is built for free space (pbc = 0) and for the
- * kernels whose translations use laplace_p or stokes_vel (LapPGrad, Stokes, RPY,
- * StokesRegVel); other cases return STK_ERR_NOT_SUPPORTED. */
+ * KIFMM far field, for LapPGrad, Stokes, RPY, StokesRegVel and PVel in free
+ * space, PXY and PXYZ; PX and the other kernels return STK_ERR_NOT_SUPPORTED.
+ * Triply periodic potentials / pressures / mean velocities carry a constant
+ * per component (drift) set by the equivalent density, as in the reference. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
                           double *trg_value, const int nDL, double *src_DL_value);
 /* Stk3DFMM-c.cpp:33-35 */
