@@ -185,7 +185,7 @@ int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
  * KIFMM far field, for LapPGrad, Stokes, RPY, StokesRegVel and PVel in free
- * space, PXY and PXYZ; PX and the other kernels return STK_ERR_NOT_SUPPORTED.
+ * space, PX, PXY and PXYZ; the other kernels return STK_ERR_NOT_SUPPORTED.
  * Triply periodic potentials / pressures / mean velocities carry a constant
  * per component (drift) set by the equivalent density, as in the reference. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,

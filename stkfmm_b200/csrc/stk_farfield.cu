@@ -113,6 +113,45 @@ __global__ void kernel_matrix_kernel(const double *__restrict__ X, int ni, const
     }
 }
 
+// Singly periodic (PX) far images: the images t = 2 .. kPxImages on both sides
+// along x, summed directly with the micro-kernel, as the reference's generator
+// does (M2L/Laplace/Laplace1D3D.cpp:18-28, SUM1D = 500000 in
+// M2L/SVD_pvfmm.hpp:35).  The sum runs from the farthest images inwards with
+// compensation; for a neutral (and force-free) root density the images' tail
+// decays like a dipole lattice, so the cut-off costs ~1e-6 / kPxImages.
+constexpr int kPxImages = 500000;
+
+template <int UK>
+__global__ void m2c_px_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
+                              double *__restrict__ M, int ld) {
+    using K = Uk<UK>;
+    const long long total = (long long)ni * nj;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % ni), j = (int)(idx / ni);
+        const double r0[3] = {X[3 * i] - Y[3 * j], X[3 * i + 1] - Y[3 * j + 1], X[3 * i + 2] - Y[3 * j + 2]};
+        for (int col = 0; col < K::SDIM; col++) {
+            double f[K::SDIM], v[K::NV], sum[K::TDIM], cmp[K::TDIM];
+            for (int q = 0; q < K::SDIM; q++) f[q] = q == col ? 1.0 : 0.0;
+            for (int q = 0; q < K::TDIM; q++) sum[q] = cmp[q] = 0.0;
+            K::stage(f, v);
+            for (int t = kPxImages; t >= 2; t--) {
+                double u[K::TDIM];
+                for (int q = 0; q < K::TDIM; q++) u[q] = 0.0;
+                K::eval(u, r0[0] + t, r0[1], r0[2], v);
+                K::eval(u, r0[0] - t, r0[1], r0[2], v);
+                for (int q = 0; q < K::TDIM; q++) {
+                    const double y = u[q] - cmp[q], s2 = sum[q] + y;
+                    cmp[q] = (s2 - sum[q]) - y;
+                    sum[q] = s2;
+                }
+            }
+            for (int q = 0; q < K::TDIM; q++)
+                M[(size_t)(K::TDIM * i + q) + (size_t)ld * (K::SDIM * j + col)] = K::SCALE * K::comp_scale(q) * sum[q];
+        }
+    }
+}
+
 // Far-image operator of the periodic unit cell: M[(i kc + a) + ld (j ke + c)] =
 // K_far(X_i - Y_j)_ac, the sum of the translation kernel over every periodic image
 // outside the block the tree's periodic lists cover (images with |s| <= 1 on each
@@ -627,6 +666,12 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
         STK_M2C(UK_STOKES_VEL, 2);
     else if (pbc == 2 && F.m2x == UK_STOKES_PVEL)
         STK_M2C(UK_STOKES_PVEL, 2);
+    else if (pbc == 1 && F.m2x == UK_LAPLACE_P)
+        m2c_px_kernel<UK_LAPLACE_P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N);
+    else if (pbc == 1 && F.m2x == UK_STOKES_VEL)
+        m2c_px_kernel<UK_STOKES_VEL><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N);
+    else if (pbc == 1 && F.m2x == UK_STOKES_PVEL)
+        m2c_px_kernel<UK_STOKES_PVEL><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N);
     else
         return STK_ERR_NOT_SUPPORTED;
 #undef STK_M2C
@@ -692,9 +737,8 @@ FarField::~FarField() {
 
 int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     const KernelInfo *ki = kd->info;
-    // free space, or periodic in x, y (and z): the far images through the root's M2C
-    // operator; singly periodic (PX) far fields are not built
-    if (f->pbc == 1) return STK_ERR_NOT_SUPPORTED;
+    // free space, or periodic in x (PX), x and y (PXY) or all axes (PXYZ): the far
+    // images through the root's M2C operator
     const int m2x = ki->slot[SLOT_M2X];
     if (m2x != UK_LAPLACE_P && m2x != UK_STOKES_VEL && m2x != UK_STOKES_PVEL) return STK_ERR_NOT_SUPPORTED;
 
@@ -730,7 +774,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             return rc;
         }
     }
-    F.periodic = f->pbc >= 2;
+    F.periodic = f->pbc >= 1;
     if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x || F.m2c_pbc != f->pbc)) {
         rc = build_periodic(F, f->pbc, s);
         if (rc) return rc;

@@ -144,12 +144,6 @@ def test_fmm_separate_targets(torch_cuda):
 def test_fmm_not_supported_cases(torch_cuda):
     import stkfmm_b200 as S
     pts = np.random.default_rng(0).random((500, 3))
-    per = S.Stk3DFMM(8, 50, 1, 8)  # singly periodic (PX) far field: not built
-    per.set_box(np.zeros(3), 1.0)
-    per.set_points(pts, pts, None)
-    per.setup_tree(8)
-    with pytest.raises(S.StkError):
-        per.evaluate_fmm(8, np.zeros((500, 3)), np.zeros((500, 3)), None)
     lg = S.Stk3DFMM(8, 50, 0, 2)  # LapPGradGrad: kernel not built
     lg.set_box(np.zeros(3), 1.0)
     lg.set_points(pts, pts, pts)

@@ -170,3 +170,34 @@ def test_periodic_translation(torch_cuda):
     b = periodic_fmm_pbc(8, 3, 10, 50, np.mod(pts + np.array([0.31, 0.17, 0.73]), 1.0), f)
     d = (b - a).mean(0)
     assert max(component_errors(b - d, a)) < TOL[10]
+
+
+@pytest.mark.parametrize("kernel", [1, 8, 128])
+def test_singly_periodic_against_image_sum(torch_cuda, kernel):
+    """PX: sources without net charge / force, dipole or quadrupole (alternating
+    signs on the corners of small cubes) against the direct sum over their
+    images |t| <= 3000 along x (the tail beyond is far below the bar)."""
+    import itertools
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(40 + kernel)
+    c = rng.random((16, 3)) * 0.8 + 0.1
+    sg = np.array(list(itertools.product([-1, 1], [-1, 1], [-1, 1])), dtype=np.float64)
+    src = np.concatenate([ci + 0.03 * sg for ci in c])
+    s = np.tile(sg.prod(1), 16)[:, None]
+    val = {1: s, 8: s * np.array([[0.3, -0.2, 0.5]]),
+           128: np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)}[kernel]
+    trg = rng.random((1500, 3)) * 0.999
+    fmm = S.Stk3DFMM(10, 32, S.PAXIS.PX, kernel)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(src, trg, None)
+    fmm.setup_tree(kernel)
+    out = np.zeros((len(trg), S.get_kernel_dimension(kernel)[2]))
+    fmm.evaluate_fmm(kernel, val, out, None)
+    T = 3000
+    sh = np.zeros((2 * T + 1, 3))
+    sh[:, 0] = np.arange(-T, T + 1)
+    imgs = (src[None] + sh[:, None]).reshape(-1, 3)
+    uk = S.kernel_slot(kernel, 0)
+    ref = O.direct(uk, imgs, np.tile(val, (len(sh), 1)), trg)
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
