@@ -19,6 +19,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
 
 #include "../../include/stkfmm_b200.h"
 #include "stk_farfield.hpp"
@@ -325,48 +327,9 @@ __global__ void upper_copy_kernel(const double *__restrict__ A, long long m, int
     }
 }
 
-// Optional tensor-core M2L for the mixed path (STK_M2L_TF32_TERMS = 3, 4 or 6;
-// 0 = off, the default): each operand is split into kTf32Pieces TF32 values
-// (cvt.rna.tf32.f32, 10 explicit mantissa bits each) a = a0 + a1 (+ a2), and the
-// product is the sum of the TF32 products listed in kTf32Terms (piece of C_d,
-// piece of the sources), smallest first, accumulated by the tensor cores.
-// Measured on B200: 2-3x faster than the FP32 SIMT GEMM, but the FMM's
-// mixed-vs-FP64 error rises from 4.5e-7 to 1.4e-6 (StokesVel, 32k points, p = 8)
-// and the LapPGrad potential's from 1.5e-7 to 2.4e-6, independent of the number
-// of pieces, so the limit is the tensor cores' FP32 accumulation over k = 240-716
-// terms, not the operand split.
-#ifndef STK_M2L_TF32_TERMS
-#define STK_M2L_TF32_TERMS 0
-#endif
-#if STK_M2L_TF32_TERMS == 3
-constexpr int kTf32Pieces = 2, kTf32Terms = 3;
-constexpr int kTf32Term[3][2] = {{1, 0}, {0, 1}, {0, 0}};
-#elif STK_M2L_TF32_TERMS == 4
-constexpr int kTf32Pieces = 2, kTf32Terms = 4;
-constexpr int kTf32Term[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};
-#elif STK_M2L_TF32_TERMS == 6
-constexpr int kTf32Pieces = 3, kTf32Terms = 6;
-constexpr int kTf32Term[6][2] = {{2, 0}, {0, 2}, {1, 1}, {1, 0}, {0, 1}, {0, 0}};
-#else
-constexpr int kTf32Pieces = 1, kTf32Terms = 1;  // one FP32 piece: the FP32 SIMT GEMM
-constexpr int kTf32Term[1][2] = {{0, 0}};
-#endif
-constexpr bool kM2LTensor = STK_M2L_TF32_TERMS != 0;
-
-__device__ __forceinline__ float tf32_rna(float x) {
-    unsigned int u;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-    return __uint_as_float(u);
-}
-
-// piece p of a (p < kTf32Pieces): a0 = tf32(a), a1 = tf32(a - a0), a2 = a - a0 - a1
-__device__ __forceinline__ void split_tf32(double a, float *out, size_t stride) {
-    double r = a;
-    for (int p = 0; p < kTf32Pieces; p++) {
-        const float v = p + 1 < kTf32Pieces ? tf32_rna((float)r) : (float)r;
-        out[p * stride] = v;
-        r -= (double)v;
-    }
+__global__ void to_float_kernel(const double *__restrict__ a, long long n, float *__restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
 }
 
 constexpr int kM2LChunk = 256;  // pairs (columns) per batched-GEMM problem of the M2L
@@ -382,19 +345,6 @@ __global__ void m2l_gather_kernel(const double *__restrict__ phi_hat, const int 
         const int r = (int)(idx - j * k);
         const int a = gsrc[j];
         X[idx] = a >= 0 ? (T)phi_hat[(size_t)a * k + r] : (T)0;
-    }
-}
-
-// the same gather, split into TF32 pieces (piece p at X + p * k * ncol)
-__global__ void m2l_gather_split_kernel(const double *__restrict__ phi_hat, const int *__restrict__ gsrc, int k,
-                                        long long ncol, float *__restrict__ X) {
-    const long long total = ncol * k;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const long long j = idx / k;
-        const int r = (int)(idx - j * k);
-        const int a = gsrc[j];
-        split_tf32(a >= 0 ? phi_hat[(size_t)a * k + r] : 0.0, X + idx, (size_t)total);
     }
 }
 
@@ -415,11 +365,6 @@ __global__ void m2l_reduce_kernel(const T *__restrict__ Y, const int *__restrict
         for (int e = e0; e < e1; e++) acc += (double)Y[(size_t)((long long)col[e] - c0) * k + r];
         psi_hat[idx] += acc;
     }
-}
-
-__global__ void split_tf32_kernel(const double *__restrict__ a, long long n, float *__restrict__ out) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        split_tf32(a[i], out + i, (size_t)n);
 }
 
 // A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
@@ -498,6 +443,214 @@ std::vector<double> scaled_surface(const std::vector<double> &unit, double cx, d
         o[i + 2] = cz + r * unit[i + 2];
     }
     return o;
+}
+
+// ---- two-level M2L: per-offset low-rank factors ----------------------------------
+//
+// In the shared bases, C_d = U^T A_d V (k x k) has a much lower numerical rank
+// for each single offset d than k (e.g. stokes_vel at p = 8: k = 716, r_d ~ 100 -
+// 280).  C_d ~ P_d Q_d^T (k x r_d each) turns a pair's 2 k^2 flops into 4 k r_d.
+// The surface points and the kernels are symmetric under the 48 signed axis
+// permutations G of the cube, A_{G d} = T_out(G) A_d T_in(G)^T (T: the point
+// permutation with the components rotated), so only the 16 offsets with
+// |dx| >= |dy| >= |dz| >= 0 need an SVD; the others get P, Q from the mapped
+// N-space factors: P_{G d} = U^T T_out L_d, Q_{G d} = V^T T_in R_d.
+
+struct SignedPerm {
+    int perm[3], sign[3];  // (G x)_a = sign[a] x[perm[a]]
+};
+
+// y[pi(i)] = G_comp x[i] for each of r columns (point-major, dim components per point);
+// vector components start at vec0 (3 of them) when vec0 >= 0, the others are scalars
+__global__ void sym_apply_kernel(const double *__restrict__ x, double *__restrict__ y, int n, int dim, int r,
+                                 const int *__restrict__ pi, SignedPerm g, int vec0) {
+    const long long total = (long long)n * r;
+    const long long N = (long long)n * dim;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n);
+        const long long c = idx / n;
+        const double *xi = x + c * N + (long long)i * dim;
+        double *yo = y + c * N + (long long)pi[i] * dim;
+        for (int a = 0; a < dim; a++) {
+            const bool vec = vec0 >= 0 && a >= vec0 && a < vec0 + 3;
+            yo[a] = vec ? g.sign[a - vec0] * xi[vec0 + g.perm[a - vec0]] : xi[a];
+        }
+    }
+}
+
+int build_m2l_lowrank(FarField &F, const std::vector<double> &unit, const double *Ut, const double *Vt,
+                      const std::function<int(int, double *, int)> &offset_matrix, DevBuf &K, DevBuf &T,
+                      cudaStream_t s) {
+    const int n = F.n, N = F.n * F.ke, k = F.m2l_rank;
+    const double one = 1.0, zero = 0.0;
+    cublasSetStream(F.blas, s);
+    // component layout of the equivalent densities (in) and check potentials (out)
+    const int vec_in = F.m2x == UK_LAPLACE_P ? -1 : 0;
+    const int vec_out = F.m2x == UK_LAPLACE_P ? -1 : F.m2x == UK_STOKES_PVEL ? 1 : 0;
+    // representative and symmetry of every well-separated offset
+    struct Rep {
+        int rep;  // index of the representative offset
+        SignedPerm g;
+    };
+    std::vector<int> rep_code;            // representative offsets (codes)
+    std::vector<Rep> of(kNumOffsets, {-1, {{0, 1, 2}, {1, 1, 1}}});
+    for (int code = 0; code < kNumOffsets; code++) {
+        if (F.m2l_slot[code] < 0) continue;
+        const int d[3] = {code % 7 - 3, (code / 7) % 7 - 3, code / 49 - 3};
+        int o[3] = {0, 1, 2};
+        std::stable_sort(o, o + 3, [&](int a, int b) { return std::abs(d[a]) > std::abs(d[b]); });
+        const int d0[3] = {std::abs(d[o[0]]), std::abs(d[o[1]]), std::abs(d[o[2]])};
+        const int rcode = (d0[0] + 3) + 7 * (d0[1] + 3) + 49 * (d0[2] + 3);
+        SignedPerm g;
+        for (int t = 0; t < 3; t++) {
+            g.perm[o[t]] = t;
+            g.sign[o[t]] = d[o[t]] < 0 ? -1 : 1;
+        }
+        int ri = (int)(std::find(rep_code.begin(), rep_code.end(), rcode) - rep_code.begin());
+        if (ri == (int)rep_code.size()) rep_code.push_back(rcode);
+        of[code] = {ri, g};
+    }
+    const int nrep = (int)rep_code.size();
+    // SVD of C_d0 = U^T A_d0 V for each representative
+    int lw = 0;
+    if (cusolverDnDgesvd_bufferSize(F.solver, k, k, &lw) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    DevBuf C, W, Zt, Sg, work, info, rwork;
+    int rc = C.reserve(sizeof(double) * (size_t)k * k);
+    if (!rc) rc = W.reserve(sizeof(double) * (size_t)nrep * k * k);
+    if (!rc) rc = Zt.reserve(sizeof(double) * (size_t)nrep * k * k);
+    if (!rc) rc = Sg.reserve(sizeof(double) * (size_t)nrep * k);
+    if (!rc) rc = work.reserve(sizeof(double) * (size_t)std::max(lw, 1));
+    if (!rc) rc = info.reserve(sizeof(int) * nrep);
+    if (!rc) rc = rwork.reserve(sizeof(double) * k);
+    if (rc) return rc;
+    cusolverDnSetStream(F.solver, s);
+    for (int ri = 0; ri < nrep; ri++) {
+        if ((rc = offset_matrix(rep_code[ri], (double *)K.ptr, N))) return rc;
+        // T = A V (N x k), C = U^T T (k x k)
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_T, N, k, N, &one, (const double *)K.ptr, N, Vt, N, &zero,
+                          (double *)T.ptr, N));
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, k, N, &one, Ut, N, (const double *)T.ptr, N, &zero,
+                          (double *)C.ptr, k));
+        if (cusolverDnDgesvd(F.solver, 'A', 'A', k, k, (double *)C.ptr, k, (double *)Sg.ptr + (size_t)ri * k,
+                             (double *)W.ptr + (size_t)ri * k * k, k, (double *)Zt.ptr + (size_t)ri * k * k, k,
+                             (double *)work.ptr, lw, (double *)rwork.ptr, (int *)info.ptr + ri) !=
+            CUSOLVER_STATUS_SUCCESS)
+            return STK_ERR_CUDA;
+    }
+    std::vector<double> sg((size_t)nrep * k);
+    std::vector<int> hinfo(nrep);
+    FCUDA(cudaMemcpyAsync(sg.data(), Sg.ptr, sizeof(double) * sg.size(), cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaMemcpyAsync(hinfo.data(), info.ptr, sizeof(int) * nrep, cudaMemcpyDeviceToHost, s));
+    FCUDA(cudaStreamSynchronize(s));
+    for (int v : hinfo)
+        if (v != 0) return STK_ERR_CUDA;
+    double smax = 0.0;
+    for (int ri = 0; ri < nrep; ri++) smax = std::max(smax, sg[(size_t)ri * k]);
+    // ranks at a tenth of the shared bases' cut, relative to the largest C_d
+    std::vector<int> rrank(nrep, 1);
+    for (int ri = 0; ri < nrep; ri++)
+        for (int i = 0; i < k; i++)
+            if (sg[(size_t)ri * k + i] > 0.1 * F.m2l_rtol * smax) rrank[ri] = i + 1;
+    int rmaxr = 1;
+    for (int r : rrank) rmaxr = std::max(rmaxr, r);
+    // N-space factors of the representatives: L = U W_r S_r, R = V Z_r (N x r each)
+    DevBuf Lrep, Rrep, Ws;
+    size_t nspace = 0;
+    std::vector<size_t> roff(nrep);
+    for (int ri = 0; ri < nrep; ri++) {
+        roff[ri] = nspace;
+        nspace += (size_t)N * rrank[ri];
+    }
+    rc = Lrep.reserve(sizeof(double) * nspace);
+    if (!rc) rc = Rrep.reserve(sizeof(double) * nspace);
+    if (!rc) rc = Ws.reserve(sizeof(double) * (size_t)k * rmaxr);
+    if (rc) return rc;
+    for (int ri = 0; ri < nrep; ri++) {
+        const int r = rrank[ri];
+        // Ws = W_r S_r (k x r)
+        FCUDA(cudaMemcpyAsync(Ws.ptr, (const double *)W.ptr + (size_t)ri * k * k, sizeof(double) * (size_t)k * r,
+                              cudaMemcpyDeviceToDevice, s));
+        FBLAS(cublasDdgmm(F.blas, CUBLAS_SIDE_RIGHT, k, r, (const double *)Ws.ptr, k,
+                          (const double *)Sg.ptr + (size_t)ri * k, 1, (double *)Ws.ptr, k));
+        // L = U Ws: U = (rows 0..k-1 of Ut)^T
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, N, r, k, &one, Ut, N, (const double *)Ws.ptr, k, &zero,
+                          (double *)Lrep.ptr + roff[ri], N));
+        // R = V Z_r, Z_r = (rows 0..r-1 of Zt)^T
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_T, CUBLAS_OP_T, N, r, k, &one, Vt, N,
+                          (const double *)Zt.ptr + (size_t)ri * k * k, k, &zero, (double *)Rrep.ptr + roff[ri], N));
+    }
+    // surface point permutations of the symmetries in use
+    std::map<long long, int> where;
+    auto key = [&](double x, double y, double z) {
+        const long long a = std::llround(x * (F.p - 1)) + 64, b = std::llround(y * (F.p - 1)) + 64,
+                        c = std::llround(z * (F.p - 1)) + 64;
+        return (a * 256 + b) * 256 + c;
+    };
+    for (int i = 0; i < n; i++) where[key(unit[3 * i], unit[3 * i + 1], unit[3 * i + 2])] = i;
+    // per offset: P = U^T T_out L_rep, Q = V^T T_in R_rep
+    size_t total = 0;
+    int nslot = 0;
+    for (int code = 0; code < kNumOffsets; code++)
+        if (F.m2l_slot[code] >= 0) nslot++;
+    F.m2l_r.assign(nslot, 0);
+    F.m2l_pq_off.assign(nslot, 0);
+    for (int code = 0; code < kNumOffsets; code++) {
+        const int sl = F.m2l_slot[code];
+        if (sl < 0) continue;
+        // ranks padded to a multiple of 32 (zero columns), so that offsets of similar
+        // rank share one uniformly sized batched GEMM
+        F.m2l_r[sl] = std::min(k, (rrank[of[code].rep] + 31) / 32 * 32);
+        F.m2l_pq_off[sl] = total;
+        total += (size_t)k * F.m2l_r[sl];
+    }
+    F.m2l_rmax = 1;
+    for (int r : F.m2l_r) F.m2l_rmax = std::max(F.m2l_rmax, r);
+    rc = F.m2l_p.reserve(sizeof(double) * std::max<size_t>(total, 1));
+    if (!rc) rc = F.m2l_q.reserve(sizeof(double) * std::max<size_t>(total, 1));
+    if (!rc) rc = F.m2l_p32.reserve(sizeof(float) * std::max<size_t>(total, 1));
+    if (!rc) rc = F.m2l_q32.reserve(sizeof(float) * std::max<size_t>(total, 1));
+    DevBuf Tm, pi;
+    if (!rc) rc = Tm.reserve(sizeof(double) * (size_t)N * rmaxr);
+    if (rc) return rc;
+    FCUDA(cudaMemsetAsync(F.m2l_p.ptr, 0, sizeof(double) * total, s));
+    FCUDA(cudaMemsetAsync(F.m2l_q.ptr, 0, sizeof(double) * total, s));
+    std::vector<int> hpi(n);
+    for (int code = 0; code < kNumOffsets; code++) {
+        const int sl = F.m2l_slot[code];
+        if (sl < 0) continue;
+        const int ri = of[code].rep, r = rrank[ri];
+        const SignedPerm g = of[code].g;
+        for (int i = 0; i < n; i++) {
+            double x[3] = {unit[3 * i], unit[3 * i + 1], unit[3 * i + 2]}, gx[3];
+            for (int a = 0; a < 3; a++) gx[a] = g.sign[a] * x[g.perm[a]];
+            auto it = where.find(key(gx[0], gx[1], gx[2]));
+            if (it == where.end()) return STK_ERR_STATE;  // the surface is symmetric by construction
+            hpi[i] = it->second;
+        }
+        rc = pi.upload(hpi.data(), sizeof(int) * n, s);
+        if (rc) return rc;
+        const int gr = grid_for((long long)n * r);
+        double *P = (double *)F.m2l_p.ptr + F.m2l_pq_off[sl], *Q = (double *)F.m2l_q.ptr + F.m2l_pq_off[sl];
+        sym_apply_kernel<<<gr, 256, 0, s>>>((const double *)Lrep.ptr + roff[ri], (double *)Tm.ptr, n, F.kc, r,
+                                            (const int *)pi.ptr, g, vec_out);
+        FCUDA(cudaGetLastError());
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, r, N, &one, Ut, N, (const double *)Tm.ptr, N, &zero, P,
+                          k));
+        sym_apply_kernel<<<gr, 256, 0, s>>>((const double *)Rrep.ptr + roff[ri], (double *)Tm.ptr, n, F.ke, r,
+                                            (const int *)pi.ptr, g, vec_in);
+        FCUDA(cudaGetLastError());
+        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, r, N, &one, Vt, N, (const double *)Tm.ptr, N, &zero, Q,
+                          k));
+        // pi and Tm are reused by the next offset: keep the stream order (no host wait needed)
+    }
+    to_float_kernel<<<grid_for((long long)total), 256, 0, s>>>((const double *)F.m2l_p.ptr, (long long)total,
+                                                              (float *)F.m2l_p32.ptr);
+    to_float_kernel<<<grid_for((long long)total), 256, 0, s>>>((const double *)F.m2l_q.ptr, (long long)total,
+                                                              (float *)F.m2l_q32.ptr);
+    FCUDA(cudaGetLastError());
+    FCUDA(cudaStreamSynchronize(s));
+    return STK_OK;
 }
 
 // Build the level-independent operators for (m2x, p).
@@ -610,8 +763,7 @@ int build_operators(FarField &F, cudaStream_t s) {
     for (int i = 0; i < N; i++)
         if (sv[i] > F.m2l_rtol * sv[0] || su[i] > F.m2l_rtol * su[0]) k = std::max(k, i + 1);
     F.m2l_rank = k;
-    rc = F.m2l_c.reserve(sizeof(double) * (size_t)nslot * k * k);
-    if (!rc) rc = F.m2l_vt.reserve(sizeof(double) * (size_t)k * N);
+    rc = F.m2l_vt.reserve(sizeof(double) * (size_t)k * N);
     if (!rc) rc = F.m2l_e.reserve(sizeof(double) * (size_t)N * k);
     if (rc) return rc;
     // V^T: the first k rows of VTv;  E = DC2DE U,  U^T = the first k rows of VTu
@@ -619,22 +771,8 @@ int build_operators(FarField &F, cudaStream_t s) {
                       (const double *)VTv.ptr, N, (double *)F.m2l_vt.ptr, k));
     FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_T, N, k, N, &one, (const double *)F.dc2de.ptr, N,
                       (const double *)VTu.ptr, N, &zero, (double *)F.m2l_e.ptr, N));
-    for (int code = 0; code < kNumOffsets; code++) {
-        const int sl = F.m2l_slot[code];
-        if (sl < 0) continue;
-        if ((rc = offset_matrix(code, (double *)K.ptr, N))) return rc;
-        // T = A_d V (N x k), C_d = U^T T (k x k)
-        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_T, N, k, N, &one, (const double *)K.ptr, N,
-                          (const double *)VTv.ptr, N, &zero, (double *)T.ptr, N));
-        FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, k, N, &one, (const double *)VTu.ptr, N,
-                          (const double *)T.ptr, N, &zero, (double *)F.m2l_c.ptr + (size_t)sl * k * k, k));
-    }
-    // TF32 pieces for the mixed path's tensor-core M2L (C_d holds no pseudo-inverse)
-    rc = F.m2l_c32.reserve(kTf32Pieces * sizeof(float) * (size_t)nslot * k * k);
+    rc = build_m2l_lowrank(F, unit, (const double *)VTu.ptr, (const double *)VTv.ptr, offset_matrix, K, T, s);
     if (rc) return rc;
-    split_tf32_kernel<<<grid_for((long long)nslot * k * k), 256, 0, s>>>(
-        (const double *)F.m2l_c.ptr, (long long)nslot * k * k, (float *)F.m2l_c32.ptr);
-    FCUDA(cudaGetLastError());
     FCUDA(cudaStreamSynchronize(s));
     return STK_OK;
 }
@@ -1043,33 +1181,56 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
         rc = F.d_m2l_gstart.upload(gstart.data(), sizeof(int) * gstart.size(), s);
         if (rc) return rc;
-        rc = F.m2l_x.reserve(std::max(sizeof(double), kTf32Pieces * sizeof(float)) * (size_t)k * gcols);
+        const int rmax = F.m2l_rmax;
+        rc = F.m2l_x.reserve(sizeof(double) * (size_t)k * gcols);
         if (!rc) rc = F.m2l_y.reserve(sizeof(double) * (size_t)k * gcols);
+        if (!rc) rc = F.m2l_z.reserve(sizeof(double) * (size_t)rmax * gcols);
         if (rc) return rc;
-        // pointer arrays of the batched GEMMs: C_d per chunk (global); X / Y chunk
-        // positions within one group (FP64 and FP32 views of the same buffers)
-        std::vector<const void *> pa(nc), pb(gc), pc(gc);
-        std::vector<const void *> qa((size_t)kTf32Pieces * nc), qb((size_t)kTf32Pieces * gc), qc(gc);
-        const size_t step = (size_t)kM2LChunk * k;
-        const size_t cpiece = (size_t)nslot * k * k, xpiece = (size_t)k * gcols;
-        for (int c = 0; c < nc; c++) {
-            pa[c] = (const double *)F.m2l_c.ptr + (size_t)chunk_slot[c] * k * k;
-            for (int p = 0; p < kTf32Pieces; p++)
-                qa[(size_t)p * nc + c] = (const float *)F.m2l_c32.ptr + p * cpiece + (size_t)chunk_slot[c] * k * k;
+        // Per group of columns and padded rank r: two batched GEMMs over that group's
+        // chunks whose offset has rank r,
+        //   Z_c = Q_d^T X_c (r x 256),  Y_c = P_d Z_c (k x 256).
+        // Pointer arrays in (group, rank, chunk) order -- A: the offset's factor; B, C:
+        // the chunk's slot in its group -- as FP64 and FP32 views of the same buffers.
+        std::vector<int> order;
+        F.m2l_seg.clear();
+        for (int g = 0; g < ngroups; g++) {
+            const int c0 = g * gc, c1e = std::min(nc, c0 + gc);
+            std::map<int, std::vector<int>> by_rank;
+            for (int c = c0; c < c1e; c++) by_rank[F.m2l_r[chunk_slot[c]]].push_back(c);
+            for (auto &kv : by_rank) {
+                F.m2l_seg.push_back({g, kv.first, (int)order.size(), (int)kv.second.size()});
+                order.insert(order.end(), kv.second.begin(), kv.second.end());
+            }
         }
-        for (int c = 0; c < gc; c++) {
-            pb[c] = (const double *)F.m2l_x.ptr + c * step;
-            pc[c] = (double *)F.m2l_y.ptr + c * step;
-            for (int p = 0; p < kTf32Pieces; p++) qb[(size_t)p * gc + c] = (const float *)F.m2l_x.ptr + p * xpiece + c * step;
-            qc[c] = (float *)F.m2l_y.ptr + c * step;
+        std::vector<const void *> a1(nc), b1(nc), a2(nc), a1f(nc), b1f(nc), a2f(nc);
+        std::vector<void *> c1(nc), c2(nc), c1f(nc), c2f(nc);
+        for (int i = 0; i < nc; i++) {
+            const int c = order[i], sl = chunk_slot[c];
+            const size_t j = (size_t)(c % gc);  // slot within its group
+            a1[i] = (const double *)F.m2l_q.ptr + F.m2l_pq_off[sl];
+            a2[i] = (const double *)F.m2l_p.ptr + F.m2l_pq_off[sl];
+            a1f[i] = (const float *)F.m2l_q32.ptr + F.m2l_pq_off[sl];
+            a2f[i] = (const float *)F.m2l_p32.ptr + F.m2l_pq_off[sl];
+            b1[i] = (const double *)F.m2l_x.ptr + j * kM2LChunk * k;
+            b1f[i] = (const float *)F.m2l_x.ptr + j * kM2LChunk * k;
+            c1[i] = (double *)F.m2l_z.ptr + j * kM2LChunk * rmax;
+            c1f[i] = (float *)F.m2l_z.ptr + j * kM2LChunk * rmax;
+            c2[i] = (double *)F.m2l_y.ptr + j * kM2LChunk * k;
+            c2f[i] = (float *)F.m2l_y.ptr + j * kM2LChunk * k;
         }
-        rc = F.d_ptr64[0].upload(pa.data(), sizeof(void *) * pa.size(), s);
-        if (!rc) rc = F.d_ptr64[1].upload(pb.data(), sizeof(void *) * pb.size(), s);
-        if (!rc) rc = F.d_ptr64[2].upload(pc.data(), sizeof(void *) * pc.size(), s);
-        if (!rc) rc = F.d_ptr32[0].upload(qa.data(), sizeof(void *) * qa.size(), s);
-        if (!rc) rc = F.d_ptr32[1].upload(qb.data(), sizeof(void *) * qb.size(), s);
-        if (!rc) rc = F.d_ptr32[2].upload(qc.data(), sizeof(void *) * qc.size(), s);
+        rc = F.d_m2l_ptr[0].upload(a1.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr[1].upload(b1.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr[2].upload(c1.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr[3].upload(a2.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr[4].upload(c2.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr32[0].upload(a1f.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr32[1].upload(b1f.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr32[2].upload(c1f.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr32[3].upload(a2f.data(), sizeof(void *) * nc, s);
+        if (!rc) rc = F.d_m2l_ptr32[4].upload(c2f.data(), sizeof(void *) * nc, s);
         if (rc) return rc;
+        F.m2l_flops = 0;
+        for (int c = 0; c < nc; c++) F.m2l_flops += 4.0 * k * F.m2l_r[chunk_slot[c]] * kM2LChunk;
         // host vectors above are pageable: their copies complete before upload returns
         int maxm = 0;
         for (int l = 0; l <= T.depth(); l++) maxm = std::max(maxm, F.parent_off[l + 1] - F.parent_off[l]);
@@ -1177,33 +1338,39 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         const int *gsrc = (const int *)F.d_m2l_gsrc.ptr + col0;
         const int gg = grid_for(ncol * k);
         t_launches += 2;
-        if (prec == PREC_MIXED) {
-            // The translation C_d carries no pseudo-inverse: FP32 operands and FP32
-            // accumulation (or the optional TF32 piece products, see kTf32Terms)
-            m2l_gather_split_kernel<<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (float *)F.m2l_x.ptr);
-            FCUDA(cudaGetLastError());
-            const float onef = 1.0f, zerof = 0.0f;
-            const void *const *qa = (const void *const *)F.d_ptr32[0].ptr;
-            const void *const *qb = (const void *const *)F.d_ptr32[1].ptr;
-            for (int t = 0; t < kTf32Terms; t++)
-                FBLAS(cublasGemmBatchedEx(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &onef,
-                                          qa + (size_t)kTf32Term[t][0] * nc + c0, CUDA_R_32F, k,
-                                          qb + (size_t)kTf32Term[t][1] * gc, CUDA_R_32F, k, t == 0 ? &zerof : &onef,
-                                          (void *const *)F.d_ptr32[2].ptr, CUDA_R_32F, k, ncg,
-                                          kM2LTensor ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F,
-                                          CUBLAS_GEMM_DEFAULT));
+        const bool mixed = prec == PREC_MIXED;
+        const int rmax = F.m2l_rmax;
+        const double one64 = 1.0, zero64 = 0.0;
+        const float one32 = 1.0f, zero32 = 0.0f;
+        const void *alpha = mixed ? (const void *)&one32 : (const void *)&one64;
+        const void *beta = mixed ? (const void *)&zero32 : (const void *)&zero64;
+        const cudaDataType_t dt = mixed ? CUDA_R_32F : CUDA_R_64F;
+        const cublasComputeType_t ct = mixed ? CUBLAS_COMPUTE_32F : CUBLAS_COMPUTE_64F;
+        DevBuf *P = mixed ? F.d_m2l_ptr32 : F.d_m2l_ptr;
+        if (mixed)
+            m2l_gather_kernel<float><<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (float *)F.m2l_x.ptr);
+        else
+            m2l_gather_kernel<double><<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (double *)F.m2l_x.ptr);
+        FCUDA(cudaGetLastError());
+        for (const M2LSeg &sg : F.m2l_seg) {
+            if (sg.group != c0 / gc) continue;
+            // Z = Q_d^T X (r x 256), then Y = P_d Z (k x 256), for the segment's chunks
+            FBLAS(cublasGemmBatchedEx(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, sg.rank, kM2LChunk, k, alpha,
+                                      (const void *const *)P[0].ptr + sg.start, dt, k,
+                                      (const void *const *)P[1].ptr + sg.start, dt, k, beta,
+                                      (void *const *)P[2].ptr + sg.start, dt, rmax, sg.count, ct,
+                                      CUBLAS_GEMM_DEFAULT));
+            FBLAS(cublasGemmBatchedEx(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, sg.rank, alpha,
+                                      (const void *const *)P[3].ptr + sg.start, dt, k,
+                                      (const void *const *)P[2].ptr + sg.start, dt, rmax, beta,
+                                      (void *const *)P[4].ptr + sg.start, dt, k, sg.count, ct, CUBLAS_GEMM_DEFAULT));
+        }
+        if (mixed)
             m2l_reduce_kernel<float><<<grid_for((long long)nn * k), 256, 0, s>>>(
                 (const float *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
-        } else {
-            m2l_gather_kernel<double><<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (double *)F.m2l_x.ptr);
-            FCUDA(cudaGetLastError());
-            FBLAS(cublasDgemmBatched(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kM2LChunk, k, &one,
-                                     (const double *const *)F.d_ptr64[0].ptr + c0, k,
-                                     (const double *const *)F.d_ptr64[1].ptr, k, &zero,
-                                     (double *const *)F.d_ptr64[2].ptr, k, ncg));
+        else
             m2l_reduce_kernel<double><<<grid_for((long long)nn * k), 256, 0, s>>>(
                 (const double *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
-        }
         FCUDA(cudaGetLastError());
     }
     FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,

@@ -36,6 +36,11 @@ struct ListPass {
     }
 };
 
+// Chunks of one group of columns whose offsets share one padded rank.
+struct M2LSeg {
+    int group, rank, start, count;
+};
+
 struct FarField {
     int p = 0, n = 0;      // multipole order, surface points per box
     int ke = 0, kc = 0;    // equivalent density and check potential dims
@@ -55,7 +60,11 @@ struct FarField {
     // compressed M2L: M2L_d = m2l_e C_d m2l_vt
     double m2l_rtol = 0;        // relative singular-value cut of the M2L bases
     int m2l_rank = 0;           // k
-    DevBuf m2l_c, m2l_c32;      // 316 blocks of k x k (FP64; TF32 pieces for the mixed path)
+    // two-level: per offset slot C_d ~ P_d Q_d^T, P and Q k x r_d (column-major, packed)
+    std::vector<int> m2l_r;         // r_d per slot
+    std::vector<size_t> m2l_pq_off;  // start of P_d / Q_d in m2l_p / m2l_q
+    int m2l_rmax = 1;
+    DevBuf m2l_p, m2l_q, m2l_p32, m2l_q32;
     DevBuf m2l_vt;              // V^T: k x (n ke)
     DevBuf m2l_e;               // DC2DE U: (n ke) x k
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
@@ -88,8 +97,10 @@ struct FarField {
     DevBuf d_m2l_gsrc;                      // per column: source node, -1 = padding
     DevBuf d_m2l_red_off, d_m2l_red_col;    // per target node: its columns (CSR, offset order)
     DevBuf d_m2l_gstart;                    // per group and target node: first entry in that group
-    DevBuf m2l_x, m2l_y;                    // one group of columns: k x columns (FP64, or FP32 pieces)
-    DevBuf d_ptr64[3], d_ptr32[3];          // batched-GEMM pointer arrays: C_d (per chunk), X and Y (per group slot)
+    DevBuf m2l_x, m2l_y, m2l_z;             // one group of columns: k x, k x, rmax x columns (FP64 or FP32)
+    DevBuf d_m2l_ptr[5], d_m2l_ptr32[5];    // per chunk: Q_d, X, Z, P_d, Y (FP64 / FP32 views)
+    std::vector<M2LSeg> m2l_seg;            // per group of columns and padded rank: chunks in the pointer arrays
+    double m2l_flops = 0;                   // flops of one M2L (both stages)
     ~FarField();
 };
 
