@@ -89,7 +89,8 @@ enum stk_ukernel {
      *   ADJ_TRG: outputs = forward targets with values w, inputs = forward sources
      *            with values (f, eps)  ->  dL/dx_trg 3 */
     STK_UK_REGVEL_ADJ_SRC = 13,     /* 3 -> 7, 4 values per output point */
-    STK_UK_REGVEL_ADJ_TRG = 14      /* 4 -> 3, 3 values per output point */
+    STK_UK_REGVEL_ADJ_TRG = 14,     /* 4 -> 3, 3 values per output point */
+    STK_UK_LAPLACE_SLDL_P = 15      /* 1+3 -> 1 laplace_p + laplace_dipolep at one point */
 };
 
 /* ---- kernel descriptors --------------------------------------------------- */

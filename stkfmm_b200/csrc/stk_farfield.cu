@@ -957,6 +957,11 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     for (int i = 0; i < nn; i++) T.centre(i, &ctr[3 * (size_t)i]);
     const int bw = f->sms * 12;  // resident warps of the list kernel, roughly
 
+    // SL and DL at the same points (the near field's fused case): the check
+    // potentials of S2M / S2L come from one pass over records carrying both
+    F.fused_src = kd->fused && (ki->id == STK_LapPGrad || ki->id == STK_PVel);
+    F.fused_check_uk = ki->id == STK_LapPGrad ? UK_LAPLACE_SLDL_P : UK_STOKES_SLDL_PVEL;
+
     // ---- S2M: leaves with sources; targets = their upward check surfaces ----
     F.s2m_nodes.clear();
     for (int b : T.leaves)
@@ -983,7 +988,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
         off[ms] = ms;
         for (int k = 0; k < 2; k++) {
-            const int uk = ki->slot[k == 0 ? SLOT_S2M_SL : SLOT_S2M_DL];
+            // SL and DL at the same points: one fused pass (its records carry both)
+            const int uk = F.fused_src ? (k == 0 ? F.fused_check_uk : -1) : ki->slot[k == 0 ? SLOT_S2M_SL : SLOT_S2M_DL];
             F.s2m[k].reset();
             if (uk < 0 || T.sets[k].n == 0) continue;
             rc = setup_pass(F.s2m[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
@@ -1055,7 +1061,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
         off[mx] = (int)ent.size();
         for (int k = 0; k < 2; k++) {
-            const int uk = ki->slot[k == 0 ? SLOT_S2L_SL : SLOT_S2L_DL];
+            const int uk = F.fused_src ? (k == 0 ? F.fused_check_uk : -1) : ki->slot[k == 0 ? SLOT_S2L_SL : SLOT_S2L_DL];
             F.s2l[k].reset();
             if (uk < 0 || T.sets[k].n == 0) continue;
             rc = setup_pass(F.s2l[k], uk, tb, te, off, ent, T.sets[k].node_begin.data(), T.sets[k].node_end.data(),
@@ -1272,9 +1278,11 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         int rc = F.rec_pts[k].reserve(sizeof(double) * (size_t)std::max(ps.n, 1) * rs);
         if (rc) return rc;
         t_launches++;
+        // fused check pass: SL values then DL values in one record
+        const bool both = F.fused_src && k == 0 && d_dl;
         if (launch_pack_records(ps.n, (const int *)kd->d_perm[k].ptr, (const double *)kd->d_xyz[k].ptr,
-                                k == 0 ? d_sl : d_dl, k == 0 ? ki->kdim_sl : ki->kdim_dl, nullptr, 0, rs,
-                                (double *)F.rec_pts[k].ptr, s) != cudaSuccess)
+                                k == 0 ? d_sl : d_dl, k == 0 ? ki->kdim_sl : ki->kdim_dl, both ? d_dl : nullptr,
+                                both ? ki->kdim_dl : 0, rs, (double *)F.rec_pts[k].ptr, s) != cudaSuccess)
             return STK_ERR_CUDA;
         return STK_OK;
     };

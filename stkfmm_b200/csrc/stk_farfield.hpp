@@ -85,6 +85,8 @@ struct FarField {
     std::vector<int> s2m_level_off, s2l_level_off;  // per level start in the compact order
     DevBuf d_s2m_nodes, d_s2l_nodes;
     ListPass s2m[2], s2l[2], m2t, l2t;  // [SL, DL]
+    bool fused_src = false;             // S2M / S2L as one SL+DL pass (s2m[0], s2l[0])
+    int fused_check_uk = -1;
     ListPass near[2];  // FMM near field per source set: U list + direct W / X entries
     // M2M / L2L per level: the parents (non-leaf nodes) of level l are
     // parents[parent_off[l] .. parent_off[l+1]) in node order

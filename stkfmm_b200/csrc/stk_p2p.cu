@@ -436,6 +436,7 @@ cudaError_t launch_list_p2p(int uk, int prec, const ListP2PArgs &a, int num_sms,
     case UK_STOKES_DOUBLEPVEL: return launch_prec<UK_STOKES_DOUBLEPVEL>(prec, a, num_sms, stream);
     case UK_LAPLACE_SLDL_PGRAD: return launch_prec<UK_LAPLACE_SLDL_PGRAD>(prec, a, num_sms, stream);
     case UK_STOKES_SLDL_PVEL: return launch_prec<UK_STOKES_SLDL_PVEL>(prec, a, num_sms, stream);
+    case UK_LAPLACE_SLDL_P: return launch_prec<UK_LAPLACE_SLDL_P>(prec, a, num_sms, stream);
     case UK_REGVEL_ADJ_SRC:
         if (!a.trg_aux) return cudaErrorInvalidValue;
         return launch_prec<UK_REGVEL_ADJ_SRC>(prec, a, num_sms, stream);

@@ -116,7 +116,8 @@ enum UkId : int {
     UK_STOKES_SLDL_PVEL = 12,    // values (f0, f1, f2, trD, D00 .. D22)
     UK_REGVEL_ADJ_SRC = 13,      // adjoint of stokes_regvel, source side (see below)
     UK_REGVEL_ADJ_TRG = 14,      // adjoint of stokes_regvel, target positions
-    UK_COUNT = 15
+    UK_LAPLACE_SLDL_P = 15,      // values (q, d0, d1, d2): laplace_p + laplace_dipolep (S2M / S2L)
+    UK_COUNT = 16
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
@@ -541,27 +542,50 @@ template <> struct Uk<UK_REGVEL_ADJ_TRG> {
     }
 };
 
+// laplace_p + laplace_dipolep at one point (the check potentials of S2M / S2L when
+// SL and DL sit at the same points): p = (q + (d.r) / r^2) / r.  staged (q, d)
+template <> struct Uk<UK_LAPLACE_SLDL_P> {
+    static constexpr int SDIM = 4, TDIM = 1, NV = 4;
+    static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = f[1];
+        v[2] = f[2];
+        v[3] = f[3];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rdn = fmav(v[1], dx, fmav(v[2], dy, v[3] * dz));
+        u[0] = fmav(fmav(rdn, rinv * rinv, v[0]), rinv, u[0]);
+    }
+};
+
 // Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
          : id == UK_LAPLACE_DIPOLEPGRAD ? 3 : id == UK_STOKES_VEL ? 3 : id == UK_RPY_U ? 4
          : id == UK_RPY_ULAPU ? 4 : id == UK_STK_ULAPU ? 3 : id == UK_STOKES_REGVEL ? 4
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 9 : id == UK_LAPLACE_SLDL_PGRAD ? 4
-         : id == UK_STOKES_SLDL_PVEL ? 13 : id == UK_REGVEL_ADJ_SRC ? 3 : id == UK_REGVEL_ADJ_TRG ? 4 : 0;
+         : id == UK_STOKES_SLDL_PVEL ? 13 : id == UK_REGVEL_ADJ_SRC ? 3 : id == UK_REGVEL_ADJ_TRG ? 4
+         : id == UK_LAPLACE_SLDL_P ? 4 : 0;
 }
 __host__ __device__ constexpr int uk_tdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 4 : id == UK_LAPLACE_DIPOLEP ? 1
          : id == UK_LAPLACE_DIPOLEPGRAD ? 4 : id == UK_STOKES_VEL ? 3 : id == UK_RPY_U ? 3
          : id == UK_RPY_ULAPU ? 6 : id == UK_STK_ULAPU ? 6 : id == UK_STOKES_REGVEL ? 3
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 4 : id == UK_LAPLACE_SLDL_PGRAD ? 4
-         : id == UK_STOKES_SLDL_PVEL ? 4 : id == UK_REGVEL_ADJ_SRC ? 7 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
+         : id == UK_STOKES_SLDL_PVEL ? 4 : id == UK_REGVEL_ADJ_SRC ? 7 : id == UK_REGVEL_ADJ_TRG ? 3
+         : id == UK_LAPLACE_SLDL_P ? 1 : 0;
 }
 // per-output-point (target-side) values a micro-kernel reads
 __host__ __device__ constexpr int uk_tvdim(int id) {
     return id == UK_REGVEL_ADJ_SRC ? 4 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
 }
 __host__ __device__ constexpr double uk_scale(int id) {
-    return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD ? kInv4Pi : kInv8Pi;
+    return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD || id == UK_LAPLACE_SLDL_P ? kInv4Pi
+                                                                                                : kInv8Pi;
 }
 
 }  // namespace stk

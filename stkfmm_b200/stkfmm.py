@@ -74,6 +74,7 @@ class UKERNEL(enum.IntEnum):
     STOKES_SLDL_PVEL = 12
     REGVEL_ADJ_SRC = 13  # adjoint of stokes_regvel: (dL/df, dL/deps, dL/dx) at the sources
     REGVEL_ADJ_TRG = 14  # adjoint of stokes_regvel: dL/dx at the targets
+    LAPLACE_SLDL_P = 15  # laplace_p + laplace_dipolep at one point (fused S2M / S2L)
 
 
 SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.Stokes, KERNEL.RPY, KERNEL.StokesRegVel, KERNEL.PVel)

@@ -17,11 +17,13 @@ GOLDEN_MAP = {
     "StokesSLPVel": [(9, slice(0, 4), slice(0, 4))],
     "StokesDLPVel": [(10, slice(0, 4), slice(0, 9))],
 }
-UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13]
-UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13, 3, 4, 4]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4, 7, 3, 1]
 UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel", "rpy_u",
             "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel", "laplace_sldl_pgrad",
-            "stokes_sldl_pvel"]
+            "stokes_sldl_pvel", "regvel_adjoint_src", "regvel_adjoint_trg", "laplace_sldl_p"]
+# forward micro-kernels (the adjoint ones, 13 and 14, need per-target values)
+UK_FORWARD = list(range(13)) + [15]
 
 
 def load_golden(name):

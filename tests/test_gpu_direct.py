@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from helpers import GOLDEN_MAP, UK_NAMES, UK_SDIM, UK_TDIM, load_golden, uk_values
+from helpers import UK_FORWARD, GOLDEN_MAP, UK_NAMES, UK_SDIM, UK_TDIM, load_golden, uk_values
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -58,7 +58,7 @@ def test_direct_golden(torch_cuda, L, name, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
-@pytest.mark.parametrize("uk", list(range(13)))
+@pytest.mark.parametrize("uk", UK_FORWARD)
 def test_direct_all_ukernels_vs_oracle(torch_cuda, L, uk, prec):
     rng = np.random.default_rng(100 + uk)
     src = rng.random((3000, 3))
@@ -69,6 +69,8 @@ def test_direct_all_ukernels_vs_oracle(torch_cuda, L, uk, prec):
         ref = O.direct(1, src, val[:, :1], trg) + O.direct(3, src, val[:, 1:4], trg)
     elif uk == 12:  # fused stokes SL+DL
         ref = O.direct(9, src, val[:, :4], trg) + O.direct(10, src, val[:, 4:13], trg)
+    elif uk == 15:  # fused laplace SL+DL potential
+        ref = O.direct(0, src, val[:, :1], trg) + O.direct(2, src, val[:, 1:4], trg)
     else:
         ref = O.direct(uk, src, val, trg)
     assert rel_l2(out, ref) < TOL[prec], (UK_NAMES[uk], rel_l2(out, ref))

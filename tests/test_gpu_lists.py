@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import component_errors, rel_l2
-from helpers import UK_NAMES, UK_TDIM, clustered_points, uk_values
+from helpers import UK_FORWARD, UK_NAMES, UK_TDIM, clustered_points, uk_values
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -49,6 +49,9 @@ def oracle_ulist(uk, tb, te, off, ent, sb, se, src_sorted, val_sorted, trg_sorte
     if uk == 12:
         return (oracle_ulist(9, tb, te, off, ent, sb, se, src_sorted, val_sorted[:, :4], trg_sorted, period)
                 + oracle_ulist(10, tb, te, off, ent, sb, se, src_sorted, val_sorted[:, 4:], trg_sorted, period))
+    if uk == 15:
+        return (oracle_ulist(0, tb, te, off, ent, sb, se, src_sorted, val_sorted[:, :1], trg_sorted, period)
+                + oracle_ulist(2, tb, te, off, ent, sb, se, src_sorted, val_sorted[:, 1:4], trg_sorted, period))
     return O.lists(uk, tb, te, off, ent >> 5, ent & 31, sb, se, src_sorted, val_sorted, trg_sorted, period=period)
 
 
@@ -65,7 +68,7 @@ def tree_case(seed, n, pbc, max_pts, dist="clustered", separate_trg=False):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
-@pytest.mark.parametrize("uk", list(range(13)))
+@pytest.mark.parametrize("uk", UK_FORWARD)
 def test_ulist_all_ukernels(torch_cuda, uk, prec):
     rng, src, trg, L = tree_case(uk, 6000, 0, 64)
     val = uk_values(rng, uk, len(src))
