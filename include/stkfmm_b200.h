@@ -90,7 +90,12 @@ enum stk_ukernel {
      *            with values (f, eps)  ->  dL/dx_trg 3 */
     STK_UK_REGVEL_ADJ_SRC = 13,     /* 3 -> 7, 4 values per output point */
     STK_UK_REGVEL_ADJ_TRG = 14,     /* 4 -> 3, 3 values per output point */
-    STK_UK_LAPLACE_SLDL_P = 15      /* 1+3 -> 1 laplace_p + laplace_dipolep at one point */
+    STK_UK_LAPLACE_SLDL_P = 15,     /* 1+3 -> 1 laplace_p + laplace_dipolep at one point */
+    /* outputs (p, grad p 3, Hessian xx xy xz yy yz zz) */
+    STK_UK_LAPLACE_PGRADGRAD = 16,       /* 1 -> 10  LaplaceLayerKernel.hpp:138-166 */
+    STK_UK_LAPLACE_DIPOLEPGRADGRAD = 17, /* 3 -> 10  LaplaceLayerKernel.hpp:168-200 */
+    STK_UK_LAPLACE_QUADP = 18,           /* 9 -> 1   LaplaceLayerKernel.hpp:202-232 (S row-major) */
+    STK_UK_LAPLACE_QUADPGRADGRAD = 19    /* 9 -> 10  LaplaceLayerKernel.hpp:234-301 */
 };
 
 /* ---- kernel descriptors --------------------------------------------------- */
@@ -296,6 +301,14 @@ void stk_ker_stokes_pvel(double *r_src, int src_cnt, double *v_src, int dof, dou
                          double *k_out, void *mem_mgr);
 void stk_ker_stokes_doublepvel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
                                double *k_out, void *mem_mgr);
+void stk_ker_laplace_pgradgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                               double *k_out, void *mem_mgr);
+void stk_ker_laplace_dipolepgradgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg,
+                                     int trg_cnt, double *k_out, void *mem_mgr);
+void stk_ker_laplace_quadp(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                           double *k_out, void *mem_mgr);
+void stk_ker_laplace_quadpgradgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                   double *k_out, void *mem_mgr);
 /* status of the last ker_poten shim call on this thread (they return void) */
 int stk_ker_last_status(void);
 

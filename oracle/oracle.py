@@ -29,17 +29,26 @@ UK_STK_ULAPU = 7
 UK_STOKES_REGVEL = 8
 UK_STOKES_PVEL = 9
 UK_STOKES_DOUBLEPVEL = 10
+# 11 .. 15 are fused / adjoint device micro-kernels without an oracle body
+UK_LAPLACE_PGRADGRAD = 16
+UK_LAPLACE_DIPOLEPGRADGRAD = 17
+UK_LAPLACE_QUADP = 18
+UK_LAPLACE_QUADPGRADGRAD = 19
 UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel",
-            "rpy_u", "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel"]
-UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9]
-UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4]
+            "rpy_u", "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel",
+            None, None, None, None, None,
+            "laplace_pgradgrad", "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad"]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10]
 
 # reference SimpleKernel selectors (oracle/ref_driver.cpp)
 REF_STOKES_SL, REF_LAP_SL_PGRAD, REF_LAP_DL_PGRAD, REF_STOKES_SL_RPY, REF_STOKES_REG_SL_VEL, \
-    REF_STOKES_SL_PVEL, REF_STOKES_DL_PVEL = range(7)
+    REF_STOKES_SL_PVEL, REF_STOKES_DL_PVEL, REF_LAP_SL_PGRADGRAD, REF_LAP_DL_PGRADGRAD, \
+    REF_LAP_QPGRADGRAD = range(10)
 REF_DIMS = {REF_STOKES_SL: (3, 6), REF_LAP_SL_PGRAD: (1, 4), REF_LAP_DL_PGRAD: (3, 4),
             REF_STOKES_SL_RPY: (4, 6), REF_STOKES_REG_SL_VEL: (4, 3), REF_STOKES_SL_PVEL: (4, 4),
-            REF_STOKES_DL_PVEL: (9, 4)}
+            REF_STOKES_DL_PVEL: (9, 4), REF_LAP_SL_PGRADGRAD: (1, 10), REF_LAP_DL_PGRADGRAD: (3, 10),
+            REF_LAP_QPGRADGRAD: (9, 10)}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -209,10 +218,11 @@ def ewald(kind: int, src, sval, trg, xi: float = 7.0, nreal: int = 1, nwave: int
 
     kind EWALD_LAPLACE: charges (n, 1) -> potential + gradient (n, 4), zero-mean Green's function;
     kind EWALD_STOKES: forces (n, 3) -> velocity (n, 3); kind EWALD_PVEL: (f, trD) (n, 4) -> pressure and
-    velocity of stokes_pvel (n, 4).  Defaults (xi = 7, one real-space image
+    velocity of stokes_pvel (n, 4); kind EWALD_LAPLACE_HESS: charges -> potential, gradient and
+    Hessian (n, 10).  Defaults (xi = 7, one real-space image
     shell, |m| <= 14) converge to ~1e-15 for points in [0, 1)^3.
     """
-    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), 2: (4, 4)}[kind]
+    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), 2: (4, 4), 3: (1, 10)}[kind]
     src, ps = _d(np.asarray(src).reshape(-1, 3))
     sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
     trg, pt = _d(np.asarray(trg).reshape(-1, 3))
@@ -225,15 +235,17 @@ def ewald(kind: int, src, sval, trg, xi: float = 7.0, nreal: int = 1, nwave: int
 
 
 EWALD_PVEL = 2
+# Laplace charges -> potential, gradient and Hessian (xx xy xz yy yz zz), laplace_pgradgrad's layout
+EWALD_LAPLACE_HESS = 3
 
 
 def ewald2d(kind: int, src, sval, trg, out=None, nthreads: int = 0):
     """out += doubly periodic (x, y; z free) sum per pair (see stk_oracle.c:oracle_ewald2d).
 
     kind EWALD_LAPLACE: (n, 1) -> (n, 4) potential + gradient; EWALD_STOKES: (n, 3) -> (n, 3);
-    EWALD_PVEL: (f, trD) (n, 4) -> (pressure, velocity) (n, 4).
+    EWALD_PVEL: (f, trD) (n, 4) -> (pressure, velocity) (n, 4); EWALD_LAPLACE_HESS: (n, 1) -> (n, 10).
     """
-    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), EWALD_PVEL: (4, 4)}[kind]
+    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), EWALD_PVEL: (4, 4), EWALD_LAPLACE_HESS: (1, 10)}[kind]
     src, ps = _d(np.asarray(src).reshape(-1, 3))
     sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
     trg, pt = _d(np.asarray(trg).reshape(-1, 3))

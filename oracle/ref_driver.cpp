@@ -17,7 +17,8 @@ typedef void (*kernel_func)(double *, double *, double *, double *);
 
 // Selector values (stable, used by oracle/oracle.py):
 //   0 StokesSL  1 LaplaceSLPGrad  2 LaplaceDLPGrad  3 StokesSLRPY
-//   4 StokesRegSLVel  5 StokesSLPVel  6 StokesDLPVel
+//   4 StokesRegSLVel  5 StokesSLPVel  6 StokesDLPVel  7 LaplaceSLPGradGrad
+//   8 LaplaceDLPGradGrad  9 LaplaceQPGradGrad
 static kernel_func pick(int which) {
     switch (which) {
     case 0: return StokesSL;
@@ -27,6 +28,9 @@ static kernel_func pick(int which) {
     case 4: return StokesRegSLVel;
     case 5: return StokesSLPVel;
     case 6: return StokesDLPVel;
+    case 7: return LaplaceSLPGradGrad;
+    case 8: return LaplaceDLPGradGrad;
+    case 9: return LaplaceQPGradGrad;
     default: return nullptr;
     }
 }

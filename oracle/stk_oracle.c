@@ -44,16 +44,23 @@ enum {
     UK_STOKES_REGVEL = 8,       /* f,eps(4)  -> u(3)              StokesRegSingleLayerKernel.hpp:17-41 */
     UK_STOKES_PVEL = 9,         /* f,trD(4)  -> p,u(4)            StokesSingleLayerKernel.hpp:27-47 */
     UK_STOKES_DOUBLEPVEL = 10,  /* D(9)      -> p,u(4)            StokesDoubleLayerKernel.hpp:25-57 */
-    UK_COUNT = 11
+    /* 11 .. 15: fused / adjoint device micro-kernels, no oracle body (tests compose them) */
+    UK_LAPLACE_PGRADGRAD = 16,       /* q(1) -> p,grad,Hessian(10)  LaplaceLayerKernel.hpp:138-166 */
+    UK_LAPLACE_DIPOLEPGRADGRAD = 17, /* d(3) -> (10)                LaplaceLayerKernel.hpp:168-200 */
+    UK_LAPLACE_QUADP = 18,           /* S(9) -> p(1)                LaplaceLayerKernel.hpp:202-232 */
+    UK_LAPLACE_QUADPGRADGRAD = 19,   /* S(9) -> (10)                LaplaceLayerKernel.hpp:234-301 */
+    UK_COUNT = 20
 };
 
-static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9};
-static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4};
+static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9};
+static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10};
+
+static int uk_valid(int uk) { return uk >= 0 && uk < UK_COUNT && uk_sdim[uk] > 0; }
 
 static const double PI_ = 3.14159265358979323846264338327950288;
 
 int oracle_uk_dims(int uk, int *sdim, int *tdim) {
-    if (uk < 0 || uk >= UK_COUNT) return 1;
+    if (!uk_valid(uk)) return 1;
     *sdim = uk_sdim[uk];
     *tdim = uk_tdim[uk];
     return 0;
@@ -62,7 +69,7 @@ int oracle_uk_dims(int uk, int *sdim, int *tdim) {
 /* ScaleFactor() of each micro-kernel: 1/(4 pi) for Laplace, 1/(8 pi) for the
  * Stokes family (e.g. LaplaceLayerKernel.hpp:44-46, RPYKernel.hpp:20-22). */
 double oracle_uk_scale(int uk) {
-    return (uk <= UK_LAPLACE_DIPOLEPGRAD) ? 1.0 / (4.0 * PI_) : 1.0 / (8.0 * PI_);
+    return (uk <= UK_LAPLACE_DIPOLEPGRAD || uk >= UK_LAPLACE_PGRADGRAD) ? 1.0 / (4.0 * PI_) : 1.0 / (8.0 * PI_);
 }
 
 /* Exact masked 1/sqrt: the reference's approx_rsqrt<digits>(r2, r2 > 0) returns
@@ -202,6 +209,97 @@ static void uk_pair(int uk, const double r[3], const double *f, double *u) {
         u[2] += dy * cc;
         u[3] += dz * cc;
     } break;
+    case UK_LAPLACE_PGRADGRAD: { /* LaplaceLayerKernel.hpp:145-165 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double sv = f[0] * rinv2 * rinv;
+        u[0] += sv * r2;
+        u[1] -= sv * dx;
+        u[2] -= sv * dy;
+        u[3] -= sv * dz;
+        sv *= rinv2;
+        u[4] += sv * (3.0 * dx * dx - r2);
+        u[5] += sv * 3.0 * dx * dy;
+        u[6] += sv * 3.0 * dx * dz;
+        u[7] += sv * (3.0 * dy * dy - r2);
+        u[8] += sv * 3.0 * dy * dz;
+        u[9] += sv * (3.0 * dz * dz - r2);
+    } break;
+    case UK_LAPLACE_DIPOLEPGRADGRAD: { /* LaplaceLayerKernel.hpp:175-199 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double rinv3 = rinv2 * rinv;
+        double rinv5 = rinv2 * rinv3;
+        double rinv7 = rinv2 * rinv5;
+        double rd = dx * f[0] + dy * f[1] + dz * f[2];
+        double t3 = 3.0 * r2;
+        u[0] += rd * rinv3;
+        u[1] += (f[0] * r2 - rd * 3.0 * dx) * rinv5;
+        u[2] += (f[1] * r2 - rd * 3.0 * dy) * rinv5;
+        u[3] += (f[2] * r2 - rd * 3.0 * dz) * rinv5;
+        u[4] += (15.0 * dx * dx * rd - r2 * (3.0 * rd + 6.0 * dx * f[0])) * rinv7;
+        u[5] += (15.0 * dx * dy * rd - t3 * (dx * f[1] + dy * f[0])) * rinv7;
+        u[6] += (15.0 * dx * dz * rd - t3 * (dx * f[2] + dz * f[0])) * rinv7;
+        u[7] += (15.0 * dy * dy * rd - r2 * (3.0 * rd + 6.0 * dy * f[1])) * rinv7;
+        u[8] += (15.0 * dy * dz * rd - t3 * (dy * f[2] + dz * f[1])) * rinv7;
+        u[9] += (15.0 * dz * dz * rd - r2 * (3.0 * rd + 6.0 * dz * f[2])) * rinv7;
+    } break;
+    case UK_LAPLACE_QUADP: { /* LaplaceLayerKernel.hpp:209-231; S row-major */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv5 = rinv * rinv;
+        rinv5 = rinv5 * rinv5 * rinv;
+        double c = f[0] * dx * dx;
+        c += (f[1] + f[3]) * dx * dy;
+        c += (f[2] + f[6]) * dx * dz;
+        c += f[4] * dy * dy;
+        c += (f[5] + f[7]) * dy * dz;
+        c += f[8] * dz * dz;
+        c *= 3.0;
+        u[0] += (c - r2 * (f[0] + f[4] + f[8])) * rinv5;
+    } break;
+    case UK_LAPLACE_QUADPGRADGRAD: { /* LaplaceLayerKernel.hpp:241-300 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double rinv3 = rinv2 * rinv;
+        double rinv5 = rinv3 * rinv2;
+        double rinv7 = rinv5 * rinv2;
+        double rinv9 = rinv7 * rinv2;
+        const double sxx = f[0], sxy = f[1], sxz = f[2], syx = f[3], syy = f[4], syz = f[5];
+        const double szx = f[6], szy = f[7], szz = f[8];
+        double rrQ = dx * dx * sxx + dx * dy * (sxy + syx) + dx * dz * (sxz + szx) + dy * dy * syy +
+                     dy * dz * (syz + szy) + dz * dz * szz;
+        double c3 = rrQ * 3.0, c5 = rrQ * 5.0;
+        double tr = sxx + syy + szz;
+        /* row (S r) and column (S^T r) products */
+        double ax = dx * sxx + dy * sxy + dz * sxz, ay = dx * syx + dy * syy + dz * syz;
+        double az = dx * szx + dy * szy + dz * szz;
+        double bx = dx * sxx + dy * syx + dz * szx, by = dx * sxy + dy * syy + dz * szy;
+        double bz = dx * sxz + dy * syz + dz * szz;
+        u[0] += (c3 - r2 * tr) * rinv5;
+        double px = dx * c5 - r2 * (ax + bx + dx * tr);
+        double py = dy * c5 - r2 * (ay + by + dy * tr);
+        double pz = dz * c5 - r2 * (az + bz + dz * tr);
+        u[1] -= 3.0 * px * rinv7;
+        u[2] -= 3.0 * py * rinv7;
+        u[3] -= 3.0 * pz * rinv7;
+        double r4 = r2 * r2;
+        u[4] += rinv9 * (105.0 * dx * dx * rrQ - r2 * 15.0 * (rrQ + dx * 2.0 * (ax + bx) + dx * dx * tr) +
+                         3.0 * r4 * (tr + 2.0 * sxx));
+        u[5] += rinv9 * (105.0 * (dx * dy * rrQ) - r2 * 15.0 * ((dy * ax + dy * bx + dx * ay + dx * by) + dx * dy * tr) +
+                         3.0 * r4 * (sxy + syx));
+        u[6] += rinv9 * (105.0 * (dx * dz * rrQ) - r2 * 15.0 * ((dz * ax + dz * bx + dx * az + dx * bz) + dx * dz * tr) +
+                         3.0 * r4 * (sxz + szx));
+        u[7] += rinv9 * (105.0 * dy * dy * rrQ - r2 * 15.0 * (rrQ + dy * 2.0 * (ay + by) + dy * dy * tr) +
+                         3.0 * r4 * (tr + 2.0 * syy));
+        u[8] += rinv9 * (105.0 * (dy * dz * rrQ) - r2 * 15.0 * ((dy * az + dy * bz + dz * ay + dz * by) + dy * dz * tr) +
+                         3.0 * r4 * (syz + szy));
+        u[9] += rinv9 * (105.0 * dz * dz * rrQ - r2 * 15.0 * (rrQ + dz * 2.0 * (az + bz) + dz * dz * tr) +
+                         3.0 * r4 * (tr + 2.0 * szz));
+    } break;
     default:
         break;
     }
@@ -224,7 +322,7 @@ static int clamp_threads(int nthreads) {
  * coordinates, accumulate into the caller's output, targets split across threads. */
 int oracle_direct(int uk, int nsrc, const double *src_xyz, const double *src_val, int ntrg,
                   const double *trg_xyz, double *trg_val, int nthreads) {
-    if (uk < 0 || uk >= UK_COUNT || nsrc < 0 || ntrg < 0) return 1;
+    if (!uk_valid(uk) || nsrc < 0 || ntrg < 0) return 1;
     const int sd = uk_sdim[uk], td = uk_tdim[uk];
     const double sc = oracle_uk_scale(uk);
     nthreads = clamp_threads(nthreads);
@@ -254,7 +352,7 @@ int oracle_lists(int uk, int n_trg_box, const int *trg_begin, const int *trg_end
                  const int *list_src, const int *list_shift, const int *src_begin, const int *src_end,
                  const double *src_xyz, const double *src_val, const double *trg_xyz, double *trg_val,
                  double period, int nthreads) {
-    if (uk < 0 || uk >= UK_COUNT) return 1;
+    if (!uk_valid(uk)) return 1;
     const int sd = uk_sdim[uk], td = uk_tdim[uk];
     const double sc = oracle_uk_scale(uk);
     nthreads = clamp_threads(nthreads);
@@ -385,7 +483,12 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
  * kind 1: f (3 values) -> velocity (3 outputs);
  * kind 2: (f, trD) (4 values) -> stokes_pvel's pressure and velocity (4 outputs):
  *         p = -grad(psi).f / 4 pi, u = G f / 8 pi + grad(psi) trD / 8 pi, with psi the
- *         Laplace sum above and G the Stokeslet sum.
+ *         Laplace sum above and G the Stokeslet sum;
+ * kind 3: q (1 value)  -> potential, gradient and Hessian (xx xy xz yy yz zz; 10 outputs)
+ *         of the Laplace sum (laplace_pgradgrad's layout).  Real-space Hessian
+ *         f'' r r^T / r^2 + f'/r (I - r r^T / r^2) of f = erfc(xi r)/r; a target on a
+ *         source gets the Hessian at 0 of the smooth remainder -erf(xi r)/r,
+ *         4 xi^3 / (3 sqrt(pi)) I; wave terms -w k k^T cos(k.r).
  * Real-space images |s_i| <= nreal around the minimum-image displacement, wave
  * vectors k = 2 pi m with 0 < max|m_i| <= nwave (structure factors per k).  A
  * target on a source point gets that source's periodic images but not the source
@@ -393,8 +496,10 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
  * ------------------------------------------------------------------------ */
 int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const double *src, const double *val,
                  int ntrg, const double *trg, double *out, int nthreads) {
-    if (kind < 0 || kind > 2 || nsrc < 0 || ntrg < 0 || nreal < 0 || nwave < 0 || !(xi > 0)) return 1;
-    const int sd = kind == 0 ? 1 : kind == 1 ? 3 : 4, td = kind == 1 ? 3 : 4;
+    if (kind < 0 || kind > 3 || nsrc < 0 || ntrg < 0 || nreal < 0 || nwave < 0 || !(xi > 0)) return 1;
+    const int hess = kind == 3;
+    if (hess) kind = 0;
+    const int sd = kind == 0 ? 1 : kind == 1 ? 3 : 4, td = hess ? 10 : kind == 1 ? 3 : 4;
     /* structure-factor columns: the values, plus f.k for kind 2 */
     const int ns = kind == 2 ? 5 : sd;
     const double sqpi = sqrt(PI_), xi2 = xi * xi;
@@ -440,7 +545,7 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
 #pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads)
     for (int t = 0; t < ntrg; t++) {
         const double *x = trg + 3 * (size_t)t;
-        double acc[4] = {0, 0, 0, 0};
+        double acc[4] = {0, 0, 0, 0}, H[6] = {0, 0, 0, 0, 0, 0};
         /* real space */
         for (int j = 0; j < nsrc; j++) {
             double d0[3];
@@ -456,9 +561,15 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
                         const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
                         if (rr < eps) {
                             /* the source itself: its self term instead (no gradient) */
-                            if (kind == 0)
+                            if (kind == 0) {
                                 acc[0] += -2 * xi / sqpi * v[0];
-                            else if (kind == 1)
+                                if (hess) {
+                                    const double h0 = 4 * xi * xi2 / (3 * sqpi) * v[0];
+                                    H[0] += h0;
+                                    H[3] += h0;
+                                    H[5] += h0;
+                                }
+                            } else if (kind == 1)
                                 for (int a = 0; a < 3; a++) acc[a] += -4 * xi / sqpi * v[a];
                             else
                                 for (int a = 0; a < 3; a++) acc[1 + a] += -4 * xi / sqpi * v[a];
@@ -470,6 +581,13 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
                         if (kind == 0) {
                             acc[0] += v[0] * ec / rr;
                             for (int a = 0; a < 3; a++) acc[1 + a] += v[0] * fp / rr * r[a];
+                            if (hess) {
+                                const double fpp = 2 * xi / sqpi * ex * (2 * xi2 + 2 / (rr * rr)) + 2 * ec / (rr * rr * rr);
+                                const double hs = v[0] * (fpp - fp / rr) / (rr * rr), hd = v[0] * fp / rr;
+                                int q = 0;
+                                for (int a = 0; a < 3; a++)
+                                    for (int b = a; b < 3; b++) H[q++] += hs * r[a] * r[b] + (a == b ? hd : 0.0);
+                            }
                         } else {
                             const double c1 = 2 * (xi * ex / (sqpi * rr * rr) + ec / (2 * rr * rr * rr));
                             const double c2 = 4 * xi / sqpi * ex;
@@ -501,6 +619,11 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
                 const double Sn = sp * Sc[ik] - cp * Ss[ik];
                 acc[0] += w * C;
                 for (int a = 0; a < 3; a++) acc[1 + a] -= w * k[a] * Sn;
+                if (hess) {
+                    int q = 0;
+                    for (int a = 0; a < 3; a++)
+                        for (int b = a; b < 3; b++) H[q++] -= w * k[a] * k[b] * C;
+                }
             } else {
                 const double w = 8 * PI_ * (1 + k2 / (4 * xi2)) * g / (k2 * k2);
                 const int o = kind == 1 ? 0 : 1;
@@ -521,6 +644,8 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
         if (kind == 0) {
             acc[0] -= PI_ / xi2 * qsum;
             for (int a = 0; a < 4; a++) out[(size_t)td * t + a] += acc[a] / (4 * PI_);
+            if (hess)
+                for (int a = 0; a < 6; a++) out[(size_t)td * t + 4 + a] += H[a] / (4 * PI_);
         } else if (kind == 1) {
             for (int a = 0; a < 3; a++) out[(size_t)td * t + a] += acc[a] / (8 * PI_);
         } else {
@@ -543,20 +668,37 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
 static const double XI2D = 2.0;
 static const int NR2D = 5, NW2D = 5;
 
-static void ewald2_laplace(const double r0[3], double *pot, double grad[3]) {
+/* Potential, gradient and (hess != NULL) Hessian xx xy xz yy yz zz.  The Hessian
+ * terms: real space as in oracle_ewald (kind 3); wave terms of
+ * pi cos(k.r) g(z) / k with g = e+ + e-, g' = k (e+ - e-) (the two Gaussian
+ * terms of the reference's gradient cancel), g'' = k^2 g - 4 xi k / sqrt(pi)
+ * exp(-k^2/4xi^2 - xi^2 z^2); the k = 0 term's d2/dz2 = -4 sqrt(pi) xi exp(-xi^2 z^2). */
+static void ewald2_laplace_h(const double r0[3], double *pot, double grad[3], double *hess) {
     const double xi = XI2D, z = r0[2], sp = sqrt(PI_);
-    double p = 0.0, g[3] = {0, 0, 0};
+    double p = 0.0, g[3] = {0, 0, 0}, H[6] = {0, 0, 0, 0, 0, 0};
     for (int a = -NR2D; a <= NR2D; a++)
         for (int b = -NR2D; b <= NR2D; b++) {
             const double r[3] = {r0[0] + a, r0[1] + b, z};
             const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
             if (rr < 1e-13) {
                 p += -2 * xi / sp;
+                const double h0 = 4 * xi * xi * xi / (3 * sp);
+                H[0] += h0;
+                H[3] += h0;
+                H[5] += h0;
                 continue;
             }
             p += erfc(xi * rr) / rr;
             const double fp = -(2. * exp(-rr * rr * xi * xi) * xi) / (sp * rr) - erfc(rr * xi) / (rr * rr);
             for (int k = 0; k < 3; k++) g[k] += fp / rr * r[k];
+            if (hess) {
+                const double fpp = 2 * xi / sp * exp(-rr * rr * xi * xi) * (2 * xi * xi + 2 / (rr * rr)) +
+                                   2 * erfc(xi * rr) / (rr * rr * rr);
+                const double hs = (fpp - fp / rr) / (rr * rr), hd = fp / rr;
+                int q = 0;
+                for (int i = 0; i < 3; i++)
+                    for (int j = i; j < 3; j++) H[q++] += hs * r[i] * r[j] + (i == j ? hd : 0.0);
+            }
         }
     for (int a = -NW2D; a <= NW2D; a++)
         for (int b = -NW2D; b <= NW2D; b++) {
@@ -572,12 +714,27 @@ static void ewald2_laplace(const double r0[3], double *pot, double grad[3]) {
             g[0] += -PI_ * sin(ph) * (ep + em) / k * kx;
             g[1] += -PI_ * sin(ph) * (ep + em) / k * ky;
             g[2] += PI_ * cos(ph) * gz / k;
+            if (hess) {
+                const double gg = ep + em, c = cos(ph), s = sin(ph);
+                const double gzz = k * k * gg - 4 * xi * k / sp * exp(-k * k / (4 * xi * xi) - xi * xi * z * z);
+                H[0] -= PI_ * c * gg / k * kx * kx;
+                H[1] -= PI_ * c * gg / k * kx * ky;
+                H[2] -= PI_ * s * gz / k * kx;
+                H[3] -= PI_ * c * gg / k * ky * ky;
+                H[4] -= PI_ * s * gz / k * ky;
+                H[5] += PI_ * c * gzz / k;
+            }
         }
     p -= 2 * sp * (exp(-xi * xi * z * z) / xi + sp * z * erf(xi * z));
     g[2] += -2 * PI_ * erf(xi * z);
+    H[5] -= 4 * sp * xi * exp(-xi * xi * z * z);
     *pot = p;
     for (int k = 0; k < 3; k++) grad[k] = g[k];
+    if (hess)
+        for (int k = 0; k < 6; k++) hess[k] = H[k];
 }
+
+static void ewald2_laplace(const double r0[3], double *pot, double grad[3]) { ewald2_laplace_h(r0, pot, grad, NULL); }
 
 static void ewald2_stokes(const double r0[3], double G[3][3]) {
     const double xi = XI2D, xi2 = xi * xi, z = r0[2], sp = sqrt(PI_);
@@ -635,21 +792,29 @@ static void ewald2_stokes(const double r0[3], double G[3][3]) {
 
 /* out += doubly periodic sum, per pair (O(ntrg nsrc)).
  * kind 0: q (1) -> potential, gradient (4); kind 1: f (3) -> velocity (3);
- * kind 2: (f, trD) (4) -> (pressure, velocity) (4) of stokes_pvel. */
+ * kind 2: (f, trD) (4) -> (pressure, velocity) (4) of stokes_pvel;
+ * kind 3: q (1) -> potential, gradient, Hessian (10). */
 int oracle_ewald2d(int kind, int nsrc, const double *src, const double *val, int ntrg, const double *trg,
                    double *out, int nthreads) {
-    if (kind < 0 || kind > 2 || nsrc < 0 || ntrg < 0) return 1;
-    const int sd = kind == 0 ? 1 : kind == 1 ? 3 : 4, td = kind == 1 ? 3 : 4;
+    if (kind < 0 || kind > 3 || nsrc < 0 || ntrg < 0) return 1;
+    const int sd = kind == 0 || kind == 3 ? 1 : kind == 1 ? 3 : 4, td = kind == 3 ? 10 : kind == 1 ? 3 : 4;
     nthreads = clamp_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
     for (int t = 0; t < ntrg; t++) {
-        double acc[4] = {0, 0, 0, 0};
+        double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int j = 0; j < nsrc; j++) {
             double r[3];
             for (int k = 0; k < 3; k++) r[k] = trg[3 * (size_t)t + k] - src[3 * (size_t)j + k];
             r[0] -= floor(r[0] + 0.5);
             r[1] -= floor(r[1] + 0.5);
             const double *v = val + (size_t)sd * j;
+            if (kind == 3) {
+                double pot, g[3], h[6];
+                ewald2_laplace_h(r, &pot, g, h);
+                acc[0] += v[0] * pot / (4 * PI_);
+                for (int k = 0; k < 3; k++) acc[1 + k] += v[0] * g[k] / (4 * PI_);
+                for (int k = 0; k < 6; k++) acc[4 + k] += v[0] * h[k] / (4 * PI_);
+            }
             if (kind == 0 || kind == 2) {
                 double pot, g[3];
                 ewald2_laplace(r, &pot, g);

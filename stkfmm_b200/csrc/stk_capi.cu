@@ -348,3 +348,7 @@ STK_KER_SHIM(stk_ulapu, UK_STK_ULAPU)
 STK_KER_SHIM(stokes_regvel, UK_STOKES_REGVEL)
 STK_KER_SHIM(stokes_pvel, UK_STOKES_PVEL)
 STK_KER_SHIM(stokes_doublepvel, UK_STOKES_DOUBLEPVEL)
+STK_KER_SHIM(laplace_pgradgrad, UK_LAPLACE_PGRADGRAD)
+STK_KER_SHIM(laplace_dipolepgradgrad, UK_LAPLACE_DIPOLEPGRADGRAD)
+STK_KER_SHIM(laplace_quadp, UK_LAPLACE_QUADP)
+STK_KER_SHIM(laplace_quadpgradgrad, UK_LAPLACE_QUADPGRADGRAD)

@@ -47,8 +47,17 @@ static const KernelInfo kKernels[] = {
      {UK_LAPLACE_PGRAD, UK_LAPLACE_DIPOLEPGRAD, UK_LAPLACE_P, UK_LAPLACE_DIPOLEP, UK_LAPLACE_P, UK_LAPLACE_PGRAD,
       UK_LAPLACE_PGRAD, UK_LAPLACE_P, UK_LAPLACE_DIPOLEP},
      {1, 2, 2, 2}, 0},
-    {2, "laplace_PGradGrad", 1, 3, 10, {-1, -1, -1, -1, -1, -1, -1, -1, -1}, {1, 2, 2, 2, 3, 3, 3, 3, 3, 3}, 0},
-    {4, "laplace_QPGradGrad", 9, 12, 10, {-1, -1, -1, -1, -1, -1, -1, -1, -1}, {3, 4, 4, 4, 5, 5, 5, 5, 5, 5}, 0},
+    // LaplaceLayerKernel<T>::PGradGrad (Lib/include/STKFMM/LaplaceLayerKernel.hpp:328-341)
+    {2, "laplace_PGradGrad", 1, 3, 10,
+     {UK_LAPLACE_PGRADGRAD, UK_LAPLACE_DIPOLEPGRADGRAD, UK_LAPLACE_P, UK_LAPLACE_DIPOLEP, UK_LAPLACE_P,
+      UK_LAPLACE_PGRADGRAD, UK_LAPLACE_PGRADGRAD, UK_LAPLACE_P, UK_LAPLACE_DIPOLEP},
+     {1, 2, 2, 2, 3, 3, 3, 3, 3, 3}, 0},
+    // LaplaceLayerKernel<T>::QPGradGrad (LaplaceLayerKernel.hpp:343-356): no double layer;
+    // quadrupole sources for S2T / S2M / S2L, laplace_pgradgrad for M2T / L2T
+    {4, "laplace_QPGradGrad", 9, 12, 10,
+     {UK_LAPLACE_QUADPGRADGRAD, -1, UK_LAPLACE_QUADP, -1, UK_LAPLACE_P, UK_LAPLACE_PGRADGRAD, UK_LAPLACE_PGRADGRAD,
+      UK_LAPLACE_QUADP, -1},
+     {3, 4, 4, 4, 5, 5, 5, 5, 5, 5}, 0},
     {8, "stokes_vel", 3, 6, 3,
      {UK_STOKES_VEL, -1, UK_STOKES_VEL, -1, UK_STOKES_VEL, UK_STOKES_VEL, UK_STOKES_VEL, UK_STOKES_VEL, -1},
      {1, 1, 1}, 0},

@@ -437,6 +437,10 @@ cudaError_t launch_list_p2p(int uk, int prec, const ListP2PArgs &a, int num_sms,
     case UK_LAPLACE_SLDL_PGRAD: return launch_prec<UK_LAPLACE_SLDL_PGRAD>(prec, a, num_sms, stream);
     case UK_STOKES_SLDL_PVEL: return launch_prec<UK_STOKES_SLDL_PVEL>(prec, a, num_sms, stream);
     case UK_LAPLACE_SLDL_P: return launch_prec<UK_LAPLACE_SLDL_P>(prec, a, num_sms, stream);
+    case UK_LAPLACE_PGRADGRAD: return launch_prec<UK_LAPLACE_PGRADGRAD>(prec, a, num_sms, stream);
+    case UK_LAPLACE_DIPOLEPGRADGRAD: return launch_prec<UK_LAPLACE_DIPOLEPGRADGRAD>(prec, a, num_sms, stream);
+    case UK_LAPLACE_QUADP: return launch_prec<UK_LAPLACE_QUADP>(prec, a, num_sms, stream);
+    case UK_LAPLACE_QUADPGRADGRAD: return launch_prec<UK_LAPLACE_QUADPGRADGRAD>(prec, a, num_sms, stream);
     case UK_REGVEL_ADJ_SRC:
         if (!a.trg_aux) return cudaErrorInvalidValue;
         return launch_prec<UK_REGVEL_ADJ_SRC>(prec, a, num_sms, stream);

@@ -30,6 +30,10 @@
 //   stokes_regvel        Lib/include/STKFMM/StokesRegSingleLayerKernel.hpp:17-41
 //   stokes_pvel          Lib/include/STKFMM/StokesSingleLayerKernel.hpp:27-47
 //   stokes_doublepvel    Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:25-57
+//   laplace_pgradgrad    Lib/include/STKFMM/LaplaceLayerKernel.hpp:138-166
+//   laplace_dipolepgradgrad Lib/include/STKFMM/LaplaceLayerKernel.hpp:168-200
+//   laplace_quadp        Lib/include/STKFMM/LaplaceLayerKernel.hpp:202-232
+//   laplace_quadpgradgrad Lib/include/STKFMM/LaplaceLayerKernel.hpp:234-301
 // Two fused variants (no single reference function) evaluate a single-layer
 // and a double-layer source at the same point in one pass:
 //   laplace_pgrad + laplace_dipolepgrad, stokes_pvel + stokes_doublepvel.
@@ -117,7 +121,11 @@ enum UkId : int {
     UK_REGVEL_ADJ_SRC = 13,      // adjoint of stokes_regvel, source side (see below)
     UK_REGVEL_ADJ_TRG = 14,      // adjoint of stokes_regvel, target positions
     UK_LAPLACE_SLDL_P = 15,      // values (q, d0, d1, d2): laplace_p + laplace_dipolep (S2M / S2L)
-    UK_COUNT = 16
+    UK_LAPLACE_PGRADGRAD = 16,
+    UK_LAPLACE_DIPOLEPGRADGRAD = 17,
+    UK_LAPLACE_QUADP = 18,
+    UK_LAPLACE_QUADPGRADGRAD = 19,
+    UK_COUNT = 20
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
@@ -562,6 +570,155 @@ template <> struct Uk<UK_LAPLACE_SLDL_P> {
     }
 };
 
+// Second derivatives: outputs (p, grad p, H_xx, H_xy, H_xz, H_yy, H_yz, H_zz).
+
+// laplace_pgradgrad: p = q/r, grad p = -q r / r^3,
+// H = q (3 r r^T - r^2 I) / r^5 = 3 q r r^T / r^5 + (grad p / r) I.  staged (q, -q, 3q)
+template <> struct Uk<UK_LAPLACE_PGRADGRAD> {
+    static constexpr int SDIM = 1, TDIM = 10, NV = 3;
+    static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = f[0];
+        v[1] = -f[0];
+        v[2] = 3.0 * f[0];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        u[0] = fmav(v[0], rinv, u[0]);
+        V w = v[1] * rinv3;  // -q / r^3
+        u[1] = fmav(w, dx, u[1]);
+        u[2] = fmav(w, dy, u[2]);
+        u[3] = fmav(w, dz, u[3]);
+        V s3 = (v[2] * rinv3) * rinv2;  // 3 q / r^5
+        V sx = s3 * dx, sy = s3 * dy;
+        u[4] = fmav(sx, dx, u[4] + w);
+        u[5] = fmav(sx, dy, u[5]);
+        u[6] = fmav(sx, dz, u[6]);
+        u[7] = fmav(sy, dy, u[7] + w);
+        u[8] = fmav(sy, dz, u[8]);
+        u[9] = fmav(s3 * dz, dz, u[9] + w);
+    }
+};
+
+// laplace_dipolepgradgrad, A = (d.r)/r^2:
+//   p = (d.r)/r^3, grad p = (d - 3 A r) / r^3,
+//   H_kl = (15 A r_k r_l - 3 (r_k d_l + r_l d_k)) / r^5 - 3 A d_kl / r^3
+//        = (r_k h_l + r_l h_k) / r^5 - 3 A d_kl / r^3  with h = 7.5 A r - 3 d.   staged (d, -3d)
+template <> struct Uk<UK_LAPLACE_DIPOLEPGRADGRAD> {
+    static constexpr int SDIM = 3, TDIM = 10, NV = 6;
+    static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        for (int k = 0; k < 3; k++) {
+            v[k] = f[k];
+            v[3 + k] = -3.0 * f[k];
+        }
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V rdn = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        V A = rdn * rinv2;
+        u[0] = fmav(rdn, rinv3, u[0]);
+        V nA = A * cst<V>(-3.0);
+        u[1] = fmav(fmav(nA, dx, v[0]), rinv3, u[1]);
+        u[2] = fmav(fmav(nA, dy, v[1]), rinv3, u[2]);
+        u[3] = fmav(fmav(nA, dz, v[2]), rinv3, u[3]);
+        V c = rinv3 * rinv2;
+        V a75 = A * cst<V>(7.5);
+        V hx = fmav(a75, dx, v[3]) * c, hy = fmav(a75, dy, v[4]) * c, hz = fmav(a75, dz, v[5]) * c;
+        V dg = nA * rinv3;
+        u[4] = fmav(dx + dx, hx, u[4] + dg);
+        u[5] = fmav(dx, hy, fmav(dy, hx, u[5]));
+        u[6] = fmav(dx, hz, fmav(dz, hx, u[6]));
+        u[7] = fmav(dy + dy, hy, u[7] + dg);
+        u[8] = fmav(dy, hz, fmav(dz, hy, u[8]));
+        u[9] = fmav(dz + dz, hz, u[9] + dg);
+    }
+};
+
+// laplace_quadp: p = (3 r^T S r - r^2 tr S) / r^5 (only the symmetric part of S
+// enters).  staged symmetric parts (3 S00, 3 S11, 3 S22, 3 (S01+S10), 3 (S02+S20),
+// 3 (S12+S21), -tr S)
+template <> struct Uk<UK_LAPLACE_QUADP> {
+    static constexpr int SDIM = 9, TDIM = 1, NV = 7;
+    static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = 3.0 * f[0];
+        v[1] = 3.0 * f[4];
+        v[2] = 3.0 * f[8];
+        v[3] = 3.0 * (f[1] + f[3]);
+        v[4] = 3.0 * (f[2] + f[6]);
+        v[5] = 3.0 * (f[5] + f[7]);
+        v[6] = -(f[0] + f[4] + f[8]);
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rr3 = Uk<UK_STOKES_DOUBLEPVEL>::rdr(dx, dy, dz, v);  // 3 r^T S r
+        u[0] = fmav(fmav(rr3, rinv2, v[6]), rinv2 * rinv, u[0]);
+    }
+};
+
+// laplace_quadpgradgrad, with P the symmetric part of S, g = P r, m = r^T P r / r^2,
+// t = tr S and gamma = 3 t - 15 m (p = S_ij d_i d_j (1/r) and its derivatives):
+//   p = (3 m - t) / r^3,  grad p = (gamma r + 6 g) / r^5,
+//   H_kl = (r_k h_l + r_l h_k + gamma d_kl + 6 P_kl) / r^5,
+//   h = ((52.5 m - 7.5 t) r - 30 g) / r^2.
+// staged (6 P00, 6 P11, 6 P22, 6 P01, 6 P02, 6 P12, 3 t, -t)
+template <> struct Uk<UK_LAPLACE_QUADPGRADGRAD> {
+    static constexpr int SDIM = 9, TDIM = 10, NV = 8;
+    static constexpr double SCALE = kInv4Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = 6.0 * f[0];
+        v[1] = 6.0 * f[4];
+        v[2] = 6.0 * f[8];
+        v[3] = 3.0 * (f[1] + f[3]);
+        v[4] = 3.0 * (f[2] + f[6]);
+        v[5] = 3.0 * (f[5] + f[7]);
+        const double t = f[0] + f[4] + f[8];
+        v[6] = 3.0 * t;
+        v[7] = -t;
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c = rinv3 * rinv2;
+        // g6 = 6 P r
+        V gx = fmav(v[0], dx, fmav(v[3], dy, v[4] * dz));
+        V gy = fmav(v[3], dx, fmav(v[1], dy, v[5] * dz));
+        V gz = fmav(v[4], dx, fmav(v[5], dy, v[2] * dz));
+        V m15 = (fmav(gx, dx, fmav(gy, dy, gz * dz)) * rinv2) * cst<V>(2.5);  // 15 m
+        u[0] = fmav(fmav(m15, cst<V>(0.2), v[7]), rinv3, u[0]);
+        V gam = v[6] - m15;
+        u[1] = fmav(fmav(gam, dx, gx), c, u[1]);
+        u[2] = fmav(fmav(gam, dy, gy), c, u[2]);
+        u[3] = fmav(fmav(gam, dz, gz), c, u[3]);
+        V ah = fmav(m15, cst<V>(3.5), v[6] * cst<V>(-2.5));  // 52.5 m - 7.5 t
+        V cr = c * rinv2;
+        V hx = fmav(ah, dx, gx * cst<V>(-5.0)) * cr;
+        V hy = fmav(ah, dy, gy * cst<V>(-5.0)) * cr;
+        V hz = fmav(ah, dz, gz * cst<V>(-5.0)) * cr;
+        u[4] = fmav(dx + dx, hx, fmav(gam + v[0], c, u[4]));
+        u[5] = fmav(dx, hy, fmav(dy, hx, fmav(v[3], c, u[5])));
+        u[6] = fmav(dx, hz, fmav(dz, hx, fmav(v[4], c, u[6])));
+        u[7] = fmav(dy + dy, hy, fmav(gam + v[1], c, u[7]));
+        u[8] = fmav(dy, hz, fmav(dz, hy, fmav(v[5], c, u[8])));
+        u[9] = fmav(dz + dz, hz, fmav(gam + v[2], c, u[9]));
+    }
+};
+
 // Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
@@ -569,7 +726,8 @@ __host__ __device__ constexpr int uk_sdim(int id) {
          : id == UK_RPY_ULAPU ? 4 : id == UK_STK_ULAPU ? 3 : id == UK_STOKES_REGVEL ? 4
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 9 : id == UK_LAPLACE_SLDL_PGRAD ? 4
          : id == UK_STOKES_SLDL_PVEL ? 13 : id == UK_REGVEL_ADJ_SRC ? 3 : id == UK_REGVEL_ADJ_TRG ? 4
-         : id == UK_LAPLACE_SLDL_P ? 4 : 0;
+         : id == UK_LAPLACE_SLDL_P ? 4 : id == UK_LAPLACE_PGRADGRAD ? 1 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 3
+         : id == UK_LAPLACE_QUADP ? 9 : id == UK_LAPLACE_QUADPGRADGRAD ? 9 : 0;
 }
 __host__ __device__ constexpr int uk_tdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 4 : id == UK_LAPLACE_DIPOLEP ? 1
@@ -577,14 +735,15 @@ __host__ __device__ constexpr int uk_tdim(int id) {
          : id == UK_RPY_ULAPU ? 6 : id == UK_STK_ULAPU ? 6 : id == UK_STOKES_REGVEL ? 3
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 4 : id == UK_LAPLACE_SLDL_PGRAD ? 4
          : id == UK_STOKES_SLDL_PVEL ? 4 : id == UK_REGVEL_ADJ_SRC ? 7 : id == UK_REGVEL_ADJ_TRG ? 3
-         : id == UK_LAPLACE_SLDL_P ? 1 : 0;
+         : id == UK_LAPLACE_SLDL_P ? 1 : id == UK_LAPLACE_PGRADGRAD ? 10 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 10
+         : id == UK_LAPLACE_QUADP ? 1 : id == UK_LAPLACE_QUADPGRADGRAD ? 10 : 0;
 }
 // per-output-point (target-side) values a micro-kernel reads
 __host__ __device__ constexpr int uk_tvdim(int id) {
     return id == UK_REGVEL_ADJ_SRC ? 4 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
 }
 __host__ __device__ constexpr double uk_scale(int id) {
-    return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD || id == UK_LAPLACE_SLDL_P ? kInv4Pi
+    return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD || id >= UK_LAPLACE_SLDL_P ? kInv4Pi
                                                                                                 : kInv8Pi;
 }
 

@@ -75,9 +75,14 @@ class UKERNEL(enum.IntEnum):
     REGVEL_ADJ_SRC = 13  # adjoint of stokes_regvel: (dL/df, dL/deps, dL/dx) at the sources
     REGVEL_ADJ_TRG = 14  # adjoint of stokes_regvel: dL/dx at the targets
     LAPLACE_SLDL_P = 15  # laplace_p + laplace_dipolep at one point (fused S2M / S2L)
+    LAPLACE_PGRADGRAD = 16
+    LAPLACE_DIPOLEPGRADGRAD = 17
+    LAPLACE_QUADP = 18
+    LAPLACE_QUADPGRADGRAD = 19
 
 
-SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.Stokes, KERNEL.RPY, KERNEL.StokesRegVel, KERNEL.PVel)
+SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.LapPGradGrad, KERNEL.LapQPGradGrad, KERNEL.Stokes, KERNEL.RPY,
+                     KERNEL.StokesRegVel, KERNEL.PVel)
 
 
 def _arr(a, cols=None, name="array"):

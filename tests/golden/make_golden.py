@@ -36,6 +36,9 @@ CASES = {
     "StokesRegSLVel": O.REF_STOKES_REG_SL_VEL,
     "StokesSLPVel": O.REF_STOKES_SL_PVEL,
     "StokesDLPVel": O.REF_STOKES_DL_PVEL,
+    "LaplaceSLPGradGrad": O.REF_LAP_SL_PGRADGRAD,
+    "LaplaceDLPGradGrad": O.REF_LAP_DL_PGRADGRAD,
+    "LaplaceQPGradGrad": O.REF_LAP_QPGRADGRAD,
 }
 EPS = 1e-2
 

@@ -52,7 +52,11 @@ def test_kernel_descriptors_match_reference():
     assert [S.kernel_slot(1, s) for s in range(9)] == [1, 3, 0, 2, 0, 1, 1, 0, 2]
     # StokesRegVel (StokesRegSingleLayerKernel.hpp:211-218)
     assert [S.kernel_slot(32, s) for s in range(9)] == [8, -1, 8, -1, 4, 4, 4, 8, -1]
+    # LapPGradGrad (LaplaceLayerKernel.hpp:328-341), LapQPGradGrad (LaplaceLayerKernel.hpp:343-356)
+    assert [S.kernel_slot(2, s) for s in range(9)] == [16, 17, 0, 2, 0, 16, 16, 0, 2]
+    assert [S.kernel_slot(4, s) for s in range(9)] == [19, -1, 18, -1, 0, 16, 16, 18, -1]
     assert S.ukernel_dims(S.UKERNEL.STOKES_SLDL_PVEL) == (13, 4)
+    assert S.ukernel_dims(S.UKERNEL.LAPLACE_QUADPGRADGRAD) == (9, 10)
 
 
 def test_status_strings():

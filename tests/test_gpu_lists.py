@@ -156,7 +156,7 @@ def handle_case(kernel, n, pbc=0, max_pts=64, seed=0, origin=(0.0, 0.0, 0.0), bo
     return pts, (dl if has_dl else None), slv, dlv, td
 
 
-@pytest.mark.parametrize("kernel", [1, 8, 16, 32, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128])
 @pytest.mark.parametrize("prec", [0, 1])
 def test_handle_evaluate_near(torch_cuda, kernel, prec):
     """Stk3DFMM_evaluate_near against the oracle on the handle's own U-list (SL and DL)."""
@@ -184,7 +184,7 @@ def test_handle_evaluate_near(torch_cuda, kernel, prec):
     assert st["u_pairs_sl"] > 0 and st["u_entries"] == len(u["list_ent"])
 
 
-@pytest.mark.parametrize("kernel", [1, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 128])
 def test_handle_separate_dl_points(torch_cuda, kernel):
     """SL and DL at different points: separate (unfused) passes."""
     import stkfmm_b200 as S
@@ -205,7 +205,7 @@ def test_handle_separate_dl_points(torch_cuda, kernel):
     assert rel_l2(out, ref) < 1e-12
 
 
-@pytest.mark.parametrize("kernel", [1, 16, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 16, 128])
 def test_handle_box_scaling(torch_cuda, kernel):
     """A box (origin o, length L) gives sF^k times the unit-box result (scaleSrc / scaleTrg)."""
     import stkfmm_b200 as S
@@ -231,7 +231,8 @@ def test_handle_box_scaling(torch_cuda, kernel):
     b = np.zeros((len(pts), td))
     unit.evaluate_near(kernel, slv, a, dlv)
     big.evaluate_near(kernel, slv_big, b, dlv_big)
-    pows = {1: [1, 2, 2, 2], 16: [1, 1, 1, 3, 3, 3], 128: [2, 1, 1, 1]}[kernel]
+    pows = {1: [1, 2, 2, 2], 2: [1, 2, 2, 2, 3, 3, 3, 3, 3, 3], 4: [3, 4, 4, 4, 5, 5, 5, 5, 5, 5],
+            16: [1, 1, 1, 3, 3, 3], 128: [2, 1, 1, 1]}[kernel]
     assert rel_l2(b, a * sf ** np.array(pows)) < 1e-12
 
 

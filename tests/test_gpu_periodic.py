@@ -172,7 +172,7 @@ def test_periodic_translation(torch_cuda):
     assert max(component_errors(b - d, a)) < TOL[10]
 
 
-@pytest.mark.parametrize("kernel", [1, 8, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 128])
 def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     """PX: sources without net charge / force, dipole or quadrupole (alternating
     signs on the corners of small cubes) against the direct sum over their
@@ -184,7 +184,8 @@ def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     sg = np.array(list(itertools.product([-1, 1], [-1, 1], [-1, 1])), dtype=np.float64)
     src = np.concatenate([ci + 0.03 * sg for ci in c])
     s = np.tile(sg.prod(1), 16)[:, None]
-    val = {1: s, 8: s * np.array([[0.3, -0.2, 0.5]]),
+    quad = s * np.array([[0.4, 0.1, -0.3, 0.2, -0.5, 0.3, 0.1, 0.6, 0.2]])
+    val = {1: s, 2: s, 4: quad, 8: s * np.array([[0.3, -0.2, 0.5]]),
            128: np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)}[kernel]
     trg = rng.random((1500, 3)) * 0.999
     fmm = S.Stk3DFMM(10, 32, S.PAXIS.PX, kernel)
@@ -201,3 +202,39 @@ def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     ref = O.direct(uk, imgs, np.tile(val, (len(sh), 1)), trg)
     errs = component_errors(out, ref)
     assert max(errs) < TOL[10], errs
+
+
+@pytest.mark.parametrize("pbc", [2, 3])
+def test_periodic_laplace_hessian(torch_cuda, pbc):
+    """LapPGradGrad (potential, gradient, Hessian) against the oracle's Ewald
+    sums with the Hessian (PXYZ potential compared with the mean removed)."""
+    pts, rng = points("clustered", 3000, 13 + pbc)
+    q = rng.uniform(-0.5, 0.5, (len(pts), 1))
+    q -= q.mean()
+    out = periodic_fmm_pbc(2, pbc, 10, 50, pts, q)
+    ref = (O.ewald if pbc == 3 else O.ewald2d)(O.EWALD_LAPLACE_HESS, pts, q, pts)
+    if pbc == 3:
+        out[:, 0] -= out[:, 0].mean()
+        ref[:, 0] -= ref[:, 0].mean()
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+
+
+@pytest.mark.parametrize("pbc", [2, 3])
+def test_periodic_quadrupole_potential(torch_cuda, pbc):
+    """LapQPGradGrad's potential S : grad grad G summed over the periodic images,
+    from the oracle's Ewald Hessians (one sum per symmetric component of S; the
+    PXYZ potential compared with the mean removed)."""
+    pts, rng = points("clustered", 2000, 15 + pbc)
+    S = rng.uniform(-1, 1, (len(pts), 9))
+    out = periodic_fmm_pbc(4, pbc, 10, 50, pts, S)
+    ew = O.ewald if pbc == 3 else O.ewald2d
+    ref = np.zeros(len(pts))
+    for col, (i, j) in enumerate(((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))):
+        w = S[:, 3 * i + j] + (S[:, 3 * j + i] if i != j else 0.0)
+        ref += ew(O.EWALD_LAPLACE_HESS, pts, w[:, None], pts)[:, 4 + col]
+    pot = out[:, 0].copy()
+    if pbc == 3:
+        pot -= pot.mean()
+        ref -= ref.mean()
+    assert np.linalg.norm(pot - ref) / np.linalg.norm(ref) < TOL[10]

@@ -28,6 +28,9 @@ def test_oracle_matches_golden(name):
     (O.REF_STOKES_REG_SL_VEL, O.UK_STOKES_REGVEL, slice(0, 3)),
     (O.REF_STOKES_SL_PVEL, O.UK_STOKES_PVEL, slice(0, 4)),
     (O.REF_STOKES_DL_PVEL, O.UK_STOKES_DOUBLEPVEL, slice(0, 4)),
+    (O.REF_LAP_SL_PGRADGRAD, O.UK_LAPLACE_PGRADGRAD, slice(0, 10)),
+    (O.REF_LAP_DL_PGRADGRAD, O.UK_LAPLACE_DIPOLEPGRADGRAD, slice(0, 10)),
+    (O.REF_LAP_QPGRADGRAD, O.UK_LAPLACE_QUADPGRADGRAD, slice(0, 10)),
 ])
 def test_oracle_matches_live_reference(which, uk, osl, rng):
     """Fresh random inputs (clustered, with coincident points) through the compiled reference."""
@@ -230,3 +233,39 @@ def test_ewald2d_matches_image_sums(kind):
     imgs = (src[None] + sh[:, None]).reshape(-1, 3)
     d = O.direct(uk, imgs, np.tile(val, (len(sh), 1)), trg)
     assert np.abs(d - ew).max() < 1e-6 * np.abs(ew).max()
+
+
+@pytest.mark.parametrize("fn", ["ewald", "ewald2d"])
+def test_ewald_laplace_hessian(fn):
+    """Potential, gradient and Hessian of the periodic Laplace sums: the Hessian
+    equals central differences of the gradient, its trace vanishes for neutral
+    charges, and at a target on a source (self image removed) it is the limit of
+    the full sum minus that source's own singular Hessian."""
+    f = getattr(O, fn)
+    rng = np.random.default_rng(34)
+    src = rng.random((40, 3))
+    q = rng.uniform(-1, 1, (40, 1))
+    q -= q.mean()
+    trg = rng.random((30, 3))
+    H = f(O.EWALD_LAPLACE_HESS, src, q, trg)
+    assert np.array_equal(H[:, :4], f(O.EWALD_LAPLACE, src, q, trg))
+    h = 1e-5
+    fd = np.zeros((len(trg), 3, 3))
+    for a in range(3):
+        e = np.zeros(3)
+        e[a] = h
+        fd[:, a] = (f(O.EWALD_LAPLACE, src, q, trg + e)[:, 1:4] - f(O.EWALD_LAPLACE, src, q, trg - e)[:, 1:4]) / (2 * h)
+    hm = np.stack([fd[:, i, j] for i, j in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))], 1)
+    scale = np.abs(hm).max()
+    assert np.abs(H[:, 4:] - hm).max() < 1e-7 * scale
+    assert np.abs(H[:, 4] + H[:, 7] + H[:, 9]).max() < 1e-12 * scale
+    # self image: second-order convergence of the symmetric limit
+    t0 = src[:5]
+    H0 = f(O.EWALD_LAPLACE_HESS, src, q, t0)[:, 4:]
+    errs = []
+    for s in (1e-3, 5e-4):
+        d = np.array([1.0, -0.7, 0.5]) * s
+        avg = 0.5 * (f(O.EWALD_LAPLACE_HESS, src, q, t0 + d) + f(O.EWALD_LAPLACE_HESS, src, q, t0 - d))[:, 4:]
+        sing = O.direct(O.UK_LAPLACE_PGRADGRAD, np.zeros((1, 3)), np.ones((1, 1)), d[None])[0, 4:]
+        errs.append(np.abs(avg - q[:5] * sing[None] - H0).max() / np.abs(H0).max())
+    assert errs[0] < 1e-3 and 3.0 < errs[0] / errs[1] < 5.0, errs
