@@ -190,8 +190,9 @@ int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:26 (not declared in the reference header) */
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
- * KIFMM far field, for LapPGrad, Stokes, RPY, StokesRegVel and PVel in free
- * space, PX, PXY and PXYZ; the other kernels return STK_ERR_NOT_SUPPORTED.
+ * KIFMM far field, for LapPGrad, LapPGradGrad, LapQPGradGrad, Stokes, RPY,
+ * StokesRegVel and PVel in free space, PX, PXY and PXYZ; the other kernels
+ * return STK_ERR_NOT_SUPPORTED.
  * Triply periodic potentials / pressures / mean velocities carry a constant
  * per component (drift) set by the equivalent density, as in the reference. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
@@ -251,6 +252,45 @@ int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
 int Stk3DFMM_get_ulist(Stk3DFMM *fmm, unsigned kernel, int *sizes, int *trg_begin, int *trg_end, int *list_off,
                        int *list_ent, int *sl_begin, int *sl_end, int *dl_begin, int *dl_end, int *sl_perm,
                        int *dl_perm, int *trg_perm);
+
+/* ---- StkWallFMM handle (STKFMM.h:19-35, Stk3DFMM-c.cpp:37-67) ---------------
+ * Stokeslets (Stokes, 3 values -> u 3) or RPY spheres (RPY, (f, b) -> (u, lap u))
+ * above a no-slip wall at z = origin_z; points lie in [o, o+L)^2 x [o_z, o_z+L/2).
+ * Each evaluation combines sub-FMMs of the sources and their mirror images
+ * (Stokes, LapPGrad, LapPGradGrad; RPY, LapPGradGrad, LapPGrad, LapQPGradGrad),
+ * StkWallFMM.cpp:154-292.  Free space, PX or PXY. */
+typedef struct StkWallFMM StkWallFMM;
+/* Stk3DFMM-c.cpp:37-39; NULL for pbc = PXYZ, without Stokes or RPY in kernelComb,
+ * on invalid arguments or when no device */
+StkWallFMM *StkWallFMM_create(int mult_order, int max_pts, int pbc, unsigned kernelComb);
+/* Stk3DFMM-c.cpp:41-43 */
+void StkWallFMM_destroy(StkWallFMM *fmm);
+/* Stk3DFMM-c.cpp:45-48; double-layer points are ignored, as in the reference.
+ * STK_ERR_OUT_OF_BOX for a point outside [o, o+L)^2 x [o_z, o_z+L/2) on a free axis */
+int StkWallFMM_set_points(StkWallFMM *fmm, const int nSL, double *src_SL_coord, const int nTrg, double *trg_coord,
+                          const int nDL, double *src_DL_coord);
+/* Stk3DFMM-c.cpp:50-52 */
+int StkWallFMM_get_kernel_dimension(unsigned kernel, int *dims);
+/* Stk3DFMM-c.cpp:54 */
+int StkWallFMM_set_box(StkWallFMM *fmm, double *origin, double len);
+/* Stk3DFMM-c.cpp:56; STK_ERR_NOT_SUPPORTED for kernels other than Stokes and RPY */
+int StkWallFMM_setup_tree(StkWallFMM *fmm, unsigned kernel);
+/* Stk3DFMM-c.cpp:58 */
+int StkWallFMM_clear_fmm(StkWallFMM *fmm, unsigned kernel);
+/* Stk3DFMM-c.cpp:60-63: trg_value += wall FMM(sources) */
+int StkWallFMM_evaluate_fmm(StkWallFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
+                            double *trg_value, const int nDL, double *src_DL_value);
+/* Stk3DFMM-c.cpp:65-67 */
+int StkWallFMM_show_active_kernels(StkWallFMM *fmm);
+/* additions with no reference C counterpart: P2P precision of the Stokes / RPY
+ * sub-FMM (the Laplace sub-FMMs, whose terms cancel near the sources, stay FP64); the
+ * evaluation on device buffers in the caller's order queued on `stream` (null: the
+ * handle's stream; the first call after setup_tree builds the sub-FMMs' far-field
+ * operators and synchronises); device time (ms) of the last evaluation */
+int StkWallFMM_set_precision(StkWallFMM *fmm, int precision);
+int StkWallFMM_evaluate_fmm_device(StkWallFMM *fmm, unsigned kernel, const double *d_src_SL_value,
+                                   double *d_trg_value, void *stream);
+int StkWallFMM_last_kernel_ms(StkWallFMM *fmm, float *ms);
 
 /* ---- host-only octree (no CUDA call) ------------------------------------------
  * The tree and KIFMM lists that Stk3DFMM_setup_tree builds, in place of PVFMM's

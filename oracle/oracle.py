@@ -256,3 +256,110 @@ def ewald2d(kind: int, src, sval, trg, out=None, nthreads: int = 0):
     assert rc == 0
     return out
 
+
+
+# ---------------------------------------------------------------------------
+# No-slip wall image systems (StkWallFMM), restated over the oracle's sums.
+# The wall is the plane z = z0; every source at height y3 = z - z0 > 0 has an
+# image at z0 - y3.  The free-space sums are direct sums in physical units;
+# pbc = 2 (PXY, unit period in x and y) uses the doubly periodic Ewald sums.
+# ---------------------------------------------------------------------------
+def _mirror(src, z0):
+    img = np.array(src, dtype=np.float64, copy=True)
+    img[:, 2] = 2.0 * z0 - img[:, 2]
+    return img
+
+
+def _ewald2d_dipole(src, d, trg):
+    """Doubly periodic laplace_dipolepgrad sum: potential -d.grad G and gradient -d.grad grad G."""
+    out = np.zeros((len(trg), 4))
+    hidx = {(0, 0): 4, (0, 1): 5, (0, 2): 6, (1, 1): 7, (1, 2): 8, (2, 2): 9}
+    for k in range(3):
+        h = ewald2d(EWALD_LAPLACE_HESS, src, np.ascontiguousarray(d[:, k:k + 1]), trg)
+        out[:, 0] -= h[:, 1 + k]
+        for j in range(3):
+            out[:, 1 + j] -= h[:, hidx[(min(j, k), max(j, k))]]
+    return out
+
+
+def wall_stokes(src, f, trg, z0: float = 0.0, pbc: int = 0):
+    """Stokeslets above a no-slip wall: StkWallFMM::evalStokes (Lib/src/StkWallFMM.cpp:154-208).
+
+    Stokes sum of (fx, fy, 0) at the sources and (-fx, -fy, 0) at the images;
+    laplace_pgrad of charges -fz/2 (sources), +fz/2 (images) plus dipoles
+    (-y3 fx, -y3 fy, y3 fz) at the images; laplace_pgradgrad of charges fz y3
+    (sources), -fz y3 (images).  u_j = uS_j + uL2_{grad j} / 2 + x3 uL1D_{grad j},
+    u_z -= uL1D_pot, with x3 the target's height above the wall.
+    """
+    src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(f, dtype=np.float64).reshape(-1, 3)
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    n = len(src)
+    img = _mirror(src, z0)
+    s2 = np.concatenate([src, img])
+    y3 = src[:, 2] - z0
+    x3 = trg[:, 2] - z0
+    v_stk = np.zeros((2 * n, 3))
+    v_stk[:n, :2] = f[:, :2]
+    v_stk[n:, :2] = -f[:, :2]
+    v_l1 = np.concatenate([-0.5 * f[:, 2], 0.5 * f[:, 2]])[:, None]
+    v_d = np.stack([-y3 * f[:, 0], -y3 * f[:, 1], y3 * f[:, 2]], 1)
+    v_l2 = np.concatenate([f[:, 2] * y3, -f[:, 2] * y3])[:, None]
+    if pbc == 0:
+        u_s = direct(UK_STOKES_VEL, s2, v_stk, trg)
+        u_l1d = direct(UK_LAPLACE_PGRAD, s2, v_l1, trg) + direct(UK_LAPLACE_DIPOLEPGRAD, img, v_d, trg)
+        g_l2 = direct(UK_LAPLACE_PGRADGRAD, s2, v_l2, trg)[:, 1:4]
+    elif pbc == 2:
+        u_s = ewald2d(EWALD_STOKES, s2, v_stk, trg)
+        u_l1d = ewald2d(EWALD_LAPLACE, s2, v_l1, trg) + _ewald2d_dipole(img, v_d, trg)
+        g_l2 = ewald2d(EWALD_LAPLACE, s2, v_l2, trg)[:, 1:4]
+    else:
+        raise ValueError("pbc must be 0 or 2")
+    u = u_s + 0.5 * g_l2 + x3[:, None] * u_l1d[:, 1:4]
+    u[:, 2] -= u_l1d[:, 0]
+    return u
+
+
+def wall_rpy(src, fb, trg, z0: float = 0.0):
+    """RPY spheres above a no-slip wall: StkWallFMM::evalRPY (Lib/src/StkWallFMM.cpp:210-292),
+    free space.  fb rows (fx, fy, fz, b); output rows (u 3, lap u 3).
+
+    rpy_ulapu of (fx, fy, 0, b) at the sources and (-fx, -fy, 0, b) at the images;
+    SD: laplace_pgradgrad of charges -fz/2 (sources), +fz/2 (images) plus dipoles
+    (-y3 fx, -y3 fy, y3 fz) at the images; SDZ: laplace_pgrad of charges y3 fz / 2,
+    -y3 fz / 2 plus dipoles (0, 0, b^2 fz / 6) at sources and images; Q:
+    laplace_quadpgradgrad of S = 2 b^2 / 6 (fz e_xx + fz e_yy + fx e_zx + fy e_zy)
+    at the images.
+    """
+    src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+    fb = np.asarray(fb, dtype=np.float64).reshape(-1, 4)
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    n = len(src)
+    img = _mirror(src, z0)
+    s2 = np.concatenate([src, img])
+    y3 = src[:, 2] - z0
+    x3 = trg[:, 2] - z0
+    f1, f2, f3, b = fb[:, 0], fb[:, 1], fb[:, 2], fb[:, 3]
+    v_rpy = np.zeros((2 * n, 4))
+    v_rpy[:n, 0], v_rpy[:n, 1], v_rpy[:n, 3] = f1, f2, b
+    v_rpy[n:, 0], v_rpy[n:, 1], v_rpy[n:, 3] = -f1, -f2, b
+    v_ls = np.concatenate([-0.5 * f3, 0.5 * f3])[:, None]
+    v_ld = np.stack([-y3 * f1, -y3 * f2, y3 * f3], 1)
+    v_lsz = np.concatenate([0.5 * y3 * f3, -0.5 * y3 * f3])[:, None]
+    v_ldz = np.zeros((2 * n, 3))
+    v_ldz[:n, 2] = b * b * f3 / 6.0
+    v_ldz[n:, 2] = b * b * f3 / 6.0
+    q = np.zeros((n, 9))
+    tb = 2.0 * b * b / 6.0
+    q[:, 0], q[:, 4], q[:, 6], q[:, 7] = tb * f3, tb * f3, tb * f1, tb * f2
+    u_rpy = direct(UK_RPY_ULAPU, s2, v_rpy, trg)
+    sd = direct(UK_LAPLACE_PGRADGRAD, s2, v_ls, trg) + direct(UK_LAPLACE_DIPOLEPGRADGRAD, img, v_ld, trg)
+    sdz = direct(UK_LAPLACE_PGRAD, s2, v_lsz, trg) + direct(UK_LAPLACE_DIPOLEPGRAD, s2, v_ldz, trg)
+    qq = direct(UK_LAPLACE_QUADPGRADGRAD, img, q, trg)
+    u = np.zeros((len(trg), 6))
+    for j in range(3):
+        u[:, j] = u_rpy[:, j] + sdz[:, 1 + j] + x3 * sd[:, 1 + j] + x3 * qq[:, 1 + j]
+    u[:, 2] -= sd[:, 0] + qq[:, 0]
+    for j, h in ((3, 6), (4, 8), (5, 9)):
+        u[:, j] = u_rpy[:, j] + 2.0 * sd[:, h] + 2.0 * qq[:, h]
+    return u

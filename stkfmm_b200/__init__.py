@@ -7,9 +7,9 @@ entry points for device-resident data.
 """
 from ._lib import StkError, lib  # noqa: F401
 from .stkfmm import (KERNEL, PAXIS, PPKERNEL, PRECISION, SUPPORTED_KERNELS, UKERNEL, Octree,  # noqa: F401
-                     Stk3DFMM, device_count, evaluate_kernel, get_kernel_dimension, get_kernel_name, kernel_slot,
+                     Stk3DFMM, StkWallFMM, device_count, evaluate_kernel, get_kernel_dimension, get_kernel_name, kernel_slot,
                      ukernel_dims)
 
-__all__ = ["KERNEL", "PAXIS", "PPKERNEL", "PRECISION", "UKERNEL", "Stk3DFMM", "Octree", "StkError",
+__all__ = ["KERNEL", "PAXIS", "PPKERNEL", "PRECISION", "UKERNEL", "Stk3DFMM", "StkWallFMM", "Octree", "StkError",
            "evaluate_kernel", "get_kernel_dimension", "get_kernel_name", "kernel_slot", "ukernel_dims",
            "device_count", "lib", "SUPPORTED_KERNELS"]

@@ -68,6 +68,18 @@ SIGNATURES = [
     ("Stk3DFMM_last_launch_count", c_int, [c_void_p, c_uint, P_i]),
     ("Stk3DFMM_get_tree_stats", c_int, [c_void_p, c_uint, P_ll]),
     ("Stk3DFMM_get_ulist", c_int, [c_void_p, c_uint, P_i] + [P_i] * 11),
+    ("StkWallFMM_create", c_void_p, [c_int, c_int, c_int, c_uint]),
+    ("StkWallFMM_destroy", None, [c_void_p]),
+    ("StkWallFMM_set_points", c_int, [c_void_p, c_int, P_d, c_int, P_d, c_int, P_d]),
+    ("StkWallFMM_get_kernel_dimension", c_int, [c_uint, P_i]),
+    ("StkWallFMM_set_box", c_int, [c_void_p, P_d, c_double]),
+    ("StkWallFMM_setup_tree", c_int, [c_void_p, c_uint]),
+    ("StkWallFMM_clear_fmm", c_int, [c_void_p, c_uint]),
+    ("StkWallFMM_evaluate_fmm", c_int, [c_void_p, c_uint, c_int, P_d, c_int, P_d, c_int, P_d]),
+    ("StkWallFMM_show_active_kernels", c_int, [c_void_p]),
+    ("StkWallFMM_set_precision", c_int, [c_void_p, c_int]),
+    ("StkWallFMM_evaluate_fmm_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p]),
+    ("StkWallFMM_last_kernel_ms", c_int, [c_void_p, P_f]),
     ("stk_octree_build", c_void_p, [P_d, c_int, c_int, c_int, P_d, c_int, P_d, c_int, P_d, c_int]),
     ("stk_octree_free", None, [c_void_p]),
     ("stk_octree_sizes", c_int, [c_void_p, P_ll]),

@@ -207,6 +207,7 @@ extern "C" int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel) {
         pts = &fmm->sl;
     else if (ndl > nsl && ndl > ntrg)
         pts = &fmm->dl;
+    if (!fmm->tree_pts.empty()) pts = &fmm->tree_pts;
     Octree &T = kd->tree;
     std::string err = T.build(pts->data(), (int)(pts->size() / 3), fmm->max_pts, kMaxDepth, fmm->pbc);
     if (err.empty()) err = T.assign(0, fmm->sl.data(), nsl);

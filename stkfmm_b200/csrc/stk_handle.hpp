@@ -64,6 +64,10 @@ struct Stk3DFMM {
     bool points_set = false, sl_dl_same = false;
     int nsl = 0, ndl = 0, ntrg = 0;
     std::vector<double> sl, dl, trg;  // scaled, wrapped coordinates (caller's order)
+    // points that refine the octree in place of the largest of sl / dl / trg
+    // (FMMData::setupTree's custom tree points, FMMData.cpp:131-135); unit-box
+    // coordinates, set by composite FMMs (StkWallFMM), empty otherwise
+    std::vector<double> tree_pts;
     std::map<unsigned, std::unique_ptr<stk::KernelData>> pool;
     ~Stk3DFMM();
 };

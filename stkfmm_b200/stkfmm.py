@@ -280,6 +280,77 @@ class Stk3DFMM:
         return {k: out[k][:v] for k, v in arrs.items()}
 
 
+class StkWallFMM:
+    """B200 counterpart of PySTKFMM.StkWallFMM (Python/PySTKFMM.py:82-127): Stokeslets
+    (KERNEL.Stokes) or RPY spheres (KERNEL.RPY) above a no-slip wall at z = origin_z,
+    points in [o, o+L)^2 x [o_z, o_z+L/2); pbc NONE, PX or PXY."""
+
+    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64):
+        self.mult_order = int(mult_order)
+        self.max_pts = int(max_pts)
+        self.pbc = int(pbc)
+        self.kernels = int(kernels)
+        L = lib()
+        self.fmm = L.StkWallFMM_create(self.mult_order, self.max_pts, self.pbc, self.kernels)
+        if not self.fmm:
+            status = 6 if L.stk_device_count() <= 0 else 1
+            raise StkError(status, "StkWallFMM_create")
+        self.set_precision(precision)
+
+    def __del__(self):
+        f = getattr(self, "fmm", None)
+        if f:
+            lib().StkWallFMM_destroy(f)
+            self.fmm = None
+
+    def set_precision(self, precision):
+        check(lib().StkWallFMM_set_precision(self.fmm, int(precision)), "set_precision")
+        self.precision = PRECISION(precision)
+
+    def set_box(self, origin, length):
+        origin = _arr(origin).reshape(3)
+        check(lib().StkWallFMM_set_box(self.fmm, origin.ctypes.data_as(P_d), float(length)), "set_box")
+
+    def get_kernel_dimension(self, kernel):
+        return get_kernel_dimension(kernel)
+
+    def set_points(self, src_SL_coord, trg_coord, src_DL_coord=None):
+        sl = _arr(src_SL_coord, 3)
+        trg = _arr(trg_coord, 3)
+        dl = _arr(src_DL_coord, 3) if src_DL_coord is not None else np.zeros((0, 3))
+        check(lib().StkWallFMM_set_points(self.fmm, len(sl), _ptr(sl), len(trg), _ptr(trg), len(dl), _ptr(dl)),
+              "set_points")
+
+    def setup_tree(self, kernel):
+        check(lib().StkWallFMM_setup_tree(self.fmm, int(kernel)), "setup_tree")
+
+    def clear_fmm(self, kernel):
+        check(lib().StkWallFMM_clear_fmm(self.fmm, int(kernel)), "clear_fmm")
+
+    def show_active_kernels(self):
+        check(lib().StkWallFMM_show_active_kernels(self.fmm), "show_active_kernels")
+
+    def evaluate_fmm(self, kernel, src_SL_value, trg_value, src_DL_value=None):
+        sd, _, td = get_kernel_dimension(kernel)
+        slv = _arr(src_SL_value, sd)
+        if not (isinstance(trg_value, np.ndarray) and trg_value.dtype == np.float64 and trg_value.flags.c_contiguous):
+            raise TypeError("trg_value must be a C-contiguous float64 numpy array (accumulated in place)")
+        ntrg = trg_value.size // td if td else 0
+        check(lib().StkWallFMM_evaluate_fmm(self.fmm, int(kernel), len(slv), _ptr(slv), ntrg, _ptr(trg_value), 0,
+                                            None), "evaluate_fmm")
+        return trg_value
+
+    def evaluate_fmm_device(self, kernel, d_sl, d_trg, stream=None):
+        """evaluate_fmm on device pointers (ints) in the caller's order, queued on `stream`."""
+        check(lib().StkWallFMM_evaluate_fmm_device(self.fmm, int(kernel), d_sl, d_trg, stream),
+              "evaluate_fmm_device")
+
+    def last_kernel_ms(self) -> float:
+        ms = ctypes.c_float()
+        check(lib().StkWallFMM_last_kernel_ms(self.fmm, ctypes.byref(ms)), "last_kernel_ms")
+        return ms.value
+
+
 class Octree:
     """Host-only octree + KIFMM lists (no GPU needed); coordinates in [0,1)^3."""
 

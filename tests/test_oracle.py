@@ -269,3 +269,25 @@ def test_ewald_laplace_hessian(fn):
         sing = O.direct(O.UK_LAPLACE_PGRADGRAD, np.zeros((1, 3)), np.ones((1, 1)), d[None])[0, 4:]
         errs.append(np.abs(avg - q[:5] * sing[None] - H0).max() / np.abs(H0).max())
     assert errs[0] < 1e-3 and 3.0 < errs[0] / errs[1] < 5.0, errs
+
+
+@pytest.mark.parametrize("kind", ["stokes", "stokes_pxy", "rpy"])
+def test_wall_image_system_no_slip(kind):
+    """The restated wall image systems (StkWallFMM.cpp:154-292) give zero velocity
+    on the wall z = z0 (to rounding), free space and doubly periodic."""
+    rng = np.random.default_rng(35)
+    z0 = 0.25
+    src = rng.random((60, 3))
+    src[:, 2] = z0 + 0.05 + 0.4 * rng.random(60)
+    f = rng.normal(size=(60, 3))
+    bulk = rng.random((20, 3))
+    bulk[:, 2] = z0 + 0.5 * bulk[:, 2]
+    wall = rng.random((20, 3))
+    wall[:, 2] = z0
+    if kind == "rpy":
+        fb = np.concatenate([f, rng.uniform(1e-3, 5e-3, (60, 1))], 1)
+        uw, ub = O.wall_rpy(src, fb, wall, z0=z0)[:, :3], O.wall_rpy(src, fb, bulk, z0=z0)[:, :3]
+    else:
+        pbc = 2 if kind == "stokes_pxy" else 0
+        uw, ub = O.wall_stokes(src, f, wall, z0=z0, pbc=pbc), O.wall_stokes(src, f, bulk, z0=z0, pbc=pbc)
+    assert np.abs(uw).max() < 1e-13 * np.abs(ub).max()
