@@ -160,6 +160,109 @@ EXTRA_FMM = [
 ]
 
 
+# no-slip wall (StkWallFMM): sources = targets, 64 Gaussian clusters in x, y, heights in [0.01, 0.49]
+WALL_FMM = [
+    {"name": "wall_stokes_1m_clustered", "kernel": 8, "pbc": 0, "p": 8, "max_pts": 256, "n": 1048576,
+     "workload": "StkWallFMM Stokeslets above a no-slip wall (free space): 1,048,576 points in 64 Gaussian "
+                 "clusters (sigma 0.02, centres U[0.1,0.9]^3) with heights mapped to [0.01, 0.49] of the unit box "
+                 "(wall at z = 0), sources = targets, f ~ N(0,1)^3, p=8, max 256 pts/leaf, seed 0"},
+    {"name": "wall_rpy_1m_clustered", "kernel": 16, "pbc": 0, "p": 8, "max_pts": 256, "n": 1048576,
+     "workload": "StkWallFMM RPY spheres above a no-slip wall (free space): the same 1,048,576 points, f ~ N(0,1)^3, "
+                 "b ~ U(1e-4, 5e-4), p=8, max 256 pts/leaf, seed 0"},
+]
+
+
+def wall_inputs(cfg, seed):
+    rng = np.random.default_rng(seed)
+    n = cfg["n"]
+    c = rng.uniform(0.1, 0.9, size=(64, 3))
+    pts = c[rng.integers(0, 64, size=n)] + rng.normal(0.0, 0.02, size=(n, 3))
+    pts = np.clip(pts, 0.0, 0.999)
+    pts[:, 2] = 0.01 + 0.48 * pts[:, 2]
+    f = rng.normal(size=(n, 3))
+    if cfg["kernel"] == 16:
+        f = np.concatenate([f, rng.uniform(1e-4, 5e-4, (n, 1))], axis=1)
+    return pts, f
+
+
+def time_wall_fmm(cfg, seed, steps, warmup, ws, flush, nsample=1000):
+    """StkWallFMM_evaluate_fmm_device of one wall workload, FP64 and mixed, CUDA events per
+    evaluation; accuracy against the oracle's image system on a target sample."""
+    import torch
+    import stkfmm_b200 as S
+    pts, val = wall_inputs(cfg, seed)
+    K = cfg["kernel"]
+    td = S.get_kernel_dimension(K)[2]
+    fmm = S.StkWallFMM(cfg["p"], cfg["max_pts"], cfg["pbc"], K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    t0 = time.perf_counter()
+    fmm.setup_tree(K)
+    res = {"workload": cfg["workload"], "setup_tree_s": time.perf_counter() - t0}
+    d_v = torch.as_tensor(val).cuda()
+    outs = {}
+    for prec, nm in ((S.PRECISION.FP64, "fp64"), (S.PRECISION.MIXED, "mixed")):
+        fmm.set_precision(prec)
+        out = torch.zeros((len(pts), td), dtype=torch.float64, device="cuda")
+        for _ in range(warmup):
+            fmm.evaluate_fmm_device(K, d_v.data_ptr(), out.data_ptr(), None)
+        torch.cuda.synchronize()
+        ms = []
+        torch.cuda.profiler.start()
+        for _ in range(steps):
+            flush.zero_()
+            out.zero_()
+            torch.cuda.synchronize()
+            fmm.evaluate_fmm_device(K, d_v.data_ptr(), out.data_ptr(), None)
+            torch.cuda.synchronize()
+            ms.append(fmm.last_kernel_ms())
+        torch.cuda.profiler.stop()
+        m = max_over_ranks([sum(ms) / steps], ws)[0]
+        res[nm] = {"evals_per_s": job_rate(1, ws, m * 1e-3), "ms_per_eval": m}
+        outs[nm] = out.cpu().numpy()
+    res["mixed_over_fp64"] = res["fp64"]["ms_per_eval"] / res["mixed"]["ms_per_eval"]
+    res["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(outs["mixed"] - outs["fp64"]) / np.linalg.norm(outs["fp64"]))
+    res["gpu_launches_per_eval"] = fmm.last_launch_count(K)
+    res["timing"] = "device time of each evaluate_fmm_device (CUDA events on the wall's stream), L2 flushed between"
+    res["_acc"] = (pts, val, outs, nsample)
+    return res
+
+
+def wall_accuracy(cfg, res):
+    """Both precisions against the oracle's image system (oracle.wall_stokes / wall_rpy) on a target sample."""
+    from oracle import oracle as O
+    O.build()
+    pts, val, outs, nsample = res.pop("_acc")
+    samp = np.random.default_rng(17).choice(len(pts), nsample, replace=False)
+    t0 = time.perf_counter()
+    fn = O.wall_stokes if cfg["kernel"] == 8 else O.wall_rpy
+    ref = fn(pts, val, pts[samp])
+    res["rel_l2_vs_image_system_sample_per_component"] = {
+        nm: [float(np.linalg.norm(o[samp, c] - ref[:, c]) / np.linalg.norm(ref[:, c])) for c in range(ref.shape[1])]
+        for nm, o in outs.items()}
+    res["sample"] = "%d targets drawn with seed 17; oracle image system over all %d sources (%.1f s on the host)" % (
+        nsample, len(pts), time.perf_counter() - t0)
+
+
+def run_one_workload(name, steps, warmup):
+    """One further FMM or wall workload alone (for profiling); prints its block as one JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for cfg in EXTRA_FMM:
+        if cfg["name"] == name:
+            r, _, _, _ = time_extra_fmm(cfg, 0, steps, warmup, 1, flush)
+            print(json.dumps({name: r}), flush=True)
+            return 0
+    for cfg in WALL_FMM:
+        if cfg["name"] == name:
+            r = time_wall_fmm(cfg, 0, steps, warmup, 1, flush)
+            r.pop("_acc")
+            print(json.dumps({name: r}), flush=True)
+            return 0
+    raise SystemExit("unknown workload %s" % name)
+
+
 def extra_fmm_inputs(cfg, seed):
     """Points, SL values and DL values (or None) of a further workload."""
     rng = np.random.default_rng(seed)
@@ -214,6 +317,7 @@ def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
         if nm == "fp64":
             res["first_evaluations_s"] = time.perf_counter() - t0  # includes the far-field operator build
         ms, phases = [], []
+        torch.cuda.profiler.start()
         for _ in range(steps):
             flush.zero_()
             out.zero_()
@@ -222,6 +326,7 @@ def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
             torch.cuda.synchronize()
             ms.append(fmm.last_kernel_ms(K))
             phases.append(fmm.last_phase_ms(K))
+        torch.cuda.profiler.stop()
         m = max_over_ranks([sum(ms) / steps], ws)[0]
         res[nm] = {"evals_per_s": job_rate(1, ws, m * 1e-3), "ms_per_eval": m,
                    "phases_ms": {k: sum(p[k] for p in phases) / steps for k in phases[0]}}
@@ -525,6 +630,7 @@ def b200_arm(args):
         # a few timed evaluations each (the largest takes about a second per evaluation)
         r, epts, eslv, eouts = time_extra_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)
         extra.append((cfg, r, epts, eslv, eouts))
+    walls = [(cfg, time_wall_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)) for cfg in WALL_FMM]
 
     if rank != 0:
         if ws > 1:
@@ -570,6 +676,9 @@ def b200_arm(args):
     extra_blocks = {}
     for cfg, r, epts, eslv, eouts in extra:
         r["rel_l2_vs_direct_sum_sample_per_component"] = extra_fmm_accuracy(cfg, epts, eslv, eouts)
+        extra_blocks[cfg["name"]] = r
+    for cfg, r in walls:
+        wall_accuracy(cfg, r)
         extra_blocks[cfg["name"]] = r
     fmm_block = {
         "workload": WORKLOAD_FMM,
@@ -637,7 +746,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--fmm-workload", default=None,
+                    help="time one further FMM / wall workload alone (%s) and print its block"
+                         % ", ".join(c["name"] for c in EXTRA_FMM + WALL_FMM))
     args = ap.parse_args()
+    if args.fmm_workload:
+        return run_one_workload(args.fmm_workload, args.steps, args.warmup)
     if args.impl == "reference":
         return reference_arm(args)
     return b200_arm(args)

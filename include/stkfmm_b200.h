@@ -291,6 +291,8 @@ int StkWallFMM_set_precision(StkWallFMM *fmm, int precision);
 int StkWallFMM_evaluate_fmm_device(StkWallFMM *fmm, unsigned kernel, const double *d_src_SL_value,
                                    double *d_trg_value, void *stream);
 int StkWallFMM_last_kernel_ms(StkWallFMM *fmm, float *ms);
+/* this library's kernels launched by the last evaluation of `kernel` (cuBLAS calls excluded) */
+int StkWallFMM_last_launch_count(StkWallFMM *fmm, unsigned kernel, int *count);
 
 /* ---- host-only octree (no CUDA call) ------------------------------------------
  * The tree and KIFMM lists that Stk3DFMM_setup_tree builds, in place of PVFMM's

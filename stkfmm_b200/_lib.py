@@ -80,6 +80,7 @@ SIGNATURES = [
     ("StkWallFMM_set_precision", c_int, [c_void_p, c_int]),
     ("StkWallFMM_evaluate_fmm_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p]),
     ("StkWallFMM_last_kernel_ms", c_int, [c_void_p, P_f]),
+    ("StkWallFMM_last_launch_count", c_int, [c_void_p, c_uint, P_i]),
     ("stk_octree_build", c_void_p, [P_d, c_int, c_int, c_int, P_d, c_int, P_d, c_int, P_d, c_int]),
     ("stk_octree_free", None, [c_void_p]),
     ("stk_octree_sizes", c_int, [c_void_p, P_ll]),

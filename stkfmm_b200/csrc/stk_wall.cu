@@ -476,6 +476,24 @@ extern "C" int StkWallFMM_evaluate_fmm(StkWallFMM *fmm, unsigned kernel, const i
     return STK_OK;
 }
 
+// this library's kernels launched by the last evaluation: the sub-FMMs' plus staging and assembly
+extern "C" int StkWallFMM_last_launch_count(StkWallFMM *fmm, unsigned kernel, int *count) {
+    if (!fmm || !count) return STK_ERR_INVALID_ARG;
+    const int f = family_of(kernel);
+    if (f < 0) return STK_ERR_NOT_SUPPORTED;
+    if (!fmm->sub[f][0]) return STK_ERR_KERNEL;
+    if (!fmm->ready[f]) return STK_ERR_STATE;
+    int total = 2;
+    for (int k = 0; k < kSubs; k++) {
+        if (!fmm->sub[f][k]) continue;
+        int c = 0;
+        if (int rc = Stk3DFMM_last_launch_count(fmm->sub[f][k], kSubKernel[f][k], &c)) return rc;
+        total += c;
+    }
+    *count = total;
+    return STK_OK;
+}
+
 extern "C" int StkWallFMM_last_kernel_ms(StkWallFMM *fmm, float *ms) {
     if (!fmm || !ms) return STK_ERR_INVALID_ARG;
     if (!fmm->timed) return STK_ERR_STATE;

@@ -350,6 +350,11 @@ class StkWallFMM:
         check(lib().StkWallFMM_last_kernel_ms(self.fmm, ctypes.byref(ms)), "last_kernel_ms")
         return ms.value
 
+    def last_launch_count(self, kernel) -> int:
+        c = ctypes.c_int()
+        check(lib().StkWallFMM_last_launch_count(self.fmm, int(kernel), ctypes.byref(c)), "last_launch_count")
+        return c.value
+
 
 class Octree:
     """Host-only octree + KIFMM lists (no GPU needed); coordinates in [0,1)^3."""
