@@ -334,9 +334,24 @@ def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
     res["mixed_over_fp64"] = res["fp64"]["ms_per_eval"] / res["mixed"]["ms_per_eval"]
     res["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(outs["mixed"] - outs["fp64"]) / np.linalg.norm(outs["fp64"]))
     res["work_per_eval"] = fmm.fmm_stats(K)
+    res["m2l_roofline"] = m2l_roofline(fmm, K, res)
     res["gpu_launches_per_eval"] = fmm.last_launch_count(K)
     res["timing"] = "device time of each evaluate_fmm_device (CUDA events on the handle's stream), L2 flushed between"
     return res, pts, slv, outs
+
+
+def m2l_roofline(fmm, K, res):
+    """Achieved FP64 / FP32 rate of the compressed M2L phase (its flops over its event time)."""
+    w = fmm.m2l_work(K)
+    out = {"flops_algorithmic": w["flops_algorithmic"], "flops_executed": w["flops_executed"]}
+    for nm in ("fp64", "mixed"):
+        ms = res[nm]["phases_ms"]["m2l"] if nm in res else None
+        if ms:
+            out[nm + "_tflops_algorithmic"] = w["flops_algorithmic"] / (ms * 1e-3) / 1e12
+            out[nm + "_tflops_executed"] = w["flops_executed"] / (ms * 1e-3) / 1e12
+    out["note"] = ("M2L phase: basis products, column gather, per-offset GEMMs, per-target reduce; "
+                   "FP64 GEMMs on the FP64 tensor pipe (DMMA), mixed GEMMs SIMT FP32")
+    return out
 
 
 def extra_fmm_accuracy(cfg, pts, slv, outs, nsample=4096):
@@ -689,6 +704,7 @@ def b200_arm(args):
         "sample": "%d targets drawn with seed 11; oracle direct sum over all %d sources (%.1f s on the host)"
                   % (FMM_SAMPLE, N_POINTS, oracle_s),
         "work_per_eval": fst,
+        "m2l_roofline": m2l_roofline(fmm, K, {"fp64": {"phases_ms": fph64}, "mixed": {"phases_ms": fphmx}}),
         "e2e": {"evals_per_s": job_rate(1, ws, fe2e_s), "ms_per_eval": fe2e_s * 1e3,
                 "api": "Stk3DFMM_evaluate_fmm (C ABI, pinned host arrays, mixed)",
                 "h2d_bytes_per_eval": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),

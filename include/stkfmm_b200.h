@@ -247,6 +247,11 @@ int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
  * pairs, [7] points per check / equivalent surface, [8] rank of the compressed M2L,
  * [9] kernels of this library launched by the last evaluation (cuBLAS calls excluded). */
 int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long *out);
+/* Floating-point work of one compressed M2L of `kernel` (after its first evaluate_fmm):
+ * out[0] = 4 k r_d per V-list pair at the offsets' true ranks plus the two basis
+ * products (4 N k per node), out[1] = the flops the GEMMs execute (ranks padded to
+ * multiples of 32, columns to 256-pair chunks). */
+int Stk3DFMM_get_m2l_work(Stk3DFMM *fmm, unsigned kernel, double *out);
 /* Copy the U-list of the last setup_tree (leaf-sorted indices, same layout as
  * stk_p2p_lists).  Pass null arrays to query sizes: sizes = {n_leaf_boxes, n_entries, nSL, nDL, nTrg}. */
 int Stk3DFMM_get_ulist(Stk3DFMM *fmm, unsigned kernel, int *sizes, int *trg_begin, int *trg_end, int *list_off,

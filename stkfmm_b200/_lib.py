@@ -65,6 +65,7 @@ SIGNATURES = [
     ("Stk3DFMM_last_kernel_ms", c_int, [c_void_p, c_uint, P_f]),
     ("Stk3DFMM_last_phase_ms", c_int, [c_void_p, c_uint, P_f]),
     ("Stk3DFMM_get_fmm_stats", c_int, [c_void_p, c_uint, P_ll]),
+    ("Stk3DFMM_get_m2l_work", c_int, [c_void_p, c_uint, P_d]),
     ("Stk3DFMM_last_launch_count", c_int, [c_void_p, c_uint, P_i]),
     ("Stk3DFMM_get_tree_stats", c_int, [c_void_p, c_uint, P_ll]),
     ("Stk3DFMM_get_ulist", c_int, [c_void_p, c_uint, P_i] + [P_i] * 11),

@@ -598,6 +598,7 @@ int build_m2l_lowrank(FarField &F, const std::vector<double> &unit, const double
     for (int code = 0; code < kNumOffsets; code++)
         if (F.m2l_slot[code] >= 0) nslot++;
     F.m2l_r.assign(nslot, 0);
+    F.m2l_rt.assign(nslot, 0);
     F.m2l_pq_off.assign(nslot, 0);
     for (int code = 0; code < kNumOffsets; code++) {
         const int sl = F.m2l_slot[code];
@@ -605,6 +606,7 @@ int build_m2l_lowrank(FarField &F, const std::vector<double> &unit, const double
         // ranks padded to a multiple of 32 (zero columns), so that offsets of similar
         // rank share one uniformly sized batched GEMM
         F.m2l_r[sl] = std::min(k, (rrank[of[code].rep] + 31) / 32 * 32);
+        F.m2l_rt[sl] = rrank[of[code].rep];
         F.m2l_pq_off[sl] = total;
         total += (size_t)k * F.m2l_r[sl];
     }
@@ -1244,6 +1246,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         if (rc) return rc;
         F.m2l_flops = 0;
         for (int c = 0; c < nc; c++) F.m2l_flops += 4.0 * k * F.m2l_r[chunk_slot[c]] * kM2LChunk;
+        F.m2l_flops_alg = 4.0 * (double)k * N * nn;
+        for (int sl = 0; sl < nslot; sl++) F.m2l_flops_alg += 4.0 * k * F.m2l_rt[sl] * (double)srcs[sl].size();
+        F.m2l_flops += 4.0 * (double)k * N * nn;
         // host vectors above are pageable: their copies complete before upload returns
         int maxm = 0;
         for (int l = 0; l <= T.depth(); l++) maxm = std::max(maxm, F.parent_off[l + 1] - F.parent_off[l]);

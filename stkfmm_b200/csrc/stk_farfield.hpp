@@ -61,7 +61,8 @@ struct FarField {
     double m2l_rtol = 0;        // relative singular-value cut of the M2L bases
     int m2l_rank = 0;           // k
     // two-level: per offset slot C_d ~ P_d Q_d^T, P and Q k x r_d (column-major, packed)
-    std::vector<int> m2l_r;         // r_d per slot
+    std::vector<int> m2l_r;         // r_d per slot (padded to a multiple of 32)
+    std::vector<int> m2l_rt;        // r_d per slot before padding
     std::vector<size_t> m2l_pq_off;  // start of P_d / Q_d in m2l_p / m2l_q
     int m2l_rmax = 1;
     DevBuf m2l_p, m2l_q, m2l_p32, m2l_q32;
@@ -102,7 +103,9 @@ struct FarField {
     DevBuf m2l_x, m2l_y, m2l_z;             // one group of columns: k x, k x, rmax x columns (FP64 or FP32)
     DevBuf d_m2l_ptr[5], d_m2l_ptr32[5];    // per chunk: Q_d, X, Z, P_d, Y (FP64 / FP32 views)
     std::vector<M2LSeg> m2l_seg;            // per group of columns and padded rank: chunks in the pointer arrays
-    double m2l_flops = 0;                   // flops of one M2L (both stages)
+    double m2l_flops = 0;                   // flops of one M2L (both stages, padded ranks and chunks)
+    double m2l_flops_alg = 0;               // the same at the true ranks over the real pairs, plus the
+                                            // two basis products (V^T phi, (DC2DE U) psi_hat)
     ~FarField();
 };
 

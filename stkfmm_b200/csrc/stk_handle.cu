@@ -510,6 +510,16 @@ extern "C" int Stk3DFMM_get_tree_stats(Stk3DFMM *fmm, unsigned kernel, long long
     return STK_OK;
 }
 
+extern "C" int Stk3DFMM_get_m2l_work(Stk3DFMM *fmm, unsigned kernel, double *out) {
+    if (!fmm || !out) return STK_ERR_INVALID_ARG;
+    KernelData *kd = get_kd(fmm, kernel);
+    if (!kd) return STK_ERR_KERNEL;
+    if (!kd->tree_ready || !kd->far_ready) return STK_ERR_STATE;
+    out[0] = kd->far->m2l_flops_alg;
+    out[1] = kd->far->m2l_flops;
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_get_fmm_stats(Stk3DFMM *fmm, unsigned kernel, long long *out) {
     if (!fmm || !out) return STK_ERR_INVALID_ARG;
     KernelData *kd = get_kd(fmm, kernel);

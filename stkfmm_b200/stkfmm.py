@@ -258,6 +258,12 @@ class Stk3DFMM:
                 "launches"]
         return dict(zip(keys, (int(v) for v in out)))
 
+    def m2l_work(self, kernel) -> dict:
+        """Flops of one compressed M2L: algorithmic (true ranks, real pairs) and executed."""
+        out = np.zeros(2)
+        check(lib().Stk3DFMM_get_m2l_work(self.fmm, int(kernel), out.ctypes.data_as(P_d)), "m2l_work")
+        return {"flops_algorithmic": float(out[0]), "flops_executed": float(out[1])}
+
     def tree_stats(self, kernel) -> dict:
         out = np.zeros(9, dtype=np.int64)
         check(lib().Stk3DFMM_get_tree_stats(self.fmm, int(kernel), out.ctypes.data_as(P_ll)), "tree_stats")
