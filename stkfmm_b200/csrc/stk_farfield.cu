@@ -367,6 +367,21 @@ __global__ void m2l_reduce_kernel(const T *__restrict__ Y, const int *__restrict
     }
 }
 
+// Complete-level M2L: Zc[row + R j] = Z[srow[row] + ldz pos] for pos = tab[q + nq j],
+// q = rowq[row] (0 where the target j has no source at that offset)
+template <class T>
+__global__ void m2l_zgather_kernel(const T *__restrict__ Z, int ldz, const int *__restrict__ tab, int nq,
+                                   const int *__restrict__ rowq, const int *__restrict__ srow, int R, int n8,
+                                   T *__restrict__ Zc) {
+    const long long total = (long long)n8 * R;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / R), row = (int)(idx - (long long)j * R);
+        const int pos = tab[(size_t)j * nq + rowq[row]];
+        Zc[idx] = pos >= 0 ? Z[(size_t)pos * ldz + srow[row]] : T(0);
+    }
+}
+
 // A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
 // at rtol * sigma_max.  A is overwritten.
 int pinv(FarField &F, double *A, int m, double *A_inv, double rtol, cudaStream_t s) {
@@ -879,6 +894,191 @@ FarField::~FarField() {
     if (solver) cusolverDnDestroy(solver);
 }
 
+// Dense M2L of the complete levels (M2LDenseLevel).  A level l >= 3 qualifies
+// when all 8^l boxes are present and its V lists hold at least 70% of 189 pairs
+// per box (periodic and deep uniform levels); the stacked factors and the work
+// buffers must fit in budgets (4 GiB each).  STKFMM_M2L_DENSE=0 turns it off.
+static int setup_m2l_dense(FarField &F, const Octree &T, int nslot, cudaStream_t s) {
+    F.dense.clear();
+    const char *env = getenv("STKFMM_M2L_DENSE");
+    if (env && env[0] == '0') return STK_OK;
+    const int k = F.m2l_rank;
+    auto type_of = [&](int b) { return (int)((T.ix[b] & 1) | (T.iy[b] & 1) << 1 | (T.iz[b] & 1) << 2); };
+    auto slot_of = [&](int b, int ent) {
+        const int a = ent >> 5, code = ent & 31;
+        const int sx = code % 3 - 1, sy = (code / 3) % 3 - 1, sz = code / 9 - 1;
+        const int64_t L = 1LL << T.level[b];
+        const int dx = (int)((int64_t)T.ix[a] + sx * L - T.ix[b]);
+        const int dy = (int)((int64_t)T.iy[a] + sy * L - T.iy[b]);
+        const int dz = (int)((int64_t)T.iz[a] + sz * L - T.iz[b]);
+        if (std::abs(dx) > 3 || std::abs(dy) > 3 || std::abs(dz) > 3) return -1;
+        return F.m2l_slot[(dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)];
+    };
+    // candidate levels
+    std::vector<int> levels;
+    for (int l = 3; l <= T.depth() && l < 10; l++) {
+        const long long n = (long long)T.level_begin[l + 1] - T.level_begin[l];
+        if (n != (1LL << (3 * l))) continue;
+        long long pairs = 0;
+        for (int b = T.level_begin[l]; b < T.level_begin[l + 1]; b++) pairs += T.V.off[b + 1] - T.V.off[b];
+        if (pairs >= 0.7 * 189.0 * (double)n) levels.push_back(l);
+    }
+    if (levels.empty()) return STK_OK;
+    // offsets per (target type, source type), one pair per (target, offset)
+    std::vector<char> in((size_t)64 * nslot, 0);
+    std::vector<int> stamp(nslot, -1);
+    for (int l : levels)
+        for (int b = T.level_begin[l]; b < T.level_begin[l + 1]; b++)
+            for (int e = T.V.off[b]; e < T.V.off[b + 1]; e++) {
+                const int sl = slot_of(b, T.V.ent[e]);
+                if (sl < 0 || stamp[sl] == b) return STK_OK;  // not the expected structure: chunked path
+                stamp[sl] = b;
+                in[(size_t)(8 * type_of(b) + type_of(T.V.ent[e] >> 5)) * nslot + sl] = 1;
+            }
+    // rows: blocks (c, c') of Pv_c in c' order; Qs_c' rows in slot order
+    std::vector<int> rows_s((size_t)8 * nslot, -1);
+    for (int cs = 0; cs < 8; cs++) {
+        int r = 0;
+        for (int sl = 0; sl < nslot; sl++) {
+            bool used = false;
+            for (int c = 0; c < 8; c++) used = used || in[(size_t)(8 * c + cs) * nslot + sl];
+            if (!used) continue;
+            rows_s[(size_t)cs * nslot + sl] = r;
+            r += F.m2l_rt[sl];
+        }
+        F.dn_rs[cs] = r;
+    }
+    size_t ops = 0, rows_total = 0;
+    for (int c = 0; c < 8; c++) {
+        int r = 0;
+        for (int cs = 0; cs < 8; cs++) {
+            const int b = 8 * c + cs;
+            F.dn_slots[b].clear();
+            F.dn_pstart[b] = r;
+            int rb = 0;
+            for (int sl = 0; sl < nslot; sl++)
+                if (in[(size_t)b * nslot + sl]) {
+                    F.dn_slots[b].push_back(sl);
+                    rb += F.m2l_rt[sl];
+                }
+            F.dn_q[b] = (int)F.dn_slots[b].size();
+            F.dn_rcc[b] = rb;
+            r += rb;
+        }
+        F.dn_rv[c] = r;
+        ops += (size_t)k * (F.dn_rv[c] + F.dn_rs[c]);
+        rows_total += r;
+    }
+    // budgets: stacked factors (FP64 + FP32) and the largest level's buffers (FP64)
+    int rs_max = 1, rcc_max = 1;
+    for (int c = 0; c < 8; c++) rs_max = std::max(rs_max, F.dn_rs[c]);
+    for (int b = 0; b < 64; b++) rcc_max = std::max(rcc_max, F.dn_rcc[b]);
+    const long long nmax = 1LL << (3 * levels.back()), n8max = nmax / 8;
+    const size_t buf = sizeof(double) * ((size_t)2 * k * nmax + (size_t)(rs_max + rcc_max) * n8max);
+    if (ops * 12 > (4ull << 30) || buf > (4ull << 30)) return STK_OK;
+
+    // stacked factors
+    int rc = F.dn_pv.reserve(sizeof(double) * (size_t)k * rows_total);
+    size_t qs_total = 0;
+    for (int c = 0; c < 8; c++) qs_total += F.dn_rs[c];
+    if (!rc) rc = F.dn_qs.reserve(sizeof(double) * (size_t)k * std::max<size_t>(qs_total, 1));
+    if (!rc) rc = F.dn_pv32.reserve(sizeof(float) * (size_t)k * rows_total);
+    if (!rc) rc = F.dn_qs32.reserve(sizeof(float) * (size_t)k * std::max<size_t>(qs_total, 1));
+    if (rc) return rc;
+    size_t off = 0;
+    for (int c = 0; c < 8; c++) {
+        F.dn_pv_off[c] = off;
+        for (int cs = 0; cs < 8; cs++)
+            for (int sl : F.dn_slots[8 * c + cs]) {
+                const size_t bytes = sizeof(double) * (size_t)k * F.m2l_rt[sl];
+                FCUDA(cudaMemcpyAsync((double *)F.dn_pv.ptr + off, (const double *)F.m2l_p.ptr + F.m2l_pq_off[sl],
+                                      bytes, cudaMemcpyDeviceToDevice, s));
+                off += (size_t)k * F.m2l_rt[sl];
+            }
+    }
+    off = 0;
+    for (int cs = 0; cs < 8; cs++) {
+        F.dn_qs_off[cs] = off;
+        for (int sl = 0; sl < nslot; sl++) {
+            if (rows_s[(size_t)cs * nslot + sl] < 0) continue;
+            FCUDA(cudaMemcpyAsync((double *)F.dn_qs.ptr + off, (const double *)F.m2l_q.ptr + F.m2l_pq_off[sl],
+                                  sizeof(double) * (size_t)k * F.m2l_rt[sl], cudaMemcpyDeviceToDevice, s));
+            off += (size_t)k * F.m2l_rt[sl];
+        }
+    }
+    to_float_kernel<<<grid_for((long long)k * rows_total), 256, 0, s>>>((const double *)F.dn_pv.ptr,
+                                                                         (long long)k * rows_total,
+                                                                         (float *)F.dn_pv32.ptr);
+    to_float_kernel<<<grid_for((long long)k * qs_total), 256, 0, s>>>((const double *)F.dn_qs.ptr,
+                                                                       (long long)k * qs_total,
+                                                                       (float *)F.dn_qs32.ptr);
+    FCUDA(cudaGetLastError());
+    // per block row: its slot index and its row in Z_c'
+    std::vector<int> rowq, srow;
+    for (int b = 0; b < 64; b++) {
+        F.dn_row_off[b] = rowq.size();
+        const int cs = b % 8;
+        for (int q = 0; q < F.dn_q[b]; q++) {
+            const int sl = F.dn_slots[b][q];
+            for (int i = 0; i < F.m2l_rt[sl]; i++) {
+                rowq.push_back(q);
+                srow.push_back(rows_s[(size_t)cs * nslot + sl] + i);
+            }
+        }
+    }
+    rc = F.dn_rowq.upload(rowq.data(), sizeof(int) * rowq.size(), s);
+    if (!rc) rc = F.dn_srow.upload(srow.data(), sizeof(int) * srow.size(), s);
+    if (rc) return rc;
+    // per level: nodes in type order and the (c, c') source tables
+    std::vector<int> qidx((size_t)64 * nslot, -1);
+    for (int b = 0; b < 64; b++)
+        for (int q = 0; q < F.dn_q[b]; q++) qidx[(size_t)b * nslot + F.dn_slots[b][q]] = q;
+    for (int l : levels) {
+        std::unique_ptr<M2LDenseLevel> D(new M2LDenseLevel());
+        D->level = l;
+        const int b0 = T.level_begin[l], n = T.level_begin[l + 1] - b0, n8 = n / 8;
+        D->n8 = n8;
+        std::vector<int> nodes, pos(n, -1), cnt(8, 0);
+        nodes.reserve(n);
+        for (int c = 0; c < 8; c++)
+            for (int b = b0; b < b0 + n; b++)
+                if (type_of(b) == c) {
+                    pos[b - b0] = cnt[c]++;
+                    nodes.push_back(b);
+                }
+        for (int c = 0; c < 8; c++)
+            if (cnt[c] != n8) return STK_ERR_STATE;
+        D->tab_off.assign(64, 0);
+        size_t tsize = 0;
+        for (int b = 0; b < 64; b++) {
+            D->tab_off[b] = tsize;
+            tsize += (size_t)n8 * F.dn_q[b];
+        }
+        std::vector<int> tab(std::max<size_t>(tsize, 1), -1);
+        for (int t = b0; t < b0 + n; t++)
+            for (int e = T.V.off[t]; e < T.V.off[t + 1]; e++) {
+                const int a = T.V.ent[e] >> 5, sl = slot_of(t, T.V.ent[e]);
+                const int b = 8 * type_of(t) + type_of(a);
+                const int q = qidx[(size_t)b * nslot + sl];
+                if (q < 0 || a < b0 || a >= b0 + n) return STK_ERR_STATE;
+                tab[D->tab_off[b] + (size_t)pos[t - b0] * F.dn_q[b] + q] = pos[a - b0];
+                D->pairs++;
+            }
+        rc = D->d_nodes.upload(nodes.data(), sizeof(int) * nodes.size(), s);
+        if (!rc) rc = D->d_tab.upload(tab.data(), sizeof(int) * tab.size(), s);
+        if (rc) return rc;
+        F.dense.push_back(std::move(D));
+    }
+    // work buffers (FP64 size, FP32 views)
+    rc = F.dn_phi.reserve(sizeof(double) * (size_t)k * nmax);
+    if (!rc) rc = F.dn_psi.reserve(sizeof(double) * (size_t)k * nmax);
+    if (!rc) rc = F.dn_z.reserve(sizeof(double) * (size_t)rs_max * n8max);
+    if (!rc) rc = F.dn_zc.reserve(sizeof(double) * (size_t)rcc_max * n8max);
+    if (rc) return rc;
+    FCUDA(cudaStreamSynchronize(s));
+    return STK_OK;
+}
+
 int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     const KernelInfo *ki = kd->info;
     // free space, or periodic in x (PX), x and y (PXY) or all axes (PXYZ): the far
@@ -1129,7 +1329,13 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     // ---- M2L: V-list pairs grouped by offset ----
     {
         const int nslot = (int)std::count_if(F.m2l_slot.begin(), F.m2l_slot.end(), [](int v) { return v >= 0; });
+        // complete levels go to the dense M2L (all pairs of their targets)
+        rc = setup_m2l_dense(F, T, nslot, s);
+        if (rc) return rc;
+        std::vector<char> dense_lvl(T.depth() + 1, 0);
+        for (auto &dl : F.dense) dense_lvl[dl->level] = 1;
         std::vector<std::vector<int>> srcs(nslot), trgs(nslot);
+        std::vector<long long> slot_pairs(nslot, 0);
         for (int b = 0; b < nn; b++)
             for (int e = T.V.off[b]; e < T.V.off[b + 1]; e++) {
                 const int a = T.V.ent[e] >> 5, code = T.V.ent[e] & 31;
@@ -1141,6 +1347,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
                 if (std::abs(dx) > 3 || std::abs(dy) > 3 || std::abs(dz) > 3) return STK_ERR_STATE;
                 const int sl = F.m2l_slot[(dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)];
                 if (sl < 0) return STK_ERR_STATE;
+                slot_pairs[sl]++;
+                if (dense_lvl[T.level[b]]) continue;
                 srcs[sl].push_back(a);
                 trgs[sl].push_back(b);
             }
@@ -1161,6 +1369,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
             }
             pairs += m;
         }
+        for (auto &dl : F.dense) pairs += dl->pairs;
         F.m2l_pairs = pairs;
         F.m2l_chunks = (int)chunk_slot.size();
         F.m2l_cols = (long long)gsrc.size();
@@ -1247,8 +1456,10 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         F.m2l_flops = 0;
         for (int c = 0; c < nc; c++) F.m2l_flops += 4.0 * k * F.m2l_r[chunk_slot[c]] * kM2LChunk;
         F.m2l_flops_alg = 4.0 * (double)k * N * nn;
-        for (int sl = 0; sl < nslot; sl++) F.m2l_flops_alg += 4.0 * k * F.m2l_rt[sl] * (double)srcs[sl].size();
+        for (int sl = 0; sl < nslot; sl++) F.m2l_flops_alg += 4.0 * k * F.m2l_rt[sl] * (double)slot_pairs[sl];
         F.m2l_flops += 4.0 * (double)k * N * nn;
+        for (auto &dl : F.dense)
+            for (int c = 0; c < 8; c++) F.m2l_flops += 2.0 * k * (F.dn_rs[c] + F.dn_rv[c]) * (double)dl->n8;
         // host vectors above are pageable: their copies complete before upload returns
         int maxm = 0;
         for (int l = 0; l <= T.depth(); l++) maxm = std::max(maxm, F.parent_off[l + 1] - F.parent_off[l]);
@@ -1260,6 +1471,46 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     FCUDA(cudaStreamSynchronize(s));
     F.ready = true;
     return STK_OK;
+}
+
+// Dense M2L of one complete level: psi_hat[:, t] += sum over the level's V-list
+// pairs, by box parity type (M2LDenseLevel), in T = double (FP64) or float (mixed).
+template <class T>
+static int m2l_dense_level(FarField &F, const M2LDenseLevel &D, const double *phi_hat, double *psi_hat,
+                           cudaStream_t s) {
+    const bool f32 = std::is_same<T, float>::value;
+    const int k = F.m2l_rank, n8 = D.n8, n = 8 * n8;
+    const cudaDataType_t dt = f32 ? CUDA_R_32F : CUDA_R_64F;
+    const cublasComputeType_t ct = f32 ? CUBLAS_COMPUTE_32F : CUBLAS_COMPUTE_64F;
+    const T one = T(1), zero = T(0);
+    T *phi = (T *)F.dn_phi.ptr, *psi = (T *)F.dn_psi.ptr, *Z = (T *)F.dn_z.ptr, *Zc = (T *)F.dn_zc.ptr;
+    const T *pv = f32 ? (const T *)F.dn_pv32.ptr : (const T *)F.dn_pv.ptr;
+    const T *qs = f32 ? (const T *)F.dn_qs32.ptr : (const T *)F.dn_qs.ptr;
+    const int *nodes = (const int *)D.d_nodes.ptr;
+    int rc = gather_cols<double, T>(phi_hat, nodes, n, k, phi, s);
+    if (rc) return rc;
+    FCUDA(cudaMemsetAsync(psi, 0, sizeof(T) * (size_t)k * n, s));
+    for (int cs = 0; cs < 8; cs++) {
+        const int rs = F.dn_rs[cs];
+        if (!rs) continue;
+        // Z = Qs_c'^T Phi_c': every offset of the source type at once
+        FBLAS(cublasGemmEx(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, rs, n8, k, &one, qs + F.dn_qs_off[cs], dt, k,
+                           phi + (size_t)cs * n8 * k, dt, k, &zero, Z, dt, rs, ct, CUBLAS_GEMM_DEFAULT));
+        for (int c = 0; c < 8; c++) {
+            const int b = 8 * c + cs, R = F.dn_rcc[b];
+            if (!R) continue;
+            t_launches++;
+            m2l_zgather_kernel<T><<<grid_for((long long)n8 * R), 256, 0, s>>>(
+                Z, rs, (const int *)D.d_tab.ptr + D.tab_off[b], F.dn_q[b], (const int *)F.dn_rowq.ptr + F.dn_row_off[b],
+                (const int *)F.dn_srow.ptr + F.dn_row_off[b], R, n8, Zc);
+            FCUDA(cudaGetLastError());
+            // Psi_c += Pv_{c,c'} Zc (source types in a fixed order: deterministic)
+            FBLAS(cublasGemmEx(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, n8, R, &one,
+                               pv + F.dn_pv_off[c] + (size_t)k * F.dn_pstart[b], dt, k, Zc, dt, R, &one,
+                               psi + (size_t)c * n8 * k, dt, k, ct, CUBLAS_GEMM_DEFAULT));
+        }
+    }
+    return scatter_cols<T>(psi, nodes, n, k, 1.0, 1, psi_hat, s);
 }
 
 int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *trg_sorted,
@@ -1392,6 +1643,12 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
             m2l_reduce_kernel<double><<<grid_for((long long)nn * k), 256, 0, s>>>(
                 (const double *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
         FCUDA(cudaGetLastError());
+    }
+    // complete levels: dense M2L by box type
+    for (auto &Dp : F.dense) {
+        const int rcd = prec == PREC_MIXED ? m2l_dense_level<float>(F, *Dp, phi_hat, psi_hat, s)
+                                           : m2l_dense_level<double>(F, *Dp, phi_hat, psi_hat, s);
+        if (rcd) return rcd;
     }
     FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,
                       psi, N));

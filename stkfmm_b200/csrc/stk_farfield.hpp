@@ -7,6 +7,7 @@
 // upward equivalent and downward check at 1.05, upward check and downward
 // equivalent at 2.95 times the box half-width, centred on the box.
 #pragma once
+#include <memory>
 #include <vector>
 
 #include <cublas_v2.h>
@@ -39,6 +40,21 @@ struct ListPass {
 // Chunks of one group of columns whose offsets share one padded rank.
 struct M2LSeg {
     int group, rank, start, count;
+};
+
+// M2L of one complete level (all 8^l boxes present, most of their V lists full):
+// boxes grouped by parity type c = (ix & 1) | (iy & 1) << 1 | (iz & 1) << 2, so
+// that every target of type c meets the same offsets V_c and every source of
+// type c' the same offsets S_c'.  Per source type one GEMM Z = Qs_c'^T Phi_c'
+// (all of its offsets at once), per (target type, source type) a gather of Z's
+// rows into the targets' order and one GEMM Psi_c += Pv_{c,c'} Zc: no per-pair
+// k-vectors, no per-target reduce.
+struct M2LDenseLevel {
+    int level = 0, n8 = 0;
+    DevBuf d_nodes;              // 8 n8 node ids, type-major (type c: [c n8, (c+1) n8))
+    DevBuf d_tab;                // per (c, c'): n8 x nq source positions within type c' (-1: no pair)
+    std::vector<size_t> tab_off;  // [8 c + c'] start in d_tab
+    long long pairs = 0;
 };
 
 struct FarField {
@@ -106,6 +122,18 @@ struct FarField {
     double m2l_flops = 0;                   // flops of one M2L (both stages, padded ranks and chunks)
     double m2l_flops_alg = 0;               // the same at the true ranks over the real pairs, plus the
                                             // two basis products (V^T phi, (DC2DE U) psi_hat)
+    // complete levels (see M2LDenseLevel); the column chunks above hold the other levels' pairs
+    std::vector<std::unique_ptr<M2LDenseLevel>> dense;
+    int dn_q[64] = {};                      // offsets of (c, c'): slots q of V_{c,c'}
+    std::vector<int> dn_slots[64];
+    int dn_rv[8] = {}, dn_rs[8] = {};       // rows of Pv_c (sum of r_d over V_c) and of Qs_c'
+    int dn_pstart[64] = {};                 // first column of block (c, c') in Pv_c
+    int dn_rcc[64] = {};                    // rows of block (c, c')
+    DevBuf dn_pv, dn_qs, dn_pv32, dn_qs32;  // Pv_0..7, Qs_0..7 (k x rows each, packed)
+    size_t dn_pv_off[8] = {}, dn_qs_off[8] = {};
+    DevBuf dn_rowq, dn_srow;                // per block row: its slot index q, its row in Z_c'
+    size_t dn_row_off[64] = {};
+    DevBuf dn_phi, dn_psi, dn_z, dn_zc;     // per-level work buffers (FP64 or FP32)
     ~FarField();
 };
 
