@@ -1100,8 +1100,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     // The cut follows the order's own truncation error: at p <= 8 (FMM error
     // ~1e-6) 3e-8 changes the error by under 1% (RPY / Stokes, 32k-200k points)
     // and drops the rank 716 -> 636 for stokes_vel; at p = 9, 10 (error ~1e-8
-    // for Laplace) 1e-8 keeps it within 15%; higher orders keep more rank.
-    const double m2l_rtol = env_rtol ? atof(env_rtol) : (p <= 8 ? 3e-8 : p <= 10 ? 1e-8 : 1e-10);
+    // for Laplace) 1e-8 keeps it within 15%; at p = 11, 12 (error ~1e-9 for
+    // PVel and Laplace) 1e-9 changes it by under 1%; higher orders keep more rank.
+    const double m2l_rtol = env_rtol ? atof(env_rtol) : (p <= 8 ? 3e-8 : p <= 10 ? 1e-8 : p <= 12 ? 1e-9 : 1e-10);
     if (F.p != p || F.m2x != m2x || F.m2l_rtol != m2l_rtol) {
         F.m2l_rtol = m2l_rtol;
         for (int c = 0; c < 4; c++) F.pot_exp[c] = F.den_exp[c] = 0.0;
