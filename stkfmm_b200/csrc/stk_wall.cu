@@ -186,6 +186,7 @@ struct StkWallFMM {
     std::vector<double> src, img, src2, trg;
     Stk3DFMM *sub[kFamilies][kSubs] = {};
     bool ready[kFamilies] = {false, false};
+    cudaEvent_t ev_staged = nullptr, ev_done[kSubs] = {};  // sub-FMMs run concurrently on their own streams
     DevBuf d_zsrc, d_ztrg, d_in, d_out, d_val[6], d_sub[kSubs];
     ~StkWallFMM() {
         for (auto &fam : sub)
@@ -193,6 +194,9 @@ struct StkWallFMM {
                 if (h) Stk3DFMM_destroy(h);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_staged) cudaEventDestroy(ev_staged);
+        for (auto &e : ev_done)
+            if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -213,11 +217,18 @@ extern "C" StkWallFMM *StkWallFMM_create(int mult_order, int max_pts, int pbc, u
     w->kernel_comb = kernelComb;
     if (cudaGetDevice(&w->device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&w->ev0) != cudaSuccess || cudaEventCreate(&w->ev1) != cudaSuccess) {
+        cudaEventCreate(&w->ev0) != cudaSuccess || cudaEventCreate(&w->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&w->ev_staged, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         delete w;
         return nullptr;
     }
+    for (auto &e : w->ev_done)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            delete w;
+            return nullptr;
+        }
     double o[3] = {0, 0, 0};
     for (int f = 0; f < kFamilies; f++) {
         if (!(kernelComb & (f == 0 ? STK_Stokes : STK_RPY))) continue;
@@ -372,6 +383,26 @@ extern "C" int StkWallFMM_set_precision(StkWallFMM *fmm, int precision) {
     return STK_OK;
 }
 
+// The sub-FMMs of one evaluation: each on its own handle's stream after the
+// staging kernel (event on s), s waits for all of them before the assembly.
+// Their near-field kernels fill the GPU; the smaller far-field kernels and
+// GEMMs of one sub-FMM overlap with the others'.
+static int run_subs(StkWallFMM *w, int f, const double *const *sv, const double *const *dv, double *const *u,
+                    cudaStream_t s) {
+    WCUDA(cudaEventRecord(w->ev_staged, s));
+    int rc = STK_OK;
+    int k = 0;
+    for (; k < kSubs && w->sub[f][k]; k++) {
+        Stk3DFMM *h = w->sub[f][k];
+        WCUDA(cudaStreamWaitEvent(h->stream, w->ev_staged, 0));
+        rc = Stk3DFMM_evaluate_fmm_device(h, kSubKernel[f][k], sv[k], u[k], dv[k], h->stream);
+        WCUDA(cudaEventRecord(w->ev_done[k], h->stream));
+        if (rc) break;
+    }
+    for (int j = 0; j < k && j < kSubs && w->sub[f][j]; j++) WCUDA(cudaStreamWaitEvent(s, w->ev_done[j], 0));
+    return rc;
+}
+
 // The wall evaluation on device buffers: d_trg_value (caller's order, kdimTrg per
 // target) += wall FMM of d_src_SL_value (caller's order, kdimSL per source).
 static int wall_eval(StkWallFMM *w, int f, const double *d_sl, double *d_out, cudaStream_t s) {
@@ -400,16 +431,13 @@ static int wall_eval(StkWallFMM *w, int f, const double *d_sl, double *d_out, cu
     double *u[kSubs];
     for (int k = 0; k < kSubs; k++) u[k] = (double *)w->d_sub[k].ptr;
     const double *zs = (const double *)w->d_zsrc.ptr, *zt = (const double *)w->d_ztrg.ptr;
-    int rc = STK_OK;
     if (f == 0) {
         if (n > 0) {
             wall_stage_stokes<<<grid_for(n), 256, 0, s>>>(n, d_sl, zs, w->sf, v[0], v[1], v[2], v[3]);
             WCUDA(cudaGetLastError());
         }
-        rc = Stk3DFMM_evaluate_fmm_device(h[0], STK_Stokes, v[0], u[0], nullptr, s);
-        if (!rc) rc = Stk3DFMM_evaluate_fmm_device(h[1], STK_LapPGrad, v[1], u[1], v[2], s);
-        if (!rc) rc = Stk3DFMM_evaluate_fmm_device(h[2], STK_LapPGradGrad, v[3], u[2], nullptr, s);
-        if (rc) return rc;
+        const double *sv[kSubs] = {v[0], v[1], v[3], nullptr}, *dv[kSubs] = {nullptr, v[2], nullptr, nullptr};
+        if (int rc2 = run_subs(w, f, sv, dv, u, s)) return rc2;
         if (nt > 0) {
             wall_assemble_stokes<<<grid_for(nt), 256, 0, s>>>(nt, zt, w->sf, sc, u[0], u[1], u[2], d_out);
             WCUDA(cudaGetLastError());
@@ -419,11 +447,8 @@ static int wall_eval(StkWallFMM *w, int f, const double *d_sl, double *d_out, cu
             wall_stage_rpy<<<grid_for(n), 256, 0, s>>>(n, d_sl, zs, w->sf, v[0], v[1], v[2], v[3], v[4], v[5]);
             WCUDA(cudaGetLastError());
         }
-        rc = Stk3DFMM_evaluate_fmm_device(h[0], STK_RPY, v[0], u[0], nullptr, s);
-        if (!rc) rc = Stk3DFMM_evaluate_fmm_device(h[1], STK_LapPGradGrad, v[1], u[1], v[2], s);
-        if (!rc) rc = Stk3DFMM_evaluate_fmm_device(h[2], STK_LapPGrad, v[3], u[2], v[4], s);
-        if (!rc) rc = Stk3DFMM_evaluate_fmm_device(h[3], STK_LapQPGradGrad, v[5], u[3], nullptr, s);
-        if (rc) return rc;
+        const double *sv[kSubs] = {v[0], v[1], v[3], v[5]}, *dv[kSubs] = {nullptr, v[2], v[4], nullptr};
+        if (int rc2 = run_subs(w, f, sv, dv, u, s)) return rc2;
         if (nt > 0) {
             wall_assemble_rpy<<<grid_for(nt), 256, 0, s>>>(nt, zt, w->sf, sc, u[0], u[1], u[2], u[3], d_out);
             WCUDA(cudaGetLastError());
