@@ -64,13 +64,29 @@ template <> __device__ __forceinline__ F2 cst<F2>(double c) { return splat((floa
 // masked reciprocal square root: 0 where r2 == 0 (the reference's
 // approx_rsqrt<digits>(r2, r2 > 0))
 #ifndef STK_RSQ64_NEWTON
-#define STK_RSQ64_NEWTON 2  // Newton steps after the hardware approximation; 0 = CUDA's rsqrt
+// refinement of the hardware approximation: -1 = one third-order step (below),
+// n > 0 = n Newton-Raphson steps, 0 = CUDA's rsqrt
+#define STK_RSQ64_NEWTON -1
 #endif
-#if STK_RSQ64_NEWTON
-// Hardware approximation (MUFU, rsqrt.approx.ftz.f64) refined by Newton-Raphson
-// steps y <- y + y e / 2 with e = 1 - r2 y^2 (quadratic convergence; e from one
-// rounded product and one fma).  r2 below the smallest normal double counts as
-// coincident (|r| < 1.5e-154).
+#if STK_RSQ64_NEWTON < 0
+// Hardware approximation (MUFU, rsqrt.approx.ftz.f64; relative error ~1e-6 as
+// measured here) refined by one step of the third-order Householder iteration
+// for 1/sqrt: with e = 1 - r2 y^2, 1/sqrt(r2) = y (1 - e)^(-1/2) and
+// (1 - e)^(-1/2) = 1 + e/2 + 3 e^2/8 + O(e^3), so y <- y + y e (1/2 + 3e/8)
+// leaves ~(5/16) e^3 ~ 1e-19 before rounding (5 FP64 operations, against 8 for
+// two Newton steps).  r2 below the smallest normal double counts as coincident
+// (|r| < 1.5e-154).
+__device__ __forceinline__ double rsq(double r2) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r2));
+    const double e = fma(-(r2 * y), y, 1.0);
+    const double t = e * fma(e, 0.375, 0.5);
+    y = fma(y, t, y);
+    return r2 >= 2.2250738585072014e-308 ? y : 0.0;
+}
+#elif STK_RSQ64_NEWTON
+// Hardware approximation refined by Newton-Raphson steps y <- y + y e / 2 with
+// e = 1 - r2 y^2 (quadratic convergence; e from one rounded product and one fma).
 __device__ __forceinline__ double rsq(double r2) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r2));

@@ -166,8 +166,8 @@ def test_invalid_arguments_fail_loudly(torch_cuda, L):
 
 
 def test_fp64_rsqrt_pointwise():
-    """The FP64 path's reciprocal square root (hardware approximation + two Newton
-    steps) to within a few ulp of 1/sqrt over 24 decades of r^2: laplace_p of one
+    """The FP64 path's reciprocal square root (hardware approximation + one third-order
+    step) to within a few ulp of 1/sqrt over 24 decades of r^2: laplace_p of one
     unit charge at the origin against q / (4 pi |r|) per target."""
     import torch
     assert torch.cuda.is_available()
