@@ -95,6 +95,16 @@ constexpr int kMixedDisp = kDispHiLo;
 #endif
 static_assert(kMixedDisp == kDispHiLo || kMixedDisp == kDispF64, "STK_MIXED_DISP must be 0 or 1");
 
+// Unroll of the source loop (tuning builds override it)
+#ifndef STK_P2P_UNROLL_MIXED
+#define STK_P2P_UNROLL_MIXED 2
+#endif
+#ifndef STK_P2P_UNROLL_FP64
+#define STK_P2P_UNROLL_FP64 2
+#endif
+#define STK_PRAGMA(x) _Pragma(#x)
+#define STK_UNROLL(n) STK_PRAGMA(unroll n)
+
 template <int UK, bool MIXED>
 __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2p_kernel(const ListP2PArgs a) {
     using K = Uk<UK>;
@@ -270,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 #pragma unroll
                 for (int k = 0; k < TDIM; k++) p0[k] = p1[k] = splat(0.0f);
                 // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
-#pragma unroll 2
+STK_UNROLL(STK_P2P_UNROLL_MIXED)
                 for (int j = 2 * sub; j < n; j += 2 * g) {
                     F2 s[NV];
 #pragma unroll
@@ -311,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                     acc1[k] = tt;
                 }
             } else {
-#pragma unroll 2
+STK_UNROLL(STK_P2P_UNROLL_FP64)
                 for (int j = sub; j < n; j += g) {
                     double s[NV];
 #pragma unroll
