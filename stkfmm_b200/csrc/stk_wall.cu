@@ -14,9 +14,9 @@
 //           (image quadrupoles, tree refined on sources and images).
 // Each sub-FMM is a unit-box Stk3DFMM handle of this library, so its trees,
 // operators and work lists stay resident.  The source values of the sub-FMMs
-// are formed on the device (one staging kernel), the sub-FMMs run back to back
-// on the wall's stream, and one assembly kernel combines their outputs with the
-// targets' heights.  The reference's box scaling (scaleSrc / scaleTrg applied
+// are formed on the device (one staging kernel), the sub-FMMs run concurrently
+// on their own handles' streams, and one assembly kernel on the wall's stream
+// combines their outputs with the targets' heights.  The reference's box scaling (scaleSrc / scaleTrg applied
 // by each sub-FMM with the wall's scale factor) is applied in the staging and
 // assembly kernels: DL values and RPY radii times sF, sub-FMM outputs times
 // sF^k (the kernel's trg_scale_pow).
