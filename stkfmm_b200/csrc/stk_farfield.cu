@@ -894,10 +894,12 @@ FarField::~FarField() {
     if (solver) cusolverDnDestroy(solver);
 }
 
-// Dense M2L of the complete levels (M2LDenseLevel).  A level l >= 3 qualifies
+// Dense M2L of the complete levels (M2LDenseLevel).  A level l >= 4 qualifies
 // when all 8^l boxes are present and its V lists hold at least 70% of 189 pairs
 // per box (periodic and deep uniform levels); the stacked factors and the work
-// buffers must fit in budgets (4 GiB each).  STKFMM_M2L_DENSE=0 turns it off.
+// buffers must fit in budgets (4 GiB each).  Smaller levels (<= 512 boxes, under
+// 1e5 pairs) stay on the chunked path, so small trees build no stacked factors.
+// STKFMM_M2L_DENSE=0 turns it off.
 static int setup_m2l_dense(FarField &F, const Octree &T, int nslot, cudaStream_t s) {
     F.dense.clear();
     const char *env = getenv("STKFMM_M2L_DENSE");
@@ -916,7 +918,7 @@ static int setup_m2l_dense(FarField &F, const Octree &T, int nslot, cudaStream_t
     };
     // candidate levels
     std::vector<int> levels;
-    for (int l = 3; l <= T.depth() && l < 10; l++) {
+    for (int l = 4; l <= T.depth() && l < 10; l++) {
         const long long n = (long long)T.level_begin[l + 1] - T.level_begin[l];
         if (n != (1LL << (3 * l))) continue;
         long long pairs = 0;

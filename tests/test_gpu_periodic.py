@@ -238,3 +238,29 @@ def test_periodic_quadrupole_potential(torch_cuda, pbc):
         pot -= pot.mean()
         ref -= ref.mean()
     assert np.linalg.norm(pot - ref) / np.linalg.norm(ref) < TOL[10]
+
+
+@pytest.mark.parametrize("kernel,pbc", [(8, 3), (1, 2)])
+def test_complete_level_m2l_matches_chunked(torch_cuda, monkeypatch, kernel, pbc):
+    """The per-type M2L of complete levels (4096 boxes at level 4 here) gives the
+    chunked per-offset M2L's result; STKFMM_M2L_DENSE=0 selects the chunked one."""
+    import stkfmm_b200 as S
+    pts, rng = points("uniform", 20000, 30 + kernel)
+    v = rng.normal(size=(len(pts), S.get_kernel_dimension(kernel)[0]))
+    v -= v.mean(0)
+    res = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("STKFMM_M2L_DENSE", mode)
+        fmm = S.Stk3DFMM(6, 8, pbc, kernel)
+        fmm.set_box(np.zeros(3), 1.0)
+        fmm.set_points(pts, pts, None)
+        fmm.setup_tree(kernel)
+        out = np.zeros((len(pts), S.get_kernel_dimension(kernel)[2]))
+        fmm.evaluate_fmm(kernel, v, out, None)
+        res[mode] = (out, fmm.m2l_work(kernel), fmm.tree_stats(kernel))
+    assert res["1"][2]["depth"] >= 4
+    # the dense path ran: no padded ranks or columns executed
+    assert res["1"][1]["flops_executed"] < res["0"][1]["flops_executed"]
+    assert res["1"][1]["flops_algorithmic"] == res["0"][1]["flops_algorithmic"]
+    a, b = res["0"][0], res["1"][0]
+    assert np.linalg.norm(b - a) / np.linalg.norm(a) < 1e-13
