@@ -95,7 +95,15 @@ enum stk_ukernel {
     STK_UK_LAPLACE_PGRADGRAD = 16,       /* 1 -> 10  LaplaceLayerKernel.hpp:138-166 */
     STK_UK_LAPLACE_DIPOLEPGRADGRAD = 17, /* 3 -> 10  LaplaceLayerKernel.hpp:168-200 */
     STK_UK_LAPLACE_QUADP = 18,           /* 9 -> 1   LaplaceLayerKernel.hpp:202-232 (S row-major) */
-    STK_UK_LAPLACE_QUADPGRADGRAD = 19    /* 9 -> 10  LaplaceLayerKernel.hpp:234-301 */
+    STK_UK_LAPLACE_QUADPGRADGRAD = 19,   /* 9 -> 10  LaplaceLayerKernel.hpp:234-301 */
+    /* Stokes derivatives: (p, u 3, grad p 3, grad u 9 as du_i/dx_j at 7 + 3i + j),
+     * (p, u 3, lap u 3), traction 3x3 row-major */
+    STK_UK_STOKES_PVELGRAD = 20,         /* 4 -> 16  StokesSingleLayerKernel.hpp:54-111 */
+    STK_UK_STOKES_DOUBLEPVELGRAD = 21,   /* 9 -> 16  StokesDoubleLayerKernel.hpp:64-143 */
+    STK_UK_STOKES_PVELLAPLACIAN = 22,    /* 4 -> 7   StokesSingleLayerKernel.hpp:118-155 */
+    STK_UK_STOKES_DOUBLELAPLACIAN = 23,  /* 9 -> 7   StokesDoubleLayerKernel.hpp:150-206 */
+    STK_UK_STOKES_TRACTION = 24,         /* 4 -> 9   StokesSingleLayerKernel.hpp:162-199 */
+    STK_UK_STOKES_DOUBLETRACTION = 25    /* 9 -> 9   StokesDoubleLayerKernel.hpp:213-276 */
 };
 
 /* ---- kernel descriptors --------------------------------------------------- */
@@ -191,8 +199,8 @@ int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
  * KIFMM far field, for LapPGrad, LapPGradGrad, LapQPGradGrad, Stokes, RPY,
- * StokesRegVel and PVel in free space, PX, PXY and PXYZ; the other kernels
- * return STK_ERR_NOT_SUPPORTED.
+ * StokesRegVel, PVel, PVelGrad, PVelLaplacian and Traction in free space, PX,
+ * PXY and PXYZ; StokesRegVelOmega returns STK_ERR_NOT_SUPPORTED.
  * Triply periodic potentials / pressures / mean velocities carry a constant
  * per component (drift) set by the equivalent density, as in the reference. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
@@ -355,6 +363,18 @@ void stk_ker_laplace_dipolepgradgrad(double *r_src, int src_cnt, double *v_src, 
 void stk_ker_laplace_quadp(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
                            double *k_out, void *mem_mgr);
 void stk_ker_laplace_quadpgradgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                   double *k_out, void *mem_mgr);
+void stk_ker_stokes_pvelgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                             double *k_out, void *mem_mgr);
+void stk_ker_stokes_doublepvelgrad(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                   double *k_out, void *mem_mgr);
+void stk_ker_stokes_pvellaplacian(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                  double *k_out, void *mem_mgr);
+void stk_ker_stokes_doublelaplacian(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                    double *k_out, void *mem_mgr);
+void stk_ker_stokes_traction(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                             double *k_out, void *mem_mgr);
+void stk_ker_stokes_doubletraction(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
                                    double *k_out, void *mem_mgr);
 /* status of the last ker_poten shim call on this thread (they return void) */
 int stk_ker_last_status(void);

@@ -18,7 +18,8 @@ typedef void (*kernel_func)(double *, double *, double *, double *);
 // Selector values (stable, used by oracle/oracle.py):
 //   0 StokesSL  1 LaplaceSLPGrad  2 LaplaceDLPGrad  3 StokesSLRPY
 //   4 StokesRegSLVel  5 StokesSLPVel  6 StokesDLPVel  7 LaplaceSLPGradGrad
-//   8 LaplaceDLPGradGrad  9 LaplaceQPGradGrad
+//   8 LaplaceDLPGradGrad  9 LaplaceQPGradGrad  10 StokesSLPVelGrad  11 StokesDLPVelGrad
+//   12 StokesSLPVelLaplacian  13 StokesDLPVelLaplacian  14 StokesSLTraction  15 StokesDLTraction
 static kernel_func pick(int which) {
     switch (which) {
     case 0: return StokesSL;
@@ -31,6 +32,12 @@ static kernel_func pick(int which) {
     case 7: return LaplaceSLPGradGrad;
     case 8: return LaplaceDLPGradGrad;
     case 9: return LaplaceQPGradGrad;
+    case 10: return StokesSLPVelGrad;
+    case 11: return StokesDLPVelGrad;
+    case 12: return StokesSLPVelLaplacian;
+    case 13: return StokesDLPVelLaplacian;
+    case 14: return StokesSLTraction;
+    case 15: return StokesDLTraction;
     default: return nullptr;
     }
 }

@@ -49,11 +49,17 @@ enum {
     UK_LAPLACE_DIPOLEPGRADGRAD = 17, /* d(3) -> (10)                LaplaceLayerKernel.hpp:168-200 */
     UK_LAPLACE_QUADP = 18,           /* S(9) -> p(1)                LaplaceLayerKernel.hpp:202-232 */
     UK_LAPLACE_QUADPGRADGRAD = 19,   /* S(9) -> (10)                LaplaceLayerKernel.hpp:234-301 */
-    UK_COUNT = 20
+    UK_STOKES_PVELGRAD = 20,         /* f,trD(4) -> (16)            StokesSingleLayerKernel.hpp:54-111 */
+    UK_STOKES_DOUBLEPVELGRAD = 21,   /* D(9) -> (16)                StokesDoubleLayerKernel.hpp:64-143 */
+    UK_STOKES_PVELLAPLACIAN = 22,    /* f,trD(4) -> (7)             StokesSingleLayerKernel.hpp:118-155 */
+    UK_STOKES_DOUBLELAPLACIAN = 23,  /* D(9) -> (7)                 StokesDoubleLayerKernel.hpp:150-206 */
+    UK_STOKES_TRACTION = 24,         /* f,trD(4) -> (9)             StokesSingleLayerKernel.hpp:162-199 */
+    UK_STOKES_DOUBLETRACTION = 25,   /* D(9) -> (9)                 StokesDoubleLayerKernel.hpp:213-276 */
+    UK_COUNT = 26
 };
 
-static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9};
-static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10};
+static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9};
+static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9};
 
 static int uk_valid(int uk) { return uk >= 0 && uk < UK_COUNT && uk_sdim[uk] > 0; }
 
@@ -69,6 +75,9 @@ int oracle_uk_dims(int uk, int *sdim, int *tdim) {
 /* ScaleFactor() of each micro-kernel: 1/(4 pi) for Laplace, 1/(8 pi) for the
  * Stokes family (e.g. LaplaceLayerKernel.hpp:44-46, RPYKernel.hpp:20-22). */
 double oracle_uk_scale(int uk) {
+    if (uk == UK_STOKES_TRACTION) return -3.0 / (4.0 * PI_);       /* StokesSingleLayerKernel.hpp:166-168 */
+    if (uk == UK_STOKES_DOUBLETRACTION) return -3.0 / (8.0 * PI_); /* StokesDoubleLayerKernel.hpp:217-219 */
+    if (uk >= UK_STOKES_PVELGRAD) return 1.0 / (8.0 * PI_);
     return (uk <= UK_LAPLACE_DIPOLEPGRAD || uk >= UK_LAPLACE_PGRADGRAD) ? 1.0 / (4.0 * PI_) : 1.0 / (8.0 * PI_);
 }
 
@@ -299,6 +308,115 @@ static void uk_pair(int uk, const double r[3], const double *f, double *u) {
                          3.0 * r4 * (syz + szy));
         u[9] += rinv9 * (105.0 * dz * dz * rrQ - r2 * 15.0 * (rrQ + dz * 2.0 * (az + bz) + dz * dz * tr) +
                          3.0 * r4 * (tr + 2.0 * szz));
+    } break;
+    case UK_STOKES_PVELGRAD:        /* StokesSingleLayerKernel.hpp:61-110 */
+    case UK_STOKES_PVELLAPLACIAN: { /* StokesSingleLayerKernel.hpp:125-154 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        const double fx = f[0], fy = f[1], fz = f[2], tr = f[3];
+        double cc = fx * dx + fy * dy + fz * dz;
+        u[0] += 2.0 * rinv3 * cc;
+        cc -= tr;
+        u[1] += rinv3 * (r2 * fx + cc * dx);
+        u[2] += rinv3 * (r2 * fy + cc * dy);
+        u[3] += rinv3 * (r2 * fz + cc * dz);
+        cc += tr;
+        u[4] += 2.0 * (r2 * fx - 3.0 * dx * cc) * rinv5;
+        u[5] += 2.0 * (r2 * fy - 3.0 * dy * cc) * rinv5;
+        u[6] += 2.0 * (r2 * fz - 3.0 * dz * cc) * rinv5;
+        if (uk == UK_STOKES_PVELLAPLACIAN) break;
+        double qxx = r2 - 3.0 * dx * dx, qxy = -3.0 * dx * dy, qxz = -3.0 * dx * dz;
+        double qyy = r2 - 3.0 * dy * dy, qyz = -3.0 * dy * dz, qzz = r2 - 3.0 * dz * dz;
+        cc -= tr;
+        u[7] += qxx * cc * rinv5;
+        u[8] += (qxy * cc + r2 * (dx * fy - dy * fx)) * rinv5;
+        u[9] += (qxz * cc + r2 * (dx * fz - dz * fx)) * rinv5;
+        u[10] += (qxy * cc + r2 * (dy * fx - dx * fy)) * rinv5;
+        u[11] += qyy * cc * rinv5;
+        u[12] += (qyz * cc + r2 * (dy * fz - dz * fy)) * rinv5;
+        u[13] += (qxz * cc + r2 * (dz * fx - dx * fz)) * rinv5;
+        u[14] += (qyz * cc + r2 * (dz * fy - dy * fz)) * rinv5;
+        u[15] += qzz * cc * rinv5;
+    } break;
+    case UK_STOKES_TRACTION: { /* StokesSingleLayerKernel.hpp:169-198 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rinv5 = rinv3 * rinv * rinv;
+        const double tr = f[3];
+        double cc = (f[0] * dx + f[1] * dy + f[2] * dz - tr) * rinv5;
+        double diag = tr * r2 * rinv5 * 0.3333333333333333333;
+        const double d[3] = {dx, dy, dz};
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) u[3 * i + j] += d[i] * d[j] * cc + (i == j ? diag : 0.0);
+    } break;
+    case UK_STOKES_DOUBLEPVELGRAD:    /* StokesDoubleLayerKernel.hpp:71-142 */
+    case UK_STOKES_DOUBLELAPLACIAN: { /* StokesDoubleLayerKernel.hpp:157-205 */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double rinv3 = rinv * rinv2;
+        double rinv5 = rinv3 * rinv2;
+        double rinv7 = rinv5 * rinv2;
+        const double sxx = f[0], sxy = f[1], sxz = f[2], syx = f[3], syy = f[4], syz = f[5];
+        const double szx = f[6], szy = f[7], szz = f[8];
+        double cc = sxx * dx * dx + syy * dy * dy + szz * dz * dz;
+        cc += (sxy + syx) * dx * dy;
+        cc += (sxz + szx) * dx * dz;
+        cc += (syz + szy) * dy * dz;
+        double ccn3 = -3.0 * cc, cc5 = 5.0 * cc;
+        const double trace = sxx + syy + szz;
+        double ax = dx * sxx + dy * sxy + dz * sxz, ay = dx * syx + dy * syy + dz * syz;
+        double az = dx * szx + dy * szy + dz * szz;
+        double bx = dx * sxx + dy * syx + dz * szx, by = dx * sxy + dy * syy + dz * szy;
+        double bz = dx * sxz + dy * syz + dz * szz;
+        u[0] += 2.0 * (ccn3 + r2 * trace) * rinv5;
+        u[1] += rinv5 * dx * ccn3;
+        u[2] += rinv5 * dy * ccn3;
+        u[3] += rinv5 * dz * ccn3;
+        rinv7 *= -3.0;
+        u[4] -= 2.0 * rinv7 * (dx * cc5 - r2 * ((ax + bx) + dx * trace));
+        u[5] -= 2.0 * rinv7 * (dy * cc5 - r2 * ((ay + by) + dy * trace));
+        u[6] -= 2.0 * rinv7 * (dz * cc5 - r2 * ((az + bz) + dz * trace));
+        if (uk == UK_STOKES_DOUBLELAPLACIAN) break;
+        /* rinv7 keeps its factor -3 here, as in the reference */
+        double ccn1 = -cc;
+        double e0 = -2.0 * dx * sxx - dy * (sxy + syx) - dz * (sxz + szx);
+        double e1 = -2.0 * dy * syy - dx * (sxy + syx) - dz * (syz + szy);
+        double e2 = -2.0 * dz * szz - dx * (sxz + szx) - dy * (syz + szy);
+        const double d[3] = {dx, dy, dz}, e[3] = {e0, e1, e2};
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                u[7 + 3 * i + j] += (5.0 * ccn1 * d[i] * d[j] - r2 * d[i] * e[j] - (i == j ? r2 * ccn1 : 0.0)) * rinv7;
+    } break;
+    case UK_STOKES_DOUBLETRACTION: { /* StokesDoubleLayerKernel.hpp:220-275; 2/3 truncated as there */
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv2 = rinv * rinv;
+        double rinv3 = rinv * rinv2;
+        double rinv5 = rinv3 * rinv2;
+        double rinv7 = rinv5 * rinv2;
+        const double sxx = f[0], sxy = f[1], sxz = f[2], syx = f[3], syy = f[4], syz = f[5];
+        const double szx = f[6], szy = f[7], szz = f[8];
+        double cc = sxx * dx * dx + syy * dy * dy + szz * dz * dz;
+        cc += (sxy + syx) * dx * dy;
+        cc += (sxz + szx) * dx * dz;
+        cc += (syz + szy) * dy * dz;
+        double ccn3 = -3.0 * cc;
+        double trace = sxx + syy + szz;
+        double e0 = -2.0 * dx * sxx - dy * (sxy + syx) - dz * (sxz + szx);
+        double e1 = -2.0 * dy * syy - dx * (sxy + syx) - dz * (syz + szy);
+        double e2 = -2.0 * dz * szz - dx * (sxz + szx) - dy * (syz + szy);
+        double np = r2 * 0.66666666666666 * rinv7 * (ccn3 + r2 * trace);
+        const double d[3] = {dx, dy, dz}, e[3] = {e0, e1, e2};
+        double tv[9];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                tv[3 * i + j] = (-5.0 * cc * d[i] * d[j] - r2 * d[i] * e[j] + (i == j ? r2 * cc : 0.0)) * rinv7;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) u[3 * i + j] += (i == j ? np : 0.0) + tv[3 * i + j] + tv[3 * j + i];
     } break;
     default:
         break;

@@ -92,7 +92,9 @@ SIGNATURES = [
 ]
 KER_SHIMS = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel", "rpy_u",
              "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel", "laplace_pgradgrad",
-             "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad"]
+             "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad", "stokes_pvelgrad",
+             "stokes_doublepvelgrad", "stokes_pvellaplacian", "stokes_doublelaplacian", "stokes_traction",
+             "stokes_doubletraction"]
 for _n in KER_SHIMS:
     SIGNATURES.append(("stk_ker_" + _n, None, [P_d, c_int, P_d, c_int, P_d, c_int, P_d, c_void_p]))
 

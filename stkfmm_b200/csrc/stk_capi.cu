@@ -352,3 +352,9 @@ STK_KER_SHIM(laplace_pgradgrad, UK_LAPLACE_PGRADGRAD)
 STK_KER_SHIM(laplace_dipolepgradgrad, UK_LAPLACE_DIPOLEPGRADGRAD)
 STK_KER_SHIM(laplace_quadp, UK_LAPLACE_QUADP)
 STK_KER_SHIM(laplace_quadpgradgrad, UK_LAPLACE_QUADPGRADGRAD)
+STK_KER_SHIM(stokes_pvelgrad, UK_STOKES_PVELGRAD)
+STK_KER_SHIM(stokes_doublepvelgrad, UK_STOKES_DOUBLEPVELGRAD)
+STK_KER_SHIM(stokes_pvellaplacian, UK_STOKES_PVELLAPLACIAN)
+STK_KER_SHIM(stokes_doublelaplacian, UK_STOKES_DOUBLELAPLACIAN)
+STK_KER_SHIM(stokes_traction, UK_STOKES_TRACTION)
+STK_KER_SHIM(stokes_doubletraction, UK_STOKES_DOUBLETRACTION)

@@ -72,10 +72,20 @@ static const KernelInfo kKernels[] = {
      {UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL, UK_STOKES_PVEL,
       UK_STOKES_PVEL, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL},
      {2, 1, 1, 1}, 1},
-    {256, "stokes_PVelGrad", 4, 9, 16, {-1, -1, -1, -1, -1, -1, -1, -1, -1},
+    // StokesLayerKernel<T>::PVelGrad / PVelLaplacian / Traction (StokesLayerKernel.hpp:52-94):
+    // stokes_PVel translations and check potentials, the derivative kernel for S2T, M2T, L2T
+    {256, "stokes_PVelGrad", 4, 9, 16,
+     {UK_STOKES_PVELGRAD, UK_STOKES_DOUBLEPVELGRAD, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL,
+      UK_STOKES_PVELGRAD, UK_STOKES_PVELGRAD, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL},
      {2, 1, 1, 1, 3, 3, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2}, 1},
-    {512, "stokes_PVelLaplacian", 4, 9, 7, {-1, -1, -1, -1, -1, -1, -1, -1, -1}, {2, 1, 1, 1, 3, 3, 3}, 1},
-    {1024, "stokes_Traction", 4, 9, 9, {-1, -1, -1, -1, -1, -1, -1, -1, -1}, {2, 2, 2, 2, 2, 2, 2, 2, 2}, 1},
+    {512, "stokes_PVelLaplacian", 4, 9, 7,
+     {UK_STOKES_PVELLAPLACIAN, UK_STOKES_DOUBLELAPLACIAN, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL,
+      UK_STOKES_PVELLAPLACIAN, UK_STOKES_PVELLAPLACIAN, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL},
+     {2, 1, 1, 1, 3, 3, 3}, 1},
+    {1024, "stokes_Traction", 4, 9, 9,
+     {UK_STOKES_TRACTION, UK_STOKES_DOUBLETRACTION, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL,
+      UK_STOKES_TRACTION, UK_STOKES_TRACTION, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL},
+     {2, 2, 2, 2, 2, 2, 2, 2, 2}, 1},
 };
 constexpr int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
 

@@ -451,6 +451,12 @@ cudaError_t launch_list_p2p(int uk, int prec, const ListP2PArgs &a, int num_sms,
     case UK_LAPLACE_DIPOLEPGRADGRAD: return launch_prec<UK_LAPLACE_DIPOLEPGRADGRAD>(prec, a, num_sms, stream);
     case UK_LAPLACE_QUADP: return launch_prec<UK_LAPLACE_QUADP>(prec, a, num_sms, stream);
     case UK_LAPLACE_QUADPGRADGRAD: return launch_prec<UK_LAPLACE_QUADPGRADGRAD>(prec, a, num_sms, stream);
+    case UK_STOKES_PVELGRAD: return launch_prec<UK_STOKES_PVELGRAD>(prec, a, num_sms, stream);
+    case UK_STOKES_DOUBLEPVELGRAD: return launch_prec<UK_STOKES_DOUBLEPVELGRAD>(prec, a, num_sms, stream);
+    case UK_STOKES_PVELLAPLACIAN: return launch_prec<UK_STOKES_PVELLAPLACIAN>(prec, a, num_sms, stream);
+    case UK_STOKES_DOUBLELAPLACIAN: return launch_prec<UK_STOKES_DOUBLELAPLACIAN>(prec, a, num_sms, stream);
+    case UK_STOKES_TRACTION: return launch_prec<UK_STOKES_TRACTION>(prec, a, num_sms, stream);
+    case UK_STOKES_DOUBLETRACTION: return launch_prec<UK_STOKES_DOUBLETRACTION>(prec, a, num_sms, stream);
     case UK_REGVEL_ADJ_SRC:
         if (!a.trg_aux) return cudaErrorInvalidValue;
         return launch_prec<UK_REGVEL_ADJ_SRC>(prec, a, num_sms, stream);

@@ -34,6 +34,12 @@
 //   laplace_dipolepgradgrad Lib/include/STKFMM/LaplaceLayerKernel.hpp:168-200
 //   laplace_quadp        Lib/include/STKFMM/LaplaceLayerKernel.hpp:202-232
 //   laplace_quadpgradgrad Lib/include/STKFMM/LaplaceLayerKernel.hpp:234-301
+//   stokes_pvelgrad      Lib/include/STKFMM/StokesSingleLayerKernel.hpp:54-111
+//   stokes_pvellaplacian Lib/include/STKFMM/StokesSingleLayerKernel.hpp:118-155
+//   stokes_traction      Lib/include/STKFMM/StokesSingleLayerKernel.hpp:162-199
+//   stokes_doublepvelgrad Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:64-143
+//   stokes_doublelaplacian Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:150-206
+//   stokes_doubletraction Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:213-276
 // Two fused variants (no single reference function) evaluate a single-layer
 // and a double-layer source at the same point in one pass:
 //   laplace_pgrad + laplace_dipolepgrad, stokes_pvel + stokes_doublepvel.
@@ -141,11 +147,21 @@ enum UkId : int {
     UK_LAPLACE_DIPOLEPGRADGRAD = 17,
     UK_LAPLACE_QUADP = 18,
     UK_LAPLACE_QUADPGRADGRAD = 19,
-    UK_COUNT = 20
+    UK_STOKES_PVELGRAD = 20,
+    UK_STOKES_DOUBLEPVELGRAD = 21,
+    UK_STOKES_PVELLAPLACIAN = 22,
+    UK_STOKES_DOUBLELAPLACIAN = 23,
+    UK_STOKES_TRACTION = 24,
+    UK_STOKES_DOUBLETRACTION = 25,
+    UK_COUNT = 26
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
 constexpr double kInv8Pi = 0.039788735772973833942220940843128591;  // 1/(8 pi)
+constexpr double kTracSL = -0.23873241463784300365332564505877155;  // -3/(4 pi), stokes_traction
+constexpr double kTracDL = -0.11936620731892150182666282252938578;  // -3/(8 pi), stokes_doubletraction
+// the reference's truncated 2/3 of stokes_doubletraction (StokesDoubleLayerKernel.hpp:234)
+constexpr double kTwoThirdsTrunc = 0.66666666666666;
 // the reference's truncated 1/3 of rpy_u / rpy_ulapu (RPYKernel.hpp:30,66)
 constexpr double kRpyThird = 0.3333333333333;
 
@@ -735,6 +751,241 @@ template <> struct Uk<UK_LAPLACE_QUADPGRADGRAD> {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Stokes pressure / velocity derivatives.  Outputs of the PVelGrad kernels:
+// (p, u 3, grad p 3, grad u 9 with u[7 + 3i + j] = d u_i / d x_j); PVelLaplacian:
+// (p, u 3, lap u 3); Traction: the 3x3 stress-like tensor, row-major.
+// ---------------------------------------------------------------------------
+
+// Single layer, values (f, trD), cc = f.r, c1 = cc - trD:
+//   p = 2 cc / r^3, u = f / r + c1 r / r^3, grad p = lap u = 2 f / r^3 - 6 cc r / r^5,
+//   d u_i / d x_j = c1 (d_ij r^2 - 3 r_i r_j) / r^5 + (r_i f_j - r_j f_i) / r^3.
+// staged (f, trD, 2 f)
+struct StokesSLGrad {
+    static __device__ void stage(const double *f, double *v) {
+        for (int k = 0; k < 4; k++) v[k] = f[k];
+        for (int k = 0; k < 3; k++) v[4 + k] = 2.0 * f[k];
+    }
+    // p, u and grad p (= lap u): outputs 0..6; returns c1
+    template <class V, int N>
+    static __device__ __forceinline__ V pvel_gradp(V (&u)[N], V dx, V dy, V dz, const V *v, V rinv, V rinv2,
+                                                   V rinv3) {
+        V cc = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz));
+        u[0] = fmav(cc + cc, rinv3, u[0]);
+        V c1 = cc - v[3];
+        V a = c1 * rinv3;
+        u[1] = fmav(a, dx, fmav(v[0], rinv, u[1]));
+        u[2] = fmav(a, dy, fmav(v[1], rinv, u[2]));
+        u[3] = fmav(a, dz, fmav(v[2], rinv, u[3]));
+        V g = (cc * rinv2) * (rinv3 * cst<V>(-6.0));
+        u[4] = fmav(g, dx, fmav(v[4], rinv3, u[4]));
+        u[5] = fmav(g, dy, fmav(v[5], rinv3, u[5]));
+        u[6] = fmav(g, dz, fmav(v[6], rinv3, u[6]));
+        return c1;
+    }
+};
+
+template <> struct Uk<UK_STOKES_PVELGRAD> {
+    static constexpr int SDIM = 4, TDIM = 16, NV = 7;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesSLGrad::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c1 = StokesSLGrad::pvel_gradp(u, dx, dy, dz, v, rinv, rinv2, rinv3);
+        V a = c1 * rinv3;                             // d_ij part
+        V b = (c1 * rinv2) * (rinv3 * cst<V>(-3.0));  // r_i r_j part
+        V bx = b * dx, by = b * dy, bz = b * dz;
+        V wxy = (dx * v[1] - dy * v[0]) * rinv3;
+        V wxz = (dx * v[2] - dz * v[0]) * rinv3;
+        V wyz = (dy * v[2] - dz * v[1]) * rinv3;
+        V sxy = bx * dy, sxz = bx * dz, syz = by * dz;
+        u[7] = u[7] + fmav(bx, dx, a);
+        u[8] = u[8] + (sxy + wxy);
+        u[9] = u[9] + (sxz + wxz);
+        u[10] = u[10] + (sxy - wxy);
+        u[11] = u[11] + fmav(by, dy, a);
+        u[12] = u[12] + (syz + wyz);
+        u[13] = u[13] + (sxz - wxz);
+        u[14] = u[14] + (syz - wyz);
+        u[15] = u[15] + fmav(bz, dz, a);
+    }
+};
+
+template <> struct Uk<UK_STOKES_PVELLAPLACIAN> {
+    static constexpr int SDIM = 4, TDIM = 7, NV = 7;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesSLGrad::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        (void)StokesSLGrad::pvel_gradp(u, dx, dy, dz, v, rinv, rinv2, rinv3);
+    }
+};
+
+// stokes_traction (scale -3/(4 pi)): T_ij = (f.r - trD) r_i r_j / r^5 + d_ij trD / (3 r^3).
+// staged (f, trD, trD / 3)
+template <> struct Uk<UK_STOKES_TRACTION> {
+    static constexpr int SDIM = 4, TDIM = 9, NV = 5;
+    static constexpr double SCALE = kTracSL;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        for (int k = 0; k < 4; k++) v[k] = f[k];
+        v[4] = f[3] * (1.0 / 3.0);
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V c = (fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) - v[3]) * (rinv3 * rinv2);
+        V dg = v[4] * rinv3;
+        V cx = c * dx, cy = c * dy, cz = c * dz;
+        u[0] = u[0] + fmav(cx, dx, dg);
+        u[1] = fmav(cx, dy, u[1]);
+        u[2] = fmav(cx, dz, u[2]);
+        u[3] = fmav(cy, dx, u[3]);
+        u[4] = u[4] + fmav(cy, dy, dg);
+        u[5] = fmav(cy, dz, u[5]);
+        u[6] = fmav(cz, dx, u[6]);
+        u[7] = fmav(cz, dy, u[7]);
+        u[8] = u[8] + fmav(cz, dz, dg);
+    }
+};
+
+// Double layer, D row-major, g = (D + D^T) r, C = r^T D r = (r.g)/2, C2 = C / r^2:
+//   p = (2 tr - 6 C2) / r^3, u = -3 C2 r / r^3, grad p = lap u = 6 ((5 C2 - tr) r - g) / r^5,
+//   d u_i / d x_j = -3 (r_i e_j + C d_ij) / r^5 with e = g - 5 C2 r.
+// staged (2 D00, 2 D11, 2 D22, D01 + D10, D02 + D20, D12 + D21, -tr, 2 tr)
+struct StokesDLGrad {
+    static __device__ void stage(const double *f, double *v) {
+        v[0] = 2.0 * f[0];
+        v[1] = 2.0 * f[4];
+        v[2] = 2.0 * f[8];
+        v[3] = f[1] + f[3];
+        v[4] = f[2] + f[6];
+        v[5] = f[5] + f[7];
+        const double tr = f[0] + f[4] + f[8];
+        v[6] = -tr;
+        v[7] = 2.0 * tr;
+    }
+    template <class V>
+    static __device__ __forceinline__ V gvec(V dx, V dy, V dz, const V *v, V &gx, V &gy, V &gz) {
+        gx = fmav(v[0], dx, fmav(v[3], dy, v[4] * dz));
+        gy = fmav(v[3], dx, fmav(v[1], dy, v[5] * dz));
+        gz = fmav(v[4], dx, fmav(v[5], dy, v[2] * dz));
+        return fmav(gx, dx, fmav(gy, dy, gz * dz)) * cst<V>(0.5);  // C
+    }
+    // p, u and grad p: outputs 0..6
+    template <class V, int N>
+    static __device__ __forceinline__ void pvel_gradp(V (&u)[N], V dx, V dy, V dz, const V *v, V rinv3, V rinv5,
+                                                      V C2, V gx, V gy, V gz) {
+        u[0] = fmav(fmav(C2, cst<V>(-6.0), v[7]), rinv3, u[0]);
+        V a = (C2 * cst<V>(-3.0)) * rinv3;
+        u[1] = fmav(a, dx, u[1]);
+        u[2] = fmav(a, dy, u[2]);
+        u[3] = fmav(a, dz, u[3]);
+        V h = fmav(C2, cst<V>(5.0), v[6]);
+        V e6 = rinv5 * cst<V>(6.0);
+        u[4] = fmav(e6, h * dx - gx, u[4]);
+        u[5] = fmav(e6, h * dy - gy, u[5]);
+        u[6] = fmav(e6, h * dz - gz, u[6]);
+    }
+};
+
+template <> struct Uk<UK_STOKES_DOUBLEPVELGRAD> {
+    static constexpr int SDIM = 9, TDIM = 16, NV = 8;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesDLGrad::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V rinv5 = rinv3 * rinv2;
+        V gx, gy, gz;
+        V C = StokesDLGrad::gvec(dx, dy, dz, v, gx, gy, gz);
+        V C2 = C * rinv2;
+        StokesDLGrad::pvel_gradp(u, dx, dy, dz, v, rinv3, rinv5, C2, gx, gy, gz);
+        V m = C2 * cst<V>(-5.0);
+        V s3 = rinv5 * cst<V>(-3.0);
+        V ex = fmav(m, dx, gx) * s3, ey = fmav(m, dy, gy) * s3, ez = fmav(m, dz, gz) * s3;
+        V dg = C * s3;
+        u[7] = u[7] + fmav(dx, ex, dg);
+        u[8] = fmav(dx, ey, u[8]);
+        u[9] = fmav(dx, ez, u[9]);
+        u[10] = fmav(dy, ex, u[10]);
+        u[11] = u[11] + fmav(dy, ey, dg);
+        u[12] = fmav(dy, ez, u[12]);
+        u[13] = fmav(dz, ex, u[13]);
+        u[14] = fmav(dz, ey, u[14]);
+        u[15] = u[15] + fmav(dz, ez, dg);
+    }
+};
+
+template <> struct Uk<UK_STOKES_DOUBLELAPLACIAN> {
+    static constexpr int SDIM = 9, TDIM = 7, NV = 8;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesDLGrad::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V gx, gy, gz;
+        V C = StokesDLGrad::gvec(dx, dy, dz, v, gx, gy, gz);
+        StokesDLGrad::pvel_gradp(u, dx, dy, dz, v, rinv3, rinv3 * rinv2, C * rinv2, gx, gy, gz);
+    }
+};
+
+// stokes_doubletraction (scale -3/(8 pi)):
+//   T_ij = np d_ij + (r_i e_j + r_j e_i + 2 C d_ij) / r^5,
+//   np = k (tr - 3 C2) / r^3 with the reference's k = 0.66666666666666.
+// staged (2 D00, 2 D11, 2 D22, D01 + D10, D02 + D20, D12 + D21, k tr)
+template <> struct Uk<UK_STOKES_DOUBLETRACTION> {
+    static constexpr int SDIM = 9, TDIM = 9, NV = 7;
+    static constexpr double SCALE = kTracDL;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        double w[8];
+        StokesDLGrad::stage(f, w);
+        for (int k = 0; k < 6; k++) v[k] = w[k];
+        v[6] = kTwoThirdsTrunc * (f[0] + f[4] + f[8]);
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv2 = rinv * rinv;
+        V rinv3 = rinv2 * rinv;
+        V rinv5 = rinv3 * rinv2;
+        V gx, gy, gz;
+        V C = StokesDLGrad::gvec(dx, dy, dz, v, gx, gy, gz);
+        V C2 = C * rinv2;
+        V np = fmav(C2, cst<V>(-3.0 * kTwoThirdsTrunc), v[6]) * rinv3;
+        V m = C2 * cst<V>(-5.0);
+        V ex = fmav(m, dx, gx) * rinv5, ey = fmav(m, dy, gy) * rinv5, ez = fmav(m, dz, gz) * rinv5;
+        V dg = fmav(C + C, rinv5, np);
+        V txy = fmav(dx, ey, dy * ex), txz = fmav(dx, ez, dz * ex), tyz = fmav(dy, ez, dz * ey);
+        u[0] = u[0] + fmav(dx + dx, ex, dg);
+        u[1] = u[1] + txy;
+        u[2] = u[2] + txz;
+        u[3] = u[3] + txy;
+        u[4] = u[4] + fmav(dy + dy, ey, dg);
+        u[5] = u[5] + tyz;
+        u[6] = u[6] + txz;
+        u[7] = u[7] + tyz;
+        u[8] = u[8] + fmav(dz + dz, ez, dg);
+    }
+};
+
 // Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
@@ -743,7 +994,9 @@ __host__ __device__ constexpr int uk_sdim(int id) {
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 9 : id == UK_LAPLACE_SLDL_PGRAD ? 4
          : id == UK_STOKES_SLDL_PVEL ? 13 : id == UK_REGVEL_ADJ_SRC ? 3 : id == UK_REGVEL_ADJ_TRG ? 4
          : id == UK_LAPLACE_SLDL_P ? 4 : id == UK_LAPLACE_PGRADGRAD ? 1 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 3
-         : id == UK_LAPLACE_QUADP ? 9 : id == UK_LAPLACE_QUADPGRADGRAD ? 9 : 0;
+         : id == UK_LAPLACE_QUADP ? 9 : id == UK_LAPLACE_QUADPGRADGRAD ? 9 : id == UK_STOKES_PVELGRAD ? 4
+         : id == UK_STOKES_DOUBLEPVELGRAD ? 9 : id == UK_STOKES_PVELLAPLACIAN ? 4 : id == UK_STOKES_DOUBLELAPLACIAN ? 9
+         : id == UK_STOKES_TRACTION ? 4 : id == UK_STOKES_DOUBLETRACTION ? 9 : 0;
 }
 __host__ __device__ constexpr int uk_tdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 4 : id == UK_LAPLACE_DIPOLEP ? 1
@@ -752,14 +1005,19 @@ __host__ __device__ constexpr int uk_tdim(int id) {
          : id == UK_STOKES_PVEL ? 4 : id == UK_STOKES_DOUBLEPVEL ? 4 : id == UK_LAPLACE_SLDL_PGRAD ? 4
          : id == UK_STOKES_SLDL_PVEL ? 4 : id == UK_REGVEL_ADJ_SRC ? 7 : id == UK_REGVEL_ADJ_TRG ? 3
          : id == UK_LAPLACE_SLDL_P ? 1 : id == UK_LAPLACE_PGRADGRAD ? 10 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 10
-         : id == UK_LAPLACE_QUADP ? 1 : id == UK_LAPLACE_QUADPGRADGRAD ? 10 : 0;
+         : id == UK_LAPLACE_QUADP ? 1 : id == UK_LAPLACE_QUADPGRADGRAD ? 10 : id == UK_STOKES_PVELGRAD ? 16
+         : id == UK_STOKES_DOUBLEPVELGRAD ? 16 : id == UK_STOKES_PVELLAPLACIAN ? 7 : id == UK_STOKES_DOUBLELAPLACIAN ? 7
+         : id == UK_STOKES_TRACTION ? 9 : id == UK_STOKES_DOUBLETRACTION ? 9 : 0;
 }
 // per-output-point (target-side) values a micro-kernel reads
 __host__ __device__ constexpr int uk_tvdim(int id) {
     return id == UK_REGVEL_ADJ_SRC ? 4 : id == UK_REGVEL_ADJ_TRG ? 3 : 0;
 }
 __host__ __device__ constexpr double uk_scale(int id) {
-    return id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD || id >= UK_LAPLACE_SLDL_P ? kInv4Pi
+    return id == UK_STOKES_TRACTION ? kTracSL
+         : id == UK_STOKES_DOUBLETRACTION ? kTracDL
+         : id >= UK_STOKES_PVELGRAD ? kInv8Pi
+         : id <= UK_LAPLACE_DIPOLEPGRAD || id == UK_LAPLACE_SLDL_PGRAD || id >= UK_LAPLACE_SLDL_P ? kInv4Pi
                                                                                                 : kInv8Pi;
 }
 

@@ -79,10 +79,16 @@ class UKERNEL(enum.IntEnum):
     LAPLACE_DIPOLEPGRADGRAD = 17
     LAPLACE_QUADP = 18
     LAPLACE_QUADPGRADGRAD = 19
+    STOKES_PVELGRAD = 20
+    STOKES_DOUBLEPVELGRAD = 21
+    STOKES_PVELLAPLACIAN = 22
+    STOKES_DOUBLELAPLACIAN = 23
+    STOKES_TRACTION = 24
+    STOKES_DOUBLETRACTION = 25
 
 
 SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.LapPGradGrad, KERNEL.LapQPGradGrad, KERNEL.Stokes, KERNEL.RPY,
-                     KERNEL.StokesRegVel, KERNEL.PVel)
+                     KERNEL.StokesRegVel, KERNEL.PVel, KERNEL.PVelGrad, KERNEL.PVelLaplacian, KERNEL.Traction)
 
 
 def _arr(a, cols=None, name="array"):

@@ -39,6 +39,12 @@ CASES = {
     "LaplaceSLPGradGrad": O.REF_LAP_SL_PGRADGRAD,
     "LaplaceDLPGradGrad": O.REF_LAP_DL_PGRADGRAD,
     "LaplaceQPGradGrad": O.REF_LAP_QPGRADGRAD,
+    "StokesSLPVelGrad": O.REF_STOKES_SL_PVELGRAD,
+    "StokesDLPVelGrad": O.REF_STOKES_DL_PVELGRAD,
+    "StokesSLPVelLaplacian": O.REF_STOKES_SL_PVELLAP,
+    "StokesDLPVelLaplacian": O.REF_STOKES_DL_PVELLAP,
+    "StokesSLTraction": O.REF_STOKES_SL_TRACTION,
+    "StokesDLTraction": O.REF_STOKES_DL_TRACTION,
 }
 EPS = 1e-2
 

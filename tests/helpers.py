@@ -19,15 +19,23 @@ GOLDEN_MAP = {
     "LaplaceSLPGradGrad": [(16, slice(0, 10), slice(0, 1))],
     "LaplaceDLPGradGrad": [(17, slice(0, 10), slice(0, 3))],
     "LaplaceQPGradGrad": [(19, slice(0, 10), slice(0, 9)), (18, slice(0, 1), slice(0, 9))],
+    "StokesSLPVelGrad": [(20, slice(0, 16), slice(0, 4))],
+    "StokesDLPVelGrad": [(21, slice(0, 16), slice(0, 9))],
+    "StokesSLPVelLaplacian": [(22, slice(0, 7), slice(0, 4))],
+    "StokesDLPVelLaplacian": [(23, slice(0, 7), slice(0, 9))],
+    "StokesSLTraction": [(24, slice(0, 9), slice(0, 4))],
+    "StokesDLTraction": [(25, slice(0, 9), slice(0, 9))],
 }
-UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13, 3, 4, 4, 1, 3, 9, 9]
-UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4, 7, 3, 1, 10, 10, 1, 10]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13, 3, 4, 4, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4, 7, 3, 1, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9]
 UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel", "rpy_u",
             "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel", "laplace_sldl_pgrad",
             "stokes_sldl_pvel", "regvel_adjoint_src", "regvel_adjoint_trg", "laplace_sldl_p", "laplace_pgradgrad",
-            "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad"]
+            "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad", "stokes_pvelgrad",
+            "stokes_doublepvelgrad", "stokes_pvellaplacian", "stokes_doublelaplacian", "stokes_traction",
+            "stokes_doubletraction"]
 # forward micro-kernels (the adjoint ones, 13 and 14, need per-target values)
-UK_FORWARD = list(range(13)) + [15, 16, 17, 18, 19]
+UK_FORWARD = list(range(13)) + list(range(15, 26))
 
 
 def load_golden(name):

@@ -57,6 +57,11 @@ def test_kernel_descriptors_match_reference():
     assert [S.kernel_slot(4, s) for s in range(9)] == [19, -1, 18, -1, 0, 16, 16, 18, -1]
     assert S.ukernel_dims(S.UKERNEL.STOKES_SLDL_PVEL) == (13, 4)
     assert S.ukernel_dims(S.UKERNEL.LAPLACE_QUADPGRADGRAD) == (9, 10)
+    # PVelGrad / PVelLaplacian / Traction (StokesLayerKernel.hpp:52-94): stokes_PVel translations
+    assert [S.kernel_slot(256, s) for s in range(9)] == [20, 21, 9, 10, 9, 20, 20, 9, 10]
+    assert [S.kernel_slot(512, s) for s in range(9)] == [22, 23, 9, 10, 9, 22, 22, 9, 10]
+    assert [S.kernel_slot(1024, s) for s in range(9)] == [24, 25, 9, 10, 9, 24, 24, 9, 10]
+    assert S.ukernel_dims(S.UKERNEL.STOKES_DOUBLEPVELGRAD) == (9, 16)
 
 
 def test_status_strings():

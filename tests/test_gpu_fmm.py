@@ -64,7 +64,7 @@ def run_fmm(kernel, p, max_pts, pts, slv, dlv, td, prec=0, box=1.0, origin=(0.0,
     return fmm, out
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128, 256, 512, 1024])
 @pytest.mark.parametrize("p", [6, 8, 10])
 def test_fmm_matches_direct_sum(torch_cuda, kernel, p):
     pts, slv, dlv, td = fmm_case(kernel, 6000, seed=10 + kernel)
@@ -85,7 +85,7 @@ def test_fmm_higher_order(torch_cuda, kernel):
     assert max(errs) < FMM_TOL[12], errs
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128, 256, 512, 1024])
 def test_fmm_mixed_close_to_fp64(torch_cuda, kernel):
     """The mixed-precision P2P passes change the FMM result by ~1e-7 at most."""
     pts, slv, dlv, td = fmm_case(kernel, 6000, seed=20 + kernel)
@@ -144,8 +144,8 @@ def test_fmm_separate_targets(torch_cuda):
 def test_fmm_not_supported_cases(torch_cuda):
     import stkfmm_b200 as S
     pts = np.random.default_rng(0).random((500, 3))
-    lg = S.Stk3DFMM(8, 50, 0, 256)  # StokesPVelGrad: kernel not built
+    lg = S.Stk3DFMM(8, 50, 0, 64)  # StokesRegVelOmega: kernel not built
     lg.set_box(np.zeros(3), 1.0)
     lg.set_points(pts, pts, pts)
     with pytest.raises(S.StkError):
-        lg.setup_tree(256)
+        lg.setup_tree(64)

@@ -172,7 +172,7 @@ def test_periodic_translation(torch_cuda):
     assert max(component_errors(b - d, a)) < TOL[10]
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 128])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 128, 256, 1024])
 def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     """PX: sources without net charge / force, dipole or quadrupole (alternating
     signs on the corners of small cubes) against the direct sum over their
@@ -185,7 +185,8 @@ def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     src = np.concatenate([ci + 0.03 * sg for ci in c])
     s = np.tile(sg.prod(1), 16)[:, None]
     quad = s * np.array([[0.4, 0.1, -0.3, 0.2, -0.5, 0.3, 0.1, 0.6, 0.2]])
-    val = {1: s, 2: s, 4: quad, 8: s * np.array([[0.3, -0.2, 0.5]]),
+    fv = np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)
+    val = {1: s, 2: s, 4: quad, 8: s * np.array([[0.3, -0.2, 0.5]]), 256: fv, 1024: fv,
            128: np.concatenate([s * np.array([[0.3, -0.2, 0.5]]), 0.7 * s], axis=1)}[kernel]
     trg = rng.random((1500, 3)) * 0.999
     fmm = S.Stk3DFMM(10, 32, S.PAXIS.PX, kernel)

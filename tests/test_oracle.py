@@ -31,6 +31,12 @@ def test_oracle_matches_golden(name):
     (O.REF_LAP_SL_PGRADGRAD, O.UK_LAPLACE_PGRADGRAD, slice(0, 10)),
     (O.REF_LAP_DL_PGRADGRAD, O.UK_LAPLACE_DIPOLEPGRADGRAD, slice(0, 10)),
     (O.REF_LAP_QPGRADGRAD, O.UK_LAPLACE_QUADPGRADGRAD, slice(0, 10)),
+    (O.REF_STOKES_SL_PVELGRAD, O.UK_STOKES_PVELGRAD, slice(0, 16)),
+    (O.REF_STOKES_DL_PVELGRAD, O.UK_STOKES_DOUBLEPVELGRAD, slice(0, 16)),
+    (O.REF_STOKES_SL_PVELLAP, O.UK_STOKES_PVELLAPLACIAN, slice(0, 7)),
+    (O.REF_STOKES_DL_PVELLAP, O.UK_STOKES_DOUBLELAPLACIAN, slice(0, 7)),
+    (O.REF_STOKES_SL_TRACTION, O.UK_STOKES_TRACTION, slice(0, 9)),
+    (O.REF_STOKES_DL_TRACTION, O.UK_STOKES_DOUBLETRACTION, slice(0, 9)),
 ])
 def test_oracle_matches_live_reference(which, uk, osl, rng):
     """Fresh random inputs (clustered, with coincident points) through the compiled reference."""
