@@ -103,7 +103,11 @@ enum stk_ukernel {
     STK_UK_STOKES_PVELLAPLACIAN = 22,    /* 4 -> 7   StokesSingleLayerKernel.hpp:118-155 */
     STK_UK_STOKES_DOUBLELAPLACIAN = 23,  /* 9 -> 7   StokesDoubleLayerKernel.hpp:150-206 */
     STK_UK_STOKES_TRACTION = 24,         /* 4 -> 9   StokesSingleLayerKernel.hpp:162-199 */
-    STK_UK_STOKES_DOUBLETRACTION = 25    /* 9 -> 9   StokesDoubleLayerKernel.hpp:213-276 */
+    STK_UK_STOKES_DOUBLETRACTION = 25,   /* 9 -> 9   StokesDoubleLayerKernel.hpp:213-276 */
+    /* regularized force + torque (f, t, eps) and the point-force (u, omega) kernel */
+    STK_UK_STOKES_REGFTVEL = 26,         /* 7 -> 3   StokesRegSingleLayerKernel.hpp:48-89   */
+    STK_UK_STOKES_REGFTVELOMEGA = 27,    /* 7 -> 6   StokesRegSingleLayerKernel.hpp:96-151  */
+    STK_UK_STOKES_VELOMEGA = 28          /* 3 -> 6   StokesRegSingleLayerKernel.hpp:158-203 */
 };
 
 /* ---- kernel descriptors --------------------------------------------------- */
@@ -198,9 +202,9 @@ int Stk3DFMM_setup_tree(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:26 (not declared in the reference header) */
 int Stk3DFMM_clear_fmm(Stk3DFMM *fmm, unsigned kernel);
 /* Stk3DFMM-c.cpp:28-31: trg_value += FMM(sources): U-list near field plus the
- * KIFMM far field, for LapPGrad, LapPGradGrad, LapQPGradGrad, Stokes, RPY,
- * StokesRegVel, PVel, PVelGrad, PVelLaplacian and Traction in free space, PX,
- * PXY and PXYZ; StokesRegVelOmega returns STK_ERR_NOT_SUPPORTED.
+ * KIFMM far field, for every kernel of STKFMM_common.hpp:46-62 (LapPGrad,
+ * LapPGradGrad, LapQPGradGrad, Stokes, RPY, StokesRegVel, StokesRegVelOmega,
+ * PVel, PVelGrad, PVelLaplacian, Traction) in free space, PX, PXY and PXYZ.
  * Triply periodic potentials / pressures / mean velocities carry a constant
  * per component (drift) set by the equivalent density, as in the reference. */
 int Stk3DFMM_evaluate_fmm(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
@@ -376,6 +380,12 @@ void stk_ker_stokes_traction(double *r_src, int src_cnt, double *v_src, int dof,
                              double *k_out, void *mem_mgr);
 void stk_ker_stokes_doubletraction(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
                                    double *k_out, void *mem_mgr);
+void stk_ker_stokes_regftvel(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                             double *k_out, void *mem_mgr);
+void stk_ker_stokes_regftvelomega(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                                  double *k_out, void *mem_mgr);
+void stk_ker_stokes_velomega(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg, int trg_cnt,
+                             double *k_out, void *mem_mgr);
 /* status of the last ker_poten shim call on this thread (they return void) */
 int stk_ker_last_status(void);
 

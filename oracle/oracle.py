@@ -35,27 +35,29 @@ UK_LAPLACE_DIPOLEPGRADGRAD = 17
 UK_LAPLACE_QUADP = 18
 UK_LAPLACE_QUADPGRADGRAD = 19
 UK_STOKES_PVELGRAD, UK_STOKES_DOUBLEPVELGRAD, UK_STOKES_PVELLAPLACIAN, UK_STOKES_DOUBLELAPLACIAN, \
-    UK_STOKES_TRACTION, UK_STOKES_DOUBLETRACTION = range(20, 26)
+    UK_STOKES_TRACTION, UK_STOKES_DOUBLETRACTION, UK_STOKES_REGFTVEL, UK_STOKES_REGFTVELOMEGA, \
+    UK_STOKES_VELOMEGA = range(20, 29)
 UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel",
             "rpy_u", "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel",
             None, None, None, None, None,
             "laplace_pgradgrad", "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad",
             "stokes_pvelgrad", "stokes_doublepvelgrad", "stokes_pvellaplacian", "stokes_doublelaplacian",
-            "stokes_traction", "stokes_doubletraction"]
-UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9]
-UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9]
+            "stokes_traction", "stokes_doubletraction", "stokes_regftvel", "stokes_regftvelomega",
+            "stokes_velomega"]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9, 7, 7, 3]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9, 3, 6, 6]
 
 # reference SimpleKernel selectors (oracle/ref_driver.cpp)
 REF_STOKES_SL, REF_LAP_SL_PGRAD, REF_LAP_DL_PGRAD, REF_STOKES_SL_RPY, REF_STOKES_REG_SL_VEL, \
     REF_STOKES_SL_PVEL, REF_STOKES_DL_PVEL, REF_LAP_SL_PGRADGRAD, REF_LAP_DL_PGRADGRAD, \
     REF_LAP_QPGRADGRAD, REF_STOKES_SL_PVELGRAD, REF_STOKES_DL_PVELGRAD, REF_STOKES_SL_PVELLAP, \
-    REF_STOKES_DL_PVELLAP, REF_STOKES_SL_TRACTION, REF_STOKES_DL_TRACTION = range(16)
+    REF_STOKES_DL_PVELLAP, REF_STOKES_SL_TRACTION, REF_STOKES_DL_TRACTION, REF_STOKES_REG_SL_VELOMEGA = range(17)
 REF_DIMS = {REF_STOKES_SL: (3, 6), REF_LAP_SL_PGRAD: (1, 4), REF_LAP_DL_PGRAD: (3, 4),
             REF_STOKES_SL_RPY: (4, 6), REF_STOKES_REG_SL_VEL: (4, 3), REF_STOKES_SL_PVEL: (4, 4),
             REF_STOKES_DL_PVEL: (9, 4), REF_LAP_SL_PGRADGRAD: (1, 10), REF_LAP_DL_PGRADGRAD: (3, 10),
             REF_LAP_QPGRADGRAD: (9, 10), REF_STOKES_SL_PVELGRAD: (4, 16), REF_STOKES_DL_PVELGRAD: (9, 16),
             REF_STOKES_SL_PVELLAP: (4, 7), REF_STOKES_DL_PVELLAP: (9, 7), REF_STOKES_SL_TRACTION: (4, 9),
-            REF_STOKES_DL_TRACTION: (9, 9)}
+            REF_STOKES_DL_TRACTION: (9, 9), REF_STOKES_REG_SL_VELOMEGA: (7, 6)}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)

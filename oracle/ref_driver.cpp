@@ -20,6 +20,7 @@ typedef void (*kernel_func)(double *, double *, double *, double *);
 //   4 StokesRegSLVel  5 StokesSLPVel  6 StokesDLPVel  7 LaplaceSLPGradGrad
 //   8 LaplaceDLPGradGrad  9 LaplaceQPGradGrad  10 StokesSLPVelGrad  11 StokesDLPVelGrad
 //   12 StokesSLPVelLaplacian  13 StokesDLPVelLaplacian  14 StokesSLTraction  15 StokesDLTraction
+//   16 StokesRegSLVelOmega
 static kernel_func pick(int which) {
     switch (which) {
     case 0: return StokesSL;
@@ -38,6 +39,7 @@ static kernel_func pick(int which) {
     case 13: return StokesDLPVelLaplacian;
     case 14: return StokesSLTraction;
     case 15: return StokesDLTraction;
+    case 16: return StokesRegSLVelOmega;
     default: return nullptr;
     }
 }

@@ -55,11 +55,16 @@ enum {
     UK_STOKES_DOUBLELAPLACIAN = 23,  /* D(9) -> (7)                 StokesDoubleLayerKernel.hpp:150-206 */
     UK_STOKES_TRACTION = 24,         /* f,trD(4) -> (9)             StokesSingleLayerKernel.hpp:162-199 */
     UK_STOKES_DOUBLETRACTION = 25,   /* D(9) -> (9)                 StokesDoubleLayerKernel.hpp:213-276 */
-    UK_COUNT = 26
+    UK_STOKES_REGFTVEL = 26,         /* f,t,eps(7) -> u(3)          StokesRegSingleLayerKernel.hpp:48-89 */
+    UK_STOKES_REGFTVELOMEGA = 27,    /* f,t,eps(7) -> u,omega(6)    StokesRegSingleLayerKernel.hpp:96-151 */
+    UK_STOKES_VELOMEGA = 28,         /* f(3) -> u,omega(6)          StokesRegSingleLayerKernel.hpp:158-203 */
+    UK_COUNT = 29
 };
 
-static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9};
-static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9};
+static const int uk_sdim[UK_COUNT] = {1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 0, 0, 0, 0, 0, 1, 3, 9, 9,
+                                      4, 9, 4, 9, 4, 9, 7, 7, 3};
+static const int uk_tdim[UK_COUNT] = {1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 0, 0, 0, 0, 0, 10, 10, 1, 10,
+                                      16, 16, 7, 7, 9, 9, 3, 6, 6};
 
 static int uk_valid(int uk) { return uk >= 0 && uk < UK_COUNT && uk_sdim[uk] > 0; }
 
@@ -390,6 +395,46 @@ static void uk_pair(int uk, const double r[3], const double *f, double *u) {
         for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++)
                 u[7 + 3 * i + j] += (5.0 * ccn1 * d[i] * d[j] - r2 * d[i] * e[j] - (i == j ? r2 * ccn1 : 0.0)) * rinv7;
+    } break;
+    case UK_STOKES_REGFTVEL:        /* StokesRegSingleLayerKernel.hpp:55-88 */
+    case UK_STOKES_REGFTVELOMEGA: { /* StokesRegSingleLayerKernel.hpp:103-150; unmasked rsqrt as there */
+        const double fx = f[0], fy = f[1], fz = f[2], tx = f[3], ty = f[4], tz = f[5], eps = f[6];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double r4 = r2 * r2;
+        double eps2 = eps * eps, eps4 = eps2 * eps2;
+        double rinv = 1.0 / sqrt(eps2 + r2);
+        double sd = rinv * rinv * rinv;
+        double rd = 0.5 * sd * rinv * rinv;
+        double dd = 0.5 * rd * rinv * rinv;
+        double rc = (2.0 * r2 + 5.0 * eps2) * rd;
+        double D1 = (10.0 * eps4 - 7.0 * eps2 * r2 - 2.0 * r4) * dd;
+        double D2 = (21.0 * eps2 + 6.0 * r2) * dd;
+        double H2 = sd, H1 = (r2 + 2.0 * eps2) * H2;
+        double fcx = fy * dz - fz * dy, fcy = fz * dx - fx * dz, fcz = fx * dy - fy * dx;
+        double tcx = ty * dz - tz * dy, tcy = tz * dx - tx * dz, tcz = tx * dy - ty * dx;
+        double fdr = fx * dx + fy * dy + fz * dz, tdr = tx * dx + ty * dy + tz * dz;
+        u[0] += H1 * fx + H2 * fdr * dx + rc * tcx;
+        u[1] += H1 * fy + H2 * fdr * dy + rc * tcy;
+        u[2] += H1 * fz + H2 * fdr * dz + rc * tcz;
+        if (uk == UK_STOKES_REGFTVEL) break;
+        u[3] += D1 * tx + D2 * tdr * dx + rc * fcx;
+        u[4] += D1 * ty + D2 * tdr * dy + rc * fcy;
+        u[5] += D1 * tz + D2 * tdr * dz + rc * fcz;
+    } break;
+    case UK_STOKES_VELOMEGA: { /* StokesRegSingleLayerKernel.hpp:165-202 */
+        const double fx = f[0], fy = f[1], fz = f[2];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = rsqrt_mask(r2);
+        double rinv3 = rinv * rinv * rinv;
+        double rc = 2.0 * r2 * (0.5 * rinv3 * rinv * rinv);
+        double H2 = rinv3, H1 = r2 * H2;
+        double fdr = fx * dx + fy * dy + fz * dz;
+        u[0] += H1 * fx + H2 * fdr * dx;
+        u[1] += H1 * fy + H2 * fdr * dy;
+        u[2] += H1 * fz + H2 * fdr * dz;
+        u[3] += rc * (fy * dz - fz * dy);
+        u[4] += rc * (fz * dx - fx * dz);
+        u[5] += rc * (fx * dy - fy * dx);
     } break;
     case UK_STOKES_DOUBLETRACTION: { /* StokesDoubleLayerKernel.hpp:220-275; 2/3 truncated as there */
         double r2 = dx * dx + dy * dy + dz * dz;

@@ -94,7 +94,7 @@ KER_SHIMS = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgr
              "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel", "laplace_pgradgrad",
              "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad", "stokes_pvelgrad",
              "stokes_doublepvelgrad", "stokes_pvellaplacian", "stokes_doublelaplacian", "stokes_traction",
-             "stokes_doubletraction"]
+             "stokes_doubletraction", "stokes_regftvel", "stokes_regftvelomega", "stokes_velomega"]
 for _n in KER_SHIMS:
     SIGNATURES.append(("stk_ker_" + _n, None, [P_d, c_int, P_d, c_int, P_d, c_int, P_d, c_void_p]))
 

@@ -358,3 +358,6 @@ STK_KER_SHIM(stokes_pvellaplacian, UK_STOKES_PVELLAPLACIAN)
 STK_KER_SHIM(stokes_doublelaplacian, UK_STOKES_DOUBLELAPLACIAN)
 STK_KER_SHIM(stokes_traction, UK_STOKES_TRACTION)
 STK_KER_SHIM(stokes_doubletraction, UK_STOKES_DOUBLETRACTION)
+STK_KER_SHIM(stokes_regftvel, UK_STOKES_REGFTVEL)
+STK_KER_SHIM(stokes_regftvelomega, UK_STOKES_REGFTVELOMEGA)
+STK_KER_SHIM(stokes_velomega, UK_STOKES_VELOMEGA)

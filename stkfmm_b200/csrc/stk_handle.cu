@@ -426,7 +426,8 @@ static int eval_host(Stk3DFMM *fmm, unsigned kernel, const int nSL, const double
     // scaleSrc (FMMData.cpp:285-317): DL values and a scaling last SL component times sF
     const double sf = fmm->scale_factor;
     if (dl) HCUDA(scale_strided((double *)kd->d_val[1].ptr, (long long)ndl_v, 1, 0, sf, s));
-    if (ki->sl_last_scales) HCUDA(scale_strided((double *)kd->d_val[0].ptr, nSL, ki->kdim_sl, ki->kdim_sl - 1, sf, s));
+    for (int c = ki->kdim_sl - ki->sl_last_scales; c < ki->kdim_sl; c++)
+        HCUDA(scale_strided((double *)kd->d_val[0].ptr, nSL, ki->kdim_sl, c, sf, s));
     rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
                      (double *)kd->d_out_user.ptr, s, far);
     if (rc) return rc;

@@ -38,7 +38,9 @@ struct KernelInfo {
     // exponent k of the target rescaling trg *= sF^k per target component
     // (FMMData::scaleTrg, Lib/src/FMMData.cpp:319-470)
     int trg_scale_pow[16];
-    // 1 when the last SL component scales like a double layer (FMMData.cpp:300-311)
+    // number of trailing SL components that scale like a double layer: 1 for the
+    // trace / radius / regularisation of PVel-type, RPY and StokesRegVel, 4 for the
+    // torque and regularisation of StokesRegVelOmega (FMMData.cpp:300-316)
     int sl_last_scales;
 };
 
@@ -67,7 +69,12 @@ static const KernelInfo kKernels[] = {
     {32, "stokes_regvel", 4, 7, 3,
      {UK_STOKES_REGVEL, -1, UK_STOKES_REGVEL, -1, UK_STOKES_VEL, UK_STOKES_VEL, UK_STOKES_VEL, UK_STOKES_REGVEL, -1},
      {1, 1, 1}, 1},
-    {64, "stokes_regftvelomega", 7, 10, 6, {-1, -1, -1, -1, -1, -1, -1, -1, -1}, {1, 1, 1, 2, 2, 2}, 0},
+    // StokesRegKernel<T>::FTVelOmega (StokesRegSingleLayerKernel.hpp:220-232): regularized
+    // force + torque at S2T / S2M / S2L, stokes_vel translations, stokes_velomega at M2T / L2T
+    {64, "stokes_regftvelomega", 7, 10, 6,
+     {UK_STOKES_REGFTVELOMEGA, -1, UK_STOKES_REGFTVEL, -1, UK_STOKES_VEL, UK_STOKES_VELOMEGA, UK_STOKES_VELOMEGA,
+      UK_STOKES_REGFTVEL, -1},
+     {1, 1, 1, 2, 2, 2}, 4},
     {128, "stokes_PVel", 4, 9, 4,
      {UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL, UK_STOKES_PVEL, UK_STOKES_PVEL,
       UK_STOKES_PVEL, UK_STOKES_PVEL, UK_STOKES_DOUBLEPVEL},

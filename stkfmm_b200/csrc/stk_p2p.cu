@@ -457,6 +457,9 @@ cudaError_t launch_list_p2p(int uk, int prec, const ListP2PArgs &a, int num_sms,
     case UK_STOKES_DOUBLELAPLACIAN: return launch_prec<UK_STOKES_DOUBLELAPLACIAN>(prec, a, num_sms, stream);
     case UK_STOKES_TRACTION: return launch_prec<UK_STOKES_TRACTION>(prec, a, num_sms, stream);
     case UK_STOKES_DOUBLETRACTION: return launch_prec<UK_STOKES_DOUBLETRACTION>(prec, a, num_sms, stream);
+    case UK_STOKES_REGFTVEL: return launch_prec<UK_STOKES_REGFTVEL>(prec, a, num_sms, stream);
+    case UK_STOKES_REGFTVELOMEGA: return launch_prec<UK_STOKES_REGFTVELOMEGA>(prec, a, num_sms, stream);
+    case UK_STOKES_VELOMEGA: return launch_prec<UK_STOKES_VELOMEGA>(prec, a, num_sms, stream);
     case UK_REGVEL_ADJ_SRC:
         if (!a.trg_aux) return cudaErrorInvalidValue;
         return launch_prec<UK_REGVEL_ADJ_SRC>(prec, a, num_sms, stream);

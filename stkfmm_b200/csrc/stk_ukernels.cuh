@@ -40,6 +40,9 @@
 //   stokes_doublepvelgrad Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:64-143
 //   stokes_doublelaplacian Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:150-206
 //   stokes_doubletraction Lib/include/STKFMM/StokesDoubleLayerKernel.hpp:213-276
+//   stokes_regftvel      Lib/include/STKFMM/StokesRegSingleLayerKernel.hpp:48-89
+//   stokes_regftvelomega Lib/include/STKFMM/StokesRegSingleLayerKernel.hpp:96-151
+//   stokes_velomega      Lib/include/STKFMM/StokesRegSingleLayerKernel.hpp:158-203
 // Two fused variants (no single reference function) evaluate a single-layer
 // and a double-layer source at the same point in one pass:
 //   laplace_pgrad + laplace_dipolepgrad, stokes_pvel + stokes_doublepvel.
@@ -153,7 +156,10 @@ enum UkId : int {
     UK_STOKES_DOUBLELAPLACIAN = 23,
     UK_STOKES_TRACTION = 24,
     UK_STOKES_DOUBLETRACTION = 25,
-    UK_COUNT = 26
+    UK_STOKES_REGFTVEL = 26,       // values (f, t, eps) -> u
+    UK_STOKES_REGFTVELOMEGA = 27,  // values (f, t, eps) -> (u, omega)
+    UK_STOKES_VELOMEGA = 28,       // values f -> (u, omega)
+    UK_COUNT = 29
 };
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1/(4 pi)
@@ -986,6 +992,94 @@ template <> struct Uk<UK_STOKES_DOUBLETRACTION> {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Regularized force + torque (values f, t, eps; R^2 = r^2 + eps^2, self term kept):
+//   u = ((r^2 + 2 eps^2) f + (f.r) r) / R^3 + (r^2 + 2.5 eps^2) (t x r) / R^5,
+//   omega = D1 t + D2 (t.r) r + (r^2 + 2.5 eps^2) (f x r) / R^5,
+//   D1 = (2.5 eps^4 - 1.75 eps^2 r^2 - 0.5 r^4) / R^7, D2 = (5.25 eps^2 + 1.5 r^2) / R^7.
+// Evaluated with q = r / R, a = eps^2 / R^2, b = r^2 / R^2 (all at most 1), so that
+// only 1/R, 1/R^2 and 1/R^3 appear: u = ((b + 2a) f + (f.q) q) / R + (b + 2.5a)(t x q) / R^2,
+// omega = ((2.5a^2 - 1.75ab - 0.5b^2) t + (5.25a + 1.5b)(t.q) q) / R^3 + (b + 2.5a)(f x q) / R^2
+// (the FP32 path would overflow 1/R^5, 1/R^7 for R below ~1e-8 at coincident points).
+// staged (f, t, eps^2)
+struct StokesRegFT {
+    static __device__ void stage(const double *f, double *v) {
+        for (int k = 0; k < 6; k++) v[k] = f[k];
+        v[6] = f[6] * f[6];
+    }
+    // velocity (outputs 0..2); returns q, a, b, 1/R^2 and (b + 2.5a) / R^2
+    template <class V, int N>
+    static __device__ __forceinline__ void vel(V (&u)[N], V dx, V dy, V dz, const V *v, V &qx, V &qy, V &qz, V &a,
+                                               V &b, V &rinv, V &rinv2, V &rc) {
+        V r2 = norm2(dx, dy, dz);
+        rinv = rsq(r2 + v[6]);
+        rinv2 = rinv * rinv;
+        a = v[6] * rinv2;
+        b = r2 * rinv2;
+        qx = dx * rinv;
+        qy = dy * rinv;
+        qz = dz * rinv;
+        V h1 = fmav(a, cst<V>(2.0), b) * rinv;
+        V h2 = fmav(v[0], qx, fmav(v[1], qy, v[2] * qz)) * rinv;
+        rc = fmav(a, cst<V>(2.5), b) * rinv2;
+        u[0] = fmav(rc, v[4] * qz - v[5] * qy, fmav(h2, qx, fmav(h1, v[0], u[0])));
+        u[1] = fmav(rc, v[5] * qx - v[3] * qz, fmav(h2, qy, fmav(h1, v[1], u[1])));
+        u[2] = fmav(rc, v[3] * qy - v[4] * qx, fmav(h2, qz, fmav(h1, v[2], u[2])));
+    }
+};
+
+template <> struct Uk<UK_STOKES_REGFTVEL> {
+    static constexpr int SDIM = 7, TDIM = 3, NV = 7;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesRegFT::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V qx, qy, qz, a, b, rinv, rinv2, rc;
+        StokesRegFT::vel(u, dx, dy, dz, v, qx, qy, qz, a, b, rinv, rinv2, rc);
+    }
+};
+
+template <> struct Uk<UK_STOKES_REGFTVELOMEGA> {
+    static constexpr int SDIM = 7, TDIM = 6, NV = 7;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) { StokesRegFT::stage(f, v); }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V qx, qy, qz, a, b, rinv, rinv2, rc;
+        StokesRegFT::vel(u, dx, dy, dz, v, qx, qy, qz, a, b, rinv, rinv2, rc);
+        V rinv3 = rinv2 * rinv;
+        V d1 = fmav(a, fmav(a, cst<V>(2.5), b * cst<V>(-1.75)), (b * b) * cst<V>(-0.5)) * rinv3;
+        V td = fmav(v[3], qx, fmav(v[4], qy, v[5] * qz)) * (fmav(a, cst<V>(5.25), b * cst<V>(1.5)) * rinv3);
+        u[3] = fmav(rc, v[1] * qz - v[2] * qy, fmav(td, qx, fmav(d1, v[3], u[3])));
+        u[4] = fmav(rc, v[2] * qx - v[0] * qz, fmav(td, qy, fmav(d1, v[4], u[4])));
+        u[5] = fmav(rc, v[0] * qy - v[1] * qx, fmav(td, qz, fmav(d1, v[5], u[5])));
+    }
+};
+
+// stokes_velomega: u = f / r + (f.r) r / r^3, omega = (f x r) / r^3 (masked at r = 0)
+template <> struct Uk<UK_STOKES_VELOMEGA> {
+    static constexpr int SDIM = 3, TDIM = 6, NV = 3;
+    static constexpr double SCALE = kInv8Pi;
+    static constexpr int TV = 0;
+    static __host__ __device__ constexpr double comp_scale(int) { return 1.0; }
+    static __device__ void stage(const double *f, double *v) {
+        for (int k = 0; k < 3; k++) v[k] = f[k];
+    }
+    template <class V> static __device__ __forceinline__ void eval(V (&u)[TDIM], V dx, V dy, V dz, const V *v) {
+        V rinv = rsq(norm2(dx, dy, dz));
+        V rinv3 = (rinv * rinv) * rinv;
+        V h2 = fmav(v[0], dx, fmav(v[1], dy, v[2] * dz)) * rinv3;
+        u[0] = fmav(h2, dx, fmav(v[0], rinv, u[0]));
+        u[1] = fmav(h2, dy, fmav(v[1], rinv, u[1]));
+        u[2] = fmav(h2, dz, fmav(v[2], rinv, u[2]));
+        u[3] = fmav(rinv3, v[1] * dz - v[2] * dy, u[3]);
+        u[4] = fmav(rinv3, v[2] * dx - v[0] * dz, u[4]);
+        u[5] = fmav(rinv3, v[0] * dy - v[1] * dx, u[5]);
+    }
+};
+
 // Host/device tables for launch-time checks.
 __host__ __device__ constexpr int uk_sdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 1 : id == UK_LAPLACE_DIPOLEP ? 3
@@ -996,7 +1090,8 @@ __host__ __device__ constexpr int uk_sdim(int id) {
          : id == UK_LAPLACE_SLDL_P ? 4 : id == UK_LAPLACE_PGRADGRAD ? 1 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 3
          : id == UK_LAPLACE_QUADP ? 9 : id == UK_LAPLACE_QUADPGRADGRAD ? 9 : id == UK_STOKES_PVELGRAD ? 4
          : id == UK_STOKES_DOUBLEPVELGRAD ? 9 : id == UK_STOKES_PVELLAPLACIAN ? 4 : id == UK_STOKES_DOUBLELAPLACIAN ? 9
-         : id == UK_STOKES_TRACTION ? 4 : id == UK_STOKES_DOUBLETRACTION ? 9 : 0;
+         : id == UK_STOKES_TRACTION ? 4 : id == UK_STOKES_DOUBLETRACTION ? 9 : id == UK_STOKES_REGFTVEL ? 7
+         : id == UK_STOKES_REGFTVELOMEGA ? 7 : id == UK_STOKES_VELOMEGA ? 3 : 0;
 }
 __host__ __device__ constexpr int uk_tdim(int id) {
     return id == UK_LAPLACE_P ? 1 : id == UK_LAPLACE_PGRAD ? 4 : id == UK_LAPLACE_DIPOLEP ? 1
@@ -1007,7 +1102,8 @@ __host__ __device__ constexpr int uk_tdim(int id) {
          : id == UK_LAPLACE_SLDL_P ? 1 : id == UK_LAPLACE_PGRADGRAD ? 10 : id == UK_LAPLACE_DIPOLEPGRADGRAD ? 10
          : id == UK_LAPLACE_QUADP ? 1 : id == UK_LAPLACE_QUADPGRADGRAD ? 10 : id == UK_STOKES_PVELGRAD ? 16
          : id == UK_STOKES_DOUBLEPVELGRAD ? 16 : id == UK_STOKES_PVELLAPLACIAN ? 7 : id == UK_STOKES_DOUBLELAPLACIAN ? 7
-         : id == UK_STOKES_TRACTION ? 9 : id == UK_STOKES_DOUBLETRACTION ? 9 : 0;
+         : id == UK_STOKES_TRACTION ? 9 : id == UK_STOKES_DOUBLETRACTION ? 9 : id == UK_STOKES_REGFTVEL ? 3
+         : id == UK_STOKES_REGFTVELOMEGA ? 6 : id == UK_STOKES_VELOMEGA ? 6 : 0;
 }
 // per-output-point (target-side) values a micro-kernel reads
 __host__ __device__ constexpr int uk_tvdim(int id) {

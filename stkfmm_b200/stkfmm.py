@@ -85,10 +85,14 @@ class UKERNEL(enum.IntEnum):
     STOKES_DOUBLELAPLACIAN = 23
     STOKES_TRACTION = 24
     STOKES_DOUBLETRACTION = 25
+    STOKES_REGFTVEL = 26
+    STOKES_REGFTVELOMEGA = 27
+    STOKES_VELOMEGA = 28
 
 
 SUPPORTED_KERNELS = (KERNEL.LapPGrad, KERNEL.LapPGradGrad, KERNEL.LapQPGradGrad, KERNEL.Stokes, KERNEL.RPY,
-                     KERNEL.StokesRegVel, KERNEL.PVel, KERNEL.PVelGrad, KERNEL.PVelLaplacian, KERNEL.Traction)
+                     KERNEL.StokesRegVel, KERNEL.StokesRegVelOmega, KERNEL.PVel, KERNEL.PVelGrad,
+                     KERNEL.PVelLaplacian, KERNEL.Traction)
 
 
 def _arr(a, cols=None, name="array"):

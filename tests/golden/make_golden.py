@@ -45,6 +45,7 @@ CASES = {
     "StokesDLPVelLaplacian": O.REF_STOKES_DL_PVELLAP,
     "StokesSLTraction": O.REF_STOKES_SL_TRACTION,
     "StokesDLTraction": O.REF_STOKES_DL_TRACTION,
+    "StokesRegSLVelOmega": O.REF_STOKES_REG_SL_VELOMEGA,
 }
 EPS = 1e-2
 
@@ -52,7 +53,7 @@ EPS = 1e-2
 def values(rng, which, n):
     sd = O.REF_DIMS[which][0]
     v = rng.uniform(-1.0, 1.0, size=(n, sd))
-    if which in (O.REF_STOKES_SL_RPY, O.REF_STOKES_REG_SL_VEL):
+    if which in (O.REF_STOKES_SL_RPY, O.REF_STOKES_REG_SL_VEL, O.REF_STOKES_REG_SL_VELOMEGA):
         v[:, -1] = np.abs(v[:, -1]) * EPS
     return v
 

@@ -25,17 +25,18 @@ GOLDEN_MAP = {
     "StokesDLPVelLaplacian": [(23, slice(0, 7), slice(0, 9))],
     "StokesSLTraction": [(24, slice(0, 9), slice(0, 4))],
     "StokesDLTraction": [(25, slice(0, 9), slice(0, 9))],
+    "StokesRegSLVelOmega": [(27, slice(0, 6), slice(0, 7)), (26, slice(0, 3), slice(0, 7))],
 }
-UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13, 3, 4, 4, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9]
-UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4, 7, 3, 1, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9]
+UK_SDIM = [1, 1, 3, 3, 3, 4, 4, 3, 4, 4, 9, 4, 13, 3, 4, 4, 1, 3, 9, 9, 4, 9, 4, 9, 4, 9, 7, 7, 3]
+UK_TDIM = [1, 4, 1, 4, 3, 3, 6, 6, 3, 4, 4, 4, 4, 7, 3, 1, 10, 10, 1, 10, 16, 16, 7, 7, 9, 9, 3, 6, 6]
 UK_NAMES = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgrad", "stokes_vel", "rpy_u",
             "rpy_ulapu", "stk_ulapu", "stokes_regvel", "stokes_pvel", "stokes_doublepvel", "laplace_sldl_pgrad",
             "stokes_sldl_pvel", "regvel_adjoint_src", "regvel_adjoint_trg", "laplace_sldl_p", "laplace_pgradgrad",
             "laplace_dipolepgradgrad", "laplace_quadp", "laplace_quadpgradgrad", "stokes_pvelgrad",
             "stokes_doublepvelgrad", "stokes_pvellaplacian", "stokes_doublelaplacian", "stokes_traction",
-            "stokes_doubletraction"]
+            "stokes_doubletraction", "stokes_regftvel", "stokes_regftvelomega", "stokes_velomega"]
 # forward micro-kernels (the adjoint ones, 13 and 14, need per-target values)
-UK_FORWARD = list(range(13)) + list(range(15, 26))
+UK_FORWARD = list(range(13)) + list(range(15, 29))
 
 
 def load_golden(name):
@@ -47,6 +48,8 @@ def uk_values(rng, uk, n, eps=1e-2):
     v = rng.uniform(-1.0, 1.0, size=(n, UK_SDIM[uk]))
     if uk in (5, 6, 8):
         v[:, 3] = np.abs(v[:, 3]) * eps
+    if uk in (26, 27):
+        v[:, 6] = np.abs(v[:, 6]) * eps
     return v
 
 

@@ -62,6 +62,8 @@ def test_kernel_descriptors_match_reference():
     assert [S.kernel_slot(512, s) for s in range(9)] == [22, 23, 9, 10, 9, 22, 22, 9, 10]
     assert [S.kernel_slot(1024, s) for s in range(9)] == [24, 25, 9, 10, 9, 24, 24, 9, 10]
     assert S.ukernel_dims(S.UKERNEL.STOKES_DOUBLEPVELGRAD) == (9, 16)
+    # StokesRegVelOmega (StokesRegSingleLayerKernel.hpp:220-232)
+    assert [S.kernel_slot(64, s) for s in range(9)] == [27, -1, 26, -1, 4, 28, 28, 26, -1]
 
 
 def test_status_strings():

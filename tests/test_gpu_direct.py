@@ -108,7 +108,7 @@ def test_direct_large_split_sources(torch_cuda, L):
 
 
 KERNELS = {1: (1, 3, 4), 2: (1, 3, 10), 4: (9, None, 10), 8: (3, None, 3), 16: (4, None, 6), 32: (4, None, 3),
-           128: (4, 9, 4), 256: (4, 9, 16), 512: (4, 9, 7), 1024: (4, 9, 9)}
+           64: (7, None, 6), 128: (4, 9, 4), 256: (4, 9, 16), 512: (4, 9, 7), 1024: (4, 9, 9)}
 
 
 @pytest.mark.parametrize("kernel", sorted(KERNELS))

@@ -40,6 +40,8 @@ def fmm_case(kernel, n, seed, box=1.0, origin=(0.0, 0.0, 0.0)):
         # translations use the plain Stokeslet (the reference's kernel
         # compositions), a model difference of relative size (eps / r)^2
         slv[:, 3] = rng.uniform(1e-4, 5e-4, n) * box
+    if kernel == 64:
+        slv[:, 6] = rng.uniform(1e-4, 5e-4, n) * box  # regularisation, as above
     dlv = rng.normal(size=(n, dd)) if has_dl else None
     return pts, slv, dlv, td
 
@@ -64,7 +66,7 @@ def run_fmm(kernel, p, max_pts, pts, slv, dlv, td, prec=0, box=1.0, origin=(0.0,
     return fmm, out
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128, 256, 512, 1024])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
 @pytest.mark.parametrize("p", [6, 8, 10])
 def test_fmm_matches_direct_sum(torch_cuda, kernel, p):
     pts, slv, dlv, td = fmm_case(kernel, 6000, seed=10 + kernel)
@@ -85,7 +87,7 @@ def test_fmm_higher_order(torch_cuda, kernel):
     assert max(errs) < FMM_TOL[12], errs
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128, 256, 512, 1024])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
 def test_fmm_mixed_close_to_fp64(torch_cuda, kernel):
     """The mixed-precision P2P passes change the FMM result by ~1e-7 at most."""
     pts, slv, dlv, td = fmm_case(kernel, 6000, seed=20 + kernel)
@@ -144,8 +146,10 @@ def test_fmm_separate_targets(torch_cuda):
 def test_fmm_not_supported_cases(torch_cuda):
     import stkfmm_b200 as S
     pts = np.random.default_rng(0).random((500, 3))
-    lg = S.Stk3DFMM(8, 50, 0, 64)  # StokesRegVelOmega: kernel not built
+    with pytest.raises(S.StkError):
+        S.Stk3DFMM(8, 50, 0, 2048)  # no STKFMM kernel has this bit
+    lg = S.Stk3DFMM(8, 50, 0, 1)
     lg.set_box(np.zeros(3), 1.0)
     lg.set_points(pts, pts, pts)
     with pytest.raises(S.StkError):
-        lg.setup_tree(64)
+        lg.setup_tree(64)  # not activated in this handle

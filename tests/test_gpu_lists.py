@@ -156,7 +156,7 @@ def handle_case(kernel, n, pbc=0, max_pts=64, seed=0, origin=(0.0, 0.0, 0.0), bo
     return pts, (dl if has_dl else None), slv, dlv, td
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 128, 256, 512, 1024])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
 @pytest.mark.parametrize("prec", [0, 1])
 def test_handle_evaluate_near(torch_cuda, kernel, prec):
     """Stk3DFMM_evaluate_near against the oracle on the handle's own U-list (SL and DL)."""
@@ -205,7 +205,7 @@ def test_handle_separate_dl_points(torch_cuda, kernel):
     assert rel_l2(out, ref) < 1e-12
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 4, 16, 128, 256, 1024])
+@pytest.mark.parametrize("kernel", [1, 2, 4, 16, 64, 128, 256, 1024])
 def test_handle_box_scaling(torch_cuda, kernel):
     """A box (origin o, length L) gives sF^k times the unit-box result (scaleSrc / scaleTrg)."""
     import stkfmm_b200 as S
@@ -226,6 +226,8 @@ def test_handle_box_scaling(torch_cuda, kernel):
     slv_big = slv.copy()
     if kernel in (16, 128, 256, 1024):
         slv_big[:, -1] /= sf
+    if kernel == 64:  # torque and regularisation scale like a double layer
+        slv_big[:, 3:] /= sf
     dlv_big = dlv / sf if dlv is not None else None
     a = np.zeros((len(pts), td))
     b = np.zeros((len(pts), td))
@@ -233,7 +235,7 @@ def test_handle_box_scaling(torch_cuda, kernel):
     big.evaluate_near(kernel, slv_big, b, dlv_big)
     pows = {1: [1, 2, 2, 2], 2: [1, 2, 2, 2, 3, 3, 3, 3, 3, 3], 4: [3, 4, 4, 4, 5, 5, 5, 5, 5, 5],
             16: [1, 1, 1, 3, 3, 3], 128: [2, 1, 1, 1], 256: [2, 1, 1, 1, 3, 3, 3] + [2] * 9,
-            1024: [2] * 9}[kernel]
+            1024: [2] * 9, 64: [1, 1, 1, 2, 2, 2]}[kernel]
     assert rel_l2(b, a * sf ** np.array(pows)) < 1e-12
 
 

@@ -37,6 +37,7 @@ def test_oracle_matches_golden(name):
     (O.REF_STOKES_DL_PVELLAP, O.UK_STOKES_DOUBLELAPLACIAN, slice(0, 7)),
     (O.REF_STOKES_SL_TRACTION, O.UK_STOKES_TRACTION, slice(0, 9)),
     (O.REF_STOKES_DL_TRACTION, O.UK_STOKES_DOUBLETRACTION, slice(0, 9)),
+    (O.REF_STOKES_REG_SL_VELOMEGA, O.UK_STOKES_REGFTVELOMEGA, slice(0, 6)),
 ])
 def test_oracle_matches_live_reference(which, uk, osl, rng):
     """Fresh random inputs (clustered, with coincident points) through the compiled reference."""
@@ -45,6 +46,8 @@ def test_oracle_matches_live_reference(which, uk, osl, rng):
     v = rng.uniform(-1, 1, size=(400, O.REF_DIMS[which][0]))
     if which in (O.REF_STOKES_SL_RPY, O.REF_STOKES_REG_SL_VEL):
         v[:, 3] = np.abs(v[:, 3]) * 1e-3
+    if which == O.REF_STOKES_REG_SL_VELOMEGA:
+        v[:, 6] = np.abs(v[:, 6]) * 1e-3
     ref = O.ref_direct(which, src, v, trg)[:, osl]
     out = O.direct(uk, src, v[:, :O.UK_SDIM[uk]], trg)
     assert rel_l2(out, ref) < 1e-13
@@ -297,3 +300,16 @@ def test_wall_image_system_no_slip(kind):
         pbc = 2 if kind == "stokes_pxy" else 0
         uw, ub = O.wall_stokes(src, f, wall, z0=z0, pbc=pbc), O.wall_stokes(src, f, bulk, z0=z0, pbc=pbc)
     assert np.abs(uw).max() < 1e-13 * np.abs(ub).max()
+
+
+
+def test_velomega_is_unregularized_force_torque(rng):
+    """stokes_velomega (the M2T / L2T kernel of StokesRegVelOmega) equals
+    stokes_regftvelomega with no torque and eps = 0 away from the sources."""
+    src = rng.random((300, 3))
+    trg = rng.random((200, 3)) + 2.0
+    f = rng.normal(size=(300, 3))
+    ft = np.concatenate([f, np.zeros((300, 4))], axis=1)
+    a = O.direct(O.UK_STOKES_VELOMEGA, src, f, trg)
+    b = O.direct(O.UK_STOKES_REGFTVELOMEGA, src, ft, trg)
+    assert np.abs(a - b).max() < 1e-13 * np.abs(b).max()
