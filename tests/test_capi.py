@@ -10,7 +10,7 @@ import pytest
 
 import stkfmm_b200 as S
 from conftest import cuda_available
-from stkfmm_b200._lib import LIB_PATH, SIGNATURES, lib
+from stkfmm_b200._lib import LIB_PATH, P_i, SIGNATURES, lib
 
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "stkfmm_b200.h")
 
@@ -86,3 +86,19 @@ def test_no_cpu_fallback():
     with pytest.raises(S.StkError):
         S.Stk3DFMM(8, 64, 0, S.KERNEL.Stokes)
     assert not L.Stk3DFMM_create(8, 64, 0, 8)
+    with pytest.raises(S.StkError):
+        S.StkWallFMM(8, 64, 0, S.KERNEL.Stokes)
+    assert not L.StkWallFMM_create(8, 64, 0, 8)
+
+
+def test_wall_create_rejects_bad_arguments():
+    """StkWallFMM_create refuses a triply periodic box, kernels without a wall
+    image system and invalid orders before it needs a device."""
+    L = lib()
+    assert not L.StkWallFMM_create(8, 64, 3, 8)  # PXYZ
+    assert not L.StkWallFMM_create(8, 64, 0, 1)  # LapPGrad only
+    assert not L.StkWallFMM_create(1, 64, 0, 8)  # order below 2
+    assert not L.StkWallFMM_create(8, 0, 0, 16)  # no points per leaf
+    dims = np.zeros(3, dtype=np.int32)
+    assert L.StkWallFMM_get_kernel_dimension(16, dims.ctypes.data_as(P_i)) == 0
+    assert tuple(dims) == (4, 7, 6)
