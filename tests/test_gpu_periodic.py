@@ -265,3 +265,29 @@ def test_complete_level_m2l_matches_chunked(torch_cuda, monkeypatch, kernel, pbc
     assert res["1"][1]["flops_algorithmic"] == res["0"][1]["flops_algorithmic"]
     a, b = res["0"][0], res["1"][0]
     assert np.linalg.norm(b - a) / np.linalg.norm(a) < 1e-13
+
+
+@pytest.mark.parametrize("pbc", [0, 2, 3])
+def test_traction_is_stress_of_pvelgrad(torch_cuda, pbc):
+    """The Traction FMM equals -p I + grad u + grad u^T of the PVelGrad FMM on the
+    same points and SL + DL values (both share the stokes_PVel far field; the
+    identity holds pair by pair for the reference's kernels, tests/test_oracle.py),
+    free space and periodic."""
+    import stkfmm_b200 as S
+    pts, rng = points("clustered", 3000, 60 + pbc)
+    v = rng.normal(size=(len(pts), 4))
+    v -= v.mean(0)
+    d = rng.normal(size=(len(pts), 9))
+    d[:, [0, 4, 8]] -= (d[:, 0] + d[:, 4] + d[:, 8]).mean() / 3
+    res = {}
+    for k in (256, 1024):
+        fmm = S.Stk3DFMM(8, 50, pbc, k)
+        fmm.set_box(np.zeros(3), 1.0)
+        fmm.set_points(pts, pts, pts)
+        fmm.setup_tree(k)
+        out = np.zeros((len(pts), S.get_kernel_dimension(k)[2]))
+        fmm.evaluate_fmm(k, v, out, d)
+        res[k] = out
+    g = res[256][:, 7:16].reshape(-1, 3, 3)
+    comb = (-res[256][:, 0][:, None, None] * np.eye(3)[None] + g + g.transpose(0, 2, 1)).reshape(-1, 9)
+    assert np.linalg.norm(comb - res[1024]) / np.linalg.norm(res[1024]) < 1e-10

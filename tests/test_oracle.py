@@ -313,3 +313,17 @@ def test_velomega_is_unregularized_force_torque(rng):
     a = O.direct(O.UK_STOKES_VELOMEGA, src, f, trg)
     b = O.direct(O.UK_STOKES_REGFTVELOMEGA, src, ft, trg)
     assert np.abs(a - b).max() < 1e-13 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("ukg,ukt,sd", [(20, 24, 4), (21, 25, 9)])
+def test_traction_is_stress_of_pvelgrad(rng, ukg, ukt, sd):
+    """stokes_traction = -p I + grad u + grad u^T of stokes_pvelgrad (SL), and the
+    same for the double layer (up to the reference's truncated 2/3)."""
+    src = rng.random((50, 3))
+    trg = rng.random((40, 3)) + 1.5
+    v = rng.normal(size=(50, sd))
+    G = O.direct(ukg, src, v, trg)
+    T = O.direct(ukt, src, v, trg)
+    g = G[:, 7:16].reshape(-1, 3, 3)
+    comb = -G[:, 0][:, None, None] * np.eye(3)[None] + g + g.transpose(0, 2, 1)
+    assert np.abs(comb.reshape(-1, 9) - T).max() < 1e-13 * np.abs(T).max()
