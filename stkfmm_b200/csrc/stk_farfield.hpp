@@ -138,8 +138,8 @@ struct FarField {
 };
 
 // Precompute the operators for (kernel, p) and the per-tree data; returns a
-// stk_status.  Supported: kernels whose translation kernel is laplace_p or
-// stokes_vel (LapPGrad, Stokes, RPY, StokesRegVel) in free space.
+// stk_status.  Supported: kernels whose translation kernel is laplace_p,
+// stokes_vel or stokes_PVel (every STKFMM kernel), free space, PX, PXY, PXYZ.
 int farfield_setup(Stk3DFMM *f, KernelData *kd);
 
 // trg_sorted += far field of the sources (values already packed / scaled as the
