@@ -105,6 +105,16 @@ static_assert(kMixedDisp == kDispHiLo || kMixedDisp == kDispF64, "STK_MIXED_DISP
 #define STK_PRAGMA(x) _Pragma(#x)
 #define STK_UNROLL(n) STK_PRAGMA(unroll n)
 
+// Target slots per lane: 2 (a warp holds 64 targets), or 4 for small micro-kernels
+// in builds with STK_P2P_TPL4 (twice the targets per staged source pair, the
+// host's lanes-per-target doubled to keep every target covered).
+#ifndef STK_P2P_TPL4
+#define STK_P2P_TPL4 0
+#endif
+template <class K> struct TargetsPerLane {
+    static constexpr int value = (STK_P2P_TPL4 && K::TDIM <= 4 && K::NV <= 8 && K::TV == 0) ? 4 : 2;
+};
+
 template <int UK, bool MIXED>
 __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2p_kernel(const ListP2PArgs a) {
     using K = Uk<UK>;
@@ -113,6 +123,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
     constexpr int TV = K::TV;  // per-output-point values (adjoint kernels)
     constexpr int NTV = NtvOf<K>::value;
     constexpr int RS = Rec<UK>::RS;
+    constexpr int TPL = TargetsPerLane<K>::value;
     constexpr bool HILO = MIXED && kMixedDisp == kDispHiLo;
     // shared tile, one row per component: coordinates (FP64, or FP32 hi x3 + lo x3)
     // and staged values (FP64 path: double, mixed path: float)
@@ -132,12 +143,18 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
         it = __shfl_sync(kFull, it, 0);
         if (it >= a.n_items) break;
         const WorkItem w = a.items[it];
-        const int glog = w.glog;
+        // the host sizes glog for 64 slots; 4 slots per lane give twice the lanes per target
+        const int glog = TPL == 4 ? min(5, w.glog + 1) : w.glog;
         const int g = 1 << glog;
         const int sub = lane & (g - 1);
-        const int ti0 = lane >> glog, ti1 = (lane + 32) >> glog;
-        const bool act0 = ti0 < w.nt, act1 = ti1 < w.nt;
-        const int t0 = w.t0 + (act0 ? ti0 : 0), t1 = w.t0 + (act1 ? ti1 : 0);
+        bool act[TPL];
+        int tt[TPL];
+#pragma unroll
+        for (int h = 0; h < TPL; h++) {
+            const int ti = (lane + 32 * h) >> glog;
+            act[h] = ti < w.nt;
+            tt[h] = w.t0 + (act[h] ? ti : 0);
+        }
 
         double c[3] = {0.0, 0.0, 0.0};
         if constexpr (MIXED) {
@@ -147,63 +164,59 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
             c[1] = o[1];
             c[2] = o[2];
         }
-        double xt0[3], xt1[3];
+        double xt[TPL][3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            xt0[k] = a.trg_xyz[3 * (size_t)t0 + k];
-            xt1[k] = a.trg_xyz[3 * (size_t)t1 + k];
-        }
+        for (int h = 0; h < TPL; h++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) xt[h][k] = a.trg_xyz[3 * (size_t)tt[h] + k];
 
         // per-output-point values, staged once per item
         using V = typename std::conditional<MIXED, F2, double>::type;
-        V ta0[NTV], ta1[NTV];
+        V ta[TPL][NTV];
         if constexpr (TV > 0) {
-            double r0[TV], r1[TV], s0[NTV], s1[NTV];
 #pragma unroll
-            for (int q = 0; q < TV; q++) {
-                r0[q] = a.trg_aux[(size_t)t0 * TV + q];
-                r1[q] = a.trg_aux[(size_t)t1 * TV + q];
-            }
-            K::stage_aux(r0, s0);
-            K::stage_aux(r1, s1);
+            for (int h = 0; h < TPL; h++) {
+                double r0[TV], s0[NTV];
 #pragma unroll
-            for (int q = 0; q < NTV; q++) {
-                if constexpr (MIXED) {
-                    ta0[q] = splat((float)s0[q]);
-                    ta1[q] = splat((float)s1[q]);
-                } else {
-                    ta0[q] = s0[q];
-                    ta1[q] = s1[q];
+                for (int q = 0; q < TV; q++) r0[q] = a.trg_aux[(size_t)tt[h] * TV + q];
+                K::stage_aux(r0, s0);
+#pragma unroll
+                for (int q = 0; q < NTV; q++) {
+                    if constexpr (MIXED)
+                        ta[h][q] = splat((float)s0[q]);
+                    else
+                        ta[h][q] = s0[q];
                 }
             }
         }
-        auto eval = [&](auto &u, V dx, V dy, V dz, const V *sv, const V *ta) {
+        auto eval = [&](auto &u, V dx, V dy, V dz, const V *sv, const V *tav) {
             if constexpr (TV > 0)
-                K::eval(u, dx, dy, dz, sv, ta);
+                K::eval(u, dx, dy, dz, sv, tav);
             else
                 K::eval(u, dx, dy, dz, sv);
         };
 
         // accumulators: FP64 path sums directly; mixed path keeps Kahan sum + compensation
-        S acc0[TDIM], acc1[TDIM], cmp0[TDIM], cmp1[TDIM];
+        S acc[TPL][TDIM], cmp[TPL][TDIM];
 #pragma unroll
-        for (int k = 0; k < TDIM; k++) acc0[k] = acc1[k] = cmp0[k] = cmp1[k] = S(0);
-        F2 th0[3], tl0[3], th1[3], tl1[3];  // hi/lo targets (HILO)
-        double tr0[3], tr1[3];               // centre-relative targets (FP64 displacement)
+        for (int h = 0; h < TPL; h++)
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            tr0[k] = xt0[k] - c[k];
-            tr1[k] = xt1[k] - c[k];
-        }
+            for (int k = 0; k < TDIM; k++) acc[h][k] = cmp[h][k] = S(0);
+        F2 th[TPL][3], tl[TPL][3];  // hi/lo targets (HILO)
+        double tr[TPL][3];          // centre-relative targets (FP64 displacement)
+#pragma unroll
+        for (int h = 0; h < TPL; h++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) tr[h][k] = xt[h][k] - c[k];
         if constexpr (HILO) {
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const float h0 = (float)tr0[k], h1 = (float)tr1[k];
-                th0[k] = splat(h0);
-                tl0[k] = splat((float)(tr0[k] - (double)h0));
-                th1[k] = splat(h1);
-                tl1[k] = splat((float)(tr1[k] - (double)h1));
-            }
+            for (int h = 0; h < TPL; h++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const float hv = (float)tr[h][k];
+                    th[h][k] = splat(hv);
+                    tl[h][k] = splat((float)(tr[h][k] - (double)hv));
+                }
         }
 
         // ---- tile iterator over the source records of entries [e0, e1) ----
@@ -249,9 +262,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 #pragma unroll
                     for (int k = 0; k < 3; k++) {
                         const double d = x[k] - c[k];
-                        const float h = (float)d;
-                        mc[k][lane] = h;
-                        mc[3 + k][lane] = (float)(d - (double)h);
+                        const float hv = (float)d;
+                        mc[k][lane] = hv;
+                        mc[3 + k][lane] = (float)(d - (double)hv);
                     }
                 } else {
 #pragma unroll
@@ -276,15 +289,17 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 
             // ---- consume the tile ----
             if constexpr (MIXED) {
-                F2 p0[TDIM], p1[TDIM];
+                F2 pp[TPL][TDIM];
 #pragma unroll
-                for (int k = 0; k < TDIM; k++) p0[k] = p1[k] = splat(0.0f);
+                for (int h = 0; h < TPL; h++)
+#pragma unroll
+                    for (int k = 0; k < TDIM; k++) pp[h][k] = splat(0.0f);
                 // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
 STK_UNROLL(STK_P2P_UNROLL_MIXED)
                 for (int j = 2 * sub; j < n; j += 2 * g) {
-                    F2 s[NV];
+                    F2 sv[NV];
 #pragma unroll
-                    for (int q = 0; q < NV; q++) s[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
+                    for (int q = 0; q < NV; q++) sv[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
                     if constexpr (HILO) {
                         F2 sh[3], sl[3];
 #pragma unroll
@@ -292,76 +307,71 @@ STK_UNROLL(STK_P2P_UNROLL_MIXED)
                             sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
                             sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
                         }
-                        eval(p0, (th0[0] - sh[0]) + (tl0[0] - sl[0]), (th0[1] - sh[1]) + (tl0[1] - sl[1]),
-                             (th0[2] - sh[2]) + (tl0[2] - sl[2]), s, ta0);
-                        eval(p1, (th1[0] - sh[0]) + (tl1[0] - sl[0]), (th1[1] - sh[1]) + (tl1[1] - sl[1]),
-                             (th1[2] - sh[2]) + (tl1[2] - sl[2]), s, ta1);
+#pragma unroll
+                        for (int h = 0; h < TPL; h++)
+                            eval(pp[h], (th[h][0] - sh[0]) + (tl[h][0] - sl[0]), (th[h][1] - sh[1]) + (tl[h][1] - sl[1]),
+                                 (th[h][2] - sh[2]) + (tl[h][2] - sl[2]), sv, ta[h]);
                     } else {
                         double2 sx[3];
 #pragma unroll
                         for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
-                        eval(p0, mk((float)(tr0[0] - sx[0].x), (float)(tr0[0] - sx[0].y)),
-                             mk((float)(tr0[1] - sx[1].x), (float)(tr0[1] - sx[1].y)),
-                             mk((float)(tr0[2] - sx[2].x), (float)(tr0[2] - sx[2].y)), s, ta0);
-                        eval(p1, mk((float)(tr1[0] - sx[0].x), (float)(tr1[0] - sx[0].y)),
-                             mk((float)(tr1[1] - sx[1].x), (float)(tr1[1] - sx[1].y)),
-                             mk((float)(tr1[2] - sx[2].x), (float)(tr1[2] - sx[2].y)), s, ta1);
+#pragma unroll
+                        for (int h = 0; h < TPL; h++)
+                            eval(pp[h], mk((float)(tr[h][0] - sx[0].x), (float)(tr[h][0] - sx[0].y)),
+                                 mk((float)(tr[h][1] - sx[1].x), (float)(tr[h][1] - sx[1].y)),
+                                 mk((float)(tr[h][2] - sx[2].x), (float)(tr[h][2] - sx[2].y)), sv, ta[h]);
                     }
                 }
                 // Kahan-compensated accumulation of the tile's partial sums
 #pragma unroll
-                for (int k = 0; k < TDIM; k++) {
-                    float y = (p0[k].v.x + p0[k].v.y) - cmp0[k];
-                    float tt = acc0[k] + y;
-                    cmp0[k] = (tt - acc0[k]) - y;
-                    acc0[k] = tt;
-                    y = (p1[k].v.x + p1[k].v.y) - cmp1[k];
-                    tt = acc1[k] + y;
-                    cmp1[k] = (tt - acc1[k]) - y;
-                    acc1[k] = tt;
-                }
+                for (int h = 0; h < TPL; h++)
+#pragma unroll
+                    for (int k = 0; k < TDIM; k++) {
+                        const float y = (pp[h][k].v.x + pp[h][k].v.y) - cmp[h][k];
+                        const float t = acc[h][k] + y;
+                        cmp[h][k] = (t - acc[h][k]) - y;
+                        acc[h][k] = t;
+                    }
             } else {
 STK_UNROLL(STK_P2P_UNROLL_FP64)
                 for (int j = sub; j < n; j += g) {
-                    double s[NV];
+                    double sv[NV];
 #pragma unroll
-                    for (int q = 0; q < NV; q++) s[q] = mv[q][j];
+                    for (int q = 0; q < NV; q++) sv[q] = mv[q][j];
                     const double sx = mc[0][j], sy = mc[1][j], sz = mc[2][j];
-                    eval(acc0, xt0[0] - sx, xt0[1] - sy, xt0[2] - sz, s, ta0);
-                    eval(acc1, xt1[0] - sx, xt1[1] - sy, xt1[2] - sz, s, ta1);
+#pragma unroll
+                    for (int h = 0; h < TPL; h++)
+                        eval(acc[h], xt[h][0] - sx, xt[h][1] - sy, xt[h][2] - sz, sv, ta[h]);
                 }
             }
             __syncwarp();
         }
 
         // ---- reduce the lanes that share a target, then accumulate ----
-        double o0[TDIM], o1[TDIM];
+        double o[TPL][TDIM];
 #pragma unroll
-        for (int k = 0; k < TDIM; k++) {
-            if constexpr (MIXED) {
-                o0[k] = double(acc0[k]) - double(cmp0[k]);
-                o1[k] = double(acc1[k]) - double(cmp1[k]);
-            } else {
-                o0[k] = acc0[k];
-                o1[k] = acc1[k];
-            }
-        }
-        for (int o = 1; o < g; o <<= 1) {
+        for (int h = 0; h < TPL; h++)
 #pragma unroll
             for (int k = 0; k < TDIM; k++) {
-                o0[k] += __shfl_xor_sync(kFull, o0[k], o);
-                o1[k] += __shfl_xor_sync(kFull, o1[k], o);
+                if constexpr (MIXED)
+                    o[h][k] = double(acc[h][k]) - double(cmp[h][k]);
+                else
+                    o[h][k] = acc[h][k];
             }
+        for (int off = 1; off < g; off <<= 1) {
+#pragma unroll
+            for (int h = 0; h < TPL; h++)
+#pragma unroll
+                for (int k = 0; k < TDIM; k++) o[h][k] += __shfl_xor_sync(kFull, o[h][k], off);
         }
         if (sub == 0) {
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const bool act = h ? act1 : act0;
-                if (!act) continue;
-                double *dst = a.trg_out + (size_t)(h ? t1 : t0) * TDIM;
+            for (int h = 0; h < TPL; h++) {
+                if (!act[h]) continue;
+                double *dst = a.trg_out + (size_t)tt[h] * TDIM;
 #pragma unroll
                 for (int k = 0; k < TDIM; k++) {
-                    const double val = K::SCALE * K::comp_scale(k) * (h ? o1[k] : o0[k]);
+                    const double val = K::SCALE * K::comp_scale(k) * o[h][k];
                     if (a.atomic_out)
                         atomicAdd(dst + k, val);
                     else
