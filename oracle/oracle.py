@@ -248,6 +248,53 @@ EWALD_PVEL = 2
 EWALD_LAPLACE_HESS = 3
 
 
+def pvel_pxyz_terms(src, sval, trg):
+    """What the reference's triply periodic StokesPVel far field adds to the Ewald
+    sum of (f, trD) sources, as (pressure, velocity) at trg (unit cell, points in
+    [0, 1)^3):
+
+    * pressure (x - 1/2) . F with F = sum f, a mean pressure gradient that balances
+      a net force (M2L/StokesPVel/StokesPVel3D3D.cpp:203-206, in the M2C operator);
+    * velocity (1/2) sum y trD, half the trD dipole moment: the M2C operator adds
+      half of each root equivalent point's position wrapped into the cell
+      (StokesPVel3D3D.cpp:211-218) and FMMData::periodizeFMM the unwrapped rest
+      (Lib/src/FMMData.cpp:203-247); the root's equivalent density has the
+      sources' trD dipole moment.
+
+    The velocity term applies to PVel, PVelGrad and PVelLaplacian.  The pressure
+    term is fitted through the local expansion like every M2C value, and with no
+    velocity beside it it is not a Stokes flow, so an FMM reproduces it only
+    approximately; it vanishes for force-free sources.
+    """
+    src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+    sval = np.asarray(sval, dtype=np.float64).reshape(len(src), 4)
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((len(trg), 4))
+    out[:, 0] = (trg - 0.5) @ sval[:, :3].sum(0)
+    out[:, 1:] = 0.5 * (src * sval[:, 3:4]).sum(0)
+    return out
+
+
+def laplace_pxyz_neutraliser(total_charge: float, trg):
+    """Potential and gradient (n, 4) at trg of the reference's triply periodic
+    Laplace neutraliser: each equivalent charge of the root is paired with an
+    opposite one at the cell centre N = (1/2, 1/2, 1/2)
+    (M2L/Laplace/Laplace3D3D.cpp:266-273), whose periodic sum is taken without
+    the 5 x 5 x 5 block of images nearest to N (DIRECTLAYER = 2,
+    M2L/SVD_pvfmm.hpp:34).  For a total charge Q it contributes
+    -Q [G_ewald(x - N) - sum_{|s_i| <= 2} 1 / (4 pi |x - N - s|)]."""
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    cen = np.array([[0.5, 0.5, 0.5]])
+    one = np.ones((1, 1))
+    g = ewald(EWALD_LAPLACE, cen, one, trg)
+    near = np.zeros((len(trg), 4))
+    for a in range(-2, 3):
+        for b in range(-2, 3):
+            for c in range(-2, 3):
+                direct(UK_LAPLACE_PGRAD, cen + np.array([a, b, c]), one, trg, out=near)
+    return -total_charge * (g - near)
+
+
 def ewald2d(kind: int, src, sval, trg, out=None, nthreads: int = 0):
     """out += doubly periodic (x, y; z free) sum per pair (see stk_oracle.c:oracle_ewald2d).
 

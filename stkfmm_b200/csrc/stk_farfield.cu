@@ -161,9 +161,16 @@ __global__ void m2c_px_kernel(const double *__restrict__ X, int ni, const double
 // directly with the micro-kernel itself).  PBC = 3: periodic in x, y, z; PBC = 2:
 // in x and y.  The Ewald sums are those of stk_ewald.cuh; for stokes_pvel the
 // pressure row is -grad(psi).f / 4 pi and the trD column grad(psi) / 8 pi.
+// Triply periodic stokes_pvel carries the reference's two extra terms
+// (M2L/StokesPVel/StokesPVel3D3D.cpp:203-218): a pressure (x_i - 1/2).f that
+// balances a net force, and on the trD column a velocity of half the source
+// point's position wrapped into the cell (the net flux of a trD dipole; the
+// unwrapped rest is added after the evaluation, pvel_net_flux_kernel).
+// row_shift (nullable): subtracted from every column of row i (the Laplace
+// neutraliser of m2c_neutral_kernel).
 template <int UK, int PBC>
 __global__ void m2c_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
-                           double *__restrict__ M, int ld) {
+                           double *__restrict__ M, int ld, const double *__restrict__ row_shift) {
     using K = Uk<UK>;
     constexpr double pi = ewald::kPi;
     const long long total = (long long)ni * nj;
@@ -210,10 +217,75 @@ __global__ void m2c_kernel(const double *__restrict__ X, int ni, const double *_
                         for (int q = 0; q < K::TDIM; q++) out[q][col] -= K::SCALE * K::comp_scale(q) * u[q];
                     }
                 }
+        if constexpr (UK == UK_STOKES_PVEL && PBC == 3) {
+            for (int q = 0; q < 3; q++) out[0][q] += X[3 * i + q] - 0.5;
+            for (int p = 0; p < 3; p++) {
+                const double y = Y[3 * j + p];
+                out[1 + p][3] += 0.5 * (y - floor(y));
+            }
+        }
+        if (row_shift)
+            for (int p = 0; p < K::TDIM; p++)
+                for (int q = 0; q < K::SDIM; q++) out[p][q] -= row_shift[K::TDIM * i + p];
         for (int p = 0; p < K::TDIM; p++)
             for (int q = 0; q < K::SDIM; q++)
                 M[(size_t)(K::TDIM * i + p) + (size_t)ld * (K::SDIM * j + q)] = out[p][q];
     }
+}
+
+// The reference's triply periodic Laplace operator pairs every equivalent
+// charge with an opposite one at the cell centre N = (1/2, 1/2, 1/2)
+// (M2L/Laplace/Laplace3D3D.cpp:266-273): w_i = K_far(X_i - N), the Ewald sum
+// minus the 5 x 5 x 5 block of images the reference's generator sums directly
+// (DIRECTLAYER = 2, M2L/SVD_pvfmm.hpp:34), is taken off every column of row i.
+// For a neutral density the columns' sum of charges is zero and so is the
+// term; for a charged one it is the reference's convention.
+__global__ void m2c_neutral_kernel(const double *__restrict__ X, int ni, double *__restrict__ w) {
+    constexpr double pi = ewald::kPi;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ni; i += gridDim.x * blockDim.x) {
+        const double r0[3] = {X[3 * i] - 0.5, X[3 * i + 1] - 0.5, X[3 * i + 2] - 0.5};
+        double pot, g[3];
+        ewald::lap3(r0, pot, g);
+        double near = 0.0;
+        for (int a = -2; a <= 2; a++)
+            for (int b = -2; b <= 2; b++)
+                for (int c = -2; c <= 2; c++) {
+                    const double x = r0[0] + a, y = r0[1] + b, z = r0[2] + c;
+                    near += 1.0 / sqrt(x * x + y * y + z * z);
+                }
+        w[i] = (pot - near) / (4 * pi);
+    }
+}
+
+// Triply periodic PVel, PVelGrad and PVelLaplacian: the net-flux correction of
+// FMMData::periodizeFMM (Lib/src/FMMData.cpp:203-247).  With y_i the root's
+// upward-equivalent points and trD_i their trD densities, every target's
+// velocity (components 1..3) gets (1/2) sum_i (y_i - wrap(y_i)) trD_i; with the
+// wrapped half inside the M2C operator that makes (1/2) sum_i y_i trD_i, half
+// the trD dipole moment.  Each block reduces the n root values itself (in the
+// same order) and adds the result to its targets.
+constexpr int kNetFluxThreads = 256;  // the block size pvel_net_flux_kernel is launched with (a power of two)
+
+__global__ void __launch_bounds__(kNetFluxThreads)
+    pvel_net_flux_kernel(const double *__restrict__ phi_root, const double *__restrict__ ue_root, int n,
+                         double *__restrict__ trg, long long ntrg, int td) {
+    __shared__ double red[3][kNetFluxThreads];
+    double u[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double trd = phi_root[4 * i + 3];
+        for (int c = 0; c < 3; c++) u[c] += floor(ue_root[3 * i + c]) * trd;
+    }
+    for (int c = 0; c < 3; c++) red[c][threadIdx.x] = u[c];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int c = 0; c < 3; c++) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+        __syncthreads();
+    }
+    const double U[3] = {0.5 * red[0][0], 0.5 * red[1][0], 0.5 * red[2][0]};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntrg;
+         t += (long long)gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) trg[t * td + 1 + c] += U[c];
 }
 
 int kernel_matrix(int uk, const double *X, int ni, const double *Y, int nj, double *M, int ld, cudaStream_t s) {
@@ -804,7 +876,7 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     const int n = F.n, N = F.n * F.ke;
     std::vector<double> unit = unit_surface(F.p);
     // the root: centre (0.5, 0.5, 0.5), half-width 0.5; its UE and DC surfaces coincide (RAD0)
-    DevBuf X, M2C;
+    DevBuf X, M2C, W;
     int rc = upload_points(X, scaled_surface(unit, 0.5, 0.5, 0.5, kRad0 * 0.5), s);
     if (!rc) rc = M2C.reserve(sizeof(double) * (size_t)N * N);
     if (!rc) rc = F.m2c_op.reserve(sizeof(double) * (size_t)N * N);
@@ -812,10 +884,15 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     const int grid = grid_for((long long)n * n);
     const double *Xp = (const double *)X.ptr;
     double *Mp = (double *)M2C.ptr;
-#define STK_M2C(UKV, P) m2c_kernel<UKV, P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N)
-    if (pbc == 3 && F.m2x == UK_LAPLACE_P)
+    const double *shift = nullptr;
+#define STK_M2C(UKV, P) m2c_kernel<UKV, P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N, shift)
+    if (pbc == 3 && F.m2x == UK_LAPLACE_P) {
+        rc = W.reserve(sizeof(double) * (size_t)n);
+        if (rc) return rc;
+        m2c_neutral_kernel<<<(n + 127) / 128, 128, 0, s>>>(Xp, n, (double *)W.ptr);
+        shift = (const double *)W.ptr;
         STK_M2C(UK_LAPLACE_P, 3);
-    else if (pbc == 3 && F.m2x == UK_STOKES_VEL)
+    } else if (pbc == 3 && F.m2x == UK_STOKES_VEL)
         STK_M2C(UK_STOKES_VEL, 3);
     else if (pbc == 3 && F.m2x == UK_STOKES_PVEL)
         STK_M2C(UK_STOKES_PVEL, 3);
@@ -1742,6 +1819,17 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
             rc = run_pass(F.m2t, prec, (const double *)F.rec_surf.ptr, (const int *)F.m2t.src_beg.ptr,
                           (const int *)F.m2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
         if (rc) return rc;
+    }
+    // periodizeFMM: PVel, PVelGrad and PVelLaplacian only (not Traction), on the
+    // first shard alone so that the shards' outputs still sum to the whole
+    const unsigned kid = ki->id;
+    if (f->pbc == STK_PAXIS_PXYZ && (kid == STK_PVel || kid == STK_PVelGrad || kid == STK_PVelLaplacian) &&
+        f->shard_rank == 0 && f->ntrg > 0) {
+        const int blocks = (int)std::min<long long>(((long long)f->ntrg + kNetFluxThreads - 1) / kNetFluxThreads, 148 * 4);
+        pvel_net_flux_kernel<<<blocks, kNetFluxThreads, 0, s>>>(phi, (const double *)F.ue_xyz.ptr, n, trg_sorted,
+                                                                f->ntrg, ki->kdim_trg);
+        FCUDA(cudaGetLastError());
+        t_launches++;
     }
     FCUDA(cudaEventRecord(kd->ph[7], s));
     F.launches = t_launches;

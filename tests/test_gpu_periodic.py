@@ -143,18 +143,55 @@ def test_doubly_periodic_laplace(torch_cuda):
 @pytest.mark.parametrize("pbc", [2, 3])
 def test_periodic_pvel(torch_cuda, pbc):
     """StokesPVel (pressure and velocity) with f and trD, neutralised as the
-    reference's periodic tests do (Test/Test.cpp:364-402).  Triply periodic
-    pressure and mean velocity are fixed only up to constants; the reference's
-    error measure reports that "drift" (mean difference per component,
-    Test/Test.cpp:143-150) apart from the error, and so does this test: PXY has
-    none, PXYZ is compared with the drift removed."""
+    reference's periodic tests do (Test/Test.cpp:364-402).  PXYZ follows the
+    reference's conventions (oracle.pvel_pxyz_terms: half the trD dipole moment
+    on the velocity), which leave the velocity without drift; the triply periodic
+    pressure is fixed only up to a constant, the "drift" the reference's error
+    measure reports apart from the error (mean difference per component,
+    Test/Test.cpp:143-150), and is compared with it removed.  PXY has none."""
     pts, rng = points("clustered", 2000, 9 + pbc)
     v = rng.normal(size=(len(pts), 4))
     v -= v.mean(0)
     out = periodic_fmm_pbc(128, pbc, 10, 50, pts, v)
-    ref = (O.ewald2d(O.EWALD_PVEL, pts, v, pts) if pbc == 2 else O.ewald(O.EWALD_PVEL, pts, v, pts))
-    if pbc == 3:
-        out = out - (out - ref).mean(0)
+    if pbc == 2:
+        ref = O.ewald2d(O.EWALD_PVEL, pts, v, pts)
+    else:
+        ref = O.ewald(O.EWALD_PVEL, pts, v, pts) + O.pvel_pxyz_terms(pts, v, pts)
+        out[:, 0] -= (out[:, 0] - ref[:, 0]).mean()
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+
+
+def test_periodic_pvel_family_net_flux(torch_cuda):
+    """PXYZ PVelGrad and PVelLaplacian share PVel's far field and its net-flux
+    correction (FMMData.cpp:214-216 names all three): their pressure and velocity
+    equal PVel's; and the velocity carries half the trD dipole moment, which a
+    shift of the trD sources changes (the reference's M2C is not translation
+    invariant, StokesPVel3D3D.cpp:362-364)."""
+    pts, rng = points("uniform", 2000, 31)
+    v = np.zeros((len(pts), 4))
+    v[:, 3] = rng.normal(size=len(pts))
+    v[:, 3] -= v[:, 3].mean()
+    res = {}
+    for k in (128, 256, 512):
+        res[k] = periodic_fmm_pbc(k, 3, 10, 50, pts, v)
+    for k in (256, 512):
+        assert np.linalg.norm(res[k][:, :4] - res[128]) / np.linalg.norm(res[128]) < 1e-11, k
+    ref = O.ewald(O.EWALD_PVEL, pts, v, pts) + O.pvel_pxyz_terms(pts, v, pts)
+    errs = component_errors(res[128][:, 1:], ref[:, 1:])
+    assert max(errs) < TOL[10], errs
+
+
+def test_periodic_laplace_charged(torch_cuda):
+    """A charged cell: the reference's PXYZ Laplace operator pairs every
+    equivalent charge with an opposite one at the cell centre
+    (M2L/Laplace/Laplace3D3D.cpp:266-273; oracle.laplace_pxyz_neutraliser).
+    The gradient is compared as is, the potential with its drift removed."""
+    pts, rng = points("clustered", 2000, 33)
+    q = rng.normal(size=(len(pts), 1)) + 0.2
+    out = periodic_fmm_pbc(1, 3, 10, 50, pts, q)
+    ref = O.ewald(O.EWALD_LAPLACE, pts, q, pts) + O.laplace_pxyz_neutraliser(q.sum(), pts)
+    out[:, 0] -= (out[:, 0] - ref[:, 0]).mean()
     errs = component_errors(out, ref)
     assert max(errs) < TOL[10], errs
 

@@ -327,3 +327,77 @@ def test_traction_is_stress_of_pvelgrad(rng, ukg, ukt, sd):
     g = G[:, 7:16].reshape(-1, 3, 3)
     comb = -G[:, 0][:, None, None] * np.eye(3)[None] + g + g.transpose(0, 2, 1)
     assert np.abs(comb.reshape(-1, 9) - T).max() < 1e-13 * np.abs(T).max()
+
+
+def _root_equivalent(uk, p, src, sval):
+    """The root's upward-equivalent density of the unit cell as PVFMM forms it:
+    check potentials on the radius-2.95 surface, a pseudo-inverse solve (cut
+    sqrt(machine eps), M2L/SVD_pvfmm.hpp:599-604) for densities on the
+    radius-1.05 surface (surface layout of stkfmm_helpers.hpp:46-85)."""
+    sd, td = O.UK_SDIM[uk], O.UK_TDIM[uk]
+    ue = O.surface(p, np.full(3, -0.025), 1.05, 0)
+    uc = O.surface(p, np.full(3, -0.975), 2.95, 0)
+    A = np.zeros((len(uc) * td, len(ue) * sd))
+    for j in range(len(ue)):
+        for c in range(sd):
+            e = np.zeros((1, sd))
+            e[0, c] = 1.0
+            A[:, j * sd + c] = O.direct(uk, ue[j:j + 1], e, uc).reshape(-1)
+    chk = O.direct(uk, src, sval, uc).reshape(-1)
+    U, s, Vt = np.linalg.svd(A, full_matrices=False)
+    keep = s > s[0] * np.sqrt(np.finfo(float).eps)
+    return ue, ((Vt[keep].T / s[keep]) @ (U[:, keep].T @ chk)).reshape(len(ue), sd)
+
+
+def _image_block(uk, src, sval, trg, layers):
+    out = np.zeros((len(trg), O.UK_TDIM[uk]))
+    r = range(-layers, layers + 1)
+    for a in r:
+        for b in r:
+            for c in r:
+                O.direct(uk, src + np.array([a, b, c]), sval, trg, out=out)
+    return out
+
+
+def test_pvel_pxyz_terms_pin_the_root_chain(rng):
+    """oracle.pvel_pxyz_terms against the reference's own root-level arithmetic:
+    the images outside the directly summed block come from the root's equivalent
+    density through the Ewald sum, plus half its wrapped trD dipole (M2C,
+    StokesPVel3D3D.cpp:211-218) and half the unwrapped rest (periodizeFMM,
+    FMMData.cpp:203-247).  The velocity is then the sources' Ewald sum plus half
+    their trD dipole moment, with no drift; without the two terms it is off by
+    half the equivalent density's dipole (its fit misses the sources' dipole)."""
+    src, trg = rng.random((300, 3)), rng.random((40, 3))
+    val = rng.normal(size=(300, 4))
+    val -= val.mean(0)
+    ue, veq = _root_equivalent(O.UK_STOKES_PVEL, 8, src, val)
+    ew = O.ewald(O.EWALD_PVEL, src, val, trg)
+    chain = (_image_block(O.UK_STOKES_PVEL, src, val, trg, 1) + O.ewald(O.EWALD_PVEL, np.mod(ue, 1.0), veq, trg)
+             - _image_block(O.UK_STOKES_PVEL, ue, veq, trg, 1))
+    chain[:, 1:] += 0.5 * (np.mod(ue, 1.0) * veq[:, 3:4]).sum(0) + 0.5 * (np.floor(ue) * veq[:, 3:4]).sum(0)
+    ref = ew + O.pvel_pxyz_terms(src, val, trg)
+    vel = chain[:, 1:] - ref[:, 1:]
+    assert np.abs(vel).max() < 1e-6 * np.abs(ref[:, 1:]).max()
+    assert np.abs(0.5 * ((ue * veq[:, 3:4]).sum(0) - (src * val[:, 3:4]).sum(0))).max() > 1e-3
+
+
+def test_laplace_pxyz_neutraliser_pins_the_root_chain(rng):
+    """oracle.laplace_pxyz_neutraliser against the reference's root-level
+    arithmetic for a charged cell: every equivalent charge is paired with an
+    opposite one at the centre (Laplace3D3D.cpp:266-273).  The gradient then
+    matches the Ewald sum plus the neutraliser exactly; the potential up to a
+    constant (the drift of a triply periodic potential)."""
+    src, trg = rng.random((300, 3)), rng.random((40, 3))
+    q = rng.normal(size=(300, 1)) + 0.3
+    ue, qeq = _root_equivalent(O.UK_LAPLACE_P, 10, src, q)
+    cen = np.array([[0.5, 0.5, 0.5]])
+    far_n = O.ewald(O.EWALD_LAPLACE, cen, np.ones((1, 1)), trg) - _image_block(O.UK_LAPLACE_PGRAD, cen, np.ones((1, 1)),
+                                                                               trg, 2)
+    chain = (_image_block(O.UK_LAPLACE_PGRAD, src, q, trg, 1) + O.ewald(O.EWALD_LAPLACE, np.mod(ue, 1.0), qeq, trg)
+             - _image_block(O.UK_LAPLACE_PGRAD, ue, qeq, trg, 1) - qeq.sum() * far_n)
+    ref = O.ewald(O.EWALD_LAPLACE, src, q, trg) + O.laplace_pxyz_neutraliser(q.sum(), trg)
+    d = chain - ref
+    assert np.abs(d[:, 1:]).max() < 1e-6 * np.abs(ref[:, 1:]).max()
+    assert np.ptp(d[:, 0]) < 1e-6 * np.abs(ref[:, 0]).max()
+    plain = chain - O.ewald(O.EWALD_LAPLACE, src, q, trg)
+    assert np.abs(plain[:, 1:] - plain[:, 1:].mean(0)).max() > 1e-2 * np.abs(ref[:, 1:]).max()
