@@ -3,9 +3,12 @@
 The oracle (oracle/stk_oracle.c:oracle_ewald) restates the periodic Green's
 functions of the reference's M2C generator (M2L/Laplace/Laplace3D3D.cpp,
 M2L/Stokeslet/Stokes3D3D.cpp) and is itself checked for independence of the
-Ewald split and against lattice sums (tests/test_oracle.py).  Inputs follow the
-reference's periodic tests: net force (charge) removed (Test/Test.cpp:332-351).
-Error measure: relative L2 per output component (Test/Test.cpp:113-151).
+Ewald split and against lattice sums (tests/test_oracle.py); the reference's
+extra PXYZ terms (PVel net flux and net force, the Laplace neutraliser) are
+oracle.pvel_pxyz_terms and oracle.laplace_pxyz_neutraliser.  Inputs follow the
+reference's periodic tests: net force (charge) removed (Test/Test.cpp:332-351),
+except where a test says otherwise.  Error measure: relative L2 per output
+component (Test/Test.cpp:113-151).
 """
 import numpy as np
 import pytest
