@@ -401,3 +401,20 @@ def test_laplace_pxyz_neutraliser_pins_the_root_chain(rng):
     assert np.ptp(d[:, 0]) < 1e-6 * np.abs(ref[:, 0]).max()
     plain = chain - O.ewald(O.EWALD_LAPLACE, src, q, trg)
     assert np.abs(plain[:, 1:] - plain[:, 1:].mean(0)).max() > 1e-2 * np.abs(ref[:, 1:]).max()
+
+
+def test_stokes_ewald_reference_three_forces(rng):
+    """The reference generator's own check (M2L/Stokeslet/Stokes3D3D.cpp:183-242):
+    three point forces in the unit cell (net force (0, 1, 0)), the near block
+    summed directly plus the root's equivalent density through the far-image
+    sum, against the Ewald sum (here at its sample point (1/2, 1/2, 1/2) and 20
+    more).  Pins the oracle's Hasimoto sum, net force included, to the
+    root-level arithmetic."""
+    src = np.array([[0.1, 0.55, 0.2], [0.5, 0.1, 0.3], [0.8, 0.5, 0.7]])
+    f = np.array([[1.0, 0.0, 0.0], [-1.0, 1.0, 1.0], [0.0, 0.0, -1.0]])
+    trg = np.concatenate([[[0.5, 0.5, 0.5]], rng.random((20, 3))])
+    ue, feq = _root_equivalent(O.UK_STOKES_VEL, 10, src, f)
+    chain = (_image_block(O.UK_STOKES_VEL, src, f, trg, 1) + O.ewald(O.EWALD_STOKES, np.mod(ue, 1.0), feq, trg)
+             - _image_block(O.UK_STOKES_VEL, ue, feq, trg, 1))
+    ew = O.ewald(O.EWALD_STOKES, src, f, trg)
+    assert np.abs(chain - ew).max() < 1e-6 * np.abs(ew).max()
