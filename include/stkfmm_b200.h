@@ -224,6 +224,13 @@ int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision);
  * all shards' evaluate_near / evaluate_fmm outputs (e.g. an all-reduce) is the
  * unsharded result.  Takes effect at the next setup_tree (default 0 of 1). */
 int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks);
+/* The periodic far field, the reference's enableFF constructor argument
+ * (STKFMM.hpp:199-200, FMMData.cpp:83-89; its C ABI always passes true).  enable = 0:
+ * no far-image operator and no periodizeFMM correction, so a periodic sum stops
+ * at the images within two cells of the unit cell on each periodic axis, the
+ * images PVFMM's periodic lists reach.  Takes effect at the next setup_tree
+ * (default 1).  No effect in free space. */
+int Stk3DFMM_set_far_field(Stk3DFMM *fmm, int enable);
 /* Near-field (U-list S2T) part of evaluate_fmm only, on the tree of setup_tree:
  * trg_value += sum over U-list leaf pairs, in the caller's coordinates/units. */
 int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value, const int nTrg,
@@ -305,6 +312,9 @@ int StkWallFMM_show_active_kernels(StkWallFMM *fmm);
  * handle's stream; the first call after setup_tree builds the sub-FMMs' far-field
  * operators and synchronises); device time (ms) of the last evaluation */
 int StkWallFMM_set_precision(StkWallFMM *fmm, int precision);
+/* Stk3DFMM_set_far_field for every sub-FMM (the reference's StkWallFMM enableFF,
+ * STKFMM.hpp:233-234); takes effect at the next setup_tree */
+int StkWallFMM_set_far_field(StkWallFMM *fmm, int enable);
 int StkWallFMM_evaluate_fmm_device(StkWallFMM *fmm, unsigned kernel, const double *d_src_SL_value,
                                    double *d_trg_value, void *stream);
 int StkWallFMM_last_kernel_ms(StkWallFMM *fmm, float *ms);

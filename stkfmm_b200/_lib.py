@@ -58,6 +58,7 @@ SIGNATURES = [
     ("Stk3DFMM_evaluate_kernel", c_int, [c_void_p, c_uint, c_int, c_uint, c_int, P_d, P_d, c_int, P_d, P_d]),
     ("Stk3DFMM_set_precision", c_int, [c_void_p, c_int]),
     ("Stk3DFMM_set_shard", c_int, [c_void_p, c_int, c_int]),
+    ("Stk3DFMM_set_far_field", c_int, [c_void_p, c_int]),
     ("stk_partition_lpt", c_int, [c_int, P_d, c_int, P_i]),
     ("Stk3DFMM_evaluate_near", c_int, [c_void_p, c_uint, c_int, P_d, c_int, P_d, c_int, P_d]),
     ("Stk3DFMM_evaluate_near_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -79,6 +80,7 @@ SIGNATURES = [
     ("StkWallFMM_evaluate_fmm", c_int, [c_void_p, c_uint, c_int, P_d, c_int, P_d, c_int, P_d]),
     ("StkWallFMM_show_active_kernels", c_int, [c_void_p]),
     ("StkWallFMM_set_precision", c_int, [c_void_p, c_int]),
+    ("StkWallFMM_set_far_field", c_int, [c_void_p, c_int]),
     ("StkWallFMM_evaluate_fmm_device", c_int, [c_void_p, c_uint, c_void_p, c_void_p, c_void_p]),
     ("StkWallFMM_last_kernel_ms", c_int, [c_void_p, P_f]),
     ("StkWallFMM_last_launch_count", c_int, [c_void_p, c_uint, P_i]),

@@ -115,13 +115,18 @@ __global__ void kernel_matrix_kernel(const double *__restrict__ X, int ni, const
     }
 }
 
-// Singly periodic (PX) far images: the images t = 2 .. kPxImages on both sides
-// along x, summed directly with the micro-kernel, as the reference's generator
-// does (M2L/Laplace/Laplace1D3D.cpp:18-28, SUM1D = 500000 in
-// M2L/SVD_pvfmm.hpp:35).  The sum runs from the farthest images inwards with
-// compensation; for a neutral (and force-free) root density the images' tail
-// decays like a dipole lattice, so the cut-off costs ~1e-6 / kPxImages.
-constexpr int kPxImages = 500000;
+// Singly periodic (PX) far images: the images t = 2 .. kPxImages - 1 on both
+// sides along x, summed directly with the micro-kernel, as the reference's
+// generators do: t < SUM1D = 500000 for laplace_p and stokes_vel
+// (M2L/Laplace/Laplace1D3D.cpp:18-28, M2L/Stokeslet/Stokes1D3D.cpp:37,
+// M2L/SVD_pvfmm.hpp:35), t < 1000000 for stokes_pvel
+// (M2L/StokesPVel/StokesPVel1D3D.cpp:36-46).  Their sums start at t = 3
+// because PVFMM's lists reach two cells; this build's reach one.  The sum
+// runs from the farthest images inwards with compensation; for a neutral
+// (and force-free) root density the images' tail decays like a dipole
+// lattice, so the cut-off costs about 1 / kPxImages of a dipole's field.
+template <int UK>
+constexpr int kPxImages = UK == UK_STOKES_PVEL ? 1000000 : 500000;
 
 template <int UK>
 __global__ void m2c_px_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
@@ -137,7 +142,7 @@ __global__ void m2c_px_kernel(const double *__restrict__ X, int ni, const double
             for (int q = 0; q < K::SDIM; q++) f[q] = q == col ? 1.0 : 0.0;
             for (int q = 0; q < K::TDIM; q++) sum[q] = cmp[q] = 0.0;
             K::stage(f, v);
-            for (int t = kPxImages; t >= 2; t--) {
+            for (int t = kPxImages<UK> - 1; t >= 2; t--) {
                 double u[K::TDIM];
                 for (int q = 0; q < K::TDIM; q++) u[q] = 0.0;
                 K::eval(u, r0[0] + t, r0[1], r0[2], v);
@@ -151,6 +156,46 @@ __global__ void m2c_px_kernel(const double *__restrict__ X, int ni, const double
             for (int q = 0; q < K::TDIM; q++)
                 M[(size_t)(K::TDIM * i + q) + (size_t)ld * (K::SDIM * j + col)] = K::SCALE * K::comp_scale(q) * sum[q];
         }
+    }
+}
+
+// Far field off (the reference's enableFF = false: no periodic far-image
+// operator, FMMData.cpp:83-89): the periodic sum stops at the images that
+// PVFMM's periodic lists reach, |s_i| <= 2 on each periodic axis (the block
+// the reference's M2C generators leave to the tree, DIRECTLAYER = 2,
+// M2L/SVD_pvfmm.hpp:34).  This build's lists reach |s_i| <= 1, so the ring of
+// images between the two blocks goes through the root's equivalent density:
+// M = sum over that ring of the translation kernel, summed directly with the
+// micro-kernel.  PBC = 1, 2, 3: periodic in x; x and y; x, y and z.
+template <int UK, int PBC>
+__global__ void m2c_ring_kernel(const double *__restrict__ X, int ni, const double *__restrict__ Y, int nj,
+                                double *__restrict__ M, int ld) {
+    using K = Uk<UK>;
+    constexpr int LB = PBC >= 2 ? 2 : 0, LC = PBC == 3 ? 2 : 0;
+    const long long total = (long long)ni * nj;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % ni), j = (int)(idx / ni);
+        const double r0[3] = {X[3 * i] - Y[3 * j], X[3 * i + 1] - Y[3 * j + 1], X[3 * i + 2] - Y[3 * j + 2]};
+        double out[K::TDIM][K::SDIM];
+        for (int p = 0; p < K::TDIM; p++)
+            for (int q = 0; q < K::SDIM; q++) out[p][q] = 0.0;
+        for (int a = -2; a <= 2; a++)
+            for (int b = -LB; b <= LB; b++)
+                for (int c = -LC; c <= LC; c++) {
+                    if (a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) continue;
+                    for (int col = 0; col < K::SDIM; col++) {
+                        double f[K::SDIM], v[K::NV], u[K::TDIM];
+                        for (int q = 0; q < K::SDIM; q++) f[q] = q == col ? 1.0 : 0.0;
+                        for (int q = 0; q < K::TDIM; q++) u[q] = 0.0;
+                        K::stage(f, v);
+                        K::eval(u, r0[0] + a, r0[1] + b, r0[2] + c, v);
+                        for (int q = 0; q < K::TDIM; q++) out[q][col] += K::SCALE * K::comp_scale(q) * u[q];
+                    }
+                }
+        for (int p = 0; p < K::TDIM; p++)
+            for (int q = 0; q < K::SDIM; q++)
+                M[(size_t)(K::TDIM * i + p) + (size_t)ld * (K::SDIM * j + q)] = out[p][q];
     }
 }
 
@@ -870,9 +915,10 @@ int build_operators(FarField &F, cudaStream_t s) {
     return STK_OK;
 }
 
-// Triply periodic far-image operator of the root: m2c_op = DC2DE M2C (FP64),
-// mapping the root's upward equivalent density to its downward one.
-int build_periodic(FarField &F, int pbc, cudaStream_t s) {
+// Periodic far-image operator of the root: m2c_op = DC2DE M2C (FP64), mapping
+// the root's upward equivalent density to its downward one.  far_field = 0:
+// only the ring of images up to two cells away (m2c_ring_kernel).
+int build_periodic(FarField &F, int pbc, int far_field, cudaStream_t s) {
     const int n = F.n, N = F.n * F.ke;
     std::vector<double> unit = unit_surface(F.p);
     // the root: centre (0.5, 0.5, 0.5), half-width 0.5; its UE and DC surfaces coincide (RAD0)
@@ -886,7 +932,25 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     double *Mp = (double *)M2C.ptr;
     const double *shift = nullptr;
 #define STK_M2C(UKV, P) m2c_kernel<UKV, P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N, shift)
-    if (pbc == 3 && F.m2x == UK_LAPLACE_P) {
+#define STK_RING(UKV, P) m2c_ring_kernel<UKV, P><<<grid, 128, 0, s>>>(Xp, n, Xp, n, Mp, N)
+    if (!far_field) {
+        if (pbc < 1 || pbc > 3) return STK_ERR_NOT_SUPPORTED;
+        if (F.m2x == UK_LAPLACE_P) {
+            if (pbc == 1) STK_RING(UK_LAPLACE_P, 1);
+            if (pbc == 2) STK_RING(UK_LAPLACE_P, 2);
+            if (pbc == 3) STK_RING(UK_LAPLACE_P, 3);
+        } else if (F.m2x == UK_STOKES_VEL) {
+            if (pbc == 1) STK_RING(UK_STOKES_VEL, 1);
+            if (pbc == 2) STK_RING(UK_STOKES_VEL, 2);
+            if (pbc == 3) STK_RING(UK_STOKES_VEL, 3);
+        } else if (F.m2x == UK_STOKES_PVEL) {
+            if (pbc == 1) STK_RING(UK_STOKES_PVEL, 1);
+            if (pbc == 2) STK_RING(UK_STOKES_PVEL, 2);
+            if (pbc == 3) STK_RING(UK_STOKES_PVEL, 3);
+        } else {
+            return STK_ERR_NOT_SUPPORTED;
+        }
+    } else if (pbc == 3 && F.m2x == UK_LAPLACE_P) {
         rc = W.reserve(sizeof(double) * (size_t)n);
         if (rc) return rc;
         m2c_neutral_kernel<<<(n + 127) / 128, 128, 0, s>>>(Xp, n, (double *)W.ptr);
@@ -911,6 +975,7 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     else
         return STK_ERR_NOT_SUPPORTED;
 #undef STK_M2C
+#undef STK_RING
     FCUDA(cudaGetLastError());
     const double one = 1.0, zero = 0.0;
     cublasSetStream(F.blas, s);
@@ -920,6 +985,7 @@ int build_periodic(FarField &F, int pbc, cudaStream_t s) {
     F.m2c_p = F.p;
     F.m2c_m2x = F.m2x;
     F.m2c_pbc = pbc;
+    F.m2c_ff = far_field;
     return STK_OK;
 }
 
@@ -1202,8 +1268,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         }
     }
     F.periodic = f->pbc >= 1;
-    if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x || F.m2c_pbc != f->pbc)) {
-        rc = build_periodic(F, f->pbc, s);
+    const int far_field = f->enable_ff ? 1 : 0;
+    if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x || F.m2c_pbc != f->pbc || F.m2c_ff != far_field)) {
+        rc = build_periodic(F, f->pbc, far_field, s);
         if (rc) return rc;
     }
     const Octree &T = kd->tree;
@@ -1820,11 +1887,12 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
                           (const int *)F.m2t.src_end.ptr, trg_xyz, trg_sorted, counter, sms, s);
         if (rc) return rc;
     }
-    // periodizeFMM: PVel, PVelGrad and PVelLaplacian only (not Traction), on the
-    // first shard alone so that the shards' outputs still sum to the whole
+    // periodizeFMM: PVel, PVelGrad and PVelLaplacian only (not Traction), with the
+    // far field on, on the first shard alone so that the shards' outputs still
+    // sum to the whole
     const unsigned kid = ki->id;
-    if (f->pbc == STK_PAXIS_PXYZ && (kid == STK_PVel || kid == STK_PVelGrad || kid == STK_PVelLaplacian) &&
-        f->shard_rank == 0 && f->ntrg > 0) {
+    if (f->pbc == STK_PAXIS_PXYZ && f->enable_ff &&
+        (kid == STK_PVel || kid == STK_PVelGrad || kid == STK_PVelLaplacian) && f->shard_rank == 0 && f->ntrg > 0) {
         const int blocks = (int)std::min<long long>(((long long)f->ntrg + kNetFluxThreads - 1) / kNetFluxThreads, 148 * 4);
         pvel_net_flux_kernel<<<blocks, kNetFluxThreads, 0, s>>>(phi, (const double *)F.ue_xyz.ptr, n, trg_sorted,
                                                                 f->ntrg, ki->kdim_trg);

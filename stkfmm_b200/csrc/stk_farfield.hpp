@@ -87,7 +87,7 @@ struct FarField {
     std::vector<int> m2l_slot;  // offset code (0..342) -> block, -1 for adjacent offsets
     // periodic (PXY, PXYZ): DC2DE M2C of the root (far images, max |s| >= 2)
     bool periodic = false;
-    int m2c_p = 0, m2c_m2x = -1, m2c_pbc = 0;
+    int m2c_p = 0, m2c_m2x = -1, m2c_pbc = 0, m2c_ff = -1;  // what m2c_op was built for (m2c_ff: far field on)
     DevBuf m2c_op;
     // per-tree data
     DevBuf unit_surf;          // n x 3 points on [-1,1]^3

@@ -296,6 +296,17 @@ extern "C" int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks) {
     return STK_OK;
 }
 
+extern "C" int Stk3DFMM_set_far_field(Stk3DFMM *fmm, int enable) {
+    if (!fmm || (enable != 0 && enable != 1)) return STK_ERR_INVALID_ARG;
+    if (fmm->enable_ff != (enable == 1))
+        for (auto &kv : fmm->pool) {
+            kv.second->tree_ready = false;  // takes effect at the next setup_tree
+            kv.second->far_ready = false;
+        }
+    fmm->enable_ff = enable == 1;
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision) {
     if (!fmm || (precision != STK_FP64 && precision != STK_MIXED)) return STK_ERR_INVALID_ARG;
     fmm->precision = precision;

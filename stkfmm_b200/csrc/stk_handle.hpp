@@ -60,6 +60,9 @@ struct Stk3DFMM {
     int precision = 0;
     int device = 0, sms = 1;
     int shard_rank = 0, shard_n = 1;  // target-side work of this handle: shard shard_rank of shard_n
+    // periodic far field (the reference's enableFF, STKFMM.hpp:199-200): off, the
+    // periodic sum stops two cells away
+    bool enable_ff = true;
     cudaStream_t stream = nullptr;
     bool points_set = false, sl_dl_same = false;
     int nsl = 0, ndl = 0, ntrg = 0;

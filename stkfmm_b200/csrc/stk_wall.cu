@@ -176,6 +176,7 @@ struct StkWallFMM {
     double origin[3] = {0, 0, 0};
     double len = 1.0, sf = 1.0;
     int precision = STK_FP64;
+    bool enable_ff = true;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -373,6 +374,20 @@ extern "C" int StkWallFMM_show_active_kernels(StkWallFMM *fmm) {
     if (!fmm) return STK_ERR_INVALID_ARG;
     if (fmm->sub[0][0]) printf("enable Stokes image kernel\n");
     if (fmm->sub[1][0]) printf("enable RPY image kernel\n");
+    return STK_OK;
+}
+
+// The reference's enableFF (StkWallFMM.cpp:5-32 hands it to every sub-FMM).
+extern "C" int StkWallFMM_set_far_field(StkWallFMM *fmm, int enable) {
+    if (!fmm || (enable != 0 && enable != 1)) return STK_ERR_INVALID_ARG;
+    for (auto &fam : fmm->sub)
+        for (int k = 0; k < kSubs; k++)
+            if (fam[k]) {
+                const int rc = Stk3DFMM_set_far_field(fam[k], enable);
+                if (rc) return rc;
+            }
+    if (fmm->enable_ff != (enable == 1)) fmm->ready[0] = fmm->ready[1] = false;  // takes effect at setup_tree
+    fmm->enable_ff = enable == 1;
     return STK_OK;
 }
 

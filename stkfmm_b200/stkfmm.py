@@ -157,7 +157,9 @@ def evaluate_kernel(kernel, p2p, src_coord, src_value, trg_coord, trg_value, pre
 class Stk3DFMM:
     """B200 counterpart of PySTKFMM.Stk3DFMM (Python/PySTKFMM.py:34-79)."""
 
-    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64):
+    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64, enable_ff=True):
+        """enable_ff: the reference's enableFF (Lib/include/STKFMM/STKFMM.hpp:199-200); False
+        stops a periodic sum at the images within two cells (no far-image operator)."""
         self.mult_order = int(mult_order)
         self.max_pts = int(max_pts)
         self.pbc = int(pbc)
@@ -168,7 +170,12 @@ class Stk3DFMM:
             status = 6 if L.stk_device_count() <= 0 else 1
             raise StkError(status, "Stk3DFMM_create")
         self.set_precision(precision)
+        self.set_far_field(enable_ff)
         self._n = (0, 0, 0)
+
+    def set_far_field(self, enable):
+        check(lib().Stk3DFMM_set_far_field(self.fmm, 1 if enable else 0), "set_far_field")
+        self.enable_ff = bool(enable)
 
     def __del__(self):
         f = getattr(self, "fmm", None)
@@ -301,7 +308,7 @@ class StkWallFMM:
     (KERNEL.Stokes) or RPY spheres (KERNEL.RPY) above a no-slip wall at z = origin_z,
     points in [o, o+L)^2 x [o_z, o_z+L/2); pbc NONE, PX or PXY."""
 
-    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64):
+    def __init__(self, mult_order, max_pts, pbc, kernels, precision=PRECISION.FP64, enable_ff=True):
         self.mult_order = int(mult_order)
         self.max_pts = int(max_pts)
         self.pbc = int(pbc)
@@ -312,6 +319,11 @@ class StkWallFMM:
             status = 6 if L.stk_device_count() <= 0 else 1
             raise StkError(status, "StkWallFMM_create")
         self.set_precision(precision)
+        self.set_far_field(enable_ff)
+
+    def set_far_field(self, enable):
+        check(lib().StkWallFMM_set_far_field(self.fmm, 1 if enable else 0), "set_far_field")
+        self.enable_ff = bool(enable)
 
     def __del__(self):
         f = getattr(self, "fmm", None)

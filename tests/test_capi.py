@@ -91,6 +91,16 @@ def test_no_cpu_fallback():
     assert not L.StkWallFMM_create(8, 64, 0, 8)
 
 
+def test_setters_reject_null_handles():
+    """The handle setters refuse a null handle and invalid flags before any device work."""
+    L = lib()
+    invalid_arg = 1  # STK_ERR_INVALID_ARG
+    for fn, arg in (("Stk3DFMM_set_far_field", 1), ("StkWallFMM_set_far_field", 0), ("Stk3DFMM_set_precision", 0),
+                    ("StkWallFMM_set_precision", 0), ("Stk3DFMM_set_shard", 0)):
+        args = (None, arg, 1) if fn == "Stk3DFMM_set_shard" else (None, arg)
+        assert getattr(L, fn)(*args) == invalid_arg, fn
+
+
 def test_wall_create_rejects_bad_arguments():
     """StkWallFMM_create refuses a triply periodic box, kernels without a wall
     image system and invalid orders before it needs a device."""

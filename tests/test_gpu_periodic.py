@@ -212,6 +212,35 @@ def test_periodic_translation(torch_cuda):
     assert max(component_errors(b - d, a)) < TOL[10]
 
 
+@pytest.mark.parametrize("kernel,pbc", [(8, 3), (1, 2), (128, 1)])
+def test_far_field_off_sums_two_cells(torch_cuda, kernel, pbc):
+    """Far field off (the reference's enableFF = false, FMMData.cpp:83-89): no
+    far-image operator, so the periodic sum stops at the images within two cells
+    on each periodic axis, the images PVFMM's periodic lists reach (the block its
+    M2C generators leave to the tree, DIRECTLAYER = 2).  Compared with that finite
+    lattice sum, summed directly by the oracle; the values need no neutrality."""
+    import stkfmm_b200 as S
+    pts, rng = points("clustered", 1500, 70 + pbc)
+    v = rng.normal(size=(len(pts), S.get_kernel_dimension(kernel)[0]))
+    fmm = S.Stk3DFMM(10, 50, pbc, kernel, enable_ff=False)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    fmm.setup_tree(kernel)
+    out = np.zeros((len(pts), S.get_kernel_dimension(kernel)[2]))
+    fmm.evaluate_fmm(kernel, v, out, None)
+    r = range(-2, 3)
+    shifts = np.array([(a, b, c) for a in r for b in (r if pbc >= 2 else [0]) for c in (r if pbc == 3 else [0])],
+                      dtype=np.float64)
+    imgs = (pts[None] + shifts[:, None]).reshape(-1, 3)
+    ref = O.direct(S.kernel_slot(kernel, 0), imgs, np.tile(v, (len(shifts), 1)), pts)
+    errs = component_errors(out, ref)
+    assert max(errs) < TOL[10], errs
+    # switching it back on needs a new setup_tree, then gives the full periodic sum
+    fmm.set_far_field(True)
+    with pytest.raises(S.StkError):
+        fmm.evaluate_fmm(kernel, v, out, None)
+
+
 @pytest.mark.parametrize("kernel", [1, 2, 4, 8, 128, 256, 1024])
 def test_singly_periodic_against_image_sum(torch_cuda, kernel):
     """PX: sources without net charge / force, dipole or quadrupole (alternating
