@@ -112,3 +112,29 @@ def test_wall_create_rejects_bad_arguments():
     dims = np.zeros(3, dtype=np.int32)
     assert L.StkWallFMM_get_kernel_dimension(16, dims.ctypes.data_as(P_i)) == 0
     assert tuple(dims) == (4, 7, 6)
+
+
+def test_header_is_plain_c(tmp_path):
+    """A C99 caller of the reference's C ABI (STKFMM.h, Stk3DFMM-c.cpp:5-67)
+    compiles against include/stkfmm_b200.h with -pedantic, links the library and
+    runs the no-device path."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include "stkfmm_b200.h"\n#include <stdio.h>\n'
+        "int main(void) {\n"
+        "    int dims[3];\n"
+        "    int rc = Stk3DFMM_get_kernel_dimension(STK_PVel, dims);\n"
+        "    StkWallFMM *w = StkWallFMM_create(8, 64, STK_PAXIS_PXYZ, STK_Stokes);\n"
+        '    printf("%d %d %d %d %d\\n", rc, dims[0], dims[1], dims[2], w == NULL);\n'
+        "    return 0;\n}\n")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(LIB_PATH)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.dirname(HEADER),
+                    str(src), "-L", libdir, "-lstkfmm_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["0", "4", "9", "4", "1"]
