@@ -53,7 +53,7 @@ WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clust
             "U[0.1,0.9]^3), max 256 pts/leaf, p=10, SL=DL=targets")
 WORKLOAD_FMM = ("LapPGrad free-space FMM (evaluate_fmm: U/W/X near field + KIFMM far field), same points and "
                 "values, p=10, max 256 pts/leaf")
-FMM_SAMPLE = 4096  # targets of the FMM accuracy check (the reference's test subsample size)
+FMM_SAMPLE = 4096  # targets of the FMM accuracy check against the direct sum
 METRIC = "P2P pair-interactions/s (U-list S2T SL+DL; mixed path, FP64 beside it; FMM evals/s in fmm)"
 
 
