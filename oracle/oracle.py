@@ -248,6 +248,31 @@ EWALD_PVEL = 2
 EWALD_LAPLACE_HESS = 3
 
 
+def ewald_stokes_laplacian(src, f, trg):
+    """Laplacian of the triply periodic Stokeslet velocity (the unit cell's
+    Hasimoto sum of stokes_vel, 1/8pi (delta/r + r r^T/r^3), k = 0 mode dropped;
+    M2L/Stokeslet/Stokes3D3D.cpp:19-68) at trg, away from the sources: the
+    laplacian output of rpy_ulapu / stk_ulapu (RPYKernel.hpp:52-129) summed over
+    all images.  In Fourier space -k^2 G(k) = -8 pi delta + 8 pi k k^T / k^2;
+    the second part is -2 d_i d_j of the periodic 1/r, the first the periodic
+    delta minus its mean, which off the sources leaves + delta_ij per unit volume.
+    So lap u_i = -sum_j H_ij[f_j] + F_i, with H[q] the Hessian of the zero-mean
+    periodic potential of charges q (ewald kind EWALD_LAPLACE_HESS) and F the
+    net force."""
+    src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(f, dtype=np.float64).reshape(len(src), 3)
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    # Hessian entries (xx xy xz yy yz zz) at columns 4..9 of the EWALD_LAPLACE_HESS output
+    sym = [[4, 5, 6], [5, 7, 8], [6, 8, 9]]
+    out = np.zeros((len(trg), 3))
+    for j in range(3):
+        h = ewald(EWALD_LAPLACE_HESS, src, f[:, j:j + 1], trg)
+        for i in range(3):
+            out[:, i] -= h[:, sym[i][j]]
+    out += f.sum(0)
+    return out
+
+
 def pvel_pxyz_terms(src, sval, trg):
     """What the reference's triply periodic StokesPVel far field adds to the Ewald
     sum of (f, trD) sources, as (pressure, velocity) at trg (unit cell, points in

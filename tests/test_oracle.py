@@ -418,3 +418,32 @@ def test_stokes_ewald_reference_three_forces(rng):
              - _image_block(O.UK_STOKES_VEL, ue, feq, trg, 1))
     ew = O.ewald(O.EWALD_STOKES, src, f, trg)
     assert np.abs(chain - ew).max() < 1e-6 * np.abs(ew).max()
+
+
+@pytest.mark.parametrize("net_force", [True, False])
+def test_ewald_stokes_laplacian_by_finite_differences(net_force):
+    """oracle.ewald_stokes_laplacian (the periodic Laplacian term of rpy_ulapu /
+    stk_ulapu, lap u = -sum_j H[f_j] + F) against central differences of the
+    oracle's own periodic Stokeslet velocity (Richardson-extrapolated, targets at
+    least 0.08 from every source image), with and without a net force."""
+    rng = np.random.default_rng(2)
+    src = rng.random((20, 3))
+    f = rng.normal(size=(20, 3))
+    if not net_force:
+        f -= f.mean(0)
+    trg = rng.random((200, 3))
+    d = np.linalg.norm(((trg[:, None] - src[None]) + 0.5) % 1.0 - 0.5, axis=-1).min(1)
+    trg = trg[d > 0.08][:30]
+
+    def second_differences(h):
+        u0 = O.ewald(O.EWALD_STOKES, src, f, trg)
+        lap = np.zeros((len(trg), 3))
+        for a in range(3):
+            e = np.zeros(3)
+            e[a] = h
+            lap += O.ewald(O.EWALD_STOKES, src, f, trg + e) - 2 * u0 + O.ewald(O.EWALD_STOKES, src, f, trg - e)
+        return lap / (h * h)
+
+    fd = (4 * second_differences(1e-3) - second_differences(2e-3)) / 3
+    an = O.ewald_stokes_laplacian(src, f, trg)
+    assert np.abs(fd - an).max() < 2e-6 * np.abs(an).max()
