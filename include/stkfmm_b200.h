@@ -326,6 +326,11 @@ int StkWallFMM_last_launch_count(StkWallFMM *fmm, unsigned kernel, int *count);
  * PtFMM_Tree::Initialize / InitFMM_Tree / SetupFMM (FMMData.cpp:107-167).  All
  * coordinates must already lie in [0,1)^3 (scaled and wrapped).  List entries
  * are (node << 5) | shift code, as for stk_p2p_lists. */
+/* The reference's public KIFMM surface helper stkfmm::surface (host only,
+ * Lib/include/STKFMM/stkfmm_helpers.hpp:46-85): out[3 n] receives the
+ * n = 6 (p - 1)^2 + 2 check / equivalent surface points, in the reference's
+ * order, on the cube of side alpha 2^-depth with lower corner c[3]. */
+int stk_surface(int p, const double *c, double alpha, int depth, double *out);
 typedef struct stk_octree stk_octree;
 stk_octree *stk_octree_build(const double *tree_pts, int n, int max_pts, int pbc, const double *sl, int nsl,
                              const double *dl, int ndl, const double *trg, int ntrg);

@@ -110,6 +110,7 @@ def ref():
                                            _dp, ctypes.c_int, ctypes.c_int]
         _ref.ref_simple_lists.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip, _ip, _ip, _dp, _dp,
                                           ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        _ref.ref_surface.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int, _dp]
     return _ref
 
 
@@ -169,6 +170,16 @@ def surface(p: int, c, alpha: float, depth: int):
     c, pc = _d(np.asarray(c, dtype=np.float64).reshape(3))
     out = np.zeros((n, 3))
     rc = lib().oracle_surface(p, pc, alpha, depth, out.ctypes.data_as(_dp))
+    assert rc == 0
+    return out
+
+
+def ref_surface(p: int, c, alpha: float, depth: int):
+    """The reference's own stkfmm::surface (stkfmm_helpers.hpp:46-85), from oracle/_ref."""
+    n = 6 * (p - 1) ** 2 + 2
+    c, pc = _d(np.asarray(c, dtype=np.float64).reshape(3))
+    out = np.zeros((n, 3))
+    rc = ref().ref_surface(p, pc, alpha, depth, out.ctypes.data_as(_dp))
     assert rc == 0
     return out
 

@@ -6,11 +6,15 @@
 // Test/Test.cpp:478-510: a zeroed 20-slot result per pair, added into the target.
 // The shared library it builds (oracle/_ref/libstk_ref.so) generates the golden
 // fixtures under tests/golden/ and is the "reference" CPU baseline of bench.py.
+// It also exposes the reference's KIFMM surface generator (stkfmm::surface,
+// Lib/include/STKFMM/stkfmm_helpers.hpp:46-85), compiled from the reference's
+// header with oracle/stub/pvfmm.hpp standing in for PVFMM's umbrella header.
 #include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
+#include "STKFMM/stkfmm_helpers.hpp"
 #include "SimpleKernel.hpp"
 
 typedef void (*kernel_func)(double *, double *, double *, double *);
@@ -97,5 +101,14 @@ extern "C" int ref_simple_lists(int which, int n_trg_box, const int *trg_begin, 
             }
         }
     }
+    return 0;
+}
+
+// out[3 n] = stkfmm::surface(p, c, alpha, depth), n = 6 (p - 1)^2 + 2.
+extern "C" int ref_surface(int p, const double *c, double alpha, int depth, double *out) {
+    if (p < 2 || !c || !out) return 1;
+    double cc[3] = {c[0], c[1], c[2]};
+    const std::vector<double> v = stkfmm::surface<double>(p, cc, alpha, depth);
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
     return 0;
 }

@@ -1905,3 +1905,14 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
 }
 
 }  // namespace stk
+
+// The reference's public surface helper stkfmm::surface(p, c, alpha, depth)
+// (Lib/include/STKFMM/stkfmm_helpers.hpp:46-85): the same points in the same
+// order, on the cube of side alpha 2^-depth with lower corner c.  Host only.
+extern "C" int stk_surface(int p, const double *c, double alpha, int depth, double *out) {
+    if (p < 2 || !c || !out || depth < 0) return STK_ERR_INVALID_ARG;
+    const std::vector<double> u = stk::unit_surface(p);
+    const double b = alpha * std::ldexp(0.5, -depth);
+    for (size_t i = 0; i < u.size(); i++) out[i] = (u[i] + 1.0) * b + c[i % 3];
+    return STK_OK;
+}

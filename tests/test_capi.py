@@ -138,3 +138,23 @@ def test_header_is_plain_c(tmp_path):
                     str(src), "-L", libdir, "-lstkfmm_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
     assert out == ["0", "4", "9", "4", "1"]
+
+
+def test_surface_helper_matches_oracle():
+    """stk_surface (host only) gives the reference's KIFMM surface points in the
+    reference's order (pinned against the reference's own stkfmm::surface in
+    tests/test_oracle.py), and refuses invalid arguments."""
+    from oracle import oracle as O
+    from stkfmm_b200._lib import P_d
+    L = lib()
+    c = np.array([0.1, -0.3, 0.7])
+    for p in (2, 6, 10, 16):
+        for depth in (0, 2):
+            for alpha in (1.05, 2.95):
+                out = np.zeros((6 * (p - 1) ** 2 + 2, 3))
+                assert L.stk_surface(p, c.ctypes.data_as(P_d), alpha, depth, out.ctypes.data_as(P_d)) == 0
+                ref = O.ref_surface(p, c, alpha, depth) if O.ref_available() else O.surface(p, c, alpha, depth)
+                assert np.abs(out - ref).max() <= 4 * np.finfo(float).eps * np.abs(ref).max()
+    out = np.zeros((2, 3))
+    assert L.stk_surface(1, c.ctypes.data_as(P_d), 1.0, 0, out.ctypes.data_as(P_d)) == 1
+    assert L.stk_surface(2, None, 1.0, 0, out.ctypes.data_as(P_d)) == 1

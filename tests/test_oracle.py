@@ -447,3 +447,17 @@ def test_ewald_stokes_laplacian_by_finite_differences(net_force):
     fd = (4 * second_differences(1e-3) - second_differences(2e-3)) / 3
     an = O.ewald_stokes_laplacian(src, f, trg)
     assert np.abs(fd - an).max() < 2e-6 * np.abs(an).max()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+def test_surface_matches_reference():
+    """The oracle's surface generator against the reference's own stkfmm::surface
+    (stkfmm_helpers.hpp:46-85, compiled from the reference tree): the same points in
+    the same order, to an ulp or two (the C++ build may contract (u + 1) b + c into
+    an FMA)."""
+    for p in (2, 3, 6, 8, 10, 12, 16):
+        for depth in (0, 1, 3):
+            for alpha in (1.05, 2.95):
+                c = np.array([0.1, -0.3, 0.7])
+                ref = O.ref_surface(p, c, alpha, depth)
+                assert np.abs(O.surface(p, c, alpha, depth) - ref).max() <= 4 * np.finfo(float).eps * np.abs(ref).max()
