@@ -111,6 +111,8 @@ def ref():
         _ref.ref_simple_lists.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip, _ip, _ip, _dp, _dp,
                                           ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int]
         _ref.ref_surface.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int, _dp]
+        _ref.ref_ukernel_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
+        _ref.ref_kernel_composition.argtypes = [ctypes.c_uint, _ip, _ip, ctypes.c_char_p, ctypes.c_int]
     return _ref
 
 
@@ -182,6 +184,35 @@ def ref_surface(p: int, c, alpha: float, depth: int):
     rc = ref().ref_surface(p, pc, alpha, depth, out.ctypes.data_as(_dp))
     assert rc == 0
     return out
+
+
+def ref_ukernel_direct(uk: int, src, sval, trg, out=None):
+    """The reference's own micro-kernel body for id `uk` (the uKerEval of the
+    STKFMM struct, Lib/include/STKFMM/*Kernel.hpp, compiled in oracle/_ref) over
+    all (target, source) pairs: out += scale * sum_s K(trg - src) sval."""
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), UK_SDIM[uk]))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), UK_TDIM[uk]))
+    assert out.dtype == np.float64 and out.flags.c_contiguous
+    rc = ref().ref_ukernel_direct(uk, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp))
+    assert rc == 0, uk
+    return out
+
+
+def ref_kernel_composition(kernel: int):
+    """(slots, dims, name) of the reference's composite for a top-level kernel, as
+    its headers' BuildKernel calls record them: slots = micro-kernel ids of (S2T
+    SL, S2T DL, S2M SL, S2M DL, M2M = M2L = L2L, M2T, L2T, S2L SL, S2L DL), -1
+    for none; dims = (ker_dim[0], surf_dim or 0 where PVFMM's default applies,
+    ker_dim[1])."""
+    slots = np.zeros(9, dtype=np.int32)
+    dims = np.zeros(3, dtype=np.int32)
+    name = ctypes.create_string_buffer(64)
+    rc = ref().ref_kernel_composition(kernel, slots.ctypes.data_as(_ip), dims.ctypes.data_as(_ip), name, 64)
+    assert rc == 0, kernel
+    return [int(x) for x in slots], [int(x) for x in dims], name.value.decode()
 
 
 def regvel_adjoint(src, sval, trg, w, nthreads: int = 0):

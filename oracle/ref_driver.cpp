@@ -6,14 +6,22 @@
 // Test/Test.cpp:478-510: a zeroed 20-slot result per pair, added into the target.
 // The shared library it builds (oracle/_ref/libstk_ref.so) generates the golden
 // fixtures under tests/golden/ and is the "reference" CPU baseline of bench.py.
-// It also exposes the reference's KIFMM surface generator (stkfmm::surface,
-// Lib/include/STKFMM/stkfmm_helpers.hpp:46-85), compiled from the reference's
-// header with oracle/stub/pvfmm.hpp standing in for PVFMM's umbrella header.
+// It also exposes, compiled from the reference's headers with
+// oracle/stub/pvfmm.hpp standing in for PVFMM's umbrella header:
+//   * the KIFMM surface generator (stkfmm::surface, stkfmm_helpers.hpp:46-85);
+//   * every micro-kernel body STKFMM defines (the uKerEval of each struct in
+//     Lib/include/STKFMM/*Kernel.hpp), run over all pairs by the stub's driver;
+//   * the composition of each top-level kernel (which micro-kernel fills which
+//     FMM slot, as BuildKernel records it in those headers).
 #include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
+#include "STKFMM/LaplaceLayerKernel.hpp"
+#include "STKFMM/RPYKernel.hpp"
+#include "STKFMM/StokesLayerKernel.hpp"
+#include "STKFMM/StokesRegSingleLayerKernel.hpp"
 #include "STKFMM/stkfmm_helpers.hpp"
 #include "SimpleKernel.hpp"
 
@@ -110,5 +118,107 @@ extern "C" int ref_surface(int p, const double *c, double alpha, int depth, doub
     double cc[3] = {c[0], c[1], c[2]};
     const std::vector<double> v = stkfmm::surface<double>(p, cc, alpha, depth);
     std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return 0;
+}
+
+typedef pvfmm::Kernel<double>::Ker_t ker_t;
+
+// The reference's micro-kernels by this project's micro-kernel ids (the
+// numbering of include/stkfmm_b200.h).  Id 4, PVFMM's stokes_vel, is the stub's
+// (its body is not in the reference tree); 11-15 have no reference struct.
+static ker_t ukernel_fn(int uk) {
+    using namespace pvfmm;
+    switch (uk) {
+    case 0: return laplace_p::Eval<double>;
+    case 1: return laplace_pgrad::Eval<double>;
+    case 2: return laplace_dipolep::Eval<double>;
+    case 3: return laplace_dipolepgrad::Eval<double>;
+    case 4: return stokes_vel::Eval<double>;
+    case 5: return rpy_u::Eval<double>;
+    case 6: return rpy_ulapu::Eval<double>;
+    case 7: return stk_ulapu::Eval<double>;
+    case 8: return stokes_regvel::Eval<double>;
+    case 9: return stokes_pvel::Eval<double>;
+    case 10: return stokes_doublepvel::Eval<double>;
+    case 16: return laplace_pgradgrad::Eval<double>;
+    case 17: return laplace_dipolepgradgrad::Eval<double>;
+    case 18: return laplace_quadp::Eval<double>;
+    case 19: return laplace_quadpgradgrad::Eval<double>;
+    case 20: return stokes_pvelgrad::Eval<double>;
+    case 21: return stokes_doublepvelgrad::Eval<double>;
+    case 22: return stokes_pvellaplacian::Eval<double>;
+    case 23: return stokes_doublelaplacian::Eval<double>;
+    case 24: return stokes_traction::Eval<double>;
+    case 25: return stokes_doubletraction::Eval<double>;
+    case 26: return stokes_regftvel::Eval<double>;
+    case 27: return stokes_regftvelomega::Eval<double>;
+    case 28: return stokes_velomega::Eval<double>;
+    default: return nullptr;
+    }
+}
+
+static int ukernel_id(ker_t fn) {
+    if (!fn) return -1;
+    for (int uk = 0; uk < 29; uk++)
+        if (ukernel_fn(uk) == fn) return uk;
+    return -9;  // a function this driver does not know
+}
+
+// out[ntrg * tdim] += the reference micro-kernel `uk` over all (target, source)
+// pairs (ScaleFactor included).  PVFMM's stokes_vel (id 4) is refused.
+extern "C" int ref_ukernel_direct(int uk, int nsrc, const double *src, const double *val, int ntrg,
+                                  const double *trg, double *out) {
+    ker_t fn = uk == 4 ? nullptr : ukernel_fn(uk);
+    if (!fn || nsrc < 0 || ntrg < 0) return 1;
+    fn(const_cast<double *>(src), nsrc, const_cast<double *>(val), 1, const_cast<double *>(trg), ntrg, out, nullptr);
+    return 0;
+}
+
+// The reference's map from KERNEL to its composite (Lib/src/STKFMM.cpp:18-31).
+static const pvfmm::Kernel<double> *composite(unsigned id) {
+    using namespace pvfmm;
+    switch (id) {
+    case 1: return &LaplaceLayerKernel<double>::PGrad();
+    case 2: return &LaplaceLayerKernel<double>::PGradGrad();
+    case 4: return &LaplaceLayerKernel<double>::QPGradGrad();
+    case 8: return &StokesLayerKernel<double>::Vel();
+    case 16: return &RPYKernel<double>::ulapu();
+    case 32: return &StokesRegKernel<double>::Vel();
+    case 64: return &StokesRegKernel<double>::FTVelOmega();
+    case 128: return &StokesLayerKernel<double>::PVel();
+    case 256: return &StokesLayerKernel<double>::PVelGrad();
+    case 512: return &StokesLayerKernel<double>::PVelLaplacian();
+    case 1024: return &StokesLayerKernel<double>::Traction();
+    default: return nullptr;
+    }
+}
+
+// For top-level kernel `id`: slots[9] = micro-kernel ids of (S2T single layer,
+// S2T double layer, S2M single, S2M double, M2M, M2T, L2T, S2L single, S2L
+// double), -1 where the slot's kernel has no such function, -2 where M2L or
+// L2L differ from M2M; dims[3] = (ker_dim[0], surf_dim as the headers set it,
+// 0 if they leave PVFMM's default, ker_dim[1]); name = ker_name.
+extern "C" int ref_kernel_composition(unsigned id, int *slots, int *dims, char *name, int namelen) {
+    const pvfmm::Kernel<double> *k = composite(id);
+    if (!k || !slots || !dims) return 1;
+    auto self = [k](const pvfmm::Kernel<double> *sub) { return sub ? sub : k; };
+    slots[0] = ukernel_id(self(k->k_s2t)->ker_poten);
+    slots[1] = ukernel_id(self(k->k_s2t)->dbl_layer_poten);
+    slots[2] = ukernel_id(self(k->k_s2m)->ker_poten);
+    slots[3] = ukernel_id(self(k->k_s2m)->dbl_layer_poten);
+    slots[4] = ukernel_id(self(k->k_m2m)->ker_poten);
+    if (ukernel_id(self(k->k_m2l)->ker_poten) != slots[4] || ukernel_id(self(k->k_l2l)->ker_poten) != slots[4])
+        slots[4] = -2;
+    slots[5] = ukernel_id(self(k->k_m2t)->ker_poten);
+    slots[6] = ukernel_id(self(k->k_l2t)->ker_poten);
+    slots[7] = ukernel_id(self(k->k_s2l)->ker_poten);
+    slots[8] = ukernel_id(self(k->k_s2l)->dbl_layer_poten);
+    dims[0] = k->ker_dim[0];
+    dims[1] = k->surf_dim;
+    dims[2] = k->ker_dim[1];
+    if (name && namelen > 0) {
+        std::strncpy(name, k->ker_name ? k->ker_name : "", (size_t)namelen - 1);
+        name[namelen - 1] = 0;
+    }
     return 0;
 }

@@ -158,3 +158,23 @@ def test_surface_helper_matches_oracle():
     out = np.zeros((2, 3))
     assert L.stk_surface(1, c.ctypes.data_as(P_d), 1.0, 0, out.ctypes.data_as(P_d)) == 1
     assert L.stk_surface(2, None, 1.0, 0, out.ctypes.data_as(P_d)) == 1
+
+
+
+def test_kernel_tables_match_reference_compositions():
+    """The library's per-slot micro-kernels, names and dimensions against the
+    reference's own compositions: the BuildKernel calls of its kernel headers
+    (LaplaceLayerKernel.hpp, StokesLayerKernel.hpp, RPYKernel.hpp,
+    StokesRegSingleLayerKernel.hpp) compiled in oracle/_ref, for every kernel of
+    Lib/src/STKFMM.cpp:18-31.  surf_dim is compared where the headers set it."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref needs the reference tree")
+    for k in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+        slots, dims, name = O.ref_kernel_composition(k)
+        assert [S.kernel_slot(k, s) for s in range(9)] == slots, k
+        assert S.get_kernel_name(k) == name, k
+        mine = tuple(S.get_kernel_dimension(k))
+        assert (mine[0], mine[2]) == (dims[0], dims[2]), k
+        if dims[1]:
+            assert mine[1] == dims[1], k

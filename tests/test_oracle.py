@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from helpers import GOLDEN_MAP, load_golden
+from helpers import GOLDEN_MAP, load_golden, uk_values
 from oracle import oracle as O
 
 
@@ -461,3 +461,22 @@ def test_surface_matches_reference():
                 c = np.array([0.1, -0.3, 0.7])
                 ref = O.ref_surface(p, c, alpha, depth)
                 assert np.abs(O.surface(p, c, alpha, depth) - ref).max() <= 4 * np.finfo(float).eps * np.abs(ref).max()
+
+
+# Every micro-kernel body STKFMM defines itself (PVFMM's stokes_vel, id 4, is not
+# in the reference tree; ids 11-15 are this project's fused and adjoint forms).
+REF_UKERNELS = [0, 1, 2, 3, 5, 6, 7, 8, 9, 10] + list(range(16, 29))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+@pytest.mark.parametrize("uk", REF_UKERNELS)
+def test_oracle_matches_reference_ukernel(uk):
+    """The oracle's restatement against the reference's own uKerEval body of the
+    same micro-kernel (Lib/include/STKFMM/*Kernel.hpp, compiled in place through
+    oracle/stub/pvfmm.hpp), sources and targets partly coincident."""
+    rng = np.random.default_rng(100 + uk)
+    src = rng.random((150, 3))
+    trg = np.concatenate([src[:25], rng.random((75, 3))])
+    v = uk_values(rng, uk, len(src))
+    ref = O.ref_ukernel_direct(uk, src, v, trg)
+    assert rel_l2(O.direct(uk, src, v, trg), ref) < 1e-14
