@@ -100,6 +100,16 @@ def ref_available() -> bool:
     return os.path.exists(_REF)
 
 
+def ref_tree():
+    """The reference source tree oracle/_ref was built from (recorded by
+    oracle/Makefile), or None where it is absent."""
+    path = os.path.join(HERE, "_ref", "ref_tree.txt")
+    if not os.path.exists(path):
+        return None
+    tree = open(path).read().strip()
+    return tree if os.path.isdir(tree) else None
+
+
 def ref():
     global _ref
     if _ref is None:

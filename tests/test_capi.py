@@ -178,3 +178,50 @@ def test_kernel_tables_match_reference_compositions():
         assert (mine[0], mine[2]) == (dims[0], dims[2]), k
         if dims[1]:
             assert mine[1] == dims[1], k
+
+
+def test_reference_python_binding_drives_this_library():
+    """The reference's own ctypes binding (Python/PySTKFMM.py, unmodified) with its
+    library load pointed at this library, as a maintainer would repoint it: every
+    call it makes binds and runs.  It reports the reference's kernel dimensions,
+    and without a device its calls on the null handle return without writing."""
+    import importlib.util
+    import sys
+    import types
+    from oracle import oracle as O
+    tree = O.ref_tree()
+    src = os.path.join(tree, "Python", "PySTKFMM.py") if tree else None
+    if not src or not os.path.exists(src):
+        pytest.skip("the reference tree is not present")
+    real = ctypes.cdll.LoadLibrary
+    saved = sys.modules.get("mpi4py")
+    sys.modules["mpi4py"] = types.SimpleNamespace(MPI=types.SimpleNamespace())  # imported, unused by these classes
+    ctypes.cdll.LoadLibrary = lambda name: real(LIB_PATH if name == "libSTKFMM_SHARED.so" else name)
+    try:
+        spec = importlib.util.spec_from_file_location("PySTKFMM_reference", src)
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+    finally:
+        ctypes.cdll.LoadLibrary = real
+        if saved is None:
+            sys.modules.pop("mpi4py", None)
+        else:
+            sys.modules["mpi4py"] = saved
+    assert m.lib._name == LIB_PATH
+    f = m.Stk3DFMM(8, 64, m.PAXIS.NONE, m.KERNEL.Stokes | m.KERNEL.PVel)
+    for k in m.KERNEL:
+        assert tuple(f.get_kernel_dimension(k)) == tuple(S.get_kernel_dimension(int(k)))
+    w = m.StkWallFMM(8, 64, m.PAXIS.PXY, m.KERNEL.Stokes)
+    assert tuple(w.get_kernel_dimension(m.KERNEL.RPY)) == (4, 7, 6)
+    if not cuda_available():
+        assert f.fmm.value is None and w.fmm.value is None
+        pts = np.random.default_rng(0).random((10, 3))
+        out = np.zeros((10, 3))
+        f.set_box(np.zeros(3), 1.0)
+        f.set_points(pts, pts, np.zeros((0, 3)))
+        f.setup_tree(m.KERNEL.Stokes)
+        f.evaluate_fmm(m.KERNEL.Stokes, pts, out, np.zeros((0, 3)))
+        f.clear_fmm(m.KERNEL.Stokes)
+        w.set_points(pts, pts, np.zeros((0, 3)))
+        assert np.all(out == 0)
+    del f, w
