@@ -225,3 +225,43 @@ def test_reference_python_binding_drives_this_library():
         w.set_points(pts, pts, np.zeros((0, 3)))
         assert np.all(out == 0)
     del f, w
+
+
+def test_reference_c_header_links_this_library(tmp_path):
+    """A C caller compiled against the reference's own C header
+    (Lib/include/STKFMM/STKFMM.h, whose functions return void) links this library
+    and runs unchanged: the names, argument lists and calling convention match.
+    Without a device, create returns NULL and the calls on it return."""
+    import shutil
+    import subprocess
+    from oracle import oracle as O
+    tree = O.ref_tree()
+    hdir = os.path.join(tree, "Lib", "include", "STKFMM") if tree else None
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not hdir or not os.path.exists(os.path.join(hdir, "STKFMM.h")) or not cc:
+        pytest.skip("the reference tree or a C compiler is not present")
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "STKFMM.h"\n'
+        "int main(void) {\n"
+        "    double xyz[6] = {0.1, 0.2, 0.3, 0.4, 0.5, 0.6}, f[6] = {1, 0, 0, 0, 1, 0}, u[6] = {0};\n"
+        "    double origin[3] = {0, 0, 0};\n"
+        "    Stk3DFMM *fmm = Stk3DFMM_create(8, 64, 0, 8);\n"
+        "    Stk3DFMM_set_box(fmm, origin, 1.0);\n"
+        "    Stk3DFMM_set_points(fmm, 2, xyz, 2, xyz, 0, NULL);\n"
+        "    Stk3DFMM_setup_tree(fmm, 8);\n"
+        "    Stk3DFMM_evaluate_fmm(fmm, 8, 2, f, 2, u, 0, NULL);\n"
+        "    Stk3DFMM_show_active_kernels(fmm);\n"
+        "    Stk3DFMM_destroy(fmm);\n"
+        "    StkWallFMM *w = StkWallFMM_create(8, 64, 2, 8);\n"
+        "    StkWallFMM_set_box(w, origin, 1.0);\n"
+        "    StkWallFMM_destroy(w);\n"
+        '    printf("%d %d %g\\n", fmm == NULL, w == NULL, u[0]);\n'
+        "    return 0;\n}\n")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(LIB_PATH)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", hdir, str(src), "-L", libdir, "-lstkfmm_b200",
+                    "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    if not cuda_available():
+        assert out[-3:] == ["1", "1", "0"]
