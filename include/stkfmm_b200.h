@@ -21,8 +21,16 @@
  * The library fails loudly (STK_ERR_NO_DEVICE) when no CUDA device is present:
  * there is no CPU fallback.
  */
-#ifndef STKFMM_B200_H_
+/* One guard per inclusion site: stkfmm_b200.hpp also includes this header inside
+ * namespace stkfmm::capi (with STKFMM_B200_IN_NAMESPACE defined), so that its C++
+ * classes can share their names with these C handle types. */
+#if (defined(STKFMM_B200_IN_NAMESPACE) && !defined(STKFMM_B200_NS_H_)) || \
+    (!defined(STKFMM_B200_IN_NAMESPACE) && !defined(STKFMM_B200_H_))
+#ifdef STKFMM_B200_IN_NAMESPACE
+#define STKFMM_B200_NS_H_
+#else
 #define STKFMM_B200_H_
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -408,4 +416,4 @@ int stk_ker_last_status(void);
 }
 #endif
 
-#endif /* STKFMM_B200_H_ */
+#endif /* STKFMM_B200_H_ / STKFMM_B200_NS_H_ */

@@ -265,3 +265,83 @@ def test_reference_c_header_links_this_library(tmp_path):
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
     if not cuda_available():
         assert out[-3:] == ["1", "1", "0"]
+
+
+def _cxx():
+    import shutil
+    return shutil.which("g++") or shutil.which("c++")
+
+
+def _build(cxx, args, tmp_path, name):
+    import subprocess
+    libdir = os.path.dirname(LIB_PATH)
+    exe = tmp_path / name
+    subprocess.run([cxx, "-std=c++14"] + args + ["-L", libdir, "-lstkfmm_b200", "-Wl,-rpath," + libdir, "-o", str(exe)],
+                   check=True)
+    return exe
+
+
+def test_cpp_interface(tmp_path):
+    """include/stkfmm_b200.hpp mirrors the reference's C++ API (STKFMM.hpp,
+    STKFMM_common.hpp): enums, asInteger, getKernelDimension / getKernelName,
+    Stk3DFMM / StkWallFMM with the reference's constructors; a global
+    `using Stk3DFMM = stkfmm::Stk3DFMM;` (as Test/Test.hpp writes) compiles; errors
+    throw stkfmm::Error with the C status (LapGrad, outside the reference's kernel
+    map, is refused; no device gives STK_ERR_NO_DEVICE)."""
+    import subprocess
+    cxx = _cxx()
+    if not cxx:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "cpp_caller.cpp"
+    src.write_text(r'''
+#include "STKFMM/STKFMM.hpp"
+#include <cstdio>
+using Stk3DFMM = stkfmm::Stk3DFMM;
+using StkWallFMM = stkfmm::StkWallFMM;
+int main() {
+    using namespace stkfmm;
+    for (unsigned k = 1; k <= 1024; k *= 2) {
+        auto d = getKernelDimension(static_cast<KERNEL>(k));
+        std::printf("%u %d %d %d %s\n", k, std::get<0>(d), std::get<1>(d), std::get<2>(d),
+                    getKernelName(static_cast<KERNEL>(k)).c_str());
+    }
+    try { getKernelDimension(KERNEL::LapGrad); } catch (const Error &e) { std::printf("lapgrad %d\n", e.status()); }
+    try {
+        auto fmm = Stk3DFMM(8, 64, PAXIS::PXY, asInteger(KERNEL::Stokes), false);
+        std::printf("device %d\n", fmm.getMultOrder());
+    } catch (const Error &e) { std::printf("nodevice %d\n", e.status()); }
+    return 0;
+}
+''')
+    exe = _build(cxx, ["-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.dirname(HEADER), str(src)], tmp_path,
+                 "cpp_caller")
+    lines = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
+    for line in lines[:11]:
+        k, a, b, c, name = line.split()
+        assert (int(a), int(b), int(c)) == tuple(S.get_kernel_dimension(int(k))) and name == S.get_kernel_name(int(k))
+    assert lines[11] == "lapgrad 2"
+    if not cuda_available():
+        assert lines[12] == "nodevice 6"
+
+
+def test_reference_demo_builds_against_this_library(tmp_path):
+    """The reference's own Demo/Demo.cpp, unmodified, compiles against
+    include/STKFMM/STKFMM.hpp (this library's C++ interface) and links
+    libstkfmm_b200.so; MPI_Init / MPI_Finalize come from a two-line stand-in, as
+    this library needs no MPI.  Without a device it stops with the library's
+    no-device error."""
+    import subprocess
+    from oracle import oracle as O
+    tree = O.ref_tree()
+    demo = os.path.join(tree, "Demo", "Demo.cpp") if tree else None
+    cxx = _cxx()
+    if not demo or not os.path.exists(demo) or not cxx:
+        pytest.skip("the reference tree or a C++ compiler is not present")
+    stub = tmp_path / "mpistub"
+    stub.mkdir()
+    (stub / "mpi.h").write_text("#pragma once\ninline int MPI_Init(int *, char ***) { return 0; }\n"
+                                "inline int MPI_Finalize() { return 0; }\n")
+    exe = _build(cxx, ["-fopenmp", "-I", os.path.dirname(HEADER), "-I", str(stub), demo], tmp_path, "demo")
+    if not cuda_available():
+        r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+        assert r.returncode != 0 and "no CUDA device" in r.stderr
