@@ -28,6 +28,7 @@
 #include <string>
 #include <tuple>
 #include <type_traits>
+#include <unordered_map>
 #include <utility>
 
 /* The C ABI, declared inside stkfmm::capi so that no global Stk3DFMM or
@@ -102,6 +103,41 @@ inline std::string getKernelName(KERNEL kernel) {
     if (!name) throw Error(capi::STK_ERR_KERNEL, "getKernelName");
     return name;
 }
+
+/* What kernelMap maps to: the fields of pvfmm::Kernel<double> that callers
+ * of the reference read (ker_name, ker_dim, surf_dim). */
+struct KernelDescriptor {
+    std::string ker_name;
+    int ker_dim[2];
+    int surf_dim;
+};
+
+namespace detail {
+inline const std::unordered_map<KERNEL, const KernelDescriptor *> &kernel_map() {
+    static const KERNEL all[11] = {KERNEL::LapPGrad,     KERNEL::LapPGradGrad,      KERNEL::LapQPGradGrad,
+                                   KERNEL::Stokes,       KERNEL::RPY,               KERNEL::StokesRegVel,
+                                   KERNEL::StokesRegVelOmega, KERNEL::PVel,         KERNEL::PVelGrad,
+                                   KERNEL::PVelLaplacian, KERNEL::Traction};
+    static KernelDescriptor desc[11];
+    static const std::unordered_map<KERNEL, const KernelDescriptor *> map = [] {
+        std::unordered_map<KERNEL, const KernelDescriptor *> m;
+        for (int i = 0; i < 11; i++) {
+            int d[3] = {0, 0, 0};
+            check(capi::stk_get_kernel_dimension(asInteger(all[i]), d), "kernelMap");
+            desc[i].ker_name = getKernelName(all[i]);
+            desc[i].ker_dim[0] = d[0];
+            desc[i].ker_dim[1] = d[2];
+            desc[i].surf_dim = d[1];
+            m[all[i]] = &desc[i];
+        }
+        return m;
+    }();
+    return map;
+}
+}  // namespace detail
+
+/* every kernel of the reference's map (STKFMM.cpp:18-31), iterable as there */
+static const std::unordered_map<KERNEL, const KernelDescriptor *> &kernelMap = detail::kernel_map();
 
 /* The common part of both FMMs (STKFMM.hpp:30-177). */
 class STKFMM {

@@ -345,3 +345,23 @@ def test_reference_demo_builds_against_this_library(tmp_path):
     if not cuda_available():
         r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
         assert r.returncode != 0 and "no CUDA device" in r.stderr
+
+
+def test_reference_test_driver_built_on_this_library(tmp_path):
+    """oracle/_ref/stkfmm_test_driver is the reference's own test driver
+    (Test/Test.cpp, main.cpp, SimpleKernel.cpp, Util/PointDistribution.cpp)
+    compiled against this library's C++ interface and a single-rank MPI stand-in
+    (oracle/Makefile, target ref-driver).  It parses the reference's options, and
+    without a device stops at the first FMM with the library's no-device error."""
+    import subprocess
+    drv = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "stkfmm_test_driver")
+    if not os.path.exists(drv):
+        pytest.skip("oracle/_ref/stkfmm_test_driver is built only where the reference tree is present")
+    h = subprocess.run([drv, "--help"], capture_output=True, text=True, timeout=60)  # exits 1, as the reference's does
+    assert "--verify" in h.stdout and "--wall" in h.stdout
+    if not cuda_available():
+        # -T is the driver's mesh parameter, not a point count: keep it small
+        r = subprocess.run([drv, "-S", "1", "-T", "20", "-K", "1", "-M", "8"], capture_output=True, text=True,
+                           timeout=120, cwd=str(tmp_path))
+        assert r.returncode != 0 and "no CUDA device" in r.stderr
