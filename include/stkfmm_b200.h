@@ -124,6 +124,11 @@ const char *stk_status_string(int status);
 int stk_get_kernel_dimension(unsigned kernel, int *dims);
 /* PVFMM kernel name of the S2T kernel (getKernelName, Lib/src/STKFMM.cpp:42-47) */
 const char *stk_get_kernel_name(unsigned kernel);
+/* Box scaling of a kernel (host only): the factors by which the single-layer
+ * values sl[kdimSL], the double-layer values dl[kdimDL] and the results
+ * trg[kdimTrg] are multiplied around the unit-box FMM for a box with scale
+ * factor sf = 1 / length (FMMData::scaleSrc / scaleTrg, FMMData.cpp:285-470). */
+int stk_kernel_scaling(unsigned kernel, double sf, double *sl, double *dl, double *trg);
 /* micro-kernel that fills a PVFMM slot of a kernel: slot 0 s2t SL, 1 s2t DL,
  * 2 s2m SL, 3 s2m DL, 4 m2m/m2l/l2l, 5 m2t, 6 l2t, 7 s2l SL, 8 s2l DL;
  * -1 when the slot is empty.  Mirrors the BuildKernel compositions, e.g.

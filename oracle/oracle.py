@@ -123,6 +123,7 @@ def ref():
         _ref.ref_surface.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int, _dp]
         _ref.ref_ukernel_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
         _ref.ref_kernel_composition.argtypes = [ctypes.c_uint, _ip, _ip, ctypes.c_char_p, ctypes.c_int]
+        _ref.ref_kernel_scaling.argtypes = [ctypes.c_uint, ctypes.c_double, _dp, _dp, _dp, _ip]
     return _ref
 
 
@@ -223,6 +224,18 @@ def ref_kernel_composition(kernel: int):
     rc = ref().ref_kernel_composition(kernel, slots.ctypes.data_as(_ip), dims.ctypes.data_as(_ip), name, 64)
     assert rc == 0, kernel
     return [int(x) for x in slots], [int(x) for x in dims], name.value.decode()
+
+
+def ref_kernel_scaling(kernel: int, sf: float):
+    """(sl, dl, trg) factors the reference's own FMMData applies around the FMM
+    for a box with scale factor sf (scaleSrc / scaleTrg, Lib/src/FMMData.cpp:285-470,
+    compiled in oracle/_ref); dl is empty for kernels without a double layer."""
+    sl, dl, trg = np.zeros(16), np.zeros(16), np.zeros(16)
+    dims = np.zeros(3, dtype=np.int32)
+    rc = ref().ref_kernel_scaling(kernel, sf, sl.ctypes.data_as(_dp), dl.ctypes.data_as(_dp), trg.ctypes.data_as(_dp),
+                                  dims.ctypes.data_as(_ip))
+    assert rc == 0, kernel
+    return sl[:dims[0]].copy(), dl[:dims[1]].copy(), trg[:dims[2]].copy()
 
 
 def regvel_adjoint(src, sval, trg, w, nthreads: int = 0):

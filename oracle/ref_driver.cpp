@@ -12,12 +12,15 @@
 //   * every micro-kernel body STKFMM defines (the uKerEval of each struct in
 //     Lib/include/STKFMM/*Kernel.hpp), run over all pairs by the stub's driver;
 //   * the composition of each top-level kernel (which micro-kernel fills which
-//     FMM slot, as BuildKernel records it in those headers).
+//     FMM slot, as BuildKernel records it in those headers);
+//   * the reference's FMMData (Lib/src/FMMData.cpp, with STKFMM.cpp for its
+//     kernel map) around a stub FMM, to read off its source and target scaling.
 #include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
+#include "STKFMM/STKFMM_impl.hpp"
 #include "STKFMM/LaplaceLayerKernel.hpp"
 #include "STKFMM/RPYKernel.hpp"
 #include "STKFMM/StokesLayerKernel.hpp"
@@ -220,5 +223,30 @@ extern "C" int ref_kernel_composition(unsigned id, int *slots, int *dims, char *
         std::strncpy(name, k->ker_name ? k->ker_name : "", (size_t)namelen - 1);
         name[namelen - 1] = 0;
     }
+    return 0;
+}
+
+// The factors the reference's FMMData applies around the FMM for a box with
+// scale factor sf (FMMData::scaleSrc / scaleTrg, Lib/src/FMMData.cpp:285-470),
+// seen through its public evaluateFMM on one point per set: the source values
+// (ones) are scaled in place before the stub FMM, which sets every target value
+// to 1, so the targets come back as the target factors.  Free space.
+// sl[kdimSL], dl[kdimDL] (empty without a double layer), trg[kdimTrg];
+// dims = (kdimSL, kdimDL or 0, kdimTrg).
+extern "C" int ref_kernel_scaling(unsigned id, double sf, double *sl, double *dl, double *trg, int *dims) {
+    using namespace stkfmm;
+    if (!composite(id) || !sl || !dl || !trg || !dims) return 1;
+    impl::FMMData fmm(static_cast<KERNEL>(id), PAXIS::NONE, 6, 50, true);
+    const std::vector<double> pt = {0.5, 0.5, 0.5}, none;
+    const bool has_dl = fmm.hasDL();
+    fmm.setupTree(pt, has_dl ? pt : none, pt);
+    std::vector<double> slv(fmm.kdimSL, 1.0), dlv(has_dl ? fmm.kdimDL : 0, 1.0), tv(fmm.kdimTrg, 0.0);
+    fmm.evaluateFMM(slv, dlv, tv, sf);
+    std::copy(slv.begin(), slv.end(), sl);
+    std::copy(dlv.begin(), dlv.end(), dl);
+    std::copy(tv.begin(), tv.end(), trg);
+    dims[0] = fmm.kdimSL;
+    dims[1] = has_dl ? fmm.kdimDL : 0;
+    dims[2] = fmm.kdimTrg;
     return 0;
 }

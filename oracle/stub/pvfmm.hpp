@@ -21,11 +21,39 @@
 //   * stokes_vel / StokesKernel<T>::velocity(): PVFMM's Stokeslet, declared so
 //     that compositions naming it compile and can be recorded; its body is not
 //     the reference's (the Stokeslet formula, 1/8pi (f/r + r (f.r)/r^3)).
+//   * PtFMM, PtFMM_Tree, PtFMM_Data, Vector, BoundaryType and PtFMM_Evaluate:
+//     enough for Lib/src/FMMData.cpp and STKFMM.cpp to compile and for an
+//     FMMData to run its own steps around the FMM.  PtFMM::Initialize does
+//     what PVFMM's kernel initialisation does for the slots (a null sub-kernel
+//     becomes the kernel itself); PtFMM_Evaluate computes nothing: it sets every
+//     target value to 1, so that what FMMData applies after it (scaleTrg) shows.
 #pragma once
+#include <mpi.h>
+
+#include <algorithm>
+#include <cassert>
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef PVFMM_MAX_DEPTH
+#define PVFMM_MAX_DEPTH 30
+#endif
+// KIFMM surface radii (in box half-widths) of PVFMM, the scaleIn / scaleOut of
+// the reference's M2C generators
+#define PVFMM_RAD0 1.05
+#define PVFMM_RAD1 2.95
 
 namespace sctl {
 
@@ -165,6 +193,70 @@ struct stokes_vel : public GenericKernel<stokes_vel> {
         for (int i = 0; i < 3; i++) u[i] += f[i] * rinv + r[i] * fr;
     }
 };
+
+template <class T>
+struct Vector {
+    std::vector<T> v;
+    Vector &operator=(const std::vector<T> &o) {
+        v = o;
+        return *this;
+    }
+    size_t Dim() const { return v.size(); }
+    void Resize(size_t n) { v.resize(n); }
+    void ReInit(size_t n) { v.assign(n, T(0)); }
+    T *Begin() { return v.data(); }
+    T &operator[](size_t i) { return v[i]; }
+    const T &operator[](size_t i) const { return v[i]; }
+};
+
+enum class BoundaryType { FreeSpace, PX, PXY, PXYZ };
+
+template <class T>
+struct PtFMM {
+    void Initialize(int, MPI_Comm, const Kernel<T> *k) {
+        Kernel<T> *kk = const_cast<Kernel<T> *>(k);
+        const Kernel<T> **slots[] = {&kk->k_s2m, &kk->k_s2l, &kk->k_s2t, &kk->k_m2m,
+                                     &kk->k_m2l, &kk->k_m2t, &kk->k_l2l, &kk->k_l2t};
+        for (auto s : slots)
+            if (!*s) *s = k;
+    }
+    void SetM2C(const double *) {}
+};
+
+template <class T>
+struct PtFMM_Data {
+    int dim = 3, max_depth = 0, max_pts = 0;
+    Vector<T> pt_coord, src_coord, src_value, surf_coord, surf_value, trg_coord, trg_value;
+    void Clear() {}
+};
+
+template <class T>
+struct PtFMM_Node_Data {
+    Vector<T> upward_equiv;
+};
+
+template <class T>
+struct PtFMM_Node {
+    PtFMM_Node_Data<T> data;
+    PtFMM_Node_Data<T> *FMMData() { return &data; }
+};
+
+template <class T>
+struct PtFMM_Tree {
+    PtFMM_Node<T> root;
+    explicit PtFMM_Tree(MPI_Comm) {}
+    void Initialize(PtFMM_Data<T> *) {}
+    void InitFMM_Tree(bool, BoundaryType) {}
+    void SetupFMM(PtFMM<T> *) {}
+    void ClearFMMData() {}
+    PtFMM_Node<T> *RootNode() { return &root; }
+};
+
+template <class T>
+inline void PtFMM_Evaluate(PtFMM_Tree<T> *, std::vector<T> &trg_val, size_t, std::vector<T> * = nullptr,
+                           std::vector<T> * = nullptr) {
+    std::fill(trg_val.begin(), trg_val.end(), T(1));
+}
 
 template <class T>
 struct StokesKernel {

@@ -58,6 +58,7 @@ SIGNATURES = [
     ("Stk3DFMM_evaluate_kernel", c_int, [c_void_p, c_uint, c_int, c_uint, c_int, P_d, P_d, c_int, P_d, P_d]),
     ("Stk3DFMM_set_precision", c_int, [c_void_p, c_int]),
     ("Stk3DFMM_set_shard", c_int, [c_void_p, c_int, c_int]),
+    ("stk_kernel_scaling", c_int, [c_uint, c_double, P_d, P_d, P_d]),
     ("stk_surface", c_int, [c_int, P_d, c_double, c_int, P_d]),
     ("Stk3DFMM_set_far_field", c_int, [c_void_p, c_int]),
     ("stk_partition_lpt", c_int, [c_int, P_d, c_int, P_i]),

@@ -66,6 +66,21 @@ extern "C" int stk_get_kernel_dimension(unsigned kernel, int *dims) {
     return STK_OK;
 }
 
+// The factors applied around the unit-box FMM for a box with scale factor sf,
+// read from the same table fields the evaluation uses (scaleSrc / scaleTrg of
+// Lib/src/FMMData.cpp:285-470): the trailing sl_last_scales single-layer
+// components, every double-layer value, and each target component to the power
+// trg_scale_pow.  Host only.
+extern "C" int stk_kernel_scaling(unsigned kernel, double sf, double *sl, double *dl, double *trg) {
+    const KernelInfo *k = find_kernel(kernel);
+    if (!k) return STK_ERR_KERNEL;
+    if (!sl || !dl || !trg) return STK_ERR_INVALID_ARG;
+    for (int c = 0; c < k->kdim_sl; c++) sl[c] = c >= k->kdim_sl - k->sl_last_scales ? sf : 1.0;
+    for (int c = 0; c < k->kdim_dl; c++) dl[c] = sf;
+    for (int c = 0; c < k->kdim_trg; c++) trg[c] = std::pow(sf, k->trg_scale_pow[c]);
+    return STK_OK;
+}
+
 extern "C" const char *stk_get_kernel_name(unsigned kernel) {
     const KernelInfo *k = find_kernel(kernel);
     return k ? k->name : nullptr;

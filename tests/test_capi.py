@@ -365,3 +365,24 @@ def test_reference_test_driver_built_on_this_library(tmp_path):
         r = subprocess.run([drv, "-S", "1", "-T", "20", "-K", "1", "-M", "8"], capture_output=True, text=True,
                            timeout=120, cwd=str(tmp_path))
         assert r.returncode != 0 and "no CUDA device" in r.stderr
+
+
+def test_box_scaling_matches_reference_fmmdata():
+    """The library's box scaling (stk_kernel_scaling: the factors its evaluation
+    applies to single-layer, double-layer and target values) against the
+    reference's own FMMData::scaleSrc / scaleTrg (Lib/src/FMMData.cpp:285-470),
+    compiled in oracle/_ref and run around a stub FMM, for every kernel."""
+    from oracle import oracle as O
+    from stkfmm_b200._lib import P_d
+    if not O.ref_available():
+        pytest.skip("oracle/_ref needs the reference tree")
+    L = lib()
+    for k in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+        for sf in (0.5, 1.0 / 3.0):
+            rsl, rdl, rtrg = O.ref_kernel_scaling(k, sf)
+            sl, dl, trg = np.zeros(16), np.zeros(16), np.zeros(16)
+            assert L.stk_kernel_scaling(k, sf, sl.ctypes.data_as(P_d), dl.ctypes.data_as(P_d),
+                                        trg.ctypes.data_as(P_d)) == 0
+            assert np.array_equal(sl[:len(rsl)], rsl), (k, sl, rsl)
+            assert np.array_equal(dl[:len(rdl)], rdl), (k, dl, rdl)
+            assert np.allclose(trg[:len(rtrg)], rtrg, rtol=1e-15, atol=0), (k, trg, rtrg)
