@@ -124,6 +124,8 @@ def ref():
         _ref.ref_ukernel_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
         _ref.ref_kernel_composition.argtypes = [ctypes.c_uint, _ip, _ip, ctypes.c_char_p, ctypes.c_int]
         _ref.ref_kernel_scaling.argtypes = [ctypes.c_uint, ctypes.c_double, _dp, _dp, _dp, _ip]
+        _ref.ref_evaluate_kernel.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
+                                             _dp]
     return _ref
 
 
@@ -224,6 +226,19 @@ def ref_kernel_composition(kernel: int):
     rc = ref().ref_kernel_composition(kernel, slots.ctypes.data_as(_ip), dims.ctypes.data_as(_ip), name, 64)
     assert rc == 0, kernel
     return [int(x) for x in slots], [int(x) for x in dims], name.value.decode()
+
+
+def ref_evaluate_kernel(kernel: int, p2p: int, src, sval, trg, tdim: int):
+    """The reference's own FMMData::evaluateKernel (Lib/src/FMMData.cpp:252-283,
+    compiled in oracle/_ref): (ntrg, tdim) += the sub-kernel p2p selects over all
+    pairs (1 SLS2T, 2 DLS2T, 4 L2T); zeros where the kernel has no such sub-kernel."""
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), -1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    out = np.zeros((len(trg), tdim))
+    rc = ref().ref_evaluate_kernel(kernel, p2p, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp))
+    assert rc == 0, kernel
+    return out
 
 
 def ref_kernel_scaling(kernel: int, sf: float):

@@ -250,3 +250,16 @@ extern "C" int ref_kernel_scaling(unsigned id, double sf, double *sl, double *dl
     dims[2] = fmm.kdimTrg;
     return 0;
 }
+
+// The reference's own direct sum (FMMData::evaluateKernel, Lib/src/FMMData.cpp:252-283):
+// out[ntrg * kdimTrg] += the sub-kernel that p2p (PPKERNEL: 1 SLS2T, 2 DLS2T,
+// 4 L2T) selects, over all pairs; out is untouched where the kernel has none.
+extern "C" int ref_evaluate_kernel(unsigned id, unsigned p2p, int nsrc, const double *src, const double *val,
+                                   int ntrg, const double *trg, double *out) {
+    using namespace stkfmm;
+    if (!composite(id) || nsrc < 0 || ntrg < 0) return 1;
+    impl::FMMData fmm(static_cast<KERNEL>(id), PAXIS::NONE, 6, 50, true);
+    fmm.evaluateKernel(1, static_cast<PPKERNEL>(p2p), nsrc, const_cast<double *>(src), const_cast<double *>(val),
+                       ntrg, const_cast<double *>(trg), out);
+    return 0;
+}

@@ -480,3 +480,27 @@ def test_oracle_matches_reference_ukernel(uk):
     v = uk_values(rng, uk, len(src))
     ref = O.ref_ukernel_direct(uk, src, v, trg)
     assert rel_l2(O.direct(uk, src, v, trg), ref) < 1e-14
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
+def test_evaluate_kernel_selection_matches_reference(kernel):
+    """The reference's own FMMData::evaluateKernel (its PPKERNEL -> sub-kernel
+    choice, FMMData.cpp:261-268, run over 4000-target chunks) against the oracle
+    micro-kernel that the library's slot table gives for SLS2T, DLS2T and L2T
+    (the table stk_evaluate_kernel uses).  A missing sub-kernel leaves the
+    reference's output untouched (it returns after a message)."""
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(kernel)
+    src = rng.random((300, 3))
+    trg = np.concatenate([src[:40], rng.random((4100, 3))])  # two 4000-target chunks
+    tdim = S.get_kernel_dimension(kernel)[2]
+    for p2p, slot in ((1, 0), (2, 1), (4, 6)):
+        uk = S.kernel_slot(kernel, slot)
+        if uk < 0:
+            v = rng.uniform(-1, 1, (len(src), 3))
+            assert not O.ref_evaluate_kernel(kernel, p2p, src, v, trg, tdim).any()
+            continue
+        v = uk_values(rng, uk, len(src))
+        ref = O.ref_evaluate_kernel(kernel, p2p, src, v, trg, tdim)
+        assert rel_l2(O.direct(uk, src, v, trg), ref) < 1e-14, (kernel, p2p, O.UK_NAMES[uk])
