@@ -126,6 +126,10 @@ def ref():
         _ref.ref_kernel_scaling.argtypes = [ctypes.c_uint, ctypes.c_double, _dp, _dp, _dp, _ip]
         _ref.ref_evaluate_kernel.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
                                              _dp]
+        _ref.ref_wall_direct.argtypes = [ctypes.c_uint, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
+                                         _dp]
+        _ref.ref_stk3d_direct.argtypes = [ctypes.c_uint, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                                          _dp, _dp, ctypes.c_int, _dp, _dp]
     return _ref
 
 
@@ -237,6 +241,37 @@ def ref_evaluate_kernel(kernel: int, p2p: int, src, sval, trg, tdim: int):
     trg, pt = _d(np.asarray(trg).reshape(-1, 3))
     out = np.zeros((len(trg), tdim))
     rc = ref().ref_evaluate_kernel(kernel, p2p, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp))
+    assert rc == 0, kernel
+    return out
+
+
+def ref_wall_direct(kernel: int, src, val, trg, origin=(0.0, 0.0, 0.0), box: float = 1.0):
+    """The reference's own StkWallFMM (Lib/src/StkWallFMM.cpp), its FMMs replaced
+    by exact direct sums: the wall image system as the reference composes it."""
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    val, pv = _d(np.asarray(val).reshape(len(src), -1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    o, po = _d(np.asarray(origin, dtype=np.float64).reshape(3))
+    out = np.zeros((len(trg), 3 if kernel == 8 else 6))
+    rc = ref().ref_wall_direct(kernel, po, box, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp))
+    assert rc == 0, kernel
+    return out
+
+
+def ref_stk3d_direct(kernel: int, sl, slv, trg, tdim: int, dl=None, dlv=None, origin=(0.0, 0.0, 0.0),
+                     box: float = 1.0):
+    """The reference's own Stk3DFMM (Lib/src/Stk3DFMM.cpp: box scaling, scaleSrc /
+    scaleTrg) in free space, its FMM replaced by the exact direct sum."""
+    sl, psl = _d(np.asarray(sl).reshape(-1, 3))
+    slv, pslv = _d(np.asarray(slv).reshape(len(sl), -1))
+    ndl = 0 if dl is None else len(dl)
+    dl, pdl = _d(np.zeros((1, 3)) if dl is None else np.asarray(dl).reshape(-1, 3))
+    dlv, pdlv = _d(np.zeros((1, 1)) if dlv is None else np.asarray(dlv).reshape(ndl, -1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    o, po = _d(np.asarray(origin, dtype=np.float64).reshape(3))
+    out = np.zeros((len(trg), tdim))
+    rc = ref().ref_stk3d_direct(kernel, po, box, len(sl), psl, pslv, ndl, pdl, pdlv, len(trg), pt,
+                                out.ctypes.data_as(_dp))
     assert rc == 0, kernel
     return out
 

@@ -14,12 +14,16 @@
 //   * the composition of each top-level kernel (which micro-kernel fills which
 //     FMM slot, as BuildKernel records it in those headers);
 //   * the reference's FMMData (Lib/src/FMMData.cpp, with STKFMM.cpp for its
-//     kernel map) around a stub FMM, to read off its source and target scaling.
+//     kernel map) around a stub FMM, to read off its source and target scaling;
+//   * the reference's Stk3DFMM and StkWallFMM (Stk3DFMM.cpp, StkWallFMM.cpp)
+//     over the stand-in FMM in its direct-sum mode: their box scaling, image
+//     systems and assembly run as the reference wrote them, exactly.
 #include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
+#include "STKFMM/STKFMM.hpp"
 #include "STKFMM/STKFMM_impl.hpp"
 #include "STKFMM/LaplaceLayerKernel.hpp"
 #include "STKFMM/RPYKernel.hpp"
@@ -125,6 +129,10 @@ extern "C" int ref_surface(int p, const double *c, double alpha, int depth, doub
 }
 
 typedef pvfmm::Kernel<double>::Ker_t ker_t;
+
+namespace pvfmm {
+int stub_fmm_direct = 0;  // the stand-in FMM's mode (oracle/stub/pvfmm.hpp)
+}
 
 // The reference's micro-kernels by this project's micro-kernel ids (the
 // numbering of include/stkfmm_b200.h).  Id 4, PVFMM's stokes_vel, is the stub's
@@ -236,6 +244,7 @@ extern "C" int ref_kernel_composition(unsigned id, int *slots, int *dims, char *
 extern "C" int ref_kernel_scaling(unsigned id, double sf, double *sl, double *dl, double *trg, int *dims) {
     using namespace stkfmm;
     if (!composite(id) || !sl || !dl || !trg || !dims) return 1;
+    pvfmm::stub_fmm_direct = 0;
     impl::FMMData fmm(static_cast<KERNEL>(id), PAXIS::NONE, 6, 50, true);
     const std::vector<double> pt = {0.5, 0.5, 0.5}, none;
     const bool has_dl = fmm.hasDL();
@@ -261,5 +270,47 @@ extern "C" int ref_evaluate_kernel(unsigned id, unsigned p2p, int nsrc, const do
     impl::FMMData fmm(static_cast<KERNEL>(id), PAXIS::NONE, 6, 50, true);
     fmm.evaluateKernel(1, static_cast<PPKERNEL>(p2p), nsrc, const_cast<double *>(src), const_cast<double *>(val),
                        ntrg, const_cast<double *>(trg), out);
+    return 0;
+}
+
+// The reference's own StkWallFMM (Lib/src/StkWallFMM.cpp: mirror images, the
+// sub-FMMs' source values and the assembly of evalStokes / evalRPY) over the
+// stand-in FMM in direct mode: the wall's exact image system in free space.
+// kernel 8 (Stokes, f -> u) or 16 (RPY, (f, b) -> (u, lap u)); out += result.
+extern "C" int ref_wall_direct(unsigned kernel, const double *origin, double len, int nsrc, const double *src,
+                               const double *val, int ntrg, const double *trg, double *out) {
+    using namespace stkfmm;
+    if ((kernel != 8 && kernel != 16) || nsrc < 1 || ntrg < 1) return 1;
+    pvfmm::stub_fmm_direct = 1;
+    {
+        StkWallFMM wall(6, 50, PAXIS::NONE, kernel, true);
+        double o[3] = {origin[0], origin[1], origin[2]};
+        wall.setBox(o, len);
+        wall.setPoints(nsrc, src, ntrg, trg);
+        wall.setupTree(static_cast<KERNEL>(kernel));
+        wall.evaluateFMM(static_cast<KERNEL>(kernel), nsrc, val, ntrg, out);
+    }
+    pvfmm::stub_fmm_direct = 0;
+    return 0;
+}
+
+// The reference's own Stk3DFMM (Lib/src/Stk3DFMM.cpp, STKFMM.cpp: box scaling,
+// wrapping, scaleSrc / scaleTrg) over the stand-in FMM in direct mode, free
+// space: out += the kernel's single- and double-layer sums in the caller's box.
+extern "C" int ref_stk3d_direct(unsigned kernel, const double *origin, double len, int nsl, const double *sl,
+                                const double *slv, int ndl, const double *dl, const double *dlv, int ntrg,
+                                const double *trg, double *out) {
+    using namespace stkfmm;
+    if (!composite(kernel) || nsl < 1 || ntrg < 1) return 1;
+    pvfmm::stub_fmm_direct = 1;
+    {
+        Stk3DFMM fmm(6, 50, PAXIS::NONE, kernel, true);
+        double o[3] = {origin[0], origin[1], origin[2]};
+        fmm.setBox(o, len);
+        fmm.setPoints(nsl, sl, ntrg, trg, ndl, ndl > 0 ? dl : nullptr);
+        fmm.setupTree(static_cast<KERNEL>(kernel));
+        fmm.evaluateFMM(static_cast<KERNEL>(kernel), nsl, slv, ntrg, out, ndl, ndl > 0 ? dlv : nullptr);
+    }
+    pvfmm::stub_fmm_direct = 0;
     return 0;
 }

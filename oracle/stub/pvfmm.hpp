@@ -25,8 +25,12 @@
 //     enough for Lib/src/FMMData.cpp and STKFMM.cpp to compile and for an
 //     FMMData to run its own steps around the FMM.  PtFMM::Initialize does
 //     what PVFMM's kernel initialisation does for the slots (a null sub-kernel
-//     becomes the kernel itself); PtFMM_Evaluate computes nothing: it sets every
-//     target value to 1, so that what FMMData applies after it (scaleTrg) shows.
+//     becomes the kernel itself).  PtFMM_Evaluate has two modes, chosen by
+//     stub_fmm_direct (defined by the program that uses this file): 0 sets every
+//     target value to 1, so that what FMMData applies after it (scaleTrg)
+//     shows; 1 returns what the FMM approximates, the direct sum of the kernel's
+//     S2T single and double layer over all sources, so that the reference's own
+//     FMMData, Stk3DFMM and StkWallFMM code around it runs as an exact method.
 #pragma once
 #include <mpi.h>
 
@@ -211,9 +215,13 @@ struct Vector {
 
 enum class BoundaryType { FreeSpace, PX, PXY, PXYZ };
 
+extern int stub_fmm_direct;
+
 template <class T>
 struct PtFMM {
+    const Kernel<T> *ker = nullptr;
     void Initialize(int, MPI_Comm, const Kernel<T> *k) {
+        ker = k;
         Kernel<T> *kk = const_cast<Kernel<T> *>(k);
         const Kernel<T> **slots[] = {&kk->k_s2m, &kk->k_s2l, &kk->k_s2t, &kk->k_m2m,
                                      &kk->k_m2l, &kk->k_m2t, &kk->k_l2l, &kk->k_l2t};
@@ -244,18 +252,34 @@ struct PtFMM_Node {
 template <class T>
 struct PtFMM_Tree {
     PtFMM_Node<T> root;
+    PtFMM_Data<T> *data = nullptr;
+    PtFMM<T> *fmm = nullptr;
     explicit PtFMM_Tree(MPI_Comm) {}
-    void Initialize(PtFMM_Data<T> *) {}
+    void Initialize(PtFMM_Data<T> *d) { data = d; }
     void InitFMM_Tree(bool, BoundaryType) {}
-    void SetupFMM(PtFMM<T> *) {}
+    void SetupFMM(PtFMM<T> *m) { fmm = m; }
     void ClearFMMData() {}
     PtFMM_Node<T> *RootNode() { return &root; }
 };
 
 template <class T>
-inline void PtFMM_Evaluate(PtFMM_Tree<T> *, std::vector<T> &trg_val, size_t, std::vector<T> * = nullptr,
-                           std::vector<T> * = nullptr) {
-    std::fill(trg_val.begin(), trg_val.end(), T(1));
+inline void PtFMM_Evaluate(PtFMM_Tree<T> *tree, std::vector<T> &trg_val, size_t, std::vector<T> *src_val = nullptr,
+                           std::vector<T> *surf_val = nullptr) {
+    if (!stub_fmm_direct) {
+        std::fill(trg_val.begin(), trg_val.end(), T(1));
+        return;
+    }
+    std::fill(trg_val.begin(), trg_val.end(), T(0));
+    const Kernel<T> *s2t = tree->fmm->ker->k_s2t;
+    PtFMM_Data<T> &d = *tree->data;
+    const int ntrg = (int)(d.trg_coord.Dim() / 3), nsrc = (int)(d.src_coord.Dim() / 3),
+              nsurf = (int)(d.surf_coord.Dim() / 3);
+    if (src_val && nsrc && s2t->ker_poten)
+        s2t->ker_poten(d.src_coord.Begin(), nsrc, src_val->data(), 1, d.trg_coord.Begin(), ntrg, trg_val.data(),
+                       nullptr);
+    if (surf_val && nsurf && s2t->dbl_layer_poten)
+        s2t->dbl_layer_poten(d.surf_coord.Begin(), nsurf, surf_val->data(), 1, d.trg_coord.Begin(), ntrg,
+                             trg_val.data(), nullptr);
 }
 
 template <class T>

@@ -504,3 +504,59 @@ def test_evaluate_kernel_selection_matches_reference(kernel):
         v = uk_values(rng, uk, len(src))
         ref = O.ref_evaluate_kernel(kernel, p2p, src, v, trg, tdim)
         assert rel_l2(O.direct(uk, src, v, trg), ref) < 1e-14, (kernel, p2p, O.UK_NAMES[uk])
+
+
+def _wall_points(rng, n, box=1.0, origin=(0.0, 0.0, 0.0)):
+    from helpers import clustered_points
+    p = np.minimum(clustered_points(rng, n, nclusters=5, sigma=0.05), 0.999)
+    p[:, 2] = 0.01 + 0.48 * p[:, 2]
+    return p * box + np.asarray(origin)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+@pytest.mark.parametrize("kernel", [8, 16])
+@pytest.mark.parametrize("box", [1.0, 3.0])
+def test_wall_image_systems_match_reference(kernel, box):
+    """oracle.wall_stokes / wall_rpy (what the GPU wall tests compare with)
+    against the reference's own StkWallFMM (Lib/src/StkWallFMM.cpp: images,
+    sub-FMM values, evalStokes / evalRPY assembly, box scaling) run with exact
+    direct sums in place of its FMMs."""
+    rng = np.random.default_rng(kernel + int(box))
+    origin = np.zeros(3) if box == 1.0 else np.array([-1.0, 2.0, 0.5])
+    src = _wall_points(rng, 300, box, origin)
+    trg = np.concatenate([src[:50], _wall_points(rng, 200, box, origin)])
+    f = rng.normal(size=(len(src), 3))
+    if kernel == 8:
+        val, mine = f, O.wall_stokes(src, f, trg, z0=origin[2])
+    else:
+        val = np.concatenate([f, rng.uniform(1e-4, 5e-4, (len(src), 1)) * box], axis=1)
+        mine = O.wall_rpy(src, val, trg, z0=origin[2])
+    ref = O.ref_wall_direct(kernel, src, val, trg, origin=origin, box=box)
+    assert rel_l2(mine, ref) < 1e-12
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+@pytest.mark.parametrize("kernel", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
+def test_box_flow_matches_reference(kernel):
+    """The reference's own Stk3DFMM in a box [o, o + L)^3 (scaling to the unit
+    box, scaleSrc / scaleTrg; Stk3DFMM.cpp, FMMData.cpp) with its FMM replaced by
+    the exact sum equals the oracle's single- plus double-layer sums in physical
+    coordinates: the physical answer the GPU box-scaling tests compare with."""
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(200 + kernel)
+    o, L = np.array([-1.0, 2.0, 0.5]), 3.0
+    sl = rng.random((200, 3)) * L + o
+    trg = np.concatenate([sl[:30], rng.random((150, 3)) * L + o])
+    uk_sl, uk_dl = S.kernel_slot(kernel, 0), S.kernel_slot(kernel, 1)
+    slv = uk_values(rng, uk_sl, len(sl))
+    if uk_sl in (5, 6, 8):
+        slv[:, 3] *= L  # radius / regularisation in physical units
+    if uk_sl in (26, 27):
+        slv[:, 6] *= L
+    want = O.direct(uk_sl, sl, slv, trg)
+    dl = dlv = None
+    if uk_dl >= 0:
+        dl, dlv = sl.copy(), uk_values(rng, uk_dl, len(sl))
+        O.direct(uk_dl, dl, dlv, trg, out=want)
+    got = O.ref_stk3d_direct(kernel, sl, slv, trg, S.get_kernel_dimension(kernel)[2], dl, dlv, origin=o, box=L)
+    assert rel_l2(got, want) < 1e-12
