@@ -126,6 +126,7 @@ def ref():
         _ref.ref_kernel_scaling.argtypes = [ctypes.c_uint, ctypes.c_double, _dp, _dp, _dp, _ip]
         _ref.ref_evaluate_kernel.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
                                              _dp]
+        _ref.ref_periodize.argtypes = [ctypes.c_uint, ctypes.c_int, _dp, ctypes.c_int, _dp, _ip]
         _ref.ref_wall_direct.argtypes = [ctypes.c_uint, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
                                          _dp]
         _ref.ref_stk3d_direct.argtypes = [ctypes.c_uint, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_int,
@@ -274,6 +275,19 @@ def ref_stk3d_direct(kernel: int, sl, slv, trg, tdim: int, dl=None, dlv=None, or
                                 out.ctypes.data_as(_dp))
     assert rc == 0, kernel
     return out
+
+
+def ref_periodize(kernel: int, p: int, equiv):
+    """1 + what the reference's own FMMData::periodizeFMM (FMMData.cpp:203-247)
+    adds to each target component, for a triply periodic FMM of order p whose
+    root upward-equivalent density is `equiv` (stand-in FMM, unit box).  Needs
+    $PVFMM_DIR/pdata/M2C_<kernel>_3D3D_p<p> to exist (its values are unused)."""
+    equiv, pe = _d(np.asarray(equiv, dtype=np.float64).reshape(-1))
+    trg = np.zeros(16)
+    kdim = np.zeros(1, dtype=np.int32)
+    rc = ref().ref_periodize(kernel, p, pe, len(equiv), trg.ctypes.data_as(_dp), kdim.ctypes.data_as(_ip))
+    assert rc == 0, kernel
+    return trg[:kdim[0]].copy()
 
 
 def ref_kernel_scaling(kernel: int, sf: float):

@@ -132,7 +132,8 @@ typedef pvfmm::Kernel<double>::Ker_t ker_t;
 
 namespace pvfmm {
 int stub_fmm_direct = 0;  // the stand-in FMM's mode (oracle/stub/pvfmm.hpp)
-}
+std::vector<double> stub_root_equiv;
+}  // namespace pvfmm
 
 // The reference's micro-kernels by this project's micro-kernel ids (the
 // numbering of include/stkfmm_b200.h).  Id 4, PVFMM's stokes_vel, is the stub's
@@ -312,5 +313,30 @@ extern "C" int ref_stk3d_direct(unsigned kernel, const double *origin, double le
         fmm.evaluateFMM(static_cast<KERNEL>(kernel), nsl, slv, ntrg, out, ndl, ndl > 0 ? dlv : nullptr);
     }
     pvfmm::stub_fmm_direct = 0;
+    return 0;
+}
+
+// The reference's own periodizeFMM (Lib/src/FMMData.cpp:203-247) for a triply
+// periodic FMMData of order p: with the root's upward-equivalent density set to
+// equiv[n * kdim] and every FMM value 1 (the stand-in in ones mode, unit box),
+// trg[kdimTrg] returns 1 + the correction periodizeFMM adds.  The reference
+// reads its M2C operator from $PVFMM_DIR/pdata (FMMData.cpp:13-56) even though
+// the stand-in FMM does not use it: the caller provides that file.
+extern "C" int ref_periodize(unsigned id, int p, const double *equiv, int nequiv, double *trg, int *kdim_trg) {
+    using namespace stkfmm;
+    if (!composite(id) || !equiv || !trg || !kdim_trg) return 1;
+    pvfmm::stub_fmm_direct = 0;
+    pvfmm::stub_root_equiv.assign(equiv, equiv + nequiv);
+    {
+        impl::FMMData fmm(static_cast<KERNEL>(id), PAXIS::PXYZ, p, 50, true);
+        const std::vector<double> pt = {0.5, 0.5, 0.5}, none;
+        const bool has_dl = fmm.hasDL();
+        fmm.setupTree(pt, has_dl ? pt : none, pt);
+        std::vector<double> slv(fmm.kdimSL, 0.0), dlv(has_dl ? fmm.kdimDL : 0, 0.0), tv(fmm.kdimTrg, 0.0);
+        fmm.evaluateFMM(slv, dlv, tv, 1.0);
+        std::copy(tv.begin(), tv.end(), trg);
+        *kdim_trg = fmm.kdimTrg;
+    }
+    pvfmm::stub_root_equiv.clear();
     return 0;
 }

@@ -27,8 +27,9 @@
 //     what PVFMM's kernel initialisation does for the slots (a null sub-kernel
 //     becomes the kernel itself).  PtFMM_Evaluate has two modes, chosen by
 //     stub_fmm_direct (defined by the program that uses this file): 0 sets every
-//     target value to 1, so that what FMMData applies after it (scaleTrg)
-//     shows; 1 returns what the FMM approximates, the direct sum of the kernel's
+//     target value to 1 (and the root's upward-equivalent density to
+//     stub_root_equiv), so that what FMMData applies after it (periodizeFMM,
+//     scaleTrg) shows; 1 returns what the FMM approximates, the direct sum of the kernel's
 //     S2T single and double layer over all sources, so that the reference's own
 //     FMMData, Stk3DFMM and StkWallFMM code around it runs as an exact method.
 #pragma once
@@ -216,6 +217,9 @@ struct Vector {
 enum class BoundaryType { FreeSpace, PX, PXY, PXYZ };
 
 extern int stub_fmm_direct;
+// ones mode: the root's upward-equivalent density the stand-in FMM leaves behind
+// (read by FMMData::periodizeFMM); empty leaves it as it is
+extern std::vector<double> stub_root_equiv;
 
 template <class T>
 struct PtFMM {
@@ -267,6 +271,7 @@ inline void PtFMM_Evaluate(PtFMM_Tree<T> *tree, std::vector<T> &trg_val, size_t,
                            std::vector<T> *surf_val = nullptr) {
     if (!stub_fmm_direct) {
         std::fill(trg_val.begin(), trg_val.end(), T(1));
+        if (!stub_root_equiv.empty()) tree->root.data.upward_equiv = stub_root_equiv;
         return;
     }
     std::fill(trg_val.begin(), trg_val.end(), T(0));

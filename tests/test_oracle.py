@@ -560,3 +560,32 @@ def test_box_flow_matches_reference(kernel):
         O.direct(uk_dl, dl, dlv, trg, out=want)
     got = O.ref_stk3d_direct(kernel, sl, slv, trg, S.get_kernel_dimension(kernel)[2], dl, dlv, origin=o, box=L)
     assert rel_l2(got, want) < 1e-12
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref needs the reference tree")
+def test_net_flux_correction_matches_reference_periodize(tmp_path, monkeypatch):
+    """The triply periodic net-flux correction this library adds after the FMM
+    (pvel_net_flux_kernel: velocity += 1/2 sum_i floor(y_i) trD_i over the root's
+    upward-equivalent points y_i) against the reference's own
+    FMMData::periodizeFMM (FMMData.cpp:203-247) on the same root density: PVel,
+    PVelGrad and PVelLaplacian get it on components 1..3, Traction does not."""
+    import stkfmm_b200 as S
+    p = 4
+    n = 6 * (p - 1) ** 2 + 2
+    size = 4 * n  # the reference reads (and checks the indices of) its M2C file first; values unused here
+    pdata = tmp_path / "pdata"
+    pdata.mkdir()
+    ij = np.indices((size, size)).reshape(2, -1).T
+    np.savetxt(pdata / ("M2C_stokes_PVel_3D3D_p%d" % p), np.c_[ij, np.zeros(len(ij))], fmt="%d %d %.1f")
+    monkeypatch.setenv("PVFMM_DIR", str(tmp_path))
+    rng = np.random.default_rng(9)
+    equiv = rng.normal(size=(n, 4))
+    ue = O.ref_surface(p, np.full(3, -0.025), 1.05, 0)
+    corr = 0.5 * (np.floor(ue) * equiv[:, 3:4]).sum(0)
+    assert np.abs(corr).max() > 0.1
+    for k in (128, 256, 512, 1024):
+        got = O.ref_periodize(k, p, equiv)
+        want = np.ones(S.get_kernel_dimension(k)[2])
+        if k != 1024:
+            want[1:4] += corr
+        assert np.allclose(got, want, rtol=0, atol=1e-14), (k, got, want)
