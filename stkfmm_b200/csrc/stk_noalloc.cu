@@ -1,21 +1,27 @@
 // stk_noalloc.cu -- a direct-sum entry point that allocates no device memory.
 //
 // Who needs it: callers that must not call cudaMalloc / cudaFree during their
-// run.  cudaMalloc and cudaFree synchronise the device and are not allowed
-// inside a region being captured into a CUDA graph; some frameworks hand the
-// whole device to their own caching allocator, and some real-time or embedded
-// hosts forbid run-time allocation outright.  stk_ukernel_direct_device keeps a
-// per-thread workspace that grows with cudaMalloc; this variant instead works
-// inside one fixed scratch array that the library reserves when it is loaded.
+// run.  cudaMalloc and cudaFree synchronise the whole device, which stalls a
+// caller that keeps several streams busy; some frameworks hand the whole device
+// to their own caching allocator, so memory taken behind its back can make it
+// fail; and some real-time or embedded hosts forbid run-time allocation
+// outright.  stk_ukernel_direct_device keeps a per-thread workspace that grows
+// with cudaMalloc; this variant instead works inside one fixed scratch array
+// that the library reserves when it is loaded.
 //
 // Mechanics: the scratch is the file-scope array g_stk_noalloc_scratch below.
 // Its host-side name is only a stand-in, so the device address is fetched with
 // cudaGetSymbolAddress, once per device, the first time the entry point runs on
 // that device (with that device current), and cached.  That first call therefore
-// does set-up work and should come before any stream capture.  Every call shares
-// the array and leaves its contents behind: the work counter that must start at
-// zero is cleared by each call, and two calls whose work overlaps on the GPU
-// (different streams, or host threads, at the same time) race on the array.
+// does set-up work and should come before any stream capture; so should the
+// first call of each (micro-kernel, precision) pair, whose list-kernel instance
+// runs a one-time occupancy query (and, with lazy module loading, its module
+// load).  The cached address belongs to the device's primary context: after a
+// cudaDeviceReset of that device the entry point must not be used again in the
+// process.  Every call shares the array and leaves its contents behind: the
+// work counter that must start at zero is cleared by each call, and two calls
+// whose work overlaps on the GPU (different streams, or host threads, at the
+// same time) race on the array.
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -89,7 +95,11 @@ __global__ void noalloc_direct_items_kernel(int ntrg, int nsrc, int nchunk, int 
 extern "C" int stk_ukernel_direct_device_noalloc(int ukernel, int nsrc, const double *d_src_coord,
                                                  const double *d_src_value, int ntrg, const double *d_trg_coord,
                                                  double *d_trg_value, int precision, void *stream) {
-    if (ukernel < 0 || ukernel >= STK_UK_STOKES_SLDL_PVEL + 1 || nsrc < 0 || ntrg < 0) return STK_ERR_INVALID_ARG;
+    // every micro-kernel the allocating direct sum takes without per-target values
+    // (the adjoint kernels, which need them, go through stk_ukernel_direct_aux_device)
+    int sdim = 0, tdim = 0;
+    if (stk_ukernel_dims(ukernel, &sdim, &tdim) != STK_OK || stk::uk_tvdim_host(ukernel) > 0 || nsrc < 0 || ntrg < 0)
+        return STK_ERR_INVALID_ARG;
     if (precision != STK_FP64 && precision != STK_MIXED) return STK_ERR_INVALID_ARG;
     if (nsrc == 0 || ntrg == 0) return STK_OK;
     if (!d_src_coord || !d_src_value || !d_trg_coord || !d_trg_value) return STK_ERR_INVALID_ARG;
@@ -134,8 +144,6 @@ extern "C" int stk_ukernel_direct_device_noalloc(int ukernel, int nsrc, const do
     noalloc_direct_items_kernel<<<grid, threads, 0, st>>>(ntrg, nsrc, (int)nchunk, (int)nsc, (int)sc, items, sbeg,
                                                           send, ent);
     if (cudaGetLastError() != cudaSuccess) return STK_ERR_CUDA;
-    int sdim = 0, tdim = 0;
-    stk_ukernel_dims(ukernel, &sdim, &tdim);
     if (stk::launch_pack_records(nsrc, nullptr, d_src_coord, d_src_value, sdim, nullptr, 0, rs, rec, st) !=
         cudaSuccess)
         return STK_ERR_CUDA;
