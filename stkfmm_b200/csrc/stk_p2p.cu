@@ -12,12 +12,17 @@
 //  * Each lane owns two target slots (lane and lane + 32).  With fewer than 64
 //    targets, 2^glog consecutive lanes share a target and split the source
 //    tile; they are reduced with warp shuffles at the end.
-//  * The warp streams the sources of its list entries through a 32-source
-//    shared-memory tile in structure-of-arrays layout: lane i loads source
-//    record i with 16-byte vector loads (the next tile is prefetched into
-//    registers while the current one is consumed), applies the periodic image
-//    shift, computes the per-source staged values (Uk<>::stage) and stores one
-//    row per component.
+//  * The sources of an item's list entries form one stream: each entry is a
+//    segment (its source box's records, with its periodic shift), and the warp
+//    walks the concatenated stream in 32-source tiles that cross segment
+//    boundaries, so only the last tile of an item is padded (with one tile per
+//    entry, padding was ~19% of the evaluated pairs on clustered trees).
+//  * Tile staging: lane i copies the raw record of stream position i of the
+//    next tile into its own shared-memory slot with cp.async (16-byte
+//    asynchronous copies, L2 -> shared) while the current tile is consumed;
+//    then it applies the periodic image shift, computes the per-source staged
+//    values (Uk<>::stage) and writes one column of the structure-of-arrays
+//    tile (one row per component).
 //  * FP64 path: one source and two targets per step; r = x_t - (x_s + shift)
 //    formed in double exactly as the oracle forms it.
 //  * Mixed path: at staging each source coordinate, shifted to the target
@@ -57,18 +62,6 @@ template <int UK> struct Rec {
     static constexpr int SDIM = Uk<UK>::SDIM;
     static constexpr int RS = (3 + SDIM + 1) & ~1;  // doubles per global record (16-byte multiple)
 };
-
-// Load N doubles (N even) from 16-byte aligned global memory with double2 loads.
-template <int N>
-__device__ __forceinline__ void load_rec_global(double (&r)[N], const double *p) {
-    static_assert(N % 2 == 0, "record stride must be even");
-#pragma unroll
-    for (int q = 0; q < N / 2; q++) {
-        double2 v = __ldg(reinterpret_cast<const double2 *>(p) + q);
-        r[2 * q] = v.x;
-        r[2 * q + 1] = v.y;
-    }
-}
 
 // Resident CTAs per SM requested from the register allocator (1: no
 // constraint; forcing 5 measured slower for the FP64 path and neutral for the
@@ -115,6 +108,33 @@ template <class K> struct TargetsPerLane {
     static constexpr int value = (STK_P2P_TPL4 && K::TDIM <= 4 && K::NV <= 8 && K::TV == 0) ? 4 : 2;
 };
 
+// Mixed path: the packed FP32 partial sums go into the Kahan accumulators every
+// kKahanTiles * g tiles, i.e. after ~32 kKahanTiles sources per lane whatever
+// the lanes per target g (STK_KAHAN_TILES overrides; the step costs ~5 FP32
+// operations per output, which per 32-source tile was ~7% of the instructions
+// when g > 1).
+#ifndef STK_KAHAN_TILES
+#define STK_KAHAN_TILES 1
+#endif
+constexpr int kKahanTiles = STK_KAHAN_TILES;
+
+// cp.async (Ampere+ asynchronous global -> shared copy, 16 bytes per lane and
+// instruction, L2 only): the next tile's raw source records land in shared memory
+// while the current tile is consumed, so no register holds a prefetched record.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared-memory stride (doubles) of a raw record: an odd number of 16-byte units,
+// so the 8 lanes of a quarter-warp reading their own records with 16-byte loads
+// hit 8 distinct bank groups.
+template <int RS> struct RawStride {
+    static constexpr int value = ((RS / 2) & 1) ? RS : RS + 2;
+};
+
 template <int UK, bool MIXED>
 __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2p_kernel(const ListP2PArgs a) {
     using K = Uk<UK>;
@@ -123,6 +143,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
     constexpr int TV = K::TV;  // per-output-point values (adjoint kernels)
     constexpr int NTV = NtvOf<K>::value;
     constexpr int RS = Rec<UK>::RS;
+    constexpr int RSS = RawStride<RS>::value;
     constexpr int TPL = TargetsPerLane<K>::value;
     constexpr bool HILO = MIXED && kMixedDisp == kDispHiLo;
     // shared tile, one row per component: coordinates (FP64, or FP32 hi x3 + lo x3)
@@ -133,9 +154,19 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 
     __shared__ __align__(16) CT tcoord[kWarpsPerCta][NCC][32];
     __shared__ __align__(16) S tval[kWarpsPerCta][NV][32];
+    __shared__ __align__(16) double traw[kWarpsPerCta][32][RSS];  // cp.async landing zone, one record per lane
+    // the item's list entries (up to 32 at a time) as segments of one source stream
+    __shared__ int sg_end[kWarpsPerCta][32];   // stream position one past the segment
+    __shared__ int sg_src[kWarpsPerCta][32];   // first record of the segment minus its stream start
+    __shared__ int sg_code[kWarpsPerCta][32];  // periodic shift code
+    const int wid = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    CT(*mc)[32] = tcoord[threadIdx.x >> 5];
-    S(*mv)[32] = tval[threadIdx.x >> 5];
+    CT(*mc)[32] = tcoord[wid];
+    S(*mv)[32] = tval[wid];
+    double *myraw = traw[wid][lane];
+    int *s_end = sg_end[wid];
+    int *s_src = sg_src[wid];
+    int *s_code = sg_code[wid];
 
     for (;;) {
         int it = 0;
@@ -202,6 +233,28 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
         for (int h = 0; h < TPL; h++)
 #pragma unroll
             for (int k = 0; k < TDIM; k++) acc[h][k] = cmp[h][k] = S(0);
+        // mixed path: packed FP32 partial sums, added into the Kahan accumulators in steps
+        F2 pp[TPL][TDIM];
+#pragma unroll
+        for (int h = 0; h < TPL; h++)
+#pragma unroll
+            for (int k = 0; k < TDIM; k++) pp[h][k] = splat(0.0f);
+        int kahan_tiles = 0;
+        auto kahan_step = [&]() {
+            if constexpr (MIXED) {
+#pragma unroll
+                for (int h = 0; h < TPL; h++)
+#pragma unroll
+                    for (int k = 0; k < TDIM; k++) {
+                        const float y = (pp[h][k].v.x + pp[h][k].v.y) - cmp[h][k];
+                        const float t = acc[h][k] + y;
+                        cmp[h][k] = (t - acc[h][k]) - y;
+                        acc[h][k] = t;
+                        pp[h][k] = splat(0.0f);
+                    }
+            }
+            kahan_tiles = 0;
+        };
         F2 th[TPL][3], tl[TPL][3];  // hi/lo targets (HILO)
         double tr[TPL][3];          // centre-relative targets (FP64 displacement)
 #pragma unroll
@@ -219,133 +272,145 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                 }
         }
 
-        // ---- tile iterator over the source records of entries [e0, e1) ----
-        int e = w.e0, base = 0, end = 0;
-        double shx = 0.0, shy = 0.0, shz = 0.0;
-        auto open_entry = [&](int ee) {
-            const int ent = a.list_ent[ee];
-            const int sb = ent >> 5;
-            const int code = ent & 31;
-            base = a.src_box_begin[sb];
-            end = a.src_box_end[sb];
-            shx = (code % 3 - 1) * a.period;
-            shy = ((code / 3) % 3 - 1) * a.period;
-            shz = (code / 9 - 1) * a.period;
-        };
-        while (e < w.e1) {
-            open_entry(e);
-            if (base < end) break;
-            e++;
-        }
-        bool have = e < w.e1;
-        double rn[RS];
-        if (have && lane < end - base) load_rec_global(rn, a.src_rec + (size_t)(base + lane) * RS);
-
-        while (have) {
-            const int n = min(32, end - base);
-            // ---- stage: lane i writes source i of the tile (or zero-strength padding) ----
-            {
-                double v[NV];
-                double x[3];
-                if (lane < n) {
-                    x[0] = rn[0] + shx;
-                    x[1] = rn[1] + shy;
-                    x[2] = rn[2] + shz;
-                    K::stage(rn + 3, v);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) x[k] = c[k] + kPadCoord;
-#pragma unroll
-                    for (int q = 0; q < NV; q++) v[q] = 0.0;
-                }
-                if constexpr (HILO) {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        const double d = x[k] - c[k];
-                        const float hv = (float)d;
-                        mc[k][lane] = hv;
-                        mc[3 + k][lane] = (float)(d - (double)hv);
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) mc[k][lane] = x[k] - c[k];  // c = 0 on the FP64 path
-                }
-#pragma unroll
-                for (int q = 0; q < NV; q++) mv[q][lane] = (S)v[q];
+        // ---- the item's sources as one stream: its list entries, 32 at a time, in
+        // order, each a segment of its source box's records; tiles of 32 stream
+        // positions cross segment boundaries, so only a chunk's last tile is padded ----
+        for (int ec = w.e0; ec < w.e1; ec += 32) {
+            const int ne = min(32, w.e1 - ec);
+            int sz = 0, sbeg = 0, code = 13;  // 13: no periodic shift
+            if (lane < ne) {
+                const int ent = a.list_ent[ec + lane];
+                const int sb = ent >> 5;
+                code = ent & 31;
+                sbeg = a.src_box_begin[sb];
+                sz = a.src_box_end[sb] - sbeg;
             }
-            // ---- advance to the next tile and prefetch it ----
-            base += 32;
-            if (base >= end) {
-                e++;
-                while (e < w.e1) {
-                    open_entry(e);
-                    if (base < end) break;
-                    e++;
-                }
-                have = e < w.e1;
+            int incl = sz;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
             }
-            if (have && lane < end - base) load_rec_global(rn, a.src_rec + (size_t)(base + lane) * RS);
+            const int total = __shfl_sync(kFull, incl, 31);
+            __syncwarp();  // the previous chunk's segment table is no longer read
+            s_end[lane] = lane < ne ? incl : 0x7fffffff;
+            s_src[lane] = sbeg - (incl - sz);
+            s_code[lane] = code;
             __syncwarp();
+            if (total == 0) continue;
 
-            // ---- consume the tile ----
-            if constexpr (MIXED) {
-                F2 pp[TPL][TDIM];
+            // per-lane cursor into the segment table; positions only grow
+            int seg = 0;
+            auto fetch = [&](int p) {  // cp.async the record at stream position p (< total) into this lane's slot
+                while (p >= s_end[seg]) seg++;
+                const double *src = a.src_rec + (size_t)(s_src[seg] + p) * RS;
 #pragma unroll
-                for (int h = 0; h < TPL; h++)
+                for (int q = 0; q < RS / 2; q++) cp_async16(myraw + 2 * q, src + 2 * q);
+                cp_async_commit();
+            };
+            int p0 = 0;
+            if (lane < total) fetch(lane);
+            while (p0 < total) {
+                const int n = min(32, total - p0);
+                // ---- stage: lane i turns stream position p0 + i (its landed record)
+                // into tile column i, or writes zero-strength padding ----
+                cp_async_wait_all();
+                __syncwarp();  // every lane has finished reading the previous tile
+                {
+                    double v[NV];
+                    double x[3];
+                    if (lane < n) {
+                        const int cd = s_code[seg];
+                        const double shx = (cd % 3 - 1) * a.period;
+                        const double shy = ((cd / 3) % 3 - 1) * a.period;
+                        const double shz = (cd / 9 - 1) * a.period;
+                        double rn[RS];
 #pragma unroll
-                    for (int k = 0; k < TDIM; k++) pp[h][k] = splat(0.0f);
-                // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
-STK_UNROLL(STK_P2P_UNROLL_MIXED)
-                for (int j = 2 * sub; j < n; j += 2 * g) {
-                    F2 sv[NV];
+                        for (int q = 0; q < RS / 2; q++) {
+                            const double2 t2 = *reinterpret_cast<const double2 *>(myraw + 2 * q);
+                            rn[2 * q] = t2.x;
+                            rn[2 * q + 1] = t2.y;
+                        }
+                        x[0] = rn[0] + shx;
+                        x[1] = rn[1] + shy;
+                        x[2] = rn[2] + shz;
+                        K::stage(rn + 3, v);
+                    } else {
 #pragma unroll
-                    for (int q = 0; q < NV; q++) sv[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
+                        for (int k = 0; k < 3; k++) x[k] = c[k] + kPadCoord;
+#pragma unroll
+                        for (int q = 0; q < NV; q++) v[q] = 0.0;
+                    }
                     if constexpr (HILO) {
-                        F2 sh[3], sl[3];
 #pragma unroll
                         for (int k = 0; k < 3; k++) {
-                            sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
-                            sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
+                            const double d = x[k] - c[k];
+                            const float hv = (float)d;
+                            mc[k][lane] = hv;
+                            mc[3 + k][lane] = (float)(d - (double)hv);
                         }
-#pragma unroll
-                        for (int h = 0; h < TPL; h++)
-                            eval(pp[h], (th[h][0] - sh[0]) + (tl[h][0] - sl[0]), (th[h][1] - sh[1]) + (tl[h][1] - sl[1]),
-                                 (th[h][2] - sh[2]) + (tl[h][2] - sl[2]), sv, ta[h]);
                     } else {
-                        double2 sx[3];
 #pragma unroll
-                        for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
+                        for (int k = 0; k < 3; k++) mc[k][lane] = x[k] - c[k];  // c = 0 on the FP64 path
+                    }
+#pragma unroll
+                    for (int q = 0; q < NV; q++) mv[q][lane] = (S)v[q];
+                }
+                // ---- prefetch the next tile into the (now free) landing zone ----
+                p0 += 32;
+                if (p0 + lane < total) fetch(p0 + lane);
+                __syncwarp();
+
+                // ---- consume the tile ----
+                if constexpr (MIXED) {
+                    // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
+STK_UNROLL(STK_P2P_UNROLL_MIXED)
+                    for (int j = 2 * sub; j < n; j += 2 * g) {
+                        F2 sv[NV];
+#pragma unroll
+                        for (int q = 0; q < NV; q++) sv[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
+                        if constexpr (HILO) {
+                            F2 sh[3], sl[3];
+#pragma unroll
+                            for (int k = 0; k < 3; k++) {
+                                sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
+                                sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
+                            }
+#pragma unroll
+                            for (int h = 0; h < TPL; h++)
+                                eval(pp[h], (th[h][0] - sh[0]) + (tl[h][0] - sl[0]),
+                                     (th[h][1] - sh[1]) + (tl[h][1] - sl[1]), (th[h][2] - sh[2]) + (tl[h][2] - sl[2]),
+                                     sv, ta[h]);
+                        } else {
+                            double2 sx[3];
+#pragma unroll
+                            for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
+#pragma unroll
+                            for (int h = 0; h < TPL; h++)
+                                eval(pp[h], mk((float)(tr[h][0] - sx[0].x), (float)(tr[h][0] - sx[0].y)),
+                                     mk((float)(tr[h][1] - sx[1].x), (float)(tr[h][1] - sx[1].y)),
+                                     mk((float)(tr[h][2] - sx[2].x), (float)(tr[h][2] - sx[2].y)), sv, ta[h]);
+                        }
+                    }
+                    // Kahan-compensated accumulation of the partial sums once a lane has
+                    // evaluated ~32 sources since the last step (every g tiles)
+                    if (++kahan_tiles >= kKahanTiles * g) kahan_step();
+                } else {
+STK_UNROLL(STK_P2P_UNROLL_FP64)
+                    for (int j = sub; j < n; j += g) {
+                        double sv[NV];
+#pragma unroll
+                        for (int q = 0; q < NV; q++) sv[q] = mv[q][j];
+                        const double sx = mc[0][j], sy = mc[1][j], sz = mc[2][j];
 #pragma unroll
                         for (int h = 0; h < TPL; h++)
-                            eval(pp[h], mk((float)(tr[h][0] - sx[0].x), (float)(tr[h][0] - sx[0].y)),
-                                 mk((float)(tr[h][1] - sx[1].x), (float)(tr[h][1] - sx[1].y)),
-                                 mk((float)(tr[h][2] - sx[2].x), (float)(tr[h][2] - sx[2].y)), sv, ta[h]);
+                            eval(acc[h], xt[h][0] - sx, xt[h][1] - sy, xt[h][2] - sz, sv, ta[h]);
                     }
-                }
-                // Kahan-compensated accumulation of the tile's partial sums
-#pragma unroll
-                for (int h = 0; h < TPL; h++)
-#pragma unroll
-                    for (int k = 0; k < TDIM; k++) {
-                        const float y = (pp[h][k].v.x + pp[h][k].v.y) - cmp[h][k];
-                        const float t = acc[h][k] + y;
-                        cmp[h][k] = (t - acc[h][k]) - y;
-                        acc[h][k] = t;
-                    }
-            } else {
-STK_UNROLL(STK_P2P_UNROLL_FP64)
-                for (int j = sub; j < n; j += g) {
-                    double sv[NV];
-#pragma unroll
-                    for (int q = 0; q < NV; q++) sv[q] = mv[q][j];
-                    const double sx = mc[0][j], sy = mc[1][j], sz = mc[2][j];
-#pragma unroll
-                    for (int h = 0; h < TPL; h++)
-                        eval(acc[h], xt[h][0] - sx, xt[h][1] - sy, xt[h][2] - sz, sv, ta[h]);
                 }
             }
-            __syncwarp();
         }
+        __syncwarp();
+        if (kahan_tiles > 0) kahan_step();
 
         // ---- reduce the lanes that share a target, then accumulate ----
         double o[TPL][TDIM];
