@@ -151,7 +151,11 @@ int stk_measure_peaks(double *out);
 int stk_evaluate_kernel(unsigned kernel, unsigned ppkernel, int nsrc, const double *src_coord,
                         const double *src_value, int ntrg, const double *trg_coord, double *trg_value,
                         int precision);
-/* Same on device pointers and a caller's cudaStream_t (passed as void *). */
+/* Same on device pointers and a caller's cudaStream_t (passed as void *).  The
+ * device-pointer entry points (this one, stk_ukernel_direct_device[_aux],
+ * stk_p2p_lists[_aux]) queue their work on `stream` and return without a host
+ * wait; the calling thread's scratch buffers are ordered across calls by an
+ * event (a later call's stream waits for the earlier call's work). */
 int stk_evaluate_kernel_device(unsigned kernel, unsigned ppkernel, int nsrc, const double *d_src_coord,
                                const double *d_src_value, int ntrg, const double *d_trg_coord,
                                double *d_trg_value, int precision, void *stream);
@@ -165,16 +169,21 @@ int stk_ukernel_direct_aux_device(int ukernel, int nsrc, const double *d_src_coo
                                   int ntrg, const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value,
                                   int precision, void *stream);
 /* The same direct sum for callers that cannot allocate device memory while they
- * run: code being captured into a CUDA graph (cudaMalloc/cudaFree are not
- * capturable and synchronise the device), frameworks whose own allocator owns
- * the device, hosts that forbid run-time allocation.  No reference counterpart.
+ * run: frameworks whose own caching allocator owns the device (memory taken
+ * behind its back can make it fail), programs that keep several streams busy
+ * and cannot afford the device-wide synchronisation of cudaMalloc/cudaFree,
+ * hosts that forbid run-time allocation.  No reference counterpart.
  * It calls no cudaMalloc/cudaFree: all scratch lives in one fixed 8 MiB array
  * that the library reserves on every GPU where it is loaded.  Sizes whose
  * scratch (work list + nsrc packed source records) exceeds 8 MiB are refused
- * with STK_ERR_SIZE (about 130k sources for 8-double records).  The first call
- * on a device looks the array up (cudaGetSymbolAddress) and should come before
- * any stream capture.  Work is queued on `stream` without a host wait.  All
- * calls share the array: calls that overlap on the GPU race; outputs accumulate. */
+ * with STK_ERR_SIZE (about 130k sources for 8-double records).  It takes every
+ * micro-kernel stk_ukernel_direct_device takes without per-target values; the
+ * adjoint ids (13, 14) are refused with STK_ERR_INVALID_ARG.  The first call on
+ * a device looks the array up (cudaGetSymbolAddress) and the first call of each
+ * (ukernel, precision) pair runs a one-time occupancy query; make those calls
+ * before any stream capture.  Not to be used again after a cudaDeviceReset of
+ * the device.  Work is queued on `stream` without a host wait.  All calls share
+ * the array: calls that overlap on the GPU race; outputs accumulate. */
 int stk_ukernel_direct_device_noalloc(int ukernel, int nsrc, const double *d_src_coord, const double *d_src_value,
                                       int ntrg, const double *d_trg_coord, double *d_trg_value, int precision,
                                       void *stream);
@@ -197,6 +206,32 @@ int stk_p2p_lists_aux(int ukernel, int precision, int n_trg_box, const int *trg_
                       const int *src_end, int nsrc, const double *d_src_coord, const double *d_src_value, int ntrg,
                       const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value, double period,
                       void *stream);
+
+/* ---- reusable asynchronous list plan -----------------------------------------
+ * Replaces, for a list evaluated many times, the per-(target box, source box)
+ * ker_poten calls that PVFMM's list loops make at every evaluation
+ * (PtFMM_Evaluate, Lib/src/FMMData.cpp:198).  stk_p2p_plan_create validates a
+ * CSR list (the layout of stk_p2p_lists, host arrays), builds its cost-sorted
+ * work items and uploads list and items into device memory owned by the plan
+ * (on the current device); *status gets STK_OK or the error, NULL is returned on
+ * error.  stk_p2p_plan_execute queues one micro-kernel over the plan's list on
+ * `stream` and returns without a host wait; outputs accumulate.  The plan's
+ * scratch (the packed source records and the work counter) is shared by its
+ * executions: executions of one plan must be ordered (one stream, or the caller
+ * synchronises between streams).  The first execution with a larger record
+ * stride allocates (and synchronises the device).  d_trg_aux: per-target values
+ * of the adjoint micro-kernels (stk_ukernel_aux_dim), else NULL.
+ * stk_p2p_plan_destroy waits for the device before freeing. */
+typedef struct stk_p2p_plan stk_p2p_plan;
+stk_p2p_plan *stk_p2p_plan_create(int n_trg_box, const int *trg_begin, const int *trg_end, const int *list_off,
+                                  const int *list_ent, int n_src_box, const int *src_begin, const int *src_end,
+                                  int nsrc, int ntrg, double period, int *status);
+int stk_p2p_plan_execute(stk_p2p_plan *plan, int ukernel, int precision, const double *d_src_coord,
+                         const double *d_src_value, const double *d_trg_coord, const double *d_trg_aux,
+                         double *d_trg_value, void *stream);
+/* (target, source point) pairs of the plan's list */
+long long stk_p2p_plan_pairs(const stk_p2p_plan *plan);
+void stk_p2p_plan_destroy(stk_p2p_plan *plan);
 
 /* ---- Stk3DFMM handle (Lib/include/STKFMM/STKFMM.h, Lib/src/Stk3DFMM-c.cpp) -- */
 typedef struct Stk3DFMM Stk3DFMM;

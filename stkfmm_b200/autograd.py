@@ -59,7 +59,9 @@ class DirectPlan:
 
 class UListPlan:
     """Near-field pairs only: the U-list of an adaptive octree over one point set
-    (sources = targets), max_pts points per leaf, coordinates in [0,1)^3."""
+    (sources = targets), max_pts points per leaf, coordinates in [0,1)^3.  The list
+    is uploaded once into a device plan (stk_p2p_plan_create) that the forward and
+    both adjoint passes execute asynchronously on torch's current stream."""
 
     mode = "ulist"
 
@@ -71,30 +73,49 @@ class UListPlan:
         assert np.array_equal(perm, tperm)
         off, ent = self.tree.list("U")
         self.n = len(pts)
-        self.arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (tb, te, off, ent, beg, end)]
         # The adjoint of "target box A sees source box B through image shift s" is
         # "output box B sees input box A through shift -s"; U(B) holds exactly (A, -s),
         # so the U-list serves as its own transpose.
-        self.arrs_t = self.arrs
+        self.arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (tb, te, off, ent, beg, end)]
         self.perm = None
         self._perm_np = perm
+        self._plan = None
+        self._plan_dev = None
+
+    def __del__(self):
+        if getattr(self, "_plan", None):
+            lib().stk_p2p_plan_destroy(self._plan)
+            self._plan = None
+
+    def plan(self, device):
+        """The device plan of the U list (created on first use, on `device`)."""
+        if self._plan is None or self._plan_dev != device:
+            if self._plan:
+                lib().stk_p2p_plan_destroy(self._plan)
+            tb, te, off, ent, beg, end = self.arrs
+            st = np.zeros(1, np.int32)
+            with torch.cuda.device(device):
+                self._plan = lib().stk_p2p_plan_create(len(tb), *(a.ctypes.data_as(P_i) for a in (tb, te, off, ent)),
+                                                       len(beg), beg.ctypes.data_as(P_i), end.ctypes.data_as(P_i),
+                                                       self.n, self.n, 1.0, st.ctypes.data_as(P_i))
+            if not self._plan:
+                check(int(st[0]) or 5, "stk_p2p_plan_create")
+            self._plan_dev = device
+        return self._plan
+
+    def pairs(self):
+        """(target, source point) pairs of one pass over the U list."""
+        return int(lib().stk_p2p_plan_pairs(self.plan(torch.device("cuda", torch.cuda.current_device()))))
 
     def _p(self, device):
         if self.perm is None or self.perm.device != device:
             self.perm = torch.as_tensor(self._perm_np.astype(np.int64), device=device)
         return self.perm
 
-    def _run(self, uk, arrs, src_s, val_s, trg_s, aux_s, out_s, prec):
-        p = [a.ctypes.data_as(P_i) for a in arrs]
-        nbox = len(arrs[0])
-        if aux_s is None:
-            rc = lib().stk_p2p_lists(int(uk), int(prec), nbox, p[0], p[1], p[2], p[3], nbox, p[4], p[5], len(src_s),
-                                     src_s.data_ptr(), val_s.data_ptr(), len(trg_s), trg_s.data_ptr(),
-                                     out_s.data_ptr(), 1.0, _stream())
-        else:
-            rc = lib().stk_p2p_lists_aux(int(uk), int(prec), nbox, p[0], p[1], p[2], p[3], nbox, p[4], p[5],
-                                         len(src_s), src_s.data_ptr(), val_s.data_ptr(), len(trg_s),
-                                         trg_s.data_ptr(), aux_s.data_ptr(), out_s.data_ptr(), 1.0, _stream())
+    def _run(self, uk, src_s, val_s, trg_s, aux_s, out_s, prec):
+        pl = self.plan(src_s.device)
+        rc = lib().stk_p2p_plan_execute(pl, int(uk), int(prec), src_s.data_ptr(), val_s.data_ptr(), trg_s.data_ptr(),
+                                        aux_s.data_ptr() if aux_s is not None else None, out_s.data_ptr(), _stream())
         check(rc, "regvel ulist")
 
     def _sorted(self, *ts):
@@ -107,19 +128,19 @@ class UListPlan:
     def forward(self, src, sval, trg, out, prec):
         src_s, val_s = self._sorted(src, sval)
         o = torch.zeros_like(out)
-        self._run(UKERNEL.STOKES_REGVEL, self.arrs, src_s, val_s, src_s, None, o, prec)
+        self._run(UKERNEL.STOKES_REGVEL, src_s, val_s, src_s, None, o, prec)
         self._unsort(o, out)
 
     def adjoint_src(self, src, sval, trg, w, gsrc, prec):
         src_s, val_s, w_s = self._sorted(src, sval, w)
         o = torch.zeros_like(gsrc)
-        self._run(UKERNEL.REGVEL_ADJ_SRC, self.arrs_t, src_s, w_s, src_s, val_s, o, prec)
+        self._run(UKERNEL.REGVEL_ADJ_SRC, src_s, w_s, src_s, val_s, o, prec)
         self._unsort(o, gsrc)
 
     def adjoint_trg(self, src, sval, trg, w, gtrg, prec):
         src_s, val_s, w_s = self._sorted(src, sval, w)
         o = torch.zeros_like(gtrg)
-        self._run(UKERNEL.REGVEL_ADJ_TRG, self.arrs, src_s, val_s, src_s, w_s, o, prec)
+        self._run(UKERNEL.REGVEL_ADJ_TRG, src_s, val_s, src_s, w_s, o, prec)
         self._unsort(o, gtrg)
 
 
@@ -143,7 +164,6 @@ class StokesRegVelP2P(torch.autograd.Function):
         ctx.plan.adjoint_src(src, sval, trg, w, gsrc, ctx.precision)
         gtrg = torch.zeros((len(trg), 3), dtype=torch.float64, device=src.device)
         ctx.plan.adjoint_trg(src, sval, trg, w, gtrg, ctx.precision)
-        torch.cuda.current_stream().synchronize()
         return gsrc[:, 4:7], gsrc[:, 0:4], gtrg, None, None
 
 

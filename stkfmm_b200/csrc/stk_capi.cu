@@ -123,6 +123,7 @@ static int direct_device(int uk, int nsrc, const double *d_src, const double *d_
     if ((uk_tvdim_host(uk) > 0) != (d_trg_aux != nullptr)) return STK_ERR_INVALID_ARG;
     int rc = ws.ensure_device();
     if (rc) return rc;
+    if ((rc = ws.begin(stream))) return rc;
     const int sd = uk_sdim_host(uk);
     const int rs = uk_record_stride(uk);
     // source records
@@ -157,8 +158,9 @@ static int direct_device(int uk, int nsrc, const double *d_src, const double *d_
     a.atomic_out = sbeg.size() > 1 ? 1 : 0;
     a.trg_aux = d_trg_aux;
     STK_CUDA(launch_list_p2p(uk, prec, a, ws.num_sms(), stream));
-    // the host staging vectors die at return: make the async copies complete first
-    STK_CUDA(cudaStreamSynchronize(stream));
+    // the host vectors may die at return: copies from pageable memory have been
+    // staged by the time cudaMemcpyAsync returns, so no host wait is needed
+    if ((rc = ws.end(stream))) return rc;
     return STK_OK;
 }
 
@@ -279,6 +281,7 @@ static int p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_b
     int rc = ws.ensure_device();
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    if ((rc = ws.begin(s))) return rc;
     std::vector<WorkItem> items;
     long long pairs = 0;
     build_list_items(n_trg_box, trg_begin, trg_end, list_off, list_ent, src_begin, src_end, items, pairs);
@@ -310,8 +313,7 @@ static int p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_b
     a.atomic_out = 0;
     a.trg_aux = d_trg_aux;
     STK_CUDA(launch_list_p2p(ukernel, precision, a, ws.num_sms(), s));
-    STK_CUDA(cudaStreamSynchronize(s));
-    return STK_OK;
+    return ws.end(s);  // queued: no host wait (see direct_device)
 }
 
 extern "C" int stk_p2p_lists(int ukernel, int precision, int n_trg_box, const int *trg_begin, const int *trg_end,

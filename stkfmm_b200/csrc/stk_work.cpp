@@ -73,7 +73,21 @@ int Workspace::ensure_device() {
         if (cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking) != cudaSuccess) return STK_ERR_CUDA;
         if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return STK_ERR_CUDA;
         if (cudaMalloc(&d.counter, 64) != cudaSuccess) return STK_ERR_CUDA;
+        if (cudaEventCreateWithFlags(&d.done, cudaEventDisableTiming) != cudaSuccess) return STK_ERR_CUDA;
     }
+    return STK_OK;
+}
+
+int Workspace::begin(cudaStream_t s) {
+    if (!cur_) return STK_ERR_CUDA;
+    if (cur_->recorded && cudaStreamWaitEvent(s, cur_->done, 0) != cudaSuccess) return STK_ERR_CUDA;
+    return STK_OK;
+}
+
+int Workspace::end(cudaStream_t s) {
+    if (!cur_) return STK_ERR_CUDA;
+    if (cudaEventRecord(cur_->done, s) != cudaSuccess) return STK_ERR_CUDA;
+    cur_->recorded = true;
     return STK_OK;
 }
 
@@ -223,19 +237,6 @@ long long pair_sources(const WorkItem &w, const int *list_ent, const int *src_be
         ns += src_end[sb] - src_begin[sb];
     }
     return ns;
-}
-
-void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner) {
-    owner.assign(n, 0);
-    if (nparts <= 1) return;
-    std::vector<double> load(nparts, 0.0);
-    for (int i = 0; i < n; i++) {
-        int best = 0;
-        for (int r = 1; r < nparts; r++)
-            if (load[r] < load[best]) best = r;
-        owner[i] = best;
-        load[best] += cost[i];
-    }
 }
 
 void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted) {

@@ -22,6 +22,12 @@ class Workspace {
     static Workspace &thread_local_ws();
     ~Workspace();
     int ensure_device();  // STK_OK, STK_ERR_NO_DEVICE or STK_ERR_CUDA
+    // Stream ordering of the workspace's buffers across calls: begin() makes
+    // `s` wait for the work that the previous call queued on its stream (which
+    // may still read the buffers), end() marks the end of this call's work on
+    // `s`.  Calls then return without a host wait.
+    int begin(cudaStream_t s);
+    int end(cudaStream_t s);
     template <class T> T *buf(int slot, size_t n) { return static_cast<T *>(raw(slot, n * sizeof(T))); }
     unsigned int *counter();
     int num_sms();
@@ -33,6 +39,8 @@ class Workspace {
         size_t cap[kNumSlots] = {};
         unsigned int *counter = nullptr;
         cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;  // end of the last call's work on its stream
+        bool recorded = false;
         int sms = 0;
     };
     std::map<int, Dev> devs_;
@@ -55,10 +63,6 @@ void build_list_items(int n_trg_box, const int *trg_begin, const int *trg_end, c
 
 // Source points of one work item (the sum over its list entries).
 long long pair_sources(const WorkItem &w, const int *list_ent, const int *src_begin, const int *src_end);
-
-// Longest-processing-time assignment: items (in the given order, largest first)
-// each go to the part with the smallest load so far; ties to the lowest part.
-void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner);
 
 // Morton order of points inside their own bounding box.
 void morton_order(const double *xyz, int n, std::vector<int> &order, std::vector<double> &sorted);
