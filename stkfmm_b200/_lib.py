@@ -46,6 +46,11 @@ SIGNATURES = [
                                   c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("stk_ukernel_direct_aux_device", c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                               c_void_p, c_int, c_void_p]),
+    ("stk_p2p_plan_create", c_void_p, [c_int, P_i, P_i, P_i, P_i, c_int, P_i, P_i, c_int, c_int, c_double, P_i]),
+    ("stk_p2p_plan_execute", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p]),
+    ("stk_p2p_plan_pairs", c_longlong, [c_void_p]),
+    ("stk_p2p_plan_destroy", None, [c_void_p]),
     ("Stk3DFMM_create", c_void_p, [c_int, c_int, c_int, c_uint]),
     ("Stk3DFMM_destroy", None, [c_void_p]),
     ("Stk3DFMM_set_points", c_int, [c_void_p, c_int, P_d, c_int, P_d, c_int, P_d]),
@@ -102,7 +107,20 @@ KER_SHIMS = ["laplace_p", "laplace_pgrad", "laplace_dipolep", "laplace_dipolepgr
 for _n in KER_SHIMS:
     SIGNATURES.append(("stk_ker_" + _n, None, [P_d, c_int, P_d, c_int, P_d, c_int, P_d, c_void_p]))
 
+# the host-only tree library (no CUDA): the octree / list C ABI and the LPT split
+OCTREE_LIB_PATH = os.path.join(HERE, "libstk_octree.so")
+OCTREE_SIGNATURES = [
+    ("stk_octree_build", c_void_p, [P_d, c_int, c_int, c_int, P_d, c_int, P_d, c_int, P_d, c_int]),
+    ("stk_octree_free", None, [c_void_p]),
+    ("stk_octree_sizes", c_int, [c_void_p, P_ll]),
+    ("stk_octree_nodes", c_int, [c_void_p, P_i, P_i, P_i, P_i]),
+    ("stk_octree_list", c_int, [c_void_p, c_int, P_i, P_i]),
+    ("stk_octree_set", c_int, [c_void_p, c_int, P_i, P_i, P_i]),
+    ("stk_partition_lpt", c_int, [c_int, P_d, c_int, P_i]),
+]
+
 _lib = None
+_octree_lib = None
 _lock = threading.Lock()
 
 
@@ -132,6 +150,22 @@ def lib():
                 f.argtypes = args
             _lib = L
     return _lib
+
+
+def octree_lib():
+    """Load (building first if needed) the host-only libstk_octree.so; it maps no CUDA library."""
+    global _octree_lib
+    with _lock:
+        if _octree_lib is None:
+            from . import build as _build
+            _build.build_octree()
+            L = ctypes.CDLL(OCTREE_LIB_PATH)
+            for name, res, args in OCTREE_SIGNATURES:
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _octree_lib = L
+    return _octree_lib
 
 
 class StkError(RuntimeError):

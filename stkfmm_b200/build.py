@@ -6,6 +6,11 @@ Every CUDA / C++ source under stkfmm_b200/csrc is compiled by nvcc for
 dense translations and operator pseudo-inverses link cuBLAS and cuSOLVER from
 the CUDA toolkit (an rpath points there).  Objects go to
 ``stkfmm_b200/_build`` and are rebuilt only when a source or header changed.
+
+The host-only octree and list builder (stk_tree.cpp, stk_octree_capi.cpp) is
+also built on its own, by the host C++ compiler and without CUDA, into
+``stkfmm_b200/libstk_octree.so``: the tree C ABI (``stk_octree_*``) for
+programs that have no GPU or must not map the GPU library.
 """
 from __future__ import annotations
 
@@ -20,6 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libstkfmm_b200.so")
+OCTREE_LIB = os.path.join(HERE, "libstk_octree.so")
+OCTREE_SOURCES = ("stk_tree.cpp", "stk_octree_capi.cpp")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -71,8 +78,24 @@ def _compile(src: str, obj: str, verbose: bool) -> None:
         sys.stderr.write(r.stderr)
 
 
+def build_octree(force: bool = False) -> str:
+    """Compile (if needed) and return the path of the host-only libstk_octree.so."""
+    srcs = [os.path.join(CSRC, f) for f in OCTREE_SOURCES]
+    deps = srcs + [os.path.join(CSRC, "stk_tree.hpp"), os.path.join(INCLUDE, "stkfmm_b200.h")]
+    if force or not os.path.exists(OCTREE_LIB) or os.path.getmtime(OCTREE_LIB) < _newest(deps):
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "c++")
+        tmp = OCTREE_LIB + ".tmp"
+        cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + INCLUDE, "-o", tmp] + srcs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed on libstk_octree.so:\n%s%s" % (r.stdout, r.stderr))
+        os.replace(tmp, OCTREE_LIB)
+    return OCTREE_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile (if needed) and return the path of libstkfmm_b200.so."""
+    """Compile (if needed) and return the path of libstkfmm_b200.so (and build libstk_octree.so)."""
+    build_octree(force)
     os.makedirs(BUILD, exist_ok=True)
     srcs = _sources()
     hdr_time = _newest(_headers())

@@ -3,13 +3,15 @@
 // Exposes the tree that Stk3DFMM_setup_tree builds (stk_tree.hpp) without any
 // CUDA call, so list construction can be inspected and tested on a machine
 // without a GPU, and so a caller can hand the same lists to stk_p2p_lists.
+// This file and stk_tree.cpp are plain C++: besides going into
+// libstkfmm_b200.so they are built on their own into libstk_octree.so, which
+// a program without a GPU (or that must not map the GPU library) loads.
 #include <cstring>
 #include <new>
 #include <string>
 
 #include "../../include/stkfmm_b200.h"
 #include "stk_tree.hpp"
-#include "stk_work.hpp"
 
 struct stk_octree {
     stk::Octree tree;

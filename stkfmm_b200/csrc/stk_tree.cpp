@@ -302,4 +302,17 @@ void Octree::build_lists() {
     X = to_csr(Xl);
 }
 
+void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner) {
+    owner.assign(n, 0);
+    if (nparts <= 1) return;
+    std::vector<double> load(nparts, 0.0);
+    for (int i = 0; i < n; i++) {
+        int best = 0;
+        for (int r = 1; r < nparts; r++)
+            if (load[r] < load[best]) best = r;
+        owner[i] = best;
+        load[best] += cost[i];
+    }
+}
+
 }  // namespace stk

@@ -90,4 +90,8 @@ class Octree {
 
 uint64_t morton_key(double x, double y, double z);
 
+// Longest-processing-time assignment: items (in the given order, largest first)
+// each go to the part with the smallest load so far; ties to the lowest part.
+void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner);
+
 }  // namespace stk

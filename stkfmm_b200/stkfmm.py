@@ -19,7 +19,7 @@ import enum
 
 import numpy as np
 
-from ._lib import P_d, P_f, P_i, P_ll, StkError, check, lib
+from ._lib import P_d, P_f, P_i, P_ll, StkError, check, lib, octree_lib
 
 
 class PAXIS(enum.IntEnum):
@@ -388,7 +388,7 @@ class Octree:
     """Host-only octree + KIFMM lists (no GPU needed); coordinates in [0,1)^3."""
 
     def __init__(self, tree_pts, max_pts, pbc=0, sl=None, dl=None, trg=None):
-        L = lib()
+        L = octree_lib()
         tp = _arr(tree_pts, 3)
         sl = _arr(sl if sl is not None else np.zeros((0, 3)), 3)
         dl = _arr(dl if dl is not None else np.zeros((0, 3)), 3)
@@ -413,14 +413,14 @@ class Octree:
     def __del__(self):
         t = getattr(self, "t", None)
         if t:
-            lib().stk_octree_free(t)
+            octree_lib().stk_octree_free(t)
             self.t = None
 
     def list(self, which: str):
         w = "UVWX".index(which)
         off = np.zeros(self.num_nodes + 1, np.int32)
         ent = np.zeros(max(self.list_sizes[which], 1), np.int32)
-        check(lib().stk_octree_list(self.t, w, off.ctypes.data_as(P_i), ent.ctypes.data_as(P_i)))
+        check(octree_lib().stk_octree_list(self.t, w, off.ctypes.data_as(P_i), ent.ctypes.data_as(P_i)))
         return off, ent[:self.list_sizes[which]]
 
     def point_set(self, k: int):
@@ -428,6 +428,6 @@ class Octree:
         perm = np.zeros(max(n, 1), np.int32)
         b = np.zeros(self.num_nodes, np.int32)
         e = np.zeros(self.num_nodes, np.int32)
-        check(lib().stk_octree_set(self.t, k, perm.ctypes.data_as(P_i), b.ctypes.data_as(P_i),
+        check(octree_lib().stk_octree_set(self.t, k, perm.ctypes.data_as(P_i), b.ctypes.data_as(P_i),
                                    e.ctypes.data_as(P_i)))
         return perm[:n], b, e
