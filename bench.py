@@ -9,9 +9,16 @@ points per leaf, multipole order 10.  Seeded synthetic data stands in for the
 reference's TOML-configured point sets.
 
 Metric: P2P pair-interactions/s (SL and DL (target, source point) pairs counted
-separately, exact counts from the U-list), mixed precision (FP64 centre-relative
-displacement, FP32 kernel, Kahan FP32 accumulation) as the headline, the plain
-FP64 path beside it, and their ratio.
+separately, exact counts from the U-list) of the plain FP64 path, the
+reference's precision, as the headline; the mixed-precision path (FP64
+centre-relative displacement, FP32 kernel, Kahan FP32 accumulation) beside it
+with its ratio to FP64 and its error against FP64.
+
+The reference arm (--impl reference) runs the reference's own micro-kernel
+bodies (LaplaceLayerKernel.hpp laplace_pgrad + laplace_dipolepgrad, compiled in
+place) in a PVFMM-style SIMD pair loop on all host cores, over the same U-list
+of the same tree (built by the host-only libstk_octree.so; the GPU library is
+not loaded), one full step per step.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -41,20 +48,20 @@ SIGMA = 0.02
 MAX_PTS = 256
 MULT_ORDER = 10
 KERNEL_LAPPGRAD = 1
-# Flops per (target, source point) pair of the fused laplace_pgrad +
+# Algorithmic flops per (target, source point) pair of the fused laplace_pgrad +
 # laplace_dipolepgrad micro-kernel (FMA = 2), counted from stk_ukernels.cuh
-# (Uk<UK_LAPLACE_SLDL_PGRAD>::eval): r^2 5, 1/r^2 1, r.d 5, w 2, potential 2,
-# radial coefficient 2, 1/r^3 1, gradient 12 = 30; mixed path adds the hi/lo
-# displacement 9 and the Newton step on the MUFU rsqrt 5 (= 44); the FP64 path
-# adds the plain displacement 3 (= 33) plus one double-precision rsqrt.
-FLOPS_PER_POINT_PAIR_FUSED = 44
-FLOPS_PER_POINT_PAIR_FP64 = 33
+# (Uk<UK_LAPLACE_SLDL_PGRAD>::eval): displacement 3, r^2 5, 1/r^2 1, r.d 5, w 2,
+# potential 2, radial coefficient 2, 1/r^3 1, gradient 12 = 33, plus one
+# reciprocal square root.  The same count serves both paths: the mixed path's
+# hi/lo displacement split (9) and Newton step on the MUFU rsqrt (5), and the
+# FP64 path's rsqrt refinement, are implementation work and are not counted.
+FLOPS_PER_POINT_PAIR = 33
 WORKLOAD = ("LapPGrad U-list P2P (S2T SL+DL), 1,048,576 pts in 64 Gaussian clusters (sigma 0.02, centres "
             "U[0.1,0.9]^3), max 256 pts/leaf, p=10, SL=DL=targets")
 WORKLOAD_FMM = ("LapPGrad free-space FMM (evaluate_fmm: U/W/X near field + KIFMM far field), same points and "
                 "values, p=10, max 256 pts/leaf")
 FMM_SAMPLE = 4096  # targets of the FMM accuracy check against the direct sum
-METRIC = "P2P pair-interactions/s (U-list S2T SL+DL; mixed path, FP64 beside it; FMM evals/s in fmm)"
+METRIC = "P2P pair-interactions/s (U-list S2T SL+DL; FP64 path, mixed beside it; FMM evals/s in fmm)"
 
 
 def make_points(seed: int):
@@ -172,6 +179,132 @@ WALL_FMM = [
 ]
 
 
+# differentiated StokesRegVel (hand-written adjoint P2P behind torch.autograd)
+ADJ = {"name": "regvel_adjoint_1m_uniform", "n": 1_048_576, "eps": 1e-3, "max_pts": 256, "fd_sample": 4096,
+       "fd_h": 1e-6,
+       "workload": "Differentiated StokesRegVel U-list P2P: 1,048,576 points ~ U[0,1)^3 as sources and targets, "
+                   "f ~ N(0,1)^3, eps = 1e-3 per source, loss = sum_t w_t . u_t with w ~ N(0,1)^3, max 256 pts/leaf, "
+                   "seed 0; one step = forward + hand-written adjoint (d loss/d f, d loss/d eps, d loss/d x)"}
+
+
+def regvel_torch(torch, src, fe, trg):
+    """Plain torch restatement of the stokes_regvel direct sum (all pairs), for FP64 autograd."""
+    import math
+    r = trg[:, None, :] - src[None, :, :]
+    f = fe[None, :, :3]
+    e2 = fe[None, :, 3] ** 2
+    r2 = (r * r).sum(-1)
+    R2 = r2 + e2
+    Rinv3 = R2 ** -1.5
+    fdr = (f * r).sum(-1)
+    u = ((r2 + 2 * e2)[..., None] * f + r * fdr[..., None]) * Rinv3[..., None]
+    return u.sum(1) / (8 * math.pi)
+
+
+def time_adjoint(steps, warmup, seed, ws, flush):
+    """Forward + adjoint of the StokesRegVel U-list P2P through torch.autograd, FP64 and mixed,
+    CUDA events per step (torch's stream); gradients kept for the checks."""
+    import torch
+    from stkfmm_b200.autograd import UListPlan, stokes_regvel
+    rng = np.random.default_rng(seed)
+    n = ADJ["n"]
+    pts = rng.random((n, 3))
+    fe = np.concatenate([rng.normal(size=(n, 3)), np.full((n, 1), ADJ["eps"])], axis=1)
+    w = rng.normal(size=(n, 3))
+    t0 = time.perf_counter()
+    plan = UListPlan(pts, max_pts=ADJ["max_pts"])
+    pairs = plan.pairs()
+    res = {"workload": ADJ["workload"], "setup_tree_s": time.perf_counter() - t0, "pairs_per_pass": pairs,
+           "pairs_per_step": 3 * pairs,
+           "step": "forward (stokes_regvel) + adjoint sources (d/df, d/deps, d/dx_s) + adjoint targets (d/dx_t), "
+                   "each one pass over the U-list pairs"}
+    x = torch.as_tensor(pts).cuda()
+    v = torch.as_tensor(fe).cuda()
+    wt = torch.as_tensor(w).cuda()
+    grads = {}
+    for prec, nm in ((0, "fp64"), (1, "mixed")):
+        def step():
+            xx = x.detach().requires_grad_(True)
+            vv = v.detach().requires_grad_(True)
+            u = stokes_regvel(xx, vv, xx, plan=plan, precision=prec)
+            (u * wt).sum().backward()
+            return xx, vv
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            xx, vv = step()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        m = max_over_ranks([sum(ms) / len(ms)], ws)[0]
+        res[nm] = {"pairs_per_s": job_rate(3 * pairs, ws, m * 1e-3), "ms_per_step": m}
+        grads[nm] = (xx.grad.cpu().numpy(), vv.grad.cpu().numpy())
+    res["mixed_over_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+    res["rel_l2_mixed_vs_fp64"] = {
+        "d_dx": float(np.linalg.norm(grads["mixed"][0] - grads["fp64"][0]) / np.linalg.norm(grads["fp64"][0])),
+        "d_df": float(np.linalg.norm(grads["mixed"][1][:, :3] - grads["fp64"][1][:, :3])
+                      / np.linalg.norm(grads["fp64"][1][:, :3]))}
+    res["timing"] = "CUDA events around forward + backward on torch's stream, L2 flushed between steps"
+    res["_chk"] = (pts, fe, w, plan, grads["fp64"])
+    return res
+
+
+def adjoint_checks(res):
+    """Central finite differences (FP64, h = 1e-6) of the 1M-point loss at a 4,096-point sample
+    (oracle, over the pairs each sampled point enters), and FP64 torch autograd of the direct sum
+    over a 4,096-point subset."""
+    import torch
+    from oracle import oracle as O
+    from stkfmm_b200.autograd import stokes_regvel
+    O.build()
+    pts, fe, w, plan, (gx, gv) = res.pop("_chk")
+    n = len(pts)
+    samp = np.sort(np.random.default_rng(21).choice(n, ADJ["fd_sample"], replace=False))
+    # each sampled point's partners: the points of the leaves in its leaf's U list (U is symmetric)
+    perm, beg, end = plan.tree.point_set(0)
+    off, ent = plan.tree.list("U")
+    leaf_of = np.empty(n, np.int64)
+    isleaf = plan.tree.first_child < 0
+    for b in np.flatnonzero(isleaf):
+        leaf_of[perm[beg[b]:end[b]]] = b
+    nb_off, nb = [0], []
+    for i in samp:
+        b = leaf_of[i]
+        lst = np.concatenate([perm[beg[sb]:end[sb]] for sb in (ent[off[b]:off[b + 1]] >> 5)])
+        nb.append(lst)
+        nb_off.append(nb_off[-1] + len(lst))
+    t0 = time.perf_counter()
+    fdx, fdf = O.regvel_fd_local(samp, np.array(nb_off), np.concatenate(nb), pts, fe, w, h=ADJ["fd_h"])
+    fd_s = time.perf_counter() - t0
+    gxs, gfs = gx[samp], gv[samp, :3]
+    per_point = lambda g, fd: float(np.max(np.linalg.norm(g - fd, axis=1) / np.linalg.norm(fd, axis=1)))
+    res["finite_differences"] = {
+        "sample": "%d points drawn with seed 21 from the 1,048,576; central differences h = %g in FP64 by the oracle "
+                  "over the pairs each point enters (%.1f s)" % (len(samp), ADJ["fd_h"], fd_s),
+        "rel_l2_d_dx": float(np.linalg.norm(gxs - fdx) / np.linalg.norm(fdx)),
+        "rel_l2_d_df": float(np.linalg.norm(gfs - fdf) / np.linalg.norm(fdf)),
+        "max_per_point_rel_d_dx": per_point(gxs, fdx),
+        "max_per_point_rel_d_df": per_point(gfs, fdf),
+        "bar": 1e-5}
+    # FP64 torch autograd of the direct sum over a 4,096-point subset
+    sub = samp
+    a = [torch.tensor(z, dtype=torch.float64, device="cuda", requires_grad=True) for z in (pts[sub], fe[sub])]
+    b = [torch.tensor(z, dtype=torch.float64, device="cuda", requires_grad=True) for z in (pts[sub], fe[sub])]
+    wt = torch.as_tensor(w[sub]).cuda()
+    (stokes_regvel(a[0], a[1], a[0]) * wt).sum().backward()
+    (regvel_torch(torch, b[0], b[1], b[0]) * wt).sum().backward()
+    res["vs_torch_autograd_direct_subset"] = {
+        "points": len(sub),
+        "rel_l2_d_dx": float(torch.linalg.norm(a[0].grad - b[0].grad) / torch.linalg.norm(b[0].grad)),
+        "rel_l2_d_df_deps": float(torch.linalg.norm(a[1].grad - b[1].grad) / torch.linalg.norm(b[1].grad))}
+
+
 def wall_inputs(cfg, seed):
     rng = np.random.default_rng(seed)
     n = cfg["n"]
@@ -260,6 +393,11 @@ def run_one_workload(name, steps, warmup):
             r.pop("_acc")
             print(json.dumps({name: r}), flush=True)
             return 0
+    if name == ADJ["name"]:
+        r = time_adjoint(steps, warmup, 0, 1, flush)
+        adjoint_checks(r)
+        print(json.dumps({name: r}), flush=True)
+        return 0
     raise SystemExit("unknown workload %s" % name)
 
 
@@ -426,83 +564,138 @@ def cpu_lists_run(w, use_ref):
     return w["out"]
 
 
-def cpu_baseline(ul, pts, q, d, target_seconds=12.0):
-    from oracle import oracle as O
-    O.build()
-    use_ref = O.ref_available()
-    cores = os.cpu_count() or 1
-    # calibrate on a small sample, then size the timed sample to ~target_seconds
-    boxes, pairs = sample_boxes(ul, 2e7)
-    w = cpu_lists_prepare(ul, pts, q, d, boxes)
-    cpu_lists_run(w, use_ref)  # thread pool and pages warm
-    t0 = time.perf_counter()
-    cpu_lists_run(w, use_ref)
-    rate = pairs / max(time.perf_counter() - t0, 1e-6)
-    boxes, pairs = sample_boxes(ul, rate * target_seconds, seed=2)
-    w = cpu_lists_prepare(ul, pts, q, d, boxes)
-    t0 = time.perf_counter()
-    cpu_lists_run(w, use_ref)
-    dt = time.perf_counter() - t0
-    kind = "reference" if use_ref else "port"
-    what = ("reference Test/SimpleKernel.cpp LaplaceSLPGrad+LaplaceDLPGrad (oracle/_ref)" if use_ref else
-            "oracle C port of laplace_pgrad+laplace_dipolepgrad")
-    return {"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
-            "sample": "%s over the U-lists of %d randomly chosen target leaves (%.3g SL+DL pairs, %.1f s, OpenMP %d "
-                      "threads)" % (what, len(boxes), pairs, dt, cores)}
-
-
-# ---------------------------------------------------------------- arms ------
-def reference_arm(args):
-    ws, rank, local = dist_env()
-    if rank != 0:
-        return 0
+def host_ulist(pts):
+    """The benchmark's U list, built by the host-only tree library (libstk_octree.so: no GPU
+    library is loaded); the same tree, lists and leaf order as the GPU handle's setup_tree.
+    Target ranges of internal nodes are emptied (U lists belong to leaves)."""
     import stkfmm_b200 as S
-    pts, q, d = make_points(0)
-    # the same adaptive tree / U-list as the GPU arm, built on the host (no GPU)
     t = S.Octree(pts, MAX_PTS, 0, sl=pts, dl=pts, trg=pts)
     ul = {}
-    off, ent = t.list("U")
-    ul["list_off"], ul["list_ent"] = off, ent
+    ul["list_off"], ul["list_ent"] = t.list("U")
+    leaf = t.first_child < 0
     for k, nm in enumerate(("sl", "dl", "trg")):
         perm, b, e = t.point_set(k)
         ul[nm + "_perm"] = perm
         if nm == "trg":
-            ul["trg_begin"], ul["trg_end"] = b, e
-        else:
-            ul[nm + "_begin"], ul[nm + "_end"] = b, e
+            e = np.where(leaf, e, b)
+        ul[nm + "_begin"], ul[nm + "_end"] = b, e
+    return ul
+
+
+def ulist_pairs(ul):
+    """Exact (target, source point) pairs of the U list (SL; DL is the same at the same points)."""
+    off, ent = ul["list_off"], ul["list_ent"]
+    cnt = (ul["sl_end"] - ul["sl_begin"]).astype(np.int64)
+    per_entry = cnt[ent >> 5]
+    csum = np.concatenate([[0], np.cumsum(per_entry)])
+    ns = csum[off[1:]] - csum[off[:-1]]
+    nt = (ul["trg_end"] - ul["trg_begin"]).astype(np.int64)
+    return int((nt * ns).sum())
+
+
+def cpu_full_prepare(ul, pts, q, d):
+    """The whole U list in the form the SIMD reference loop takes: leaf-ordered points and
+    values, list arrays (set-up, not timed: the reference keeps its points in tree order
+    inside PVFMM)."""
+    sp, tp = ul["sl_perm"], ul["trg_perm"]
+    as_i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    ent = ul["list_ent"]
+    return {"tb": as_i32(ul["trg_begin"]), "te": as_i32(ul["trg_end"]), "off": as_i32(ul["list_off"]),
+            "src_box": as_i32(ent >> 5), "shift": as_i32(ent & 31), "sl_b": as_i32(ul["sl_begin"]),
+            "sl_e": as_i32(ul["sl_end"]), "dl_b": as_i32(ul["dl_begin"]), "dl_e": as_i32(ul["dl_end"]),
+            "src": np.ascontiguousarray(pts[sp]), "trg": np.ascontiguousarray(pts[tp]),
+            "q": np.ascontiguousarray(q[sp]), "d": np.ascontiguousarray(d[ul["dl_perm"]]),
+            "out": np.zeros((len(pts), 4))}
+
+
+def cpu_full_step(w, nthreads=0):
+    """One full step on the host: the reference's laplace_pgrad and laplace_dipolepgrad
+    bodies over the whole U list (PVFMM-style SIMD loop, OpenMP over target leaves)."""
+    from oracle import oracle as O
+    O.ref_simd_lists(O.REF_SIMD_LAP_PGRAD, w["tb"], w["te"], w["off"], w["src_box"], w["shift"], w["sl_b"],
+                     w["sl_e"], w["src"], w["q"], w["trg"], out=w["out"], nthreads=nthreads)
+    O.ref_simd_lists(O.REF_SIMD_LAP_DIPOLEPGRAD, w["tb"], w["te"], w["off"], w["src_box"], w["shift"], w["dl_b"],
+                     w["dl_e"], w["src"], w["d"], w["trg"], out=w["out"], nthreads=nthreads)
+    return w["out"]
+
+
+def cpu_isa():
+    from oracle import oracle as O
+    return os.path.basename(O.ref_simd_path())
+
+
+def cpu_baseline(ul, pts, q, d, pairs, target_seconds=15.0):
+    """The reference's micro-kernels in PVFMM's SIMD loop over the whole step's U list, full
+    steps on all host cores; the reference's scalar test kernel (SimpleKernel) beside it on a
+    bounded sample."""
     from oracle import oracle as O
     O.build()
-    use_ref = O.ref_available()
-    # each step: a bounded sample of the workload, sized so the whole run ends in a few minutes
-    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    boxes, pairs = sample_boxes(ul, 2e7)
-    w = cpu_lists_prepare(ul, pts, q, d, boxes)
-    cpu_lists_run(w, use_ref)  # thread pool and pages warm
+    cores = os.cpu_count() or 1
+    w = cpu_full_prepare(ul, pts, q, d)
+    cpu_full_step(w)  # thread pool and pages warm
     t0 = time.perf_counter()
-    cpu_lists_run(w, use_ref)
-    rate = pairs / max(time.perf_counter() - t0, 1e-6)
-    boxes, pairs = sample_boxes(ul, rate * per_step, seed=3)
-    w = cpu_lists_prepare(ul, pts, q, d, boxes)
+    cpu_full_step(w)
+    one = time.perf_counter() - t0
+    reps = int(max(1, min(10, target_seconds / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cpu_full_step(w)
+    dt = (time.perf_counter() - t0) / reps
+    out = {"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
+           "sample": "the whole step (%.4g SL+DL pairs), %d repeats: the reference's laplace_pgrad + "
+                     "laplace_dipolepgrad uKerEval bodies (Lib/include/STKFMM/LaplaceLayerKernel.hpp, compiled in "
+                     "place) in a PVFMM-style SIMD pair loop (%s, OpenMP %d threads), FP64"
+                     % (pairs, reps, cpu_isa(), cores),
+           "ms_per_step": dt * 1e3}
+    if O.ref_available():
+        boxes, spairs = sample_boxes(ul, 2e8, seed=2)
+        ws = cpu_lists_prepare(ul, pts, q, d, boxes)
+        t0 = time.perf_counter()
+        cpu_lists_run(ws, True)
+        sdt = time.perf_counter() - t0
+        out["simple_kernel"] = {"value": spairs / sdt, "unit": "pairs/s", "cores": cores,
+                                "sample": "the reference's scalar test kernels Test/SimpleKernel.cpp LaplaceSLPGrad + "
+                                          "LaplaceDLPGrad over the U lists of %d random target leaves (%.3g pairs)"
+                                          % (len(boxes), spairs)}
+    return out
+
+
+# ---------------------------------------------------------------- arms ------
+def reference_arm(args):
+    """The reference's CPU implementation of the step (its micro-kernel bodies in PVFMM's SIMD
+    loop, all host cores) on the same config: each step is the whole U-list pass."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    if not O.ref_simd_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent "
+                                                              "where the library was built)"}), flush=True)
+        return 0
+    pts, q, d = make_points(0)
+    ul = host_ulist(pts)
+    pairs = 2 * ulist_pairs(ul)
+    w = cpu_full_prepare(ul, pts, q, d)
     for _ in range(args.warmup):
-        cpu_lists_run(w, use_ref)
+        cpu_full_step(w)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        cpu_lists_run(w, use_ref)
+        cpu_full_step(w)
         times.append(time.perf_counter() - t0)
     dt = sum(times) / len(times)
     value = pairs / dt
     cores = os.cpu_count() or 1
-    kind = "reference" if use_ref else "port"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "step": "bounded sample: U-lists of %d target leaves (%.3g pairs)"
-                       % (len(boxes), pairs)},
-            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind,
-                             "sample": "%s, %d target leaves, OpenMP %d threads" % (
-                                 "reference Test/SimpleKernel.cpp via oracle/_ref" if use_ref else "oracle port",
-                                 len(boxes), cores)},
+            "config": {"workload": WORKLOAD, "n_points": N_POINTS, "pairs_per_step": pairs, "same_config": True,
+                       "step": "the whole U-list S2T pass (SL + DL), as the GPU arm's step"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
+                             "sample": "the whole step: the reference's laplace_pgrad + laplace_dipolepgrad uKerEval "
+                                       "bodies (LaplaceLayerKernel.hpp, compiled in place) in a PVFMM-style SIMD pair "
+                                       "loop (%s), OpenMP %d threads, FP64" % (cpu_isa(), cores)},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -620,32 +813,37 @@ def b200_arm(args):
     fst = fmm.fmm_stats(K)
     clk = clocks.stop() if clocks else None
 
-    value = job_rate(pairs, ws, msmx * 1e-3)
-    value64 = job_rate(pairs, ws, ms64 * 1e-3)
+    value = job_rate(pairs, ws, ms64 * 1e-3)  # the headline: FP64, the reference's precision
+    value_mx = job_rate(pairs, ws, msmx * 1e-3)
     o64 = outs[S.PRECISION.FP64].double()
     omx = outs[S.PRECISION.MIXED].double()
     err_mx = float(torch.linalg.norm(omx - o64) / torch.linalg.norm(o64))
     err_cols = [float(torch.linalg.norm(omx[:, c] - o64[:, c]) / torch.linalg.norm(o64[:, c])) for c in range(4)]
 
-    # ---- e2e: the C-ABI host call (pinned host buffers in and out, copies inside) ----
-    fmm.set_precision(S.PRECISION.MIXED)
+    # ---- e2e: the C-ABI host call (pinned host buffers in and out, copies inside), both paths ----
     qh = torch.as_tensor(q).pin_memory().numpy()
     dh = torch.as_tensor(d).pin_memory().numpy()
     oh = torch.zeros((N_POINTS, 4), dtype=torch.float64).pin_memory().numpy()
-    for _ in range(args.warmup):
-        fmm.evaluate_near(K, qh, oh, dh)
-    barrier()
-    e2e_t = []
-    for _ in range(args.steps):
-        oh[:] = 0.0
-        t0 = time.perf_counter()
-        fmm.evaluate_near(K, qh, oh, dh)
-        e2e_t.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks([sum(e2e_t) / len(e2e_t)], ws)[0]
-    e2e_val = job_rate(pairs, ws, e2e_s)
 
-    # ---- FMM e2e: Stk3DFMM_evaluate_fmm with pinned host arrays (mixed) ----
-    fmm.set_precision(S.PRECISION.MIXED)
+    def e2e_near(prec):
+        fmm.set_precision(prec)
+        for _ in range(args.warmup):
+            fmm.evaluate_near(K, qh, oh, dh)
+        barrier()
+        tt = []
+        for _ in range(args.steps):
+            oh[:] = 0.0
+            t0 = time.perf_counter()
+            fmm.evaluate_near(K, qh, oh, dh)
+            tt.append(time.perf_counter() - t0)
+        return max_over_ranks([sum(tt) / len(tt)], ws)[0]
+
+    e2e_s = e2e_near(S.PRECISION.FP64)
+    e2e_val = job_rate(pairs, ws, e2e_s)
+    e2e_mx_s = e2e_near(S.PRECISION.MIXED)
+
+    # ---- FMM e2e: Stk3DFMM_evaluate_fmm with pinned host arrays (FP64) ----
+    fmm.set_precision(S.PRECISION.FP64)
     for _ in range(args.warmup):
         fmm.evaluate_fmm(K, qh, oh, dh)
     barrier()
@@ -664,6 +862,7 @@ def b200_arm(args):
         r, epts, eslv, eouts = time_extra_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)
         extra.append((cfg, r, epts, eslv, eouts))
     walls = [(cfg, time_wall_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)) for cfg in WALL_FMM]
+    adj = time_adjoint(min(args.steps, 5), args.warmup, rank, ws, flush)
 
     if rank != 0:
         if ws > 1:
@@ -681,19 +880,22 @@ def b200_arm(args):
     gpu64 = o64.cpu().numpy()[ul["trg_perm"][sel]]
     parity64 = float(np.linalg.norm(gpu64 - ref_sorted[sel]) / np.linalg.norm(ref_sorted[sel]))
 
-    # ---- roofline of the dominant kernel (the fused mixed P2P kernel) ----
+    # ---- roofline of the dominant kernel (the fused FP64 P2P kernel of the headline) ----
     peaks = np.zeros(6)
     lib().stk_measure_peaks(peaks.ctypes.data_as(__import__("stkfmm_b200._lib", fromlist=["P_d"]).P_d))
-    achieved = point_pairs * FLOPS_PER_POINT_PAIR_FUSED / (kmx * 1e-3) / 1e12
-    traffic = None
+    achieved = point_pairs * FLOPS_PER_POINT_PAIR / (k64 * 1e-3) / 1e12
+    achieved_mx = point_pairs * FLOPS_PER_POINT_PAIR / (kmx * 1e-3) / 1e12
+    traffic, traffic_mx = None, None
     tj = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tj):
         try:
-            traffic = json.load(open(tj)).get("list_p2p_kernel<LAPLACE_SLDL_PGRAD,mixed>")
+            tt = json.load(open(tj))
+            traffic = tt.get("list_p2p_kernel<LAPLACE_SLDL_PGRAD,fp64>")
+            traffic_mx = tt.get("list_p2p_kernel<LAPLACE_SLDL_PGRAD,mixed>")
         except Exception:
             traffic = None
 
-    cpu = cpu_baseline(ul, pts, q, d) if ws == 1 else None
+    cpu = cpu_baseline(ul, pts, q, d, pairs) if ws == 1 else None
 
     # ---- FMM accuracy: both precisions against the oracle's direct sum on a target sample ----
     samp = np.random.default_rng(11).choice(N_POINTS, FMM_SAMPLE, replace=False)
@@ -713,6 +915,7 @@ def b200_arm(args):
     for cfg, r in walls:
         wall_accuracy(cfg, r)
         extra_blocks[cfg["name"]] = r
+    adjoint_checks(adj)
     fmm_block = {
         "workload": WORKLOAD_FMM,
         "fp64": {"evals_per_s": job_rate(1, ws, fms64 * 1e-3), "ms_per_eval": fms64, "phases_ms": fph64},
@@ -724,7 +927,7 @@ def b200_arm(args):
         "work_per_eval": fst,
         "m2l_roofline": m2l_roofline(fmm, K, {"fp64": {"phases_ms": fph64}, "mixed": {"phases_ms": fphmx}}),
         "e2e": {"evals_per_s": job_rate(1, ws, fe2e_s), "ms_per_eval": fe2e_s * 1e3,
-                "api": "Stk3DFMM_evaluate_fmm (C ABI, pinned host arrays, mixed)",
+                "api": "Stk3DFMM_evaluate_fmm (C ABI, pinned host arrays, FP64)",
                 "h2d_bytes_per_eval": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
                 "d2h_bytes_per_eval": int(N_POINTS * 4 * 8)},
         "gpu_launches_per_eval": fmm_launches,
@@ -734,37 +937,43 @@ def b200_arm(args):
     line = {
         "metric": METRIC,
         "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (f64 displacement, Kahan f32 accumulation)", "data": "synthetic",
+        "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_points": N_POINTS, "tree_nodes": st["nodes"], "leaves": st["leaves"],
                    "depth": st["depth"], "u_entries": st["u_entries"], "pairs_per_step": pairs,
                    "point_pairs_per_step": point_pairs, "l2": "256 MB write between timed steps (inputs < L2)",
                    "parallelism": "replica per GPU" if ws > 1 else "1 GPU", "setup_tree_s": tree_s},
-        "fp64": {"value": value64, "unit": "pairs/s", "ms_per_step": ms64, "kernel_ms": k64},
-        "mixed_over_fp64": value / value64,
+        "fp64": {"value": value, "unit": "pairs/s", "ms_per_step": ms64, "kernel_ms": k64},
+        "mixed": {"value": value_mx, "unit": "pairs/s", "ms_per_step": msmx, "kernel_ms": kmx,
+                  "dtype": "f32 kernel tensor (f64 displacement split hi/lo, Kahan f32 accumulation)",
+                  "e2e": {"value": job_rate(pairs, ws, e2e_mx_s), "unit": "pairs/s", "ms_per_step": e2e_mx_s * 1e3}},
+        "mixed_over_fp64": value_mx / value,
+        "mixed_over_fp64_kernel": k64 / kmx,
         "rel_l2_mixed_vs_fp64": err_mx, "rel_l2_mixed_vs_fp64_per_component": err_cols,
         "rel_l2_fp64_vs_oracle_sample": parity64,
-        "fmm_evals_per_s": job_rate(1, ws, fmsmx * 1e-3),
+        "fmm_evals_per_s": job_rate(1, ws, fms64 * 1e-3),
         "fmm": fmm_block,
         "fmm_other_workloads": extra_blocks,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peaks[0]), "unit": "TFLOP/s",
-                     "frac": achieved / float(peaks[0]) if peaks[0] > 0 else None, "traffic": traffic,
-                     "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, mixed>", "kernel_ms": kmx,
-                     "flops_per_point_pair": FLOPS_PER_POINT_PAIR_FUSED,
-                     "peak_source": "measured FP32 FMA probe (stk_measure_peaks) on this GPU",
+        "adjoint": adj,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": float(peaks[1]), "unit": "TFLOP/s",
+                     "frac": achieved / float(peaks[1]) if peaks[1] > 0 else None, "traffic": traffic,
+                     "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, fp64>", "kernel_ms": k64,
+                     "flops_per_point_pair": FLOPS_PER_POINT_PAIR,
+                     "peak_source": "measured FP64 FMA probe (stk_measure_peaks) on this GPU, of measured",
                      "probe": {"fp32_tflops": float(peaks[0]), "fp64_tflops": float(peaks[1]),
                                "mufu_rsqrt_gops": float(peaks[2]), "probe_sm_mhz": float(peaks[3]),
                                "fp32x2_tflops": float(peaks[5])},
-                     "fp64_path": {"achieved": point_pairs * FLOPS_PER_POINT_PAIR_FP64 / (k64 * 1e-3) / 1e12,
-                                   "peak": float(peaks[1]),
-                                   "frac": (point_pairs * FLOPS_PER_POINT_PAIR_FP64 / (k64 * 1e-3) / 1e12)
-                                   / float(peaks[1]) if peaks[1] > 0 else None}},
+                     "mixed_path": {"bound": "fp32", "achieved": achieved_mx, "peak": float(peaks[0]),
+                                    "frac": achieved_mx / float(peaks[0]) if peaks[0] > 0 else None,
+                                    "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, mixed>", "kernel_ms": kmx,
+                                    "traffic": traffic_mx}},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": "pairs/s", "h2d_bytes_per_step": int(q.nbytes + d.nbytes + N_POINTS * 4 * 8),
                 "d2h_bytes_per_step": int(N_POINTS * 4 * 8), "ms_per_step": e2e_s * 1e3,
-                "api": "Stk3DFMM_evaluate_near (C ABI, pinned host arrays)"},
+                "api": "Stk3DFMM_evaluate_near (C ABI, pinned host arrays, FP64)"},
         "gpu_launches": args.steps * (2 * near_launches + 2 * fmm_launches
-                                      + sum(2 * b["gpu_launches_per_eval"] for b in extra_blocks.values())),
+                                      + sum(2 * b["gpu_launches_per_eval"] for b in extra_blocks.values())
+                                      + 2 * 6),
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -782,7 +991,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--fmm-workload", default=None,
                     help="time one further FMM / wall workload alone (%s) and print its block"
-                         % ", ".join(c["name"] for c in EXTRA_FMM + WALL_FMM))
+                         % ", ".join([c["name"] for c in EXTRA_FMM + WALL_FMM] + [ADJ["name"]]))
     args = ap.parse_args()
     if args.fmm_workload:
         return run_one_workload(args.fmm_workload, args.steps, args.warmup)

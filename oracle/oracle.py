@@ -63,9 +63,16 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
 
+# Where this recipe looks for the reference source tree (STKFMM_REF_TREE overrides).
+REF_TREE = os.environ.get("STKFMM_REF_TREE", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and oracle/_ref when the reference tree is present)."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    cmd = ["make", "-C", HERE]
+    if os.path.isdir(REF_TREE):
+        cmd.append("REF=" + REF_TREE)
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
@@ -346,6 +353,102 @@ def ref_lists(which: int, trg_begin, trg_end, list_off, list_src, src_begin, src
                                 out.ctypes.data_as(_dp), td, nthreads)
     assert rc == 0
     return out
+
+
+# The reference's micro-kernel bodies in a PVFMM-style SIMD pair loop
+# (ref_simd.cpp, oracle/_ref/libstk_ref_simd_{avx512,avx2}.so): selector -> (micro-kernel id, sdim, tdim)
+REF_SIMD = {0: (UK_LAPLACE_PGRAD, 1, 4), 1: (UK_LAPLACE_DIPOLEPGRAD, 3, 4), 2: (UK_RPY_ULAPU, 4, 6),
+            3: (UK_STOKES_REGVEL, 4, 3), 4: (UK_STOKES_PVEL, 4, 4), 5: (UK_STOKES_DOUBLEPVEL, 9, 4)}
+REF_SIMD_LAP_PGRAD, REF_SIMD_LAP_DIPOLEPGRAD = 0, 1
+_ref_simd = None
+
+
+def _cpu_has_avx512() -> bool:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                return " avx512f " in line + " "
+    except OSError:
+        pass
+    return False
+
+
+def ref_simd_path():
+    """The SIMD baseline library for this host's vector ISA (AVX-512 when the CPU has it)."""
+    return os.path.join(HERE, "_ref", "libstk_ref_simd_%s.so" % ("avx512" if _cpu_has_avx512() else "avx2"))
+
+
+def ref_simd_available() -> bool:
+    return os.path.exists(ref_simd_path())
+
+
+def ref_simd():
+    global _ref_simd
+    if _ref_simd is None:
+        L = ctypes.CDLL(ref_simd_path())
+        L.ref_simd_lists.argtypes = [ctypes.c_int, ctypes.c_int] + [_ip] * 7 + [_dp] * 3 + [ctypes.c_double, _dp,
+                                                                                         ctypes.c_int]
+        L.ref_simd_direct.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        _ref_simd = L
+    return _ref_simd
+
+
+def ref_simd_lists(which: int, trg_begin, trg_end, list_off, list_src, list_shift, src_begin, src_end, src, sval,
+                   trg, out=None, period: float = 1.0, nthreads: int = 0):
+    """out += the reference micro-kernel `which` (REF_SIMD) over an explicit list, PVFMM's SIMD loop."""
+    _, sd, td = REF_SIMD[which]
+    tb, ptb = _i(trg_begin)
+    te, pte = _i(trg_end)
+    lo, plo = _i(list_off)
+    ls, pls = _i(list_src)
+    lsh, plsh = _i(list_shift) if list_shift is not None else (None, None)
+    sb, psb = _i(src_begin)
+    se, pse = _i(src_end)
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    assert out.dtype == np.float64 and out.flags.c_contiguous and out.shape[1] == td
+    rc = ref_simd().ref_simd_lists(which, len(tb), ptb, pte, plo, pls, plsh, psb, pse, ps, pv, pt, period,
+                                   out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return out
+
+
+def ref_simd_direct(which: int, src, sval, trg, out=None, nthreads: int = 0):
+    """out += the reference micro-kernel `which` (REF_SIMD) over all sources, PVFMM's SIMD loop."""
+    _, sd, td = REF_SIMD[which]
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(-1))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    rc = ref_simd().ref_simd_direct(which, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return out
+
+
+def regvel_fd_local(idx, nb_off, nb, x, val, w, h=1e-6, nthreads=0):
+    """Central differences (step h, FP64) of L = sum w.u for the regularized-Stokeslet sum over a
+    fixed pair set with sources = targets: dL/dx_i (point moved as source and target) and dL/df_i
+    for each checked point i = idx[c], over the pairs that involve it (its neighbour list
+    nb[nb_off[c]:nb_off[c+1]], i included).  Returns (gx, gf), each (len(idx), 3)."""
+    idx, pidx = _i(idx)
+    nb_off, po = _i(nb_off)
+    nb, pn = _i(nb)
+    x, px = _d(np.asarray(x).reshape(-1, 3))
+    val, pv = _d(np.asarray(val).reshape(-1, 4))
+    w, pw = _d(np.asarray(w).reshape(-1, 3))
+    gx = np.zeros((len(idx), 3))
+    gf = np.zeros((len(idx), 3))
+    L = lib()
+    L.oracle_regvel_fd_local.argtypes = [ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp, ctypes.c_double, _dp, _dp,
+                                         ctypes.c_int]
+    rc = L.oracle_regvel_fd_local(len(idx), pidx, po, pn, px, pv, pw, h, gx.ctypes.data_as(_dp),
+                                  gf.ctypes.data_as(_dp), nthreads)
+    assert rc == 0
+    return gx, gf
 
 
 EWALD_LAPLACE, EWALD_STOKES = 0, 1

@@ -631,6 +631,69 @@ int oracle_regvel_adjoint(int nsrc, const double *src_xyz, const double *src_val
     return 0;
 }
 
+/* Central finite differences (step h) of L = sum_t w_t . u_t, u the regularized-
+ * Stokeslet sum (uk_pair's stokes_regvel, scale 1/8 pi) over a fixed set of
+ * (target, source) pairs with sources = targets = the points x, with respect to
+ * the position x_i (moved as a source and as a target) and the force f_i of each
+ * checked point i.  The pairs that involve point i are given per checked point
+ * as its neighbour list nb[nb_off[c] .. nb_off[c+1]) (i included: the pair
+ * (i, i) has r = 0 whatever x_i is): those are the only terms of L that x_i or
+ * f_i enter, so each difference is taken over them alone, in FP64.  Writes
+ * gx[3c + k] = dL/dx_{i,k} and gf[3c + k] = dL/df_{i,k}.
+ * val holds (f, eps) per point.  No reference counterpart (test infrastructure). */
+static double regvel_local_loss(int i, const double *xi, const double *fi, int nn, const int *nb, const double *x,
+                                const double *val, const double *w) {
+    double acc = 0.0;
+    for (int q = 0; q < nn; q++) {
+        const int j = nb[q];
+        if (j == i) { /* self pair: r = 0, G_eps(0) f_i = 2 f_i / eps */
+            double r0[3] = {0.0, 0.0, 0.0}, u[3] = {0, 0, 0}, fe[4] = {fi[0], fi[1], fi[2], val[4 * (size_t)i + 3]};
+            uk_pair(UK_STOKES_REGVEL, r0, fe, u);
+            acc += w[3 * (size_t)i] * u[0] + w[3 * (size_t)i + 1] * u[1] + w[3 * (size_t)i + 2] * u[2];
+            continue;
+        }
+        const double *xj = x + 3 * (size_t)j;
+        /* i as a source seen at target j */
+        double r1[3] = {xj[0] - xi[0], xj[1] - xi[1], xj[2] - xi[2]};
+        double u1[3] = {0, 0, 0}, fe[4] = {fi[0], fi[1], fi[2], val[4 * (size_t)i + 3]};
+        uk_pair(UK_STOKES_REGVEL, r1, fe, u1);
+        acc += w[3 * (size_t)j] * u1[0] + w[3 * (size_t)j + 1] * u1[1] + w[3 * (size_t)j + 2] * u1[2];
+        /* j as a source seen at target i */
+        double r2[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+        double u2[3] = {0, 0, 0};
+        uk_pair(UK_STOKES_REGVEL, r2, val + 4 * (size_t)j, u2);
+        acc += w[3 * (size_t)i] * u2[0] + w[3 * (size_t)i + 1] * u2[1] + w[3 * (size_t)i + 2] * u2[2];
+    }
+    return acc / (8.0 * PI_);
+}
+
+int oracle_regvel_fd_local(int ncheck, const int *idx, const int *nb_off, const int *nb, const double *x,
+                           const double *val, const double *w, double h, double *gx, double *gf, int nthreads) {
+    nthreads = clamp_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int c = 0; c < ncheck; c++) {
+        const int i = idx[c];
+        const int nn = nb_off[c + 1] - nb_off[c];
+        const int *lst = nb + nb_off[c];
+        for (int k = 0; k < 3; k++) {
+            double xp[3] = {x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2]};
+            double xm[3] = {xp[0], xp[1], xp[2]};
+            xp[k] += h;
+            xm[k] -= h;
+            const double *fi = val + 4 * (size_t)i;
+            gx[3 * (size_t)c + k] = (regvel_local_loss(i, xp, fi, nn, lst, x, val, w) -
+                                     regvel_local_loss(i, xm, fi, nn, lst, x, val, w)) / (2.0 * h);
+            const double *x0 = x + 3 * (size_t)i;
+            double fp[3] = {fi[0], fi[1], fi[2]}, fm[3] = {fi[0], fi[1], fi[2]};
+            fp[k] += h;
+            fm[k] -= h;
+            gf[3 * (size_t)c + k] = (regvel_local_loss(i, x0, fp, nn, lst, x, val, w) -
+                                     regvel_local_loss(i, x0, fm, nn, lst, x, val, w)) / (2.0 * h);
+        }
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------------
  * Triply periodic sums (unit cell) by Ewald summation.
  *

@@ -589,3 +589,49 @@ def test_net_flux_correction_matches_reference_periodize(tmp_path, monkeypatch):
         if k != 1024:
             want[1:4] += corr
         assert np.allclose(got, want, rtol=0, atol=1e-14), (k, got, want)
+
+
+def test_regvel_local_finite_differences_match_full_recomputation():
+    """The oracle's neighbourhood-local central differences of L = sum w.u (the regularized
+    Stokeslet U-list sum, sources = targets) equal differences of the whole loss recomputed
+    over every U-list pair (the check bench.py runs at 1M points on a 4,096-point sample)."""
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(31)
+    n = 1500
+    pts = rng.random((n, 3))
+    fe = np.concatenate([rng.normal(size=(n, 3)), np.full((n, 1), 1e-3)], axis=1)
+    w = rng.normal(size=(n, 3))
+    t = S.Octree(pts, 40, 0, sl=pts, trg=pts)
+    perm, beg, end = t.point_set(0)
+    off, ent = t.list("U")
+    leaf = t.first_child < 0
+    tb, te = beg, np.where(leaf, end, beg)
+
+    def loss(x, v):
+        out = O.lists(O.UK_STOKES_REGVEL, tb, te, off, ent >> 5, ent & 31, beg, end, x[perm], v[perm], x[perm])
+        return float((out * w[perm]).sum())
+
+    leaf_of = np.empty(n, np.int64)
+    for b in np.flatnonzero(leaf):
+        leaf_of[perm[beg[b]:end[b]]] = b
+    samp = rng.choice(n, 6, replace=False)
+    nb_off, nb = [0], []
+    for i in samp:
+        b = leaf_of[i]
+        lst = np.concatenate([perm[beg[sb]:end[sb]] for sb in (ent[off[b]:off[b + 1]] >> 5)])
+        nb.append(lst)
+        nb_off.append(nb_off[-1] + len(lst))
+    h = 1e-6
+    gx, gf = O.regvel_fd_local(samp, np.array(nb_off), np.concatenate(nb), pts, fe, w, h=h)
+    for c, i in enumerate(samp):
+        for k in range(3):
+            xp, xm = pts.copy(), pts.copy()
+            xp[i, k] += h
+            xm[i, k] -= h
+            full = (loss(xp, fe) - loss(xm, fe)) / (2 * h)
+            assert abs(full - gx[c, k]) <= 1e-6 * max(abs(full), np.linalg.norm(gx[c])), (i, k, full, gx[c, k])
+            fp, fm = fe.copy(), fe.copy()
+            fp[i, k] += h
+            fm[i, k] -= h
+            full = (loss(pts, fp) - loss(pts, fm)) / (2 * h)
+            assert abs(full - gf[c, k]) <= 1e-6 * max(abs(full), np.linalg.norm(gf[c])), (i, k, full, gf[c, k])
