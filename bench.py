@@ -475,7 +475,42 @@ def time_extra_fmm(cfg, seed, steps, warmup, ws, flush):
     res["m2l_roofline"] = m2l_roofline(fmm, K, res)
     res["gpu_launches_per_eval"] = fmm.last_launch_count(K)
     res["timing"] = "device time of each evaluate_fmm_device (CUDA events on the handle's stream), L2 flushed between"
+    if cfg["pbc"]:
+        res["convergence_vs_p%d" % (cfg["p"] + 2)] = periodic_convergence(cfg, K, pts, slv, dlv, d_sl, dlp, outs)
     return res, pts, slv, outs
+
+
+def periodic_convergence(cfg, K, pts, slv, dlv, d_sl, dlp, outs):
+    """Accuracy of a periodic workload at full size by the reference's own protocol for periodic
+    boxes (Test/Test.cpp's errorConvergence: the FMM against the same FMM at a higher order; the
+    reference's periodic tests check convergence and translation, not an Ewald sum): both
+    precisions against FP64 at p + 2, relative L2 per output component, as is and with the mean
+    difference (the reference's "drift", Test/Test.cpp:143-150) removed."""
+    import torch
+    import stkfmm_b200 as S
+    pc = cfg["p"] + 2
+    td = S.get_kernel_dimension(K)[2]
+    f = S.Stk3DFMM(pc, cfg["max_pts"], cfg["pbc"], K)
+    f.set_box(np.zeros(3), 1.0)
+    f.set_points(pts, pts, pts if dlv is not None else None)
+    f.setup_tree(K)
+    t0 = time.perf_counter()
+    out = torch.zeros((len(pts), td), dtype=torch.float64, device="cuda")
+    f.evaluate_fmm_device(K, d_sl.data_ptr(), out.data_ptr(), dlp, None)
+    torch.cuda.synchronize()
+    ref = out.cpu().numpy()
+    res = {"reference": "FP64 FMM at p = %d, same points and tree rules (%.1f s incl. its operator build)"
+                        % (pc, time.perf_counter() - t0)}
+    for nm, o in outs.items():
+        d = o - ref
+        res[nm] = {"rel_l2_per_component": [float(np.linalg.norm(d[:, c]) / np.linalg.norm(ref[:, c]))
+                                            for c in range(td)],
+                   "rel_l2_drift_removed_per_component": [
+                       float(np.linalg.norm(d[:, c] - d[:, c].mean()) / np.linalg.norm(ref[:, c] - ref[:, c].mean()))
+                       for c in range(td)],
+                   "drift_per_component": [float(d[:, c].mean()) for c in range(td)]}
+    del f
+    return res
 
 
 def m2l_roofline(fmm, K, res):
@@ -503,6 +538,53 @@ def extra_fmm_accuracy(cfg, pts, slv, outs, nsample=4096):
     ref = O.direct(uk, pts, slv, pts[samp])
     return {nm: [float(np.linalg.norm(o[samp, c] - ref[:, c]) / np.linalg.norm(ref[:, c]))
                  for c in range(ref.shape[1])] for nm, o in outs.items()}
+
+
+def time_fmm_sharded(steps, warmup, ws, rank, stream, flush):
+    """Multi-GPU (ws > 1): ONE LapPGrad FMM problem (the seed-0 points on every rank) split over
+    the ranks -- near field, L2T and M2T by work items (set_shard), M2L / S2L by target node with
+    one NCCL all-reduce of the downward densities per evaluation (set_allreduce) -- timed with CUDA
+    events, max over ranks (strong scaling).  Returns the block and the all-reduced output."""
+    import torch
+    import torch.distributed as dist
+    import stkfmm_b200 as S
+    from stkfmm_b200.stkfmm import torch_allreduce
+    K = KERNEL_LAPPGRAD
+    pts, q, d = make_points(0)
+    fmm = S.Stk3DFMM(MULT_ORDER, MAX_PTS, S.PAXIS.NONE, K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts)
+    fmm.set_shard(rank, ws)
+    fmm.set_allreduce(torch_allreduce())
+    fmm.setup_tree(K)
+    qd, dd = torch.as_tensor(q).cuda(), torch.as_tensor(d).cuda()
+    sp = stream.cuda_stream
+    out = torch.zeros((N_POINTS, 4), dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            out.zero_()
+            fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+    stream.synchronize()
+    ms = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            out.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), sp)
+            e1.record(stream)
+        stream.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    m = max_over_ranks([sum(ms) / len(ms)], ws)[0]
+    total = out.clone()
+    dist.all_reduce(total)
+    block = {"workload": WORKLOAD_FMM + "; one problem split over %d GPUs" % ws, "ranks": ws,
+             "evals_per_s": 1e3 / m, "ms_per_eval": m, "scaling": "strong",
+             "split": "near field / L2T / M2T by cost-dealt work items; M2L / S2L by target node; one NCCL "
+                      "all-reduce of the downward equivalent densities per evaluation",
+             "timing": "CUDA events on the evaluation stream, max over ranks, L2 flushed between"}
+    return block, total
 
 
 # ---------------------------------------------------------- CPU baseline ----
@@ -863,6 +945,7 @@ def b200_arm(args):
         extra.append((cfg, r, epts, eslv, eouts))
     walls = [(cfg, time_wall_fmm(cfg, rank, min(args.steps, 3), args.warmup, ws, flush)) for cfg in WALL_FMM]
     adj = time_adjoint(min(args.steps, 5), args.warmup, rank, ws, flush)
+    sharded = time_fmm_sharded(min(args.steps, 5), args.warmup, ws, rank, stream, flush) if ws > 1 else None
 
     if rank != 0:
         if ws > 1:
@@ -916,6 +999,11 @@ def b200_arm(args):
         wall_accuracy(cfg, r)
         extra_blocks[cfg["name"]] = r
     adjoint_checks(adj)
+    if sharded is not None:
+        # rank 0's own FMM leg ran the same seed-0 points unsharded
+        blk, total = sharded
+        blk["rel_l2_vs_unsharded_fp64"] = float(torch.linalg.norm(total - fout64) / torch.linalg.norm(fout64))
+        sharded = blk
     fmm_block = {
         "workload": WORKLOAD_FMM,
         "fp64": {"evals_per_s": job_rate(1, ws, fms64 * 1e-3), "ms_per_eval": fms64, "phases_ms": fph64},
@@ -955,6 +1043,7 @@ def b200_arm(args):
         "fmm": fmm_block,
         "fmm_other_workloads": extra_blocks,
         "adjoint": adj,
+        "fmm_sharded": sharded,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": float(peaks[1]), "unit": "TFLOP/s",
                      "frac": achieved / float(peaks[1]) if peaks[1] > 0 else None, "traffic": traffic,
                      "kernel": "list_p2p_kernel<LAPLACE_SLDL_PGRAD, fp64>", "kernel_ms": k64,

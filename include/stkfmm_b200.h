@@ -207,6 +207,18 @@ int stk_p2p_lists_aux(int ukernel, int precision, int n_trg_box, const int *trg_
                       const double *d_trg_coord, const double *d_trg_aux, double *d_trg_value, double period,
                       void *stream);
 
+/* ---- tensor-core GEMM of the mixed-precision M2L ------------------------------
+ * No reference counterpart (the reference's far field is PVFMM's FP64 BLAS).
+ * C[m + n ldc] (beta 0: =, 1: +=) sum_k A[m lda + k] B[n ldb + k] for m < M,
+ * n < N: FP32 in and out, computed on the sm_100a tensor cores (tcgen05, TF32)
+ * to FP32 accuracy: each operand split into a TF32 high part and an FP32
+ * remainder (3 products), every 32-wide K-block accumulated on its own and
+ * drained into FP32 registers.  Device pointers; the call copies the operands
+ * into padded, split scratch that it allocates, and waits for the result.
+ * STK_ERR_NOT_SUPPORTED off sm_100. */
+int stk_gemm_3xtf32(int M, int N, int K, const float *d_A, int lda, const float *d_B, int ldb, float *d_C, int ldc,
+                    int beta, void *stream);
+
 /* ---- reusable asynchronous list plan -----------------------------------------
  * Replaces, for a list evaluated many times, the per-(target box, source box)
  * ker_poten calls that PVFMM's list loops make at every evaluation
@@ -272,6 +284,23 @@ int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision);
  * all shards' evaluate_near / evaluate_fmm outputs (e.g. an all-reduce) is the
  * unsharded result.  Takes effect at the next setup_tree (default 0 of 1). */
 int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks);
+/* Collective of a sharded handle: sum the n doubles at d_buf (device memory of the
+ * handle's GPU) in place over the ranks of the shard group, ordered after the work
+ * already queued on `stream` (a cudaStream_t) and before the work queued after the
+ * call returns.  Returns 0 on success.  No reference counterpart: the reference
+ * distributes its FMM with MPI inside PVFMM (Lib/src/FMMData.cpp:63).  With a
+ * collective set and set_shard(rank, n > 1), evaluate_fmm also splits the far
+ * field: each rank runs the M2L and S2L of its share of the target nodes (nodes
+ * of complete levels by parity type, the others by cost) and the ranks' downward
+ * equivalent densities are summed with one call of fn (nodes x n_surface x kdim
+ * doubles) before the L2L.  Every rank then holds the whole downward pass; the
+ * near field, L2T and M2T stay split as set_shard describes, so the sum of the
+ * ranks' target outputs is still the unsharded result.  fn = NULL: the far field
+ * is not split (each rank computes all of it).  Takes effect at the next
+ * setup_tree. */
+typedef int (*stk_allreduce_fn)(double *d_buf, long long n, void *stream, void *user);
+int Stk3DFMM_set_allreduce(Stk3DFMM *fmm, stk_allreduce_fn fn, void *user);
+
 /* The periodic far field, the reference's enableFF constructor argument
  * (STKFMM.hpp:199-200, FMMData.cpp:83-89; its C ABI always passes true).  enable = 0:
  * no far-image operator and no periodizeFMM correction, so a periodic sum stops
@@ -395,6 +424,9 @@ int stk_octree_nodes(const stk_octree *t, int *level, int *parent, int *first_ch
 int stk_octree_list(const stk_octree *t, int which, int *off, int *ent);
 /* set: 0 SL, 1 DL, 2 targets; perm (sorted position -> caller index), per-node ranges */
 int stk_octree_set(const stk_octree *t, int set, int *perm, int *node_begin, int *node_end);
+/* owner[node] (0 .. nranks-1): the rank that runs the node's M2L and S2L when
+ * Stk3DFMM's far field is split over nranks (Stk3DFMM_set_allreduce); host only. */
+int stk_octree_far_owners(const stk_octree *t, int nranks, int *owner);
 
 /* ---- ker_poten-signature shims (pvfmm::Kernel<double>::Ker_t) -----------------
  * void (*)(double *r_src, int src_cnt, double *v_src, int dof, double *r_trg,

@@ -46,6 +46,8 @@ SIGNATURES = [
                                   c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("stk_ukernel_direct_aux_device", c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                               c_void_p, c_int, c_void_p]),
+    ("stk_gemm_3xtf32", c_int, [c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
+                                c_void_p]),
     ("stk_p2p_plan_create", c_void_p, [c_int, P_i, P_i, P_i, P_i, c_int, P_i, P_i, c_int, c_int, c_double, P_i]),
     ("stk_p2p_plan_execute", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_void_p]),
@@ -63,6 +65,8 @@ SIGNATURES = [
     ("Stk3DFMM_evaluate_kernel", c_int, [c_void_p, c_uint, c_int, c_uint, c_int, P_d, P_d, c_int, P_d, P_d]),
     ("Stk3DFMM_set_precision", c_int, [c_void_p, c_int]),
     ("Stk3DFMM_set_shard", c_int, [c_void_p, c_int, c_int]),
+    ("Stk3DFMM_set_allreduce", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("stk_octree_far_owners", c_int, [c_void_p, c_int, P_i]),
     ("stk_kernel_scaling", c_int, [c_uint, c_double, P_d, P_d, P_d]),
     ("stk_surface", c_int, [c_int, P_d, c_double, c_int, P_d]),
     ("Stk3DFMM_set_far_field", c_int, [c_void_p, c_int]),
@@ -117,7 +121,11 @@ OCTREE_SIGNATURES = [
     ("stk_octree_list", c_int, [c_void_p, c_int, P_i, P_i]),
     ("stk_octree_set", c_int, [c_void_p, c_int, P_i, P_i, P_i]),
     ("stk_partition_lpt", c_int, [c_int, P_d, c_int, P_i]),
+    ("stk_octree_far_owners", c_int, [c_void_p, c_int, P_i]),
 ]
+
+# the collective a sharded handle calls (Stk3DFMM_set_allreduce)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_longlong, c_void_p, c_void_p)
 
 _lib = None
 _octree_lib = None

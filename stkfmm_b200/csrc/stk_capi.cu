@@ -17,6 +17,7 @@
 #include "stk_kernel_table.hpp"
 #include "stk_p2p.cuh"
 #include "stk_tree.hpp"
+#include "stk_umma.cuh"
 #include "stk_work.hpp"
 
 using namespace stk;
@@ -332,6 +333,52 @@ extern "C" int stk_p2p_lists_aux(int ukernel, int precision, int n_trg_box, cons
     return p2p_lists(ukernel, precision, n_trg_box, trg_begin, trg_end, list_off, list_ent, n_src_box, src_begin,
                      src_end, nsrc, d_src_coord, d_src_value, ntrg, d_trg_coord, d_trg_aux, d_trg_value, period,
                      stream);
+}
+
+// ---------------------------------------------------------------------------
+// the tensor-core GEMM of the mixed M2L (3xTF32 on tcgen05), for direct use and tests
+// ---------------------------------------------------------------------------
+extern "C" int stk_gemm_3xtf32(int M, int N, int K, const float *d_A, int lda, const float *d_B, int ldb, float *d_C,
+                               int ldc, int beta, void *stream) {
+    if (M < 0 || N < 0 || K < 0 || (beta != 0 && beta != 1)) return STK_ERR_INVALID_ARG;
+    if (M == 0 || N == 0) return STK_OK;
+    if (!d_A || !d_B || !d_C || lda < K || ldb < K || ldc < M) return STK_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return STK_ERR_NO_DEVICE;
+    }
+    if (!umma_available()) return STK_ERR_NOT_SUPPORTED;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int la = (K + 3) / 4 * 4;
+    float *buf = nullptr;
+    int *err = nullptr;
+    const size_t na = (size_t)M * la, nb = (size_t)N * la;
+    if (cudaMalloc(&buf, sizeof(float) * 2 * (na + nb) + 64) != cudaSuccess) {
+        cudaGetLastError();
+        return STK_ERR_CUDA;
+    }
+    err = reinterpret_cast<int *>(buf + 2 * (na + nb));
+    float *ah = buf, *al = ah + na, *bh = al + na, *bl = bh + nb;
+    // K-major copies padded to a multiple of 4 floats per row, split into hi / lo
+    int rc = STK_OK;
+    if (cudaMemsetAsync(buf, 0, sizeof(float) * 2 * (na + nb) + 64, s) != cudaSuccess ||
+        cudaMemcpy2DAsync(ah, sizeof(float) * la, d_A, sizeof(float) * lda, sizeof(float) * K, M,
+                          cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpy2DAsync(bh, sizeof(float) * la, d_B, sizeof(float) * ldb, sizeof(float) * K, N,
+                          cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        tf32_split(ah, (long long)na, ah, al, s) != cudaSuccess || tf32_split(bh, (long long)nb, bh, bl, s) != cudaSuccess ||
+        umma_gemm_3xtf32(M, N, K, Tf32Split{ah, al, la}, Tf32Split{bh, bl, la}, d_C, ldc, beta, err, s) != cudaSuccess)
+        rc = STK_ERR_CUDA;
+    int e = 0;
+    if (!rc && (cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess))
+        rc = STK_ERR_CUDA;
+    if (!rc && e) rc = STK_ERR_CUDA;
+    cudaStreamSynchronize(s);
+    cudaFree(buf);
+    cudaGetLastError();
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

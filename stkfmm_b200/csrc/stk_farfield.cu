@@ -15,6 +15,8 @@
 // and L2T run on the list P2P kernel with the surface points as sources or
 // targets.
 #include <algorithm>
+#include <tuple>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +28,7 @@
 #include "stk_farfield.hpp"
 #include "stk_ewald.cuh"
 #include "stk_ukernels.cuh"
+#include "stk_umma.cuh"
 #include "stk_work.hpp"
 
 namespace stk {
@@ -499,6 +502,75 @@ __global__ void m2l_zgather_kernel(const T *__restrict__ Z, int ldz, const int *
     }
 }
 
+// ---- operands of the tensor-core (3xTF32) M2L ----------------------------------
+// the value in FP32, split into TF32 hi / lo parts (tf32_split_value)
+__device__ __forceinline__ void tf32_hilo(double v, float &hi, float &lo) { tf32_split_value((float)v, hi, lo); }
+
+// rows of a column-major k x rows FP64 matrix (its columns) as K-major rows of ld floats
+__global__ void tc_rows_kernel(const double *__restrict__ src, int k, long long rows, int ld, float *__restrict__ hi,
+                               float *__restrict__ lo) {
+    const long long total = rows * ld;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / ld;
+        const int j = (int)(idx - r * ld);
+        float h = 0.f, l = 0.f;
+        if (j < k) tf32_hilo(src[r * k + j], h, l);
+        hi[idx] = h;
+        lo[idx] = l;
+    }
+}
+
+// the transpose: a column-major k x R FP64 block (ld k) as k K-major rows of ld floats
+__global__ void tc_trows_kernel(const double *__restrict__ src, int k, int R, int ld, float *__restrict__ hi,
+                                float *__restrict__ lo) {
+    const long long total = (long long)k * ld;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(idx / ld), j = (int)(idx - (long long)m * ld);
+        float h = 0.f, l = 0.f;
+        if (j < R) tf32_hilo(src[(size_t)j * k + m], h, l);
+        hi[idx] = h;
+        lo[idx] = l;
+    }
+}
+
+// phi_hat columns cols[j] (k values each, FP64) as K-major rows of ld floats, split
+__global__ void tc_gather_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int n, int k,
+                                      int ld, float *__restrict__ hi, float *__restrict__ lo) {
+    const long long total = (long long)n * ld;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / ld), r = (int)(idx - (long long)j * ld);
+        float h = 0.f, l = 0.f;
+        if (r < k) tf32_hilo(src[(size_t)cols[j] * k + r], h, l);
+        hi[idx] = h;
+        lo[idx] = l;
+    }
+}
+
+// m2l_zgather_kernel's rows of one block, split, as the first `width` floats of
+// each target's K-major row (pitch ld; zero beyond R)
+__global__ void tc_zgather_kernel(const float *__restrict__ Z, int ldz, const int *__restrict__ tab, int nq,
+                                  const int *__restrict__ rowq, const int *__restrict__ srow, int R, int width, int ld,
+                                  int n8, float *__restrict__ hi, float *__restrict__ lo) {
+    const long long total = (long long)n8 * width;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / width), row = (int)(i - (long long)j * width);
+        const long long idx = (long long)j * ld + row;
+        float v = 0.f;
+        if (row < R) {
+            const int pos = tab[(size_t)j * nq + rowq[row]];
+            v = pos >= 0 ? Z[(size_t)pos * ldz + srow[row]] : 0.f;
+        }
+        float h, l;
+        tf32_split_value(v, h, l);
+        hi[idx] = h;
+        lo[idx] = l;
+    }
+}
+
 // A_inv = pinv(A) for an m x m column-major matrix (cuSOLVER SVD, FP64), cut
 // at rtol * sigma_max.  A is overwritten.
 int pinv(FarField &F, double *A, int m, double *A_inv, double rtol, cudaStream_t s) {
@@ -531,28 +603,64 @@ int pinv(FarField &F, double *A, int m, double *A_inv, double rtol, cudaStream_t
     return h_info == 0 ? STK_OK : STK_ERR_CUDA;
 }
 
-// Singular values S and right singular vectors VT (N x N, rows v_i^T) of a tall
-// m x N matrix A (m >= N, column-major, overwritten): Householder QR A = Q R,
-// then the SVD of the N x N factor R, which has the same S and V.
-int tall_svd(FarField &F, double *A, long long m, int N, double *S, double *VT, cudaStream_t s) {
+// zero the strictly lower triangle of the leading n x n block of A (column-major, lda)
+__global__ void zero_lower_kernel(double *A, long long lda, int n) {
+    const long long total = (long long)n * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n), j = (int)(idx / n);
+        if (i > j) A[(long long)j * lda + i] = 0.0;
+    }
+}
+
+// Singular values and right singular vectors of a stack of nblocks N x N blocks
+// [B_0; B_1; ...] without holding the stack: a blockwise R-only QR.  A work
+// matrix of (g + 1) N rows holds the running triangular factor R on top of the
+// next g blocks (fill(b, dst, ld) writes block b); each QR of it leaves the new
+// R in its first N rows, whose strictly lower part is cleared before the next
+// group.  R^T R equals the stack's Gram matrix, so the SVD of the final R gives
+// the stack's singular values and right singular vectors.  The group size keeps
+// the work matrix within budget_bytes.
+int stack_svd(FarField &F, int nblocks, int N, const std::function<int(int, double *, long long)> &fill, double *S,
+              double *VT, cudaStream_t s, size_t budget_bytes) {
+    const size_t blk = sizeof(double) * (size_t)N * N;
+    int g = (int)std::max<size_t>(1, std::min<size_t>(nblocks, budget_bytes / blk > 1 ? budget_bytes / blk - 1 : 1));
+    const long long m = (long long)(g + 1) * N;
     if (m > 0x7fffffffLL) return STK_ERR_SIZE;
     cusolverDnSetStream(F.solver, s);
+    DevBuf W, work, tau, R, info, rwork;
+    int rc = W.reserve(blk * (size_t)(g + 1));
+    if (rc) return rc;
     int lq = 0, ls = 0;
-    if (cusolverDnDgeqrf_bufferSize(F.solver, (int)m, N, A, (int)m, &lq) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
+    if (cusolverDnDgeqrf_bufferSize(F.solver, (int)m, N, (double *)W.ptr, (int)m, &lq) != CUSOLVER_STATUS_SUCCESS)
+        return STK_ERR_CUDA;
     if (cusolverDnDgesvd_bufferSize(F.solver, N, N, &ls) != CUSOLVER_STATUS_SUCCESS) return STK_ERR_CUDA;
-    DevBuf work, tau, R, info, rwork;
-    int rc = work.reserve(sizeof(double) * (size_t)std::max(std::max(lq, ls), 1));
+    rc = work.reserve(sizeof(double) * (size_t)std::max(std::max(lq, ls), 1));
     if (!rc) rc = tau.reserve(sizeof(double) * N);
-    if (!rc) rc = R.reserve(sizeof(double) * (size_t)N * N);
+    if (!rc) rc = R.reserve(blk);
     if (!rc) rc = info.reserve(2 * sizeof(int));
     if (!rc) rc = rwork.reserve(sizeof(double) * N);
     if (rc) return rc;
-    if (cusolverDnDgeqrf(F.solver, (int)m, N, A, (int)m, (double *)tau.ptr, (double *)work.ptr, lq, (int *)info.ptr) !=
-        CUSOLVER_STATUS_SUCCESS)
-        return STK_ERR_CUDA;
-    // R: the upper triangle of the first N rows
-    FCUDA(cudaMemsetAsync(R.ptr, 0, sizeof(double) * (size_t)N * N, s));
-    upper_copy_kernel<<<grid_for((long long)N * N), 256, 0, s>>>(A, m, N, (double *)R.ptr);
+    double *Wp = (double *)W.ptr;
+    FCUDA(cudaMemsetAsync(W.ptr, 0, blk * (size_t)(g + 1), s));  // R = 0 before the first group
+    for (int b0 = 0; b0 < nblocks; b0 += g) {
+        const int nb = std::min(g, nblocks - b0);
+        for (int b = 0; b < g; b++) {
+            double *dst = Wp + (size_t)(b + 1) * N;  // rows (b + 1) N .. of the work matrix
+            if (b < nb) {
+                if ((rc = fill(b0 + b, dst, m))) return rc;
+            } else {
+                FCUDA(cudaMemset2DAsync(dst, sizeof(double) * m, 0, sizeof(double) * N, N, s));
+            }
+        }
+        if (cusolverDnDgeqrf(F.solver, (int)m, N, Wp, (int)m, (double *)tau.ptr, (double *)work.ptr, lq,
+                             (int *)info.ptr) != CUSOLVER_STATUS_SUCCESS)
+            return STK_ERR_CUDA;
+        zero_lower_kernel<<<grid_for((long long)N * N), 256, 0, s>>>(Wp, m, N);
+        FCUDA(cudaGetLastError());
+    }
+    FCUDA(cudaMemsetAsync(R.ptr, 0, blk, s));
+    upper_copy_kernel<<<grid_for((long long)N * N), 256, 0, s>>>(Wp, m, N, (double *)R.ptr);
     FCUDA(cudaGetLastError());
     if (cusolverDnDgesvd(F.solver, 'N', 'A', N, N, (double *)R.ptr, N, S, nullptr, N, VT, N, (double *)work.ptr, ls,
                          (double *)rwork.ptr, (int *)info.ptr + 1) != CUSOLVER_STATUS_SUCCESS)
@@ -869,29 +977,35 @@ int build_operators(FarField &F, cudaStream_t s) {
         if (!r) r = kernel_matrix(F.m2x, (const double *)X.ptr, n, (const double *)Y.ptr, n, M, ld, s);
         return r;
     };
-    const long long m = (long long)nslot * N;
-    DevBuf stack, VTv, VTu, Sv, Su;
-    rc = stack.reserve(sizeof(double) * (size_t)m * N);
-    if (!rc) rc = VTv.reserve(sizeof(double) * (size_t)N * N);
+    // the 316-offset stack is never formed: blockwise R-only QR (stack_svd), at most
+    // STKFMM_M2L_QR_BUDGET_MB (default 2048) MB of work matrix
+    DevBuf VTv, VTu, Sv, Su;
+    rc = VTv.reserve(sizeof(double) * (size_t)N * N);
     if (!rc) rc = VTu.reserve(sizeof(double) * (size_t)N * N);
     if (!rc) rc = Sv.reserve(sizeof(double) * N);
     if (!rc) rc = Su.reserve(sizeof(double) * N);
     if (rc) return rc;
-    double *A = (double *)stack.ptr;
-    // rows of [A_d; ...] -> V
+    const char *env_budget = getenv("STKFMM_M2L_QR_BUDGET_MB");
+    const size_t budget = (size_t)(env_budget ? atof(env_budget) : 2048.0) << 20;
+    std::vector<int> slot_code(nslot);
     for (int code = 0; code < kNumOffsets; code++)
-        if (F.m2l_slot[code] >= 0 && (rc = offset_matrix(code, A + (size_t)F.m2l_slot[code] * N, (int)m))) return rc;
-    rc = tall_svd(F, A, m, N, (double *)Sv.ptr, (double *)VTv.ptr, s);
+        if (F.m2l_slot[code] >= 0) slot_code[F.m2l_slot[code]] = code;
+    // rows of [A_d; ...] -> V
+    rc = stack_svd(F, nslot, N, [&](int b, double *dst, long long ld) { return offset_matrix(slot_code[b], dst, (int)ld); },
+                   (double *)Sv.ptr, (double *)VTv.ptr, s, budget);
     if (rc) return rc;
     // columns of [A_d ...] = rows of [A_d^T; ...] -> U
-    for (int code = 0; code < kNumOffsets; code++) {
-        const int sl = F.m2l_slot[code];
-        if (sl < 0) continue;
-        if ((rc = offset_matrix(code, (double *)K.ptr, N))) return rc;
-        FBLAS(cublasDgeam(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, &one, (const double *)K.ptr, N, &zero,
-                          (const double *)K.ptr, N, A + (size_t)sl * N, (int)m));
-    }
-    rc = tall_svd(F, A, m, N, (double *)Su.ptr, (double *)VTu.ptr, s);
+    rc = stack_svd(
+        F, nslot, N,
+        [&](int b, double *dst, long long ld) {
+            int r = offset_matrix(slot_code[b], (double *)K.ptr, N);
+            if (r) return r;
+            if (cublasDgeam(F.blas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, &one, (const double *)K.ptr, N, &zero,
+                            (const double *)K.ptr, N, dst, (int)ld) != CUBLAS_STATUS_SUCCESS)
+                return (int)STK_ERR_CUDA;
+            return (int)STK_OK;
+        },
+        (double *)Su.ptr, (double *)VTu.ptr, s, budget);
     if (rc) return rc;
     std::vector<double> sv(N), su(N);
     FCUDA(cudaMemcpyAsync(sv.data(), Sv.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
@@ -1035,7 +1149,75 @@ int run_pass(const ListPass &P, int prec, const double *rec, const int *src_beg,
 FarField::~FarField() {
     if (blas) cublasDestroy(blas);
     if (solver) cusolverDnDestroy(solver);
+    if (built) cudaEventDestroy(built);
+    for (int i = 0; i < 8; i++) {
+        if (tc_stream[i]) cudaStreamDestroy(tc_stream[i]);
+        if (tc_ev[i]) cudaEventDestroy(tc_ev[i]);
+    }
+    if (tc_fork) cudaEventDestroy(tc_fork);
 }
+
+// ---- process-wide operator cache -------------------------------------------
+// The level-independent operators depend only on (translation kernel, p, M2L
+// cut) and the periodic M2C in addition on (pbc, far field on/off); the
+// reference loads both from precomputed files (Lib/src/FMMData.cpp:13-56) instead
+// of rebuilding them per FMM object.  Here the first handle that needs an entry
+// builds it on its device and every later handle on that device aliases its
+// buffers (DevBuf::share): the wall's Laplace sub-FMMs, repeated handles of one
+// configuration.  Entries live while a handle holds them.
+namespace {
+
+struct OpsKey {
+    int dev, m2x, p, pbc, ff;
+    double rtol;
+    bool operator<(const OpsKey &o) const {
+        return std::tie(dev, m2x, p, pbc, ff, rtol) < std::tie(o.dev, o.m2x, o.p, o.pbc, o.ff, o.rtol);
+    }
+};
+std::mutex g_ops_mu;
+std::map<OpsKey, std::weak_ptr<FarField>> g_ops, g_m2c;
+
+std::shared_ptr<FarField> cache_find(std::map<OpsKey, std::weak_ptr<FarField>> &m, const OpsKey &k) {
+    std::lock_guard<std::mutex> lock(g_ops_mu);
+    auto it = m.find(k);
+    if (it == m.end()) return nullptr;
+    auto sp = it->second.lock();
+    if (!sp) m.erase(it);
+    return sp;
+}
+
+void cache_put(std::map<OpsKey, std::weak_ptr<FarField>> &m, const OpsKey &k, const std::shared_ptr<FarField> &e) {
+    std::lock_guard<std::mutex> lock(g_ops_mu);
+    m[k] = e;
+}
+
+// dst aliases src's level-independent operators
+void share_operators(FarField &dst, const FarField &src) {
+    dst.m2l_rank = src.m2l_rank;
+    dst.m2l_r = src.m2l_r;
+    dst.m2l_rt = src.m2l_rt;
+    dst.m2l_pq_off = src.m2l_pq_off;
+    dst.m2l_rmax = src.m2l_rmax;
+    dst.m2l_slot = src.m2l_slot;
+    dst.uc2ue.share(src.uc2ue);
+    dst.dc2de.share(src.dc2de);
+    dst.m2m.share(src.m2m);
+    dst.l2l.share(src.l2l);
+    dst.m2l_p.share(src.m2l_p);
+    dst.m2l_q.share(src.m2l_q);
+    dst.m2l_p32.share(src.m2l_p32);
+    dst.m2l_q32.share(src.m2l_q32);
+    dst.m2l_vt.share(src.m2l_vt);
+    dst.m2l_e.share(src.m2l_e);
+}
+
+// an event recorded on s after the work queued so far (the entry's build)
+int record_built(FarField &e, cudaStream_t s) {
+    if (!e.built && cudaEventCreateWithFlags(&e.built, cudaEventDisableTiming) != cudaSuccess) return STK_ERR_CUDA;
+    return cudaEventRecord(e.built, s) == cudaSuccess ? STK_OK : STK_ERR_CUDA;
+}
+
+}  // namespace
 
 // Dense M2L of the complete levels (M2LDenseLevel).  A level l >= 4 qualifies
 // when all 8^l boxes are present and its V lists hold at least 70% of 189 pairs
@@ -1158,6 +1340,43 @@ static int setup_m2l_dense(FarField &F, const Octree &T, int nslot, cudaStream_t
                                                                        (long long)k * qs_total,
                                                                        (float *)F.dn_qs32.ptr);
     FCUDA(cudaGetLastError());
+    // tensor-core operands of the mixed path (3xTF32 hi / lo, K-major rows of a multiple
+    // of 4 floats): Qs_c'^T per source type and Pv_{c,c'}^T per block, within 4 GiB
+    F.tc = false;
+    const char *env_tc = getenv("STKFMM_M2L_TC");
+    if (!(env_tc && env_tc[0] == '0') && umma_available()) {
+        const int k4 = (k + 3) / 4 * 4;
+        size_t qa = 0, pa = 0;
+        for (int cs = 0; cs < 8; cs++) {
+            F.tc_qa_off[cs] = qa;
+            qa += (size_t)F.dn_rs[cs] * k4;
+        }
+        for (int c = 0; c < 8; c++) {
+            F.tc_pa_off[c] = pa;
+            pa += (size_t)k * ((F.dn_rv[c] + 3) / 4 * 4);
+        }
+        if ((qa + pa) * 8 <= (4ull << 30)) {
+            rc = F.tc_qa_hi.reserve(sizeof(float) * std::max<size_t>(qa, 4));
+            if (!rc) rc = F.tc_qa_lo.reserve(sizeof(float) * std::max<size_t>(qa, 4));
+            if (!rc) rc = F.tc_pa_hi.reserve(sizeof(float) * std::max<size_t>(pa, 4));
+            if (!rc) rc = F.tc_pa_lo.reserve(sizeof(float) * std::max<size_t>(pa, 4));
+            if (!rc) rc = F.tc_err.reserve(sizeof(int) * 4);
+            if (rc) return rc;
+            for (int cs = 0; cs < 8; cs++)
+                if (F.dn_rs[cs])
+                    tc_rows_kernel<<<grid_for((long long)F.dn_rs[cs] * k4), 256, 0, s>>>(
+                        (const double *)F.dn_qs.ptr + F.dn_qs_off[cs], k, F.dn_rs[cs], k4,
+                        (float *)F.tc_qa_hi.ptr + F.tc_qa_off[cs], (float *)F.tc_qa_lo.ptr + F.tc_qa_off[cs]);
+            for (int c = 0; c < 8; c++)
+                if (F.dn_rv[c])
+                    tc_trows_kernel<<<grid_for((long long)k * F.dn_rv[c]), 256, 0, s>>>(
+                        (const double *)F.dn_pv.ptr + F.dn_pv_off[c], k, F.dn_rv[c], (F.dn_rv[c] + 3) / 4 * 4,
+                        (float *)F.tc_pa_hi.ptr + F.tc_pa_off[c], (float *)F.tc_pa_lo.ptr + F.tc_pa_off[c]);
+            FCUDA(cudaGetLastError());
+            FCUDA(cudaMemsetAsync(F.tc_err.ptr, 0, sizeof(int) * 4, s));
+            F.tc = true;
+        }
+    }
     // per block row: its slot index and its row in Z_c'
     std::vector<int> rowq, srow;
     for (int b = 0; b < 64; b++) {
@@ -1219,6 +1438,41 @@ static int setup_m2l_dense(FarField &F, const Octree &T, int nslot, cudaStream_t
     if (!rc) rc = F.dn_psi.reserve(sizeof(double) * (size_t)k * nmax);
     if (!rc) rc = F.dn_z.reserve(sizeof(double) * (size_t)rs_max * n8max);
     if (!rc) rc = F.dn_zc.reserve(sizeof(double) * (size_t)rcc_max * n8max);
+    if (!rc && F.tc) {
+        // tensor-core work per level: phi operands (nmax rows of k4), the Z of all source types
+        // (sum_c' rs_c' x n8max), and one concatenated Zc operand (n8max rows of ceil4(rv_max))
+        // per concurrent target-type stream, within 16 GiB (fewer streams, else the SIMT path)
+        const size_t k4 = (size_t)(k + 3) / 4 * 4;
+        int rv_max = 1;
+        size_t rs_sum = 0;
+        for (int c = 0; c < 8; c++) {
+            rv_max = std::max(rv_max, F.dn_rv[c]);
+            rs_sum += F.dn_rs[c];
+        }
+        const size_t r4 = (size_t)(rv_max + 3) / 4 * 4;
+        const size_t fixed = sizeof(float) * (2 * k4 * nmax + rs_sum * n8max);
+        const size_t per_stream = sizeof(float) * 2 * r4 * n8max;
+        F.tc_streams = 0;
+        for (int ns = 8; ns >= 1 && !F.tc_streams; ns /= 2)
+            if (fixed + ns * per_stream <= (16ull << 30)) F.tc_streams = ns;
+        if (!F.tc_streams) {
+            F.tc = false;
+        } else {
+            F.tc_zc_ld = (int)r4;
+            rc = F.tc_b_hi.reserve(sizeof(float) * k4 * nmax);
+            if (!rc) rc = F.tc_b_lo.reserve(sizeof(float) * k4 * nmax);
+            if (!rc) rc = F.tc_z.reserve(sizeof(float) * std::max<size_t>(rs_sum * n8max, 4));
+            if (!rc) rc = F.tc_zc_hi.reserve(per_stream / 2 * F.tc_streams);
+            if (!rc) rc = F.tc_zc_lo.reserve(per_stream / 2 * F.tc_streams);
+            for (int i = 0; i < F.tc_streams && !rc; i++) {
+                if (!F.tc_stream[i] && cudaStreamCreateWithFlags(&F.tc_stream[i], cudaStreamNonBlocking) != cudaSuccess)
+                    rc = STK_ERR_CUDA;
+                if (!F.tc_ev[i] && cudaEventCreateWithFlags(&F.tc_ev[i], cudaEventDisableTiming) != cudaSuccess)
+                    rc = STK_ERR_CUDA;
+            }
+            if (!F.tc_fork && cudaEventCreateWithFlags(&F.tc_fork, cudaEventDisableTiming) != cudaSuccess) rc = STK_ERR_CUDA;
+        }
+    }
     if (rc) return rc;
     FCUDA(cudaStreamSynchronize(s));
     return STK_OK;
@@ -1261,17 +1515,50 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         F.ke = ke;
         F.kc = kc;
         F.m2x = m2x;
-        rc = build_operators(F, s);
-        if (rc) {
-            F.p = 0;
-            return rc;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const OpsKey key{dev, m2x, p, 0, 0, m2l_rtol};
+        std::shared_ptr<FarField> e = cache_find(g_ops, key);
+        if (e) {
+            share_operators(F, *e);
+            if (e->built && cudaStreamWaitEvent(s, e->built, 0) != cudaSuccess) return STK_ERR_CUDA;
+        } else {
+            rc = build_operators(F, s);
+            if (rc) {
+                F.p = 0;
+                return rc;
+            }
+            e = std::make_shared<FarField>();
+            share_operators(*e, F);
+            if ((rc = record_built(*e, s))) return rc;
+            cache_put(g_ops, key, e);
         }
+        F.ops_ref = e;
+        F.m2c_p = 0;  // the periodic operator follows the (possibly new) operators
     }
     F.periodic = f->pbc >= 1;
     const int far_field = f->enable_ff ? 1 : 0;
     if (F.periodic && (F.m2c_p != F.p || F.m2c_m2x != F.m2x || F.m2c_pbc != f->pbc || F.m2c_ff != far_field)) {
-        rc = build_periodic(F, f->pbc, far_field, s);
-        if (rc) return rc;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const OpsKey key{dev, F.m2x, F.p, f->pbc, far_field, F.m2l_rtol};
+        std::shared_ptr<FarField> e = cache_find(g_m2c, key);
+        if (e) {
+            F.m2c_op.share(e->m2c_op);
+            F.m2c_p = F.p;
+            F.m2c_m2x = F.m2x;
+            F.m2c_pbc = f->pbc;
+            F.m2c_ff = far_field;
+            if (e->built && cudaStreamWaitEvent(s, e->built, 0) != cudaSuccess) return STK_ERR_CUDA;
+        } else {
+            rc = build_periodic(F, f->pbc, far_field, s);
+            if (rc) return rc;
+            e = std::make_shared<FarField>();
+            e->m2c_op.share(F.m2c_op);
+            if ((rc = record_built(*e, s))) return rc;
+            cache_put(g_m2c, key, e);
+        }
+        F.m2c_ref = e;
     }
     const Octree &T = kd->tree;
     const int nn = T.num_nodes(), n = F.n, N = n * ke;
@@ -1313,6 +1600,10 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     // potentials of S2M / S2L come from one pass over records carrying both
     F.fused_src = kd->fused && (ki->id == STK_LapPGrad || ki->id == STK_PVel);
     F.fused_check_uk = ki->id == STK_LapPGrad ? UK_LAPLACE_SLDL_P : UK_STOKES_SLDL_PVEL;
+
+    // far field split over the shard group (Stk3DFMM_set_allreduce): M2L / S2L by target node
+    F.split = f->shard_n > 1 && f->allreduce != nullptr;
+    for (int c = 0; c < 8; c++) F.dn_own[c] = !F.split || c % f->shard_n == f->shard_rank;
 
     // ---- S2M: leaves with sources; targets = their upward check surfaces ----
     F.s2m_nodes.clear();
@@ -1403,10 +1694,11 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     {
         std::vector<int> tb(mx), te(mx), off(mx + 1, 0), ent;
         std::vector<double> cc(3 * (size_t)std::max(mx, 1));
+        const std::vector<int> owner = far_owners(T, f->shard_n);
         for (int i = 0; i < mx; i++) {
             const int b = F.s2l_nodes[i];
             tb[i] = i * n;
-            te[i] = (i + 1) * n;
+            te[i] = (!F.split || owner[b] == f->shard_rank) ? (i + 1) * n : i * n;
             off[i] = (int)ent.size();
             for (int e = T.X.off[b]; e < T.X.off[b + 1]; e++) ent.push_back(T.X.ent[e]);
             for (int d = 0; d < 3; d++) cc[3 * i + d] = ctr[3 * (size_t)b + d];
@@ -1476,6 +1768,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     // ---- M2L: V-list pairs grouped by offset ----
     {
         const int nslot = (int)std::count_if(F.m2l_slot.begin(), F.m2l_slot.end(), [](int v) { return v >= 0; });
+        // far field split over the shard group: owners of the M2L / S2L target nodes
+        const std::vector<int> owner = far_owners(T, f->shard_n);
+        auto own = [&](int b) { return !F.split || owner[b] == f->shard_rank; };
         // complete levels go to the dense M2L (all pairs of their targets)
         rc = setup_m2l_dense(F, T, nslot, s);
         if (rc) return rc;
@@ -1495,7 +1790,7 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
                 const int sl = F.m2l_slot[(dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)];
                 if (sl < 0) return STK_ERR_STATE;
                 slot_pairs[sl]++;
-                if (dense_lvl[T.level[b]]) continue;
+                if (dense_lvl[T.level[b]] || !own(b)) continue;
                 srcs[sl].push_back(a);
                 trgs[sl].push_back(b);
             }
@@ -1620,6 +1915,79 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
     return STK_OK;
 }
 
+// The mixed path's dense M2L of one complete level on the tensor cores
+// (3xTF32 tcgen05 GEMMs, stk_umma.cu; Z and Psi FP32 as on the SIMT path):
+//   1. Z_c' = Qs_c'^T Phi_c' for the 8 source types, all kept (one GEMM each);
+//   2. per target type c: the rows of every block (c, c') gathered into one
+//      operand Zcat_c (dn_rv[c] rows per target, blocks in c' order), and
+//      Psi_c = Pv_c Zcat_c as ONE GEMM over K = dn_rv[c] -- the sum over the
+//      source types runs inside the GEMM's K loop, in a fixed order
+//      (deterministic) -- the 8 target types on concurrent streams, so that the
+//      narrow GEMMs (M = k, N = boxes per type) together fill the GPU.
+static int m2l_dense_level_tc(FarField &F, const M2LDenseLevel &D, const double *phi_hat, double *psi_hat,
+                              cudaStream_t s) {
+    const int k = F.m2l_rank, n8 = D.n8, n = 8 * n8, k4 = (k + 3) / 4 * 4;
+    const int *nodes = (const int *)D.d_nodes.ptr;
+    float *psi = (float *)F.dn_psi.ptr, *Z = (float *)F.tc_z.ptr;
+    float *bh = (float *)F.tc_b_hi.ptr, *bl = (float *)F.tc_b_lo.ptr;
+    int *err = (int *)F.tc_err.ptr;
+    t_launches++;
+    tc_gather_cols_kernel<<<grid_for((long long)n * k4), 256, 0, s>>>(phi_hat, nodes, n, k, k4, bh, bl);
+    FCUDA(cudaGetLastError());
+    FCUDA(cudaMemsetAsync(psi, 0, sizeof(float) * (size_t)k * n, s));  // types this rank does not own stay 0
+    size_t zoff[8];
+    size_t zo = 0;
+    for (int cs = 0; cs < 8; cs++) {
+        zoff[cs] = zo;
+        const int rs = F.dn_rs[cs];
+        if (!rs) continue;
+        t_launches++;
+        FCUDA(umma_gemm_3xtf32(rs, n8, k,
+                               Tf32Split{(const float *)F.tc_qa_hi.ptr + F.tc_qa_off[cs],
+                                         (const float *)F.tc_qa_lo.ptr + F.tc_qa_off[cs], k4},
+                               Tf32Split{bh + (size_t)cs * n8 * k4, bl + (size_t)cs * n8 * k4, k4}, Z + zo, rs, 0, err,
+                               s));
+        zo += (size_t)rs * n8;
+    }
+    // fork: target types round-robin over the streams, each with its own Zcat buffer
+    FCUDA(cudaEventRecord(F.tc_fork, s));
+    const int ns = F.tc_streams, ld = F.tc_zc_ld;
+    bool used[8] = {};
+    for (int c = 0; c < 8; c++) {
+        const int rv = F.dn_rv[c];
+        if (!rv || !F.dn_own[c]) continue;
+        const int si = c % ns;
+        cudaStream_t st = F.tc_stream[si];
+        if (!used[si]) FCUDA(cudaStreamWaitEvent(st, F.tc_fork, 0));
+        used[si] = true;
+        float *zh = (float *)F.tc_zc_hi.ptr + (size_t)si * ld * n8, *zl = (float *)F.tc_zc_lo.ptr + (size_t)si * ld * n8;
+        const int rv4 = (rv + 3) / 4 * 4;  // row pitch; the GEMM reads K = rv (TMA zero-fills beyond)
+        for (int cs = 0; cs < 8; cs++) {
+            const int b = 8 * c + cs, R = F.dn_rcc[b];
+            if (!R) continue;
+            t_launches++;
+            // rows [pstart_b, pstart_b + R) of every target's Zcat_c row (pitch rv4)
+            tc_zgather_kernel<<<grid_for((long long)n8 * R), 256, 0, st>>>(
+                Z + zoff[cs], F.dn_rs[cs], (const int *)D.d_tab.ptr + D.tab_off[b], F.dn_q[b],
+                (const int *)F.dn_rowq.ptr + F.dn_row_off[b], (const int *)F.dn_srow.ptr + F.dn_row_off[b], R, R, rv4,
+                n8, zh + F.dn_pstart[b], zl + F.dn_pstart[b]);
+            FCUDA(cudaGetLastError());
+        }
+        t_launches++;
+        FCUDA(umma_gemm_3xtf32(k, n8, rv,
+                               Tf32Split{(const float *)F.tc_pa_hi.ptr + F.tc_pa_off[c],
+                                         (const float *)F.tc_pa_lo.ptr + F.tc_pa_off[c], rv4},
+                               Tf32Split{zh, zl, rv4}, psi + (size_t)c * n8 * k, k, 0, err, st));
+    }
+    // join
+    for (int si = 0; si < ns; si++)
+        if (used[si]) {
+            FCUDA(cudaEventRecord(F.tc_ev[si], F.tc_stream[si]));
+            FCUDA(cudaStreamWaitEvent(s, F.tc_ev[si], 0));
+        }
+    return scatter_cols<float>(psi, nodes, n, k, 1.0, 1, psi_hat, s);
+}
+
 // Dense M2L of one complete level: psi_hat[:, t] += sum over the level's V-list
 // pairs, by box parity type (M2LDenseLevel), in T = double (FP64) or float (mixed).
 template <class T>
@@ -1634,6 +2002,9 @@ static int m2l_dense_level(FarField &F, const M2LDenseLevel &D, const double *ph
     const T *pv = f32 ? (const T *)F.dn_pv32.ptr : (const T *)F.dn_pv.ptr;
     const T *qs = f32 ? (const T *)F.dn_qs32.ptr : (const T *)F.dn_qs.ptr;
     const int *nodes = (const int *)D.d_nodes.ptr;
+    if constexpr (std::is_same<T, float>::value) {
+        if (F.tc) return m2l_dense_level_tc(F, D, phi_hat, psi_hat, s);
+    }
     int rc = gather_cols<double, T>(phi_hat, nodes, n, k, phi, s);
     if (rc) return rc;
     FCUDA(cudaMemsetAsync(psi, 0, sizeof(T) * (size_t)k * n, s));
@@ -1645,7 +2016,7 @@ static int m2l_dense_level(FarField &F, const M2LDenseLevel &D, const double *ph
                            phi + (size_t)cs * n8 * k, dt, k, &zero, Z, dt, rs, ct, CUBLAS_GEMM_DEFAULT));
         for (int c = 0; c < 8; c++) {
             const int b = 8 * c + cs, R = F.dn_rcc[b];
-            if (!R) continue;
+            if (!R || !F.dn_own[c]) continue;
             t_launches++;
             m2l_zgather_kernel<T><<<grid_for((long long)n8 * R), 256, 0, s>>>(
                 Z, rs, (const int *)D.d_tab.ptr + D.tab_off[b], F.dn_q[b], (const int *)F.dn_rowq.ptr + F.dn_row_off[b],
@@ -1800,7 +2171,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,
                       psi, N));
     // triply periodic: the root's far images (FP64)
-    if (F.periodic)
+    if (F.periodic && (!F.split || f->shard_rank == 0))
         FBLAS(cublasDgemv(F.blas, CUBLAS_OP_N, N, N, &one, (const double *)F.m2c_op.ptr, N, phi, 1, &one, psi, 1));
     FCUDA(cudaEventRecord(kd->ph[3], s));
     // S2L (X list): downward check potentials, solved per level
@@ -1838,6 +2209,9 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
                 if (rc) return rc;
             }
     }
+    // split far field: every rank holds its target nodes' M2L / S2L contributions;
+    // one sum over the shard group gives all ranks the whole downward densities
+    if (F.split && f->allreduce(psi, (long long)nn * N, (void *)s, f->allreduce_user) != 0) return STK_ERR_CUDA;
     FCUDA(cudaEventRecord(kd->ph[4], s));
     // L2L, top down: the level-l children block of the level-(l-1) parents
     for (int l = 1; l <= T.depth(); l++) {
@@ -1902,6 +2276,16 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     FCUDA(cudaEventRecord(kd->ph[7], s));
     F.launches = t_launches;
     return STK_OK;
+}
+
+int farfield_status(KernelData *kd) {
+    if (!kd->far || !kd->far->tc || !kd->far->tc_err.ptr) return STK_OK;
+    int e = 0;
+    if (cudaMemcpy(&e, kd->far->tc_err.ptr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return STK_ERR_CUDA;
+    if (e == 0) return STK_OK;
+    cudaMemset(kd->far->tc_err.ptr, 0, sizeof(int));
+    fprintf(stderr, "stkfmm_b200: a tensor-core M2L GEMM stopped at a pipeline wait (code %d)\n", e);
+    return STK_ERR_CUDA;
 }
 
 }  // namespace stk

@@ -134,6 +134,29 @@ struct FarField {
     DevBuf dn_rowq, dn_srow;                // per block row: its slot index q, its row in Z_c'
     size_t dn_row_off[64] = {};
     DevBuf dn_phi, dn_psi, dn_z, dn_zc;     // per-level work buffers (FP64 or FP32)
+    // mixed path on the tensor cores (stk_umma.cu): 3xTF32 hi / lo operands, K-major
+    bool tc = false;
+    DevBuf tc_qa_hi, tc_qa_lo;              // Qs_c'^T per source type: dn_rs[c'] rows of k4 floats
+    DevBuf tc_pa_hi, tc_pa_lo;              // Pv_c^T per target type: k rows of ceil4(dn_rv[c]) floats
+    size_t tc_qa_off[8] = {}, tc_pa_off[8] = {};
+    DevBuf tc_b_hi, tc_b_lo;                // per level: Phi operands (8 n8 rows of k4)
+    DevBuf tc_z;                            // per level: Z of every source type
+    DevBuf tc_zc_hi, tc_zc_lo;              // per stream: the concatenated Zc operand (n8 rows of tc_zc_ld)
+    int tc_streams = 0, tc_zc_ld = 0;
+    cudaStream_t tc_stream[8] = {};         // target types of the dense M2L run concurrently
+    cudaEvent_t tc_ev[8] = {}, tc_fork = nullptr;
+    DevBuf tc_err;                          // set by a tensor-core GEMM whose pipeline wait gave up
+    // Operators shared through the process-wide cache: the level-independent
+    // operators (and the periodic M2C) are built once per (device, translation
+    // kernel, p, M2L cut) and aliased by every handle that needs them; each
+    // holder keeps the cache entry alive.  `built` is recorded on the stream that
+    // built an entry; a handle reusing it makes its stream wait for it.
+    std::shared_ptr<FarField> ops_ref, m2c_ref;
+    // far field split over a shard group (Stk3DFMM_set_allreduce): this rank's M2L /
+    // S2L target nodes; dense levels by parity type (dn_own[c])
+    bool split = false;
+    bool dn_own[8] = {true, true, true, true, true, true, true, true};
+    cudaEvent_t built = nullptr;
     ~FarField();
 };
 
@@ -146,5 +169,9 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd);
 // near field uses them: d_sl, d_dl in the caller's order).
 int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *trg_sorted,
                       cudaStream_t s);
+
+// After the evaluation has completed (the caller synchronised): STK_ERR_CUDA, once,
+// when a tensor-core M2L GEMM gave up at a pipeline wait, else STK_OK.
+int farfield_status(KernelData *kd);
 
 }  // namespace stk

@@ -47,20 +47,22 @@ static bool verbose() {
     } while (0)
 
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    owner.reset();  // cudaFree when this was the last owner
     ptr = nullptr;
     bytes = 0;
 }
 
 int DevBuf::reserve(size_t n) {
     if (n == 0) n = 16;
-    if (n <= bytes) return STK_OK;
+    if (n <= bytes && !shared()) return STK_OK;
     release();
-    if (cudaMalloc(&ptr, n) != cudaSuccess) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, n) != cudaSuccess) {
         cudaGetLastError();
-        ptr = nullptr;
         return STK_ERR_CUDA;
     }
+    owner = std::shared_ptr<void>(p, [](void *q) { cudaFree(q); });
+    ptr = p;
     bytes = n;
     return STK_OK;
 }
@@ -85,6 +87,8 @@ KernelData::~KernelData() {
 Stk3DFMM::~Stk3DFMM() {
     pool.clear();
     if (stream) cudaStreamDestroy(stream);
+    if (aux_stream) cudaStreamDestroy(aux_stream);
+    if (ev_out) cudaEventDestroy(ev_out);
 }
 
 extern "C" Stk3DFMM *Stk3DFMM_create(int mult_order, int max_pts, int pbc, unsigned kernelComb) {
@@ -296,6 +300,18 @@ extern "C" int Stk3DFMM_set_shard(Stk3DFMM *fmm, int rank, int nranks) {
     return STK_OK;
 }
 
+extern "C" int Stk3DFMM_set_allreduce(Stk3DFMM *fmm, stk_allreduce_fn fn, void *user) {
+    if (!fmm) return STK_ERR_INVALID_ARG;
+    if (fmm->allreduce != fn)
+        for (auto &kv : fmm->pool) {
+            kv.second->tree_ready = false;  // the far-field split is rebuilt by the next setup_tree
+            kv.second->far_ready = false;
+        }
+    fmm->allreduce = fn;
+    fmm->allreduce_user = user;
+    return STK_OK;
+}
+
 extern "C" int Stk3DFMM_set_far_field(Stk3DFMM *fmm, int enable) {
     if (!fmm || (enable != 0 && enable != 1)) return STK_ERR_INVALID_ARG;
     if (fmm->enable_ff != (enable == 1))
@@ -318,7 +334,7 @@ extern "C" int Stk3DFMM_set_precision(Stk3DFMM *fmm, int precision) {
 // (scaleSrc); d_out_user receives trg += sF^k * result (scaleTrg) in the
 // caller's order.
 int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *d_out_user,
-                     cudaStream_t s, bool far) {
+                     cudaStream_t s, bool far, const std::function<int()> &before_scatter) {
     const KernelInfo *ki = kd->info;
     Octree &T = kd->tree;
     const int nn = T.num_nodes();
@@ -379,6 +395,7 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
     rc = kd->d_alpha.upload(alpha, sizeof(double) * td, s);
     if (rc) return rc;
     (void)nn;
+    if (before_scatter && (rc = before_scatter())) return rc;
     HCUDA(launch_scatter_add(ntrg, td, (const int *)kd->d_perm[2].ptr, out, (const double *)kd->d_alpha.ptr,
                              d_out_user, s));
     kd->launches = launches + (ntrg > 0 ? 1 : 0) + (far ? kd->far->launches : 0);
@@ -432,19 +449,32 @@ static int eval_host(Stk3DFMM *fmm, unsigned kernel, const int nSL, const double
     const size_t ntrg_v = (size_t)nTrg * ki->kdim_trg;
     rc = kd->d_val[0].upload(src_SL_value, nsl_v * sizeof(double), s);
     if (!rc && dl) rc = kd->d_val[1].upload(src_DL_value, ndl_v * sizeof(double), s);
-    if (!rc) rc = kd->d_out_user.upload(trg_value, ntrg_v * sizeof(double), s);
+    if (!rc) rc = kd->d_out_user.reserve(std::max<size_t>(ntrg_v, 1) * sizeof(double));
     if (rc) return rc;
+    if (!fmm->aux_stream && cudaStreamCreateWithFlags(&fmm->aux_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return STK_ERR_CUDA;
+    if (!fmm->ev_out && cudaEventCreateWithFlags(&fmm->ev_out, cudaEventDisableTiming) != cudaSuccess)
+        return STK_ERR_CUDA;
+    // the caller's target values go up on the side stream while the kernels run
+    auto upload_out = [&]() -> int {
+        if (ntrg_v)
+            HCUDA(cudaMemcpyAsync(kd->d_out_user.ptr, trg_value, ntrg_v * sizeof(double), cudaMemcpyHostToDevice,
+                                  fmm->aux_stream));
+        HCUDA(cudaEventRecord(fmm->ev_out, fmm->aux_stream));
+        HCUDA(cudaStreamWaitEvent(s, fmm->ev_out, 0));
+        return STK_OK;
+    };
     // scaleSrc (FMMData.cpp:285-317): DL values and a scaling last SL component times sF
     const double sf = fmm->scale_factor;
     if (dl) HCUDA(scale_strided((double *)kd->d_val[1].ptr, (long long)ndl_v, 1, 0, sf, s));
     for (int c = ki->kdim_sl - ki->sl_last_scales; c < ki->kdim_sl; c++)
         HCUDA(scale_strided((double *)kd->d_val[0].ptr, nSL, ki->kdim_sl, c, sf, s));
     rc = near_device(fmm, kd, (const double *)kd->d_val[0].ptr, dl ? (const double *)kd->d_val[1].ptr : nullptr,
-                     (double *)kd->d_out_user.ptr, s, far);
+                     (double *)kd->d_out_user.ptr, s, far, upload_out);
     if (rc) return rc;
     if (ntrg_v) HCUDA(cudaMemcpyAsync(trg_value, kd->d_out_user.ptr, ntrg_v * sizeof(double), cudaMemcpyDeviceToHost, s));
     HCUDA(cudaStreamSynchronize(s));
-    return STK_OK;
+    return far ? farfield_status(kd) : STK_OK;
 }
 
 extern "C" int Stk3DFMM_evaluate_near(Stk3DFMM *fmm, unsigned kernel, const int nSL, double *src_SL_value,
@@ -475,7 +505,7 @@ extern "C" int Stk3DFMM_last_kernel_ms(Stk3DFMM *fmm, unsigned kernel, float *ms
     if (!kd->timed) return STK_ERR_STATE;
     if (cudaEventSynchronize(kd->ev1) != cudaSuccess) return STK_ERR_CUDA;
     if (cudaEventElapsedTime(ms, kd->ev0, kd->ev1) != cudaSuccess) return STK_ERR_CUDA;
-    return STK_OK;
+    return kd->last_far ? farfield_status(kd) : STK_OK;
 }
 
 extern "C" int Stk3DFMM_last_phase_ms(Stk3DFMM *fmm, unsigned kernel, float *ms) {

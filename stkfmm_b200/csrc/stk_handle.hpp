@@ -1,5 +1,6 @@
 // stk_handle.hpp -- state behind the opaque Stk3DFMM handle.
 #pragma once
+#include <functional>
 #include <map>
 #include <memory>
 #include <vector>
@@ -15,6 +16,11 @@ namespace stk {
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    // owner of the allocation: share() makes another DevBuf an alias of the same
+    // memory (read-only use, e.g. far-field operators shared between handles); the
+    // memory is freed with its last owner.  reserve() never writes into memory that
+    // another DevBuf shares: it allocates afresh instead.
+    std::shared_ptr<void> owner;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
@@ -22,6 +28,12 @@ struct DevBuf {
     void release();
     int reserve(size_t n);
     int upload(const void *src, size_t n, cudaStream_t s);
+    void share(const DevBuf &o) {
+        owner = o.owner;
+        ptr = o.ptr;
+        bytes = o.bytes;
+    }
+    bool shared() const { return owner && owner.use_count() > 1; }
 };
 
 struct FarField;
@@ -60,10 +72,17 @@ struct Stk3DFMM {
     int precision = 0;
     int device = 0, sms = 1;
     int shard_rank = 0, shard_n = 1;  // target-side work of this handle: shard shard_rank of shard_n
+    // collective of the shard group: with it the far field's M2L / S2L are split too
+    int (*allreduce)(double *, long long, void *, void *) = nullptr;
+    void *allreduce_user = nullptr;
     // periodic far field (the reference's enableFF, STKFMM.hpp:199-200): off, the
     // periodic sum stops two cells away
     bool enable_ff = true;
     cudaStream_t stream = nullptr;
+    // host-array evaluations: the caller's target array is uploaded on aux_stream
+    // while the P2P kernels run (ev_out joins it before the final scatter)
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_out = nullptr;
     bool points_set = false, sl_dl_same = false;
     int nsl = 0, ndl = 0, ntrg = 0;
     std::vector<double> sl, dl, trg;  // scaled, wrapped coordinates (caller's order)
@@ -76,6 +95,9 @@ struct Stk3DFMM {
 };
 
 namespace stk {
+// before_scatter (optional) runs on the host right before the final scatter into
+// d_out_user is queued on s (after every P2P / far-field launch): host-array
+// callers upload the target array there, overlapping the kernels.
 int near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const double *d_dl, double *d_out_user,
-                cudaStream_t s, bool far);
+                cudaStream_t s, bool far, const std::function<int()> &before_scatter = nullptr);
 }

@@ -95,3 +95,12 @@ extern "C" int stk_partition_lpt(int n, const double *cost, int nparts, int *own
     if (n) std::memcpy(owner, o.data(), sizeof(int) * n);
     return STK_OK;
 }
+
+// Owners of the M2L / S2L target nodes when Stk3DFMM's far field is split over
+// nranks ranks (Stk3DFMM_set_allreduce): owner[node] in 0 .. nranks-1.  Host only.
+extern "C" int stk_octree_far_owners(const stk_octree *t, int nranks, int *owner) {
+    if (!t || nranks < 1 || !owner) return STK_ERR_INVALID_ARG;
+    const std::vector<int> o = stk::far_owners(t->tree, nranks);
+    if (!o.empty()) std::memcpy(owner, o.data(), sizeof(int) * o.size());
+    return STK_OK;
+}

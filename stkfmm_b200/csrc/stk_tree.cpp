@@ -315,4 +315,40 @@ void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owne
     }
 }
 
+// Owners of the M2L / S2L target nodes when the far field is split over nranks:
+// the nodes of complete levels (all 8^l boxes, l >= 1) by parity type
+// ((ix & 1) | (iy & 1) << 1 | (iz & 1) << 2) mod nranks -- the dense M2L splits
+// its work by target type -- and every other node, largest first by its V-list
+// and X-list size, to the least loaded rank (LPT).  Host only, deterministic.
+std::vector<int> far_owners(const Octree &T, int nranks) {
+    const int nn = T.num_nodes();
+    std::vector<int> owner(nn, 0);
+    if (nranks <= 1) return owner;
+    std::vector<double> load(nranks, 0.0);
+    std::vector<char> done(nn, 0);
+    auto cost = [&](int b) { return 1.0 + (T.V.off[b + 1] - T.V.off[b]) + (T.X.off[b + 1] - T.X.off[b]); };
+    for (int l = 1; l <= T.depth(); l++) {
+        const long long cnt = (long long)T.level_begin[l + 1] - T.level_begin[l];
+        if (cnt != (1LL << (3 * l))) continue;
+        for (int b = T.level_begin[l]; b < T.level_begin[l + 1]; b++) {
+            const int c = (int)((T.ix[b] & 1) | (T.iy[b] & 1) << 1 | (T.iz[b] & 1) << 2);
+            owner[b] = c % nranks;
+            load[owner[b]] += cost(b);
+            done[b] = 1;
+        }
+    }
+    std::vector<int> rest;
+    for (int b = 0; b < nn; b++)
+        if (!done[b]) rest.push_back(b);
+    std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    for (int b : rest) {
+        int best = 0;
+        for (int r = 1; r < nranks; r++)
+            if (load[r] < load[best]) best = r;
+        owner[b] = best;
+        load[best] += cost(b);
+    }
+    return owner;
+}
+
 }  // namespace stk

@@ -94,4 +94,8 @@ uint64_t morton_key(double x, double y, double z);
 // each go to the part with the smallest load so far; ties to the lowest part.
 void partition_lpt(int n, const double *cost, int nparts, std::vector<int> &owner);
 
+// Owners (0 .. nranks-1) of the M2L / S2L target nodes when the far field is split
+// over nranks ranks: complete levels by parity type, the other nodes by cost (LPT).
+std::vector<int> far_owners(const Octree &T, int nranks);
+
 }  // namespace stk

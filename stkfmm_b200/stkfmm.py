@@ -261,6 +261,28 @@ class Stk3DFMM:
         """Evaluate only shard `rank` of `nranks` of the target-side work (sum over shards = full result)."""
         check(lib().Stk3DFMM_set_shard(self.fmm, int(rank), int(nranks)), "set_shard")
 
+    def set_allreduce(self, fn):
+        """The shard group's collective (Stk3DFMM_set_allreduce): fn(ptr, n, stream) sums the n
+        float64 values at device address ptr over the ranks, ordered on the CUDA stream handle
+        `stream`, and returns 0.  With it a sharded handle splits the far field's M2L / S2L as
+        well.  None clears it."""
+        from ._lib import ALLREDUCE_FN
+        if fn is None:
+            self._allreduce = None
+            check(lib().Stk3DFMM_set_allreduce(self.fmm, None, None), "set_allreduce")
+            return
+
+        def _cb(ptr, n, stream, user):
+            try:
+                return int(fn(ptr, n, stream) or 0)
+            except Exception:  # an exception cannot cross the C ABI: report a failed collective
+                import traceback
+                traceback.print_exc()
+                return 1
+        self._allreduce = ALLREDUCE_FN(_cb)  # kept alive as long as the handle
+        check(lib().Stk3DFMM_set_allreduce(self.fmm, ctypes.cast(self._allreduce, ctypes.c_void_p), None),
+              "set_allreduce")
+
     def last_launch_count(self, kernel) -> int:
         n = ctypes.c_int()
         check(lib().Stk3DFMM_last_launch_count(self.fmm, int(kernel), ctypes.byref(n)), "last_launch_count")
@@ -423,6 +445,12 @@ class Octree:
         check(octree_lib().stk_octree_list(self.t, w, off.ctypes.data_as(P_i), ent.ctypes.data_as(P_i)))
         return off, ent[:self.list_sizes[which]]
 
+    def far_owners(self, nranks: int):
+        """Owner rank of each node's M2L / S2L in a far field split over nranks (stk_octree_far_owners)."""
+        o = np.zeros(self.num_nodes, np.int32)
+        check(octree_lib().stk_octree_far_owners(self.t, int(nranks), o.ctypes.data_as(P_i)))
+        return o
+
     def point_set(self, k: int):
         n = self.n[k]
         perm = np.zeros(max(n, 1), np.int32)
@@ -431,3 +459,28 @@ class Octree:
         check(octree_lib().stk_octree_set(self.t, k, perm.ctypes.data_as(P_i), b.ctypes.data_as(P_i),
                                    e.ctypes.data_as(P_i)))
         return perm[:n], b, e
+
+
+def device_view(ptr: int, n: int, dtype="float64"):
+    """A torch CUDA tensor aliasing n values at device address ptr (no copy)."""
+    import torch
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dtype).str, "data": (int(ptr), False),
+                                    "version": 2}
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+def torch_allreduce(group=None):
+    """A collective for Stk3DFMM.set_allreduce over a torch.distributed process group
+    (NCCL for one process per GPU): all_reduce (sum) of the library's device buffer on
+    the library's stream."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(ptr, n, stream):
+        t = device_view(ptr, n)
+        with torch.cuda.stream(torch.cuda.ExternalStream(int(stream) if stream else 0)):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return 0
+    return fn

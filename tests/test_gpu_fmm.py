@@ -153,3 +153,41 @@ def test_fmm_not_supported_cases(torch_cuda):
     lg.set_points(pts, pts, pts)
     with pytest.raises(S.StkError):
         lg.setup_tree(64)  # not activated in this handle
+
+
+@pytest.mark.parametrize("pbc", [0, 3])
+def test_operators_shared_between_handles(torch_cuda, pbc):
+    """A second handle of the same (translation kernel, p) reuses the first handle's
+    far-field operators (and periodic M2C): its first evaluation does no operator
+    build, and both handles give the same answer as a handle that built its own."""
+    import time
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(77 + pbc)
+    n = 6000
+    pts = rng.random((n, 3))
+    q = rng.uniform(-0.5, 0.5, (n, 1))
+    q -= q.mean()  # a neutral cell for the periodic sum
+
+    def first_eval(fmm):
+        out = np.zeros((n, 4))
+        t0 = time.perf_counter()
+        fmm.evaluate_fmm(1, q, out, None)
+        return time.perf_counter() - t0, out
+
+    def handle():
+        f = S.Stk3DFMM(10, 128, pbc, 1)
+        f.set_box(np.zeros(3), 1.0)
+        f.set_points(pts, pts, None)
+        f.setup_tree(1)
+        return f
+
+    a = handle()
+    ta, oa = first_eval(a)
+    b = handle()  # a is alive: b aliases its operators
+    tb, ob = first_eval(b)
+    assert tb < 0.5 * ta, (ta, tb)
+    assert rel_l2(ob, oa) < 1e-13
+    del a, b
+    c = handle()  # no holder left: c builds its own
+    tc, oc = first_eval(c)
+    assert rel_l2(oc, oa) < 1e-13
