@@ -480,6 +480,42 @@ EWALD_PVEL = 2
 EWALD_LAPLACE_HESS = 3
 
 
+def ewald_cells(kind: int, src, sval, trg, xi: float = 16.0, nwave: int = 28, out=None, nthreads: int = 0):
+    """The triply periodic sums of ewald() (kinds EWALD_LAPLACE, EWALD_STOKES, EWALD_LAPLACE_HESS) for
+    millions of sources: real space through a cell list (cutoff 5.3 / xi, below 1/3), wave space
+    through structure factors over the sphere |m| <= nwave (stk_oracle.c:oracle_ewald_cells).  The
+    defaults converge to ~1e-13 for points in [0, 1)^3."""
+    sd, td = {EWALD_LAPLACE: (1, 4), EWALD_STOKES: (3, 3), 3: (1, 10)}[kind]
+    src, ps = _d(np.asarray(src).reshape(-1, 3))
+    sval, pv = _d(np.asarray(sval).reshape(len(src), sd))
+    trg, pt = _d(np.asarray(trg).reshape(-1, 3))
+    if out is None:
+        out = np.zeros((len(trg), td))
+    L = lib()
+    L.oracle_ewald_cells.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                     ctypes.c_int, _dp, _dp, ctypes.c_int]
+    rc = L.oracle_ewald_cells(kind, xi, nwave, len(src), ps, pv, len(trg), pt, out.ctypes.data_as(_dp), nthreads)
+    assert rc == 0, rc
+    return out
+
+
+def ewald_stokes_laplacian_cells(src, f, trg, **kw):
+    """ewald_stokes_laplacian through ewald_cells (for millions of sources)."""
+    src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(f, dtype=np.float64).reshape(len(src), 3)
+    trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+    sym = [[4, 5, 6], [5, 7, 8], [6, 8, 9]]
+    out = np.zeros((len(trg), 3))
+    for j in range(3):
+        h = ewald_cells(EWALD_LAPLACE_HESS, src, f[:, j:j + 1], trg, **kw)
+        for i in range(3):
+            out[:, i] -= h[:, sym[i][j]]
+    out += f.sum(0)
+    return out
+
+
+
+
 def ewald_stokes_laplacian(src, f, trg):
     """Laplacian of the triply periodic Stokeslet velocity (the unit cell's
     Hasimoto sum of stokes_vel, 1/8pi (delta/r + r r^T/r^3), k = 0 mode dropped;

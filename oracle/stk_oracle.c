@@ -884,6 +884,241 @@ int oracle_ewald(int kind, double xi, int nreal, int nwave, int nsrc, const doub
     return 0;
 }
 
+/* The sums of oracle_ewald kinds 0 / 3 (Laplace) and 1 (Stokes) for many
+ * sources, same conventions and formulas, arranged for millions of sources:
+ *   real space: pairs closer than rc = 5.3 / xi (erfc(5.3) < 1e-13), found with a
+ *     cell list of the unit cell (cells of side >= rc, the 27 around the
+ *     target's cell, periodic wrap, minimum image), so rc must stay below 1/3;
+ *   wave space: k = 2 pi m with |m| <= nwave (a sphere), half of it (the terms
+ *     are even in k: each counted twice), structure factors summed source by
+ *     source with per-axis phase recurrences (e^{i 2 pi m x} from m = 1).
+ * Test infrastructure: pinned against oracle_ewald in tests/test_oracle.py. */
+typedef struct {
+    int mx, my, mz;
+} KVec;
+
+int oracle_ewald_cells(int kind, double xi, int nwave, int nsrc, const double *src, const double *val, int ntrg,
+                       const double *trg, double *out, int nthreads) {
+    if (!(kind == 0 || kind == 1 || kind == 3) || nsrc < 0 || ntrg < 0 || nwave < 1 || !(xi > 0)) return 1;
+    const double rc = 5.3 / xi;
+    int nc = (int)floor(1.0 / rc);
+    if (nc < 3) return 3; /* rc >= 1/3: use oracle_ewald */
+    const int hess = kind == 3;
+    const int lap = kind != 1;
+    const int sd = lap ? 1 : 3, td = hess ? 10 : lap ? 4 : 3;
+    const double sqpi = sqrt(PI_), xi2 = xi * xi;
+    nthreads = clamp_threads(nthreads);
+    /* ---- wave vectors: half of the sphere |m| <= nwave ---- */
+    const int M = nwave;
+    int nk = 0;
+    KVec *kv = (KVec *)malloc(sizeof(KVec) * (size_t)(2 * M + 1) * (2 * M + 1) * (2 * M + 1));
+    if (!kv) return 2;
+    for (int mx = 0; mx <= M; mx++)
+        for (int my = -M; my <= M; my++)
+            for (int mz = -M; mz <= M; mz++) {
+                if (mx * mx + my * my + mz * mz > M * M) continue;
+                if (mx == 0 && (my < 0 || (my == 0 && mz <= 0))) continue; /* the other half and k = 0 */
+                kv[nk].mx = mx;
+                kv[nk].my = my;
+                kv[nk].mz = mz;
+                nk++;
+            }
+    /* ---- structure factors S(k) = sum_j v_j e^{-i k.x_j}: per-thread partial sums ---- */
+    double *S = (double *)calloc((size_t)nthreads * nk * sd * 2, sizeof(double));
+    if (!S) {
+        free(kv);
+        return 2;
+    }
+#pragma omp parallel num_threads(nthreads)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        double *Sp = S + (size_t)tid * nk * sd * 2;
+        double *E = (double *)malloc(sizeof(double) * 3 * (2 * M + 1) * 2);
+#pragma omp for schedule(static)
+        for (int j = 0; j < nsrc; j++) {
+            /* E[a][m + M] = e^{-i 2 pi m x_a}, m = -M .. M */
+            for (int a = 0; a < 3; a++) {
+                const double ph = 2 * PI_ * src[3 * (size_t)j + a];
+                const double c1 = cos(ph), s1 = -sin(ph);
+                double *e = E + (size_t)a * (2 * M + 1) * 2;
+                e[2 * M] = 1.0;
+                e[2 * M + 1] = 0.0;
+                double c = 1.0, sn = 0.0;
+                for (int m = 1; m <= M; m++) {
+                    const double cn = c * c1 - sn * s1, snn = c * s1 + sn * c1;
+                    c = cn;
+                    sn = snn;
+                    e[2 * (M + m)] = c;
+                    e[2 * (M + m) + 1] = sn;
+                    e[2 * (M - m)] = c;
+                    e[2 * (M - m) + 1] = -sn;
+                }
+            }
+            const double *v = val + (size_t)sd * j;
+            const double *ex = E, *ey = E + (size_t)(2 * M + 1) * 2, *ez = E + (size_t)2 * (2 * M + 1) * 2;
+            for (int q = 0; q < nk; q++) {
+                const double *a = ex + 2 * (kv[q].mx + M), *b = ey + 2 * (kv[q].my + M), *cc = ez + 2 * (kv[q].mz + M);
+                const double abr = a[0] * b[0] - a[1] * b[1], abi = a[0] * b[1] + a[1] * b[0];
+                const double pr = abr * cc[0] - abi * cc[1], pi = abr * cc[1] + abi * cc[0];
+                double *o = Sp + (size_t)q * sd * 2;
+                for (int t = 0; t < sd; t++) {
+                    o[2 * t] += v[t] * pr;
+                    o[2 * t + 1] += v[t] * pi;
+                }
+            }
+        }
+        free(E);
+    }
+    for (int th = 1; th < nthreads; th++)
+        for (size_t i = 0; i < (size_t)nk * sd * 2; i++) S[i] += S[(size_t)th * nk * sd * 2 + i];
+    double qsum = 0;
+    if (lap)
+        for (int j = 0; j < nsrc; j++) qsum += val[j];
+    /* ---- cell list of the sources ---- */
+    const double h = 1.0 / nc;
+    const int ncell = nc * nc * nc;
+    int *cstart = (int *)calloc((size_t)ncell + 1, sizeof(int)), *order = (int *)malloc(sizeof(int) * (size_t)(nsrc > 0 ? nsrc : 1));
+    int *cof = (int *)malloc(sizeof(int) * (size_t)(nsrc > 0 ? nsrc : 1));
+    if (!cstart || !order || !cof) {
+        free(kv);
+        free(S);
+        free(cstart);
+        free(order);
+        free(cof);
+        return 2;
+    }
+    for (int j = 0; j < nsrc; j++) {
+        int ci[3];
+        for (int a = 0; a < 3; a++) {
+            double x = src[3 * (size_t)j + a];
+            x -= floor(x);
+            ci[a] = (int)(x / h);
+            if (ci[a] >= nc) ci[a] = nc - 1;
+        }
+        cof[j] = ci[0] + nc * (ci[1] + nc * ci[2]);
+        cstart[cof[j] + 1]++;
+    }
+    for (int c = 0; c < ncell; c++) cstart[c + 1] += cstart[c];
+    {
+        int *fill = (int *)malloc(sizeof(int) * (size_t)ncell);
+        for (int c = 0; c < ncell; c++) fill[c] = cstart[c];
+        for (int j = 0; j < nsrc; j++) order[fill[cof[j]]++] = j;
+        free(fill);
+    }
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int t = 0; t < ntrg; t++) {
+        const double *x = trg + 3 * (size_t)t;
+        double acc[4] = {0, 0, 0, 0}, H[6] = {0, 0, 0, 0, 0, 0};
+        int ci[3];
+        for (int a = 0; a < 3; a++) {
+            double xx = x[a] - floor(x[a]);
+            ci[a] = (int)(xx / h);
+            if (ci[a] >= nc) ci[a] = nc - 1;
+        }
+        /* real space over the 27 cells around the target's */
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int cx = (ci[0] + dx + nc) % nc, cy = (ci[1] + dy + nc) % nc, cz = (ci[2] + dz + nc) % nc;
+                    const int c = cx + nc * (cy + nc * cz);
+                    for (int e = cstart[c]; e < cstart[c + 1]; e++) {
+                        const int j = order[e];
+                        double r[3];
+                        for (int a = 0; a < 3; a++) {
+                            r[a] = x[a] - src[3 * (size_t)j + a];
+                            r[a] -= floor(r[a] + 0.5);
+                        }
+                        const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                        const double *v = val + (size_t)sd * j;
+                        if (rr < 1e-13) {
+                            if (lap) {
+                                acc[0] += -2 * xi / sqpi * v[0];
+                                if (hess) {
+                                    const double h0 = 4 * xi * xi2 / (3 * sqpi) * v[0];
+                                    H[0] += h0;
+                                    H[3] += h0;
+                                    H[5] += h0;
+                                }
+                            } else
+                                for (int a = 0; a < 3; a++) acc[a] += -4 * xi / sqpi * v[a];
+                            continue;
+                        }
+                        if (rr > rc) continue;
+                        const double ex = exp(-xi2 * rr * rr), ec = erfc(xi * rr);
+                        const double fp = -(2. * ex * xi) / (sqpi * rr) - ec / (rr * rr);
+                        if (lap) {
+                            acc[0] += v[0] * ec / rr;
+                            for (int a = 0; a < 3; a++) acc[1 + a] += v[0] * fp / rr * r[a];
+                            if (hess) {
+                                const double fpp = 2 * xi / sqpi * ex * (2 * xi2 + 2 / (rr * rr)) + 2 * ec / (rr * rr * rr);
+                                const double hs = v[0] * (fpp - fp / rr) / (rr * rr), hd = v[0] * fp / rr;
+                                int q = 0;
+                                for (int a = 0; a < 3; a++)
+                                    for (int b = a; b < 3; b++) H[q++] += hs * r[a] * r[b] + (a == b ? hd : 0.0);
+                            }
+                        } else {
+                            const double c1 = 2 * (xi * ex / (sqpi * rr * rr) + ec / (2 * rr * rr * rr));
+                            const double c2 = 4 * xi / sqpi * ex;
+                            const double rf = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
+                            for (int a = 0; a < 3; a++) acc[a] += c1 * (rr * rr * v[a] + r[a] * rf) - c2 * v[a];
+                        }
+                    }
+                }
+        /* wave space: the half sphere, each term twice */
+        double ph[3][2];
+        for (int a = 0; a < 3; a++) {
+            ph[a][0] = cos(2 * PI_ * x[a]);
+            ph[a][1] = sin(2 * PI_ * x[a]);
+        }
+        for (int q = 0; q < nk; q++) {
+            const double k[3] = {2 * PI_ * kv[q].mx, 2 * PI_ * kv[q].my, 2 * PI_ * kv[q].mz};
+            const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+            const double pk = k[0] * x[0] + k[1] * x[1] + k[2] * x[2];
+            const double cp = cos(pk), sp = sin(pk);
+            const double g = exp(-k2 / (4 * xi2));
+            const double *Sq = S + (size_t)q * sd * 2;
+            /* S stores sum v e^{-i k.x_j} = Sc - i Ss with oracle_ewald's Sc, Ss */
+            if (lap) {
+                const double Sc = Sq[0], Ss = -Sq[1];
+                const double w = 2 * 4 * PI_ * g / k2;
+                const double C = cp * Sc + sp * Ss, Sn = sp * Sc - cp * Ss;
+                acc[0] += w * C;
+                for (int a = 0; a < 3; a++) acc[1 + a] -= w * k[a] * Sn;
+                if (hess) {
+                    int qq = 0;
+                    for (int a = 0; a < 3; a++)
+                        for (int b = a; b < 3; b++) H[qq++] -= w * k[a] * k[b] * C;
+                }
+            } else {
+                const double w = 2 * 8 * PI_ * (1 + k2 / (4 * xi2)) * g / (k2 * k2);
+                double C[3];
+                for (int a = 0; a < 3; a++) C[a] = cp * Sq[2 * a] - sp * Sq[2 * a + 1];
+                const double kC = k[0] * C[0] + k[1] * C[1] + k[2] * C[2];
+                for (int a = 0; a < 3; a++) acc[a] += w * (k2 * C[a] - k[a] * kC);
+            }
+        }
+        (void)ph;
+        if (lap) {
+            acc[0] -= PI_ / xi2 * qsum;
+            for (int a = 0; a < 4; a++) out[(size_t)td * t + a] += acc[a] / (4 * PI_);
+            if (hess)
+                for (int a = 0; a < 6; a++) out[(size_t)td * t + 4 + a] += H[a] / (4 * PI_);
+        } else {
+            for (int a = 0; a < 3; a++) out[(size_t)td * t + a] += acc[a] / (8 * PI_);
+        }
+    }
+    free(kv);
+    free(S);
+    free(cstart);
+    free(order);
+    free(cof);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------
  * Doubly periodic sums (period 1 in x and y, z free), per pair, restating the
  * reference's generator: Laplace potential M2L/Laplace/Laplace2D3D.cpp:12-83,

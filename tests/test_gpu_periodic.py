@@ -106,6 +106,39 @@ def test_periodic_rpy_laplacian(torch_cuda):
     assert max(errs) < 1e-4, errs
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rpy_pxyz_2m_against_ewald(torch_cuda, precision):
+    """The full-size RPY PXYZ workload (2,097,152 uniform points, p = 8, 256 points per
+    leaf) against its Ewald-summed fixture at 4,096 sampled targets (u and lap u,
+    tests/golden/make_rpy_pxyz_ewald.py).  Bars: the per-component relative L2 errors
+    measured on B200 (FP64 and mixed), with headroom of about 2x."""
+    import os
+    import sys
+    import stkfmm_b200 as S
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_rpy_pxyz_ewald as G
+    z = np.load(os.path.join(here, "rpy_pxyz_2m_ewald.npz"))
+    pts, f, b = G.workload()
+    assert (z["idx"] == G.sample()).all()
+    slv = np.concatenate([f, b], axis=1)
+    fmm = S.Stk3DFMM(8, 256, S.PAXIS.PXYZ, 16)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, None)
+    fmm.setup_tree(16)
+    fmm.set_precision(S.PRECISION.FP64 if precision == "fp64" else S.PRECISION.MIXED)
+    out = np.zeros((len(pts), 6))
+    fmm.evaluate_fmm(16, slv, out, None)
+    errs = component_errors(out[z["idx"]], z["truth"])
+    print(precision, errs)
+    assert max(errs[:3]) < RPY2M_TOL[precision][0], errs
+    assert max(errs[3:]) < RPY2M_TOL[precision][1], errs
+
+
+# (u, lap u) bars of test_rpy_pxyz_2m_against_ewald
+RPY2M_TOL = {"fp64": (1e-3, 1e-3), "mixed": (1e-3, 1e-3)}
+
+
 def test_periodic_mixed_close_to_fp64(torch_cuda):
     import stkfmm_b200 as S
     pts, rng = points("clustered", 5000, 6)

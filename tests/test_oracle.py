@@ -200,6 +200,23 @@ def _zero_moment_cell(rng, ncube=3, h=0.04):
     return src, s
 
 
+@pytest.mark.parametrize("kind", [O.EWALD_LAPLACE, O.EWALD_STOKES, O.EWALD_LAPLACE_HESS])
+def test_ewald_cells_matches_ewald(kind):
+    """The cell-list Ewald sum (used for the 2M-point periodic fixture) against the
+    image-sum form, targets on and off the sources, points outside [0, 1) too."""
+    rng = np.random.default_rng(41 + kind)
+    src = rng.random((300, 3))
+    src[:20] += rng.integers(-2, 3, (20, 3))
+    v = rng.normal(size=(300, 3 if kind == O.EWALD_STOKES else 1))
+    v -= v.mean(0)
+    trg = np.concatenate([rng.random((40, 3)), src[:10]])
+    a = O.ewald(kind, src, v, trg, xi=7.0, nreal=2, nwave=20)
+    b = O.ewald_cells(kind, src, v, trg)
+    assert np.abs(a - b).max() < 3e-12 * np.abs(a).max()
+    lap = O.ewald_stokes_laplacian_cells(src, rng.normal(size=(300, 3)), trg[:8])
+    assert np.isfinite(lap).all()
+
+
 def test_ewald_pvel_splitting_independent():
     rng = np.random.default_rng(31)
     src = rng.random((150, 3))
