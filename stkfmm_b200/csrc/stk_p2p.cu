@@ -48,6 +48,7 @@ constexpr int kWarpsPerCta = 4;
 constexpr int kThreads = 32 * kWarpsPerCta;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kPadCoord = 1.0e4;  // offset of zero-strength padding sources
+constexpr int kShiftNoneCode = 13;   // list-entry shift code of the unshifted source box
 
 // Number of staged per-output-point values of a micro-kernel (1 as a dummy
 // array size when it has none).
@@ -126,7 +127,28 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// wait until at most N of this thread's most recent groups are still in flight
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Tiles in flight per warp (STK_P2P_DEPTH builds deeper pipelines where the landing
+// zones fit the 48 KB of static shared memory per block).  One tile ahead is the
+// default: two measured 0.5% slower on the clustered 1M-point LapPGrad U list
+// (3.100 against 3.084 ms mixed, 4.446 against 4.409 ms FP64), so the L2 round
+// trip is hidden behind one tile's consumption even for items of 8 targets.
+#ifndef STK_P2P_DEPTH
+#define STK_P2P_DEPTH 1
+#endif
+template <int RS> struct StageDepth {
+    static constexpr int value = RS <= 10 ? STK_P2P_DEPTH : 1;
+};
+
+// FP32 hi part of a double by truncation: the top 24 significant bits (the low
+// 29 mantissa bits cleared), so (float)hi is exact and d - hi is exact in FP64.
+__device__ __forceinline__ double trunc_to_f32_bits(double d) {
+    return __hiloint2double(__double2hiint(d), __double2loint(d) & (int)0xE0000000u);
+}
 
 // Shared-memory stride (doubles) of a raw record: an odd number of 16-byte units,
 // so the 8 lanes of a quarter-warp reading their own records with 16-byte loads
@@ -154,7 +176,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 
     __shared__ __align__(16) CT tcoord[kWarpsPerCta][NCC][32];
     __shared__ __align__(16) S tval[kWarpsPerCta][NV][32];
-    __shared__ __align__(16) double traw[kWarpsPerCta][32][RSS];  // cp.async landing zone, one record per lane
+    constexpr int DEPTH = StageDepth<RS>::value;
+    // cp.async landing zones, one record per lane and tile in flight
+    __shared__ __align__(16) double traw[kWarpsPerCta][DEPTH][32][RSS];
     // the item's list entries (up to 32 at a time) as segments of one source stream
     __shared__ int sg_end[kWarpsPerCta][32];   // stream position one past the segment
     __shared__ int sg_src[kWarpsPerCta][32];   // first record of the segment minus its stream start
@@ -163,7 +187,6 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
     const int lane = threadIdx.x & 31;
     CT(*mc)[32] = tcoord[wid];
     S(*mv)[32] = tval[wid];
-    double *myraw = traw[wid][lane];
     int *s_end = sg_end[wid];
     int *s_src = sg_src[wid];
     int *s_code = sg_code[wid];
@@ -277,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
         // positions cross segment boundaries, so only a chunk's last tile is padded ----
         for (int ec = w.e0; ec < w.e1; ec += 32) {
             const int ne = min(32, w.e1 - ec);
-            int sz = 0, sbeg = 0, code = 13;  // 13: no periodic shift
+            int sz = 0, sbeg = 0, code = kShiftNoneCode;
             if (lane < ne) {
                 const int ent = a.list_ent[ec + lane];
                 const int sb = ent >> 5;
@@ -301,39 +324,53 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 
             // per-lane cursor into the segment table; positions only grow
             int seg = 0;
-            auto fetch = [&](int p) {  // cp.async the record at stream position p (< total) into this lane's slot
-                while (p >= s_end[seg]) seg++;
-                const double *src = a.src_rec + (size_t)(s_src[seg] + p) * RS;
+            // segment of the record in each landing zone, oldest first (registers:
+            // every index below is a compile-time constant)
+            int zseg[DEPTH];
+            // cp.async the record at stream position p into this lane's slot of zone z,
+            // or nothing past the stream's end; one commit group per call either way,
+            // so every lane counts the same groups
+            auto fetch = [&](int p, int z, int &zs) {
+                if (p < total) {
+                    while (p >= s_end[seg]) seg++;
+                    const double *src = a.src_rec + (size_t)(s_src[seg] + p) * RS;
+                    double *dst = traw[wid][z][lane];
 #pragma unroll
-                for (int q = 0; q < RS / 2; q++) cp_async16(myraw + 2 * q, src + 2 * q);
+                    for (int q = 0; q < RS / 2; q++) cp_async16(dst + 2 * q, src + 2 * q);
+                    zs = seg;
+                }
                 cp_async_commit();
             };
-            int p0 = 0;
-            if (lane < total) fetch(lane);
+#pragma unroll
+            for (int z = 0; z < DEPTH; z++) fetch(32 * z + lane, z, zseg[z]);
+            int p0 = 0, zone = 0;
             while (p0 < total) {
                 const int n = min(32, total - p0);
                 // ---- stage: lane i turns stream position p0 + i (its landed record)
                 // into tile column i, or writes zero-strength padding ----
-                cp_async_wait_all();
+                cp_async_wait_group<DEPTH - 1>();  // this tile's group; later ones may still fly
                 __syncwarp();  // every lane has finished reading the previous tile
                 {
                     double v[NV];
                     double x[3];
                     if (lane < n) {
-                        const int cd = s_code[seg];
-                        const double shx = (cd % 3 - 1) * a.period;
-                        const double shy = ((cd / 3) % 3 - 1) * a.period;
-                        const double shz = (cd / 9 - 1) * a.period;
+                        const double *raw = traw[wid][zone][lane];
                         double rn[RS];
 #pragma unroll
                         for (int q = 0; q < RS / 2; q++) {
-                            const double2 t2 = *reinterpret_cast<const double2 *>(myraw + 2 * q);
+                            const double2 t2 = *reinterpret_cast<const double2 *>(raw + 2 * q);
                             rn[2 * q] = t2.x;
                             rn[2 * q + 1] = t2.y;
                         }
-                        x[0] = rn[0] + shx;
-                        x[1] = rn[1] + shy;
-                        x[2] = rn[2] + shz;
+                        x[0] = rn[0];
+                        x[1] = rn[1];
+                        x[2] = rn[2];
+                        const int cd = s_code[zseg[0]];
+                        if (cd != kShiftNoneCode) {  // periodic image
+                            x[0] += (cd % 3 - 1) * a.period;
+                            x[1] += ((cd / 3) % 3 - 1) * a.period;
+                            x[2] += (cd / 9 - 1) * a.period;
+                        }
                         K::stage(rn + 3, v);
                     } else {
 #pragma unroll
@@ -345,9 +382,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 #pragma unroll
                         for (int k = 0; k < 3; k++) {
                             const double d = x[k] - c[k];
-                            const float hv = (float)d;
-                            mc[k][lane] = hv;
-                            mc[3 + k][lane] = (float)(d - (double)hv);
+                            const double hd = trunc_to_f32_bits(d);
+                            mc[k][lane] = (float)hd;
+                            mc[3 + k][lane] = (float)(d - hd);
                         }
                     } else {
 #pragma unroll
@@ -356,9 +393,12 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 #pragma unroll
                     for (int q = 0; q < NV; q++) mv[q][lane] = (S)v[q];
                 }
-                // ---- prefetch the next tile into the (now free) landing zone ----
+                // ---- prefetch the tile DEPTH ahead into the zone just staged ----
+#pragma unroll
+                for (int z = 0; z + 1 < DEPTH; z++) zseg[z] = zseg[z + 1];
+                fetch(p0 + 32 * DEPTH + lane, zone, zseg[DEPTH - 1]);
                 p0 += 32;
-                if (p0 + lane < total) fetch(p0 + lane);
+                zone = DEPTH > 1 ? (zone + 1 == DEPTH ? 0 : zone + 1) : 0;
                 __syncwarp();
 
                 // ---- consume the tile ----

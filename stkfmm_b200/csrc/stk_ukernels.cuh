@@ -91,7 +91,9 @@ __device__ __forceinline__ double rsq(double r2) {
     const double e = fma(-(r2 * y), y, 1.0);
     const double t = e * fma(e, 0.375, 0.5);
     y = fma(y, t, y);
-    return r2 >= 2.2250738585072014e-308 ? y : 0.0;
+    // r2 >= smallest normal double, read off the high word (an integer compare
+    // instead of an FP64 one; r2 is a sum of squares, so never negative)
+    return __double2hiint(r2) >= 0x00100000 ? y : 0.0;
 }
 #elif STK_RSQ64_NEWTON
 // Hardware approximation refined by Newton-Raphson steps y <- y + y e / 2 with
