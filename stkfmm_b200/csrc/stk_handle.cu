@@ -379,6 +379,8 @@ int stk::near_device(Stk3DFMM *f, KernelData *kd, const double *d_sl, const doub
         a.box_centre = (const double *)kd->d_centre.ptr;
         a.period = 1.0;
         a.atomic_out = 0;
+        // one octree holds the sources and the targets: coincident points share a leaf
+        a.coincident_own_box = 1;
         HCUDA(launch_list_p2p(uk, f->precision, a, f->sms, s));
         launches += 2;  // record packing + list kernel
     }

@@ -49,6 +49,7 @@ constexpr int kThreads = 32 * kWarpsPerCta;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kPadCoord = 1.0e4;  // offset of zero-strength padding sources
 constexpr int kShiftNoneCode = 13;   // list-entry shift code of the unshifted source box
+constexpr int kMayCoincide = 32;     // segment-table flag above the 5-bit shift code
 
 // Number of staged per-output-point values of a micro-kernel (1 as a dummy
 // array size when it has none).
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                 }
             }
         }
-        auto eval = [&](auto &u, V dx, V dy, V dz, const V *sv, const V *tav) {
+        auto eval = [&](auto &u, auto dx, auto dy, auto dz, const auto *sv, const auto *tav) {
             if constexpr (TV > 0)
                 K::eval(u, dx, dy, dz, sv, tav);
             else
@@ -307,6 +308,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                 code = ent & 31;
                 sbeg = a.src_box_begin[sb];
                 sz = a.src_box_end[sb] - sbeg;
+                // bit 5: the segment may hold a source at a target's position (always,
+                // unless the lists guarantee coincidence only in the unshifted own box)
+                if (!a.coincident_own_box || sb == w.trg_box || code != kShiftNoneCode) code |= kMayCoincide;
             }
             int incl = sz;
 #pragma unroll
@@ -350,6 +354,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                 // into tile column i, or writes zero-strength padding ----
                 cp_async_wait_group<DEPTH - 1>();  // this tile's group; later ones may still fly
                 __syncwarp();  // every lane has finished reading the previous tile
+                int may_coincide = 0;
                 {
                     double v[NV];
                     double x[3];
@@ -365,7 +370,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
                         x[0] = rn[0];
                         x[1] = rn[1];
                         x[2] = rn[2];
-                        const int cd = s_code[zseg[0]];
+                        const int cdf = s_code[zseg[0]];
+                        may_coincide = cdf & kMayCoincide;
+                        const int cd = cdf & 31;
                         if (cd != kShiftNoneCode) {  // periodic image
                             x[0] += (cd % 3 - 1) * a.period;
                             x[1] += ((cd / 3) % 3 - 1) * a.period;
@@ -403,35 +410,57 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2
 
                 // ---- consume the tile ----
                 if constexpr (MIXED) {
-                    // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding
+                    // sources j, j+1 in one packed pair; entries [n, n+1] are zero-strength padding.
+                    // P: F2 (rsqrt masks coincident pairs) or F2U (no source of the tile can sit
+                    // at a target's position)
+                    auto consume = [&](auto proto) {
+                        using P = decltype(proto);
 STK_UNROLL(STK_P2P_UNROLL_MIXED)
-                    for (int j = 2 * sub; j < n; j += 2 * g) {
-                        F2 sv[NV];
+                        for (int j = 2 * sub; j < n; j += 2 * g) {
+                            P sv[NV];
 #pragma unroll
-                        for (int q = 0; q < NV; q++) sv[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
-                        if constexpr (HILO) {
-                            F2 sh[3], sl[3];
+                            for (int q = 0; q < NV; q++) sv[q].v = *reinterpret_cast<const float2 *>(&mv[q][j]);
+                            P dxyz[TPL][3];
+                            if constexpr (HILO) {
+                                F2 sh[3], sl[3];
 #pragma unroll
-                            for (int k = 0; k < 3; k++) {
-                                sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
-                                sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
+                                for (int k = 0; k < 3; k++) {
+                                    sh[k].v = *reinterpret_cast<const float2 *>(&mc[k][j]);
+                                    sl[k].v = *reinterpret_cast<const float2 *>(&mc[3 + k][j]);
+                                }
+#pragma unroll
+                                for (int h = 0; h < TPL; h++)
+#pragma unroll
+                                    for (int k = 0; k < 3; k++)
+                                        dxyz[h][k].v = ((th[h][k] - sh[k]) + (tl[h][k] - sl[k])).v;
+                            } else {
+                                double2 sx[3];
+#pragma unroll
+                                for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
+#pragma unroll
+                                for (int h = 0; h < TPL; h++)
+#pragma unroll
+                                    for (int k = 0; k < 3; k++)
+                                        dxyz[h][k].v = make_float2((float)(tr[h][k] - sx[k].x),
+                                                                   (float)(tr[h][k] - sx[k].y));
                             }
 #pragma unroll
-                            for (int h = 0; h < TPL; h++)
-                                eval(pp[h], (th[h][0] - sh[0]) + (tl[h][0] - sl[0]),
-                                     (th[h][1] - sh[1]) + (tl[h][1] - sl[1]), (th[h][2] - sh[2]) + (tl[h][2] - sl[2]),
-                                     sv, ta[h]);
-                        } else {
-                            double2 sx[3];
+                            for (int h = 0; h < TPL; h++) {
+                                P u[TDIM], tv[NTV];
 #pragma unroll
-                            for (int k = 0; k < 3; k++) sx[k] = *reinterpret_cast<const double2 *>(&mc[k][j]);
+                                for (int k = 0; k < TDIM; k++) u[k].v = pp[h][k].v;
 #pragma unroll
-                            for (int h = 0; h < TPL; h++)
-                                eval(pp[h], mk((float)(tr[h][0] - sx[0].x), (float)(tr[h][0] - sx[0].y)),
-                                     mk((float)(tr[h][1] - sx[1].x), (float)(tr[h][1] - sx[1].y)),
-                                     mk((float)(tr[h][2] - sx[2].x), (float)(tr[h][2] - sx[2].y)), sv, ta[h]);
+                                for (int q = 0; q < NTV; q++) tv[q].v = ta[h][q].v;
+                                eval(u, dxyz[h][0], dxyz[h][1], dxyz[h][2], sv, tv);
+#pragma unroll
+                                for (int k = 0; k < TDIM; k++) pp[h][k].v = u[k].v;
+                            }
                         }
-                    }
+                    };
+                    if (__any_sync(kFull, may_coincide))
+                        consume(F2{});
+                    else
+                        consume(F2U{});
                     // Kahan-compensated accumulation of the partial sums once a lane has
                     // evaluated ~32 sources since the last step (every g tiles)
                     if (++kahan_tiles >= kKahanTiles * g) kahan_step();

@@ -35,6 +35,10 @@ struct ListP2PArgs {
     double period;             // periodic image length (1 for the unit box)
     int atomic_out;            // 1 when several items may write the same target
     const double *trg_aux;     // per-target values (TV doubles each) of the adjoint kernels, else null
+    int coincident_own_box;    // 1: a source can sit at a target's position only in an unshifted
+                               // entry of the target's own box (lists of one octree over both
+                               // point sets); the mixed path then skips the coincidence mask
+                               // elsewhere.  0: every pair is masked.
 };
 
 // Record stride (doubles) for a micro-kernel: 3 coordinates + SDIM values,

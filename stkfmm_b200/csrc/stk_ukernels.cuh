@@ -52,23 +52,33 @@
 namespace stk {
 
 // ---------------------------------------------------------------------------
-// packed FP32 pair (two sources in one register pair)
+// packed FP32 pair (two sources in one register pair).  MASK: whether rsq()
+// zeroes coincident pairs; the list kernel evaluates tiles that cannot hold a
+// source at a target's position with the unmasked type (F2U), which saves two
+// compare-and-select steps per packed rsqrt.
 // ---------------------------------------------------------------------------
-struct F2 {
+template <bool MASK> struct F2T {
     float2 v;
 };
+using F2 = F2T<true>;
+using F2U = F2T<false>;
 __device__ __forceinline__ F2 splat(float a) { return {make_float2(a, a)}; }
 __device__ __forceinline__ F2 mk(float a, float b) { return {make_float2(a, b)}; }
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return {__fadd2_rn(a.v, b.v)}; }
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return {__fmul2_rn(a.v, b.v)}; }
+template <bool M> __device__ __forceinline__ F2T<M> operator+(F2T<M> a, F2T<M> b) { return {__fadd2_rn(a.v, b.v)}; }
+template <bool M> __device__ __forceinline__ F2T<M> operator*(F2T<M> a, F2T<M> b) { return {__fmul2_rn(a.v, b.v)}; }
 // a - b as one exactly rounded fma(b, -1, a)
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return {__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
-__device__ __forceinline__ F2 fmav(F2 a, F2 b, F2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+template <bool M> __device__ __forceinline__ F2T<M> operator-(F2T<M> a, F2T<M> b) {
+    return {__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)};
+}
+template <bool M> __device__ __forceinline__ F2T<M> fmav(F2T<M> a, F2T<M> b, F2T<M> c) {
+    return {__ffma2_rn(a.v, b.v, c.v)};
+}
 __device__ __forceinline__ double fmav(double a, double b, double c) { return fma(a, b, c); }
 
 template <class V> __device__ __forceinline__ V cst(double c);
 template <> __device__ __forceinline__ double cst<double>(double c) { return c; }
 template <> __device__ __forceinline__ F2 cst<F2>(double c) { return splat((float)c); }
+template <> __device__ __forceinline__ F2U cst<F2U>(double c) { return {make_float2((float)c, (float)c)}; }
 
 // masked reciprocal square root: 0 where r2 == 0 (the reference's
 // approx_rsqrt<digits>(r2, r2 > 0))
@@ -113,18 +123,21 @@ __device__ __forceinline__ double rsq(double r2) { return r2 > 0.0 ? rsqrt(r2) :
 #endif
 
 // Mixed path: hardware approximate rsqrt (MUFU, one per lane half) plus one
-// Newton-Raphson step y <- y (3 - r2 y^2) / 2 in packed FP32.  Pairs closer
-// than the smallest normal FP32 r^2 (|r| < 1.1e-19) count as coincident.
-__device__ __forceinline__ F2 rsq(F2 r2) {
+// Newton-Raphson step y <- y (3 - r2 y^2) / 2 in packed FP32.  Masked (F2):
+// pairs closer than the smallest normal FP32 r^2 (|r| < 1.1e-19) count as
+// coincident.  Unmasked (F2U): only for pairs known to be apart.
+template <bool M> __device__ __forceinline__ F2T<M> rsq(F2T<M> r2) {
     float y0, y1;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(r2.v.x));
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(r2.v.y));
-    F2 y = mk(y0, y1);
-    F2 h = r2 * splat(-0.5f);
-    F2 t = fmav(h, y * y, splat(1.5f));
+    F2T<M> y{make_float2(y0, y1)};
+    const F2T<M> h = r2 * F2T<M>{make_float2(-0.5f, -0.5f)};
+    const F2T<M> t = fmav(h, y * y, F2T<M>{make_float2(1.5f, 1.5f)});
     y = y * t;
-    y.v.x = r2.v.x >= 1.17549435e-38f ? y.v.x : 0.0f;
-    y.v.y = r2.v.y >= 1.17549435e-38f ? y.v.y : 0.0f;
+    if constexpr (M) {
+        y.v.x = r2.v.x >= 1.17549435e-38f ? y.v.x : 0.0f;
+        y.v.y = r2.v.y >= 1.17549435e-38f ? y.v.y : 0.0f;
+    }
     return y;
 }
 

@@ -184,6 +184,40 @@ def test_handle_evaluate_near(torch_cuda, kernel, prec):
     assert st["u_pairs_sl"] > 0 and st["u_entries"] == len(u["list_ent"])
 
 
+@pytest.mark.parametrize("pbc", [0, 3])
+@pytest.mark.parametrize("kernel", [1, 2, 128])
+def test_handle_mixed_coincident_on_leaf_faces(torch_cuda, kernel, pbc):
+    """The handle's mixed near field masks the coincidence only on tiles that can hold a
+    source at a target's position (the target's own leaf, periodic images): targets that
+    duplicate sources exactly, many of them on leaf faces and cell faces (coordinates on
+    a 1/64 grid, 0 included), stay finite and within the mixed bar of the oracle."""
+    import stkfmm_b200 as S
+    rng = np.random.default_rng(7)
+    grid = rng.integers(0, 64, size=(1500, 3)) / 64.0     # on the faces of leaves down to level 6
+    free = clustered_points(rng, 2500, nclusters=4, sigma=0.03)
+    pts = np.concatenate([grid, free, grid[:300]])         # exact duplicates inside the source set too
+    sd, dd, td = S.get_kernel_dimension(kernel)
+    slv = uk_values(rng, S.kernel_slot(kernel, 0), len(pts))
+    has_dl = S.kernel_slot(kernel, 1) >= 0
+    dlv = rng.normal(size=(len(pts), dd)) if has_dl else None
+    fmm = S.Stk3DFMM(8, 40, pbc, kernel, precision=1)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts if has_dl else None)
+    fmm.setup_tree(kernel)
+    out = np.zeros((len(pts), td))
+    fmm.evaluate_near(kernel, slv, out, dlv)
+    assert np.all(np.isfinite(out))
+    u = fmm.ulist(kernel)
+    lst = (u["trg_begin"], u["trg_end"], u["list_off"], u["list_ent"])
+    ref = np.zeros_like(out)
+    ref[u["trg_perm"]] = oracle_ulist(S.kernel_slot(kernel, 0), *lst, u["sl_begin"], u["sl_end"], pts[u["sl_perm"]],
+                                      slv[u["sl_perm"]], pts[u["trg_perm"]])
+    if has_dl:
+        ref[u["trg_perm"]] += oracle_ulist(S.kernel_slot(kernel, 1), *lst, u["dl_begin"], u["dl_end"],
+                                           pts[u["dl_perm"]], dlv[u["dl_perm"]], pts[u["trg_perm"]])
+    assert rel_l2(out, ref) < 1e-6, component_errors(out, ref)
+
+
 @pytest.mark.parametrize("kernel", [1, 2, 128])
 def test_handle_separate_dl_points(torch_cuda, kernel):
     """SL and DL at different points: separate (unfused) passes."""
