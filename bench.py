@@ -535,7 +535,7 @@ def m2l_roofline(fmm, K, res):
             out[nm + "_tflops_algorithmic"] = w["flops_algorithmic"] / (ms * 1e-3) / 1e12
             out[nm + "_tflops_executed"] = w["flops_executed"] / (ms * 1e-3) / 1e12
     out["note"] = ("M2L phase: basis products, column gather, per-offset GEMMs, per-target reduce; "
-                   "FP64 GEMMs on the FP64 tensor pipe (DMMA), mixed GEMMs SIMT FP32")
+                   "FP64 GEMMs on the FP64 tensor pipe (DMMA), mixed GEMMs on the tcgen05 tensor cores (3xTF32), basis products FP64")
     return out
 
 

@@ -535,15 +535,18 @@ __global__ void tc_trows_kernel(const double *__restrict__ src, int k, int R, in
     }
 }
 
-// phi_hat columns cols[j] (k values each, FP64) as K-major rows of ld floats, split
-__global__ void tc_gather_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, int n, int k,
-                                      int ld, float *__restrict__ hi, float *__restrict__ lo) {
-    const long long total = (long long)n * ld;
+// phi_hat columns cols[j] (k values each, FP64) as K-major rows of ld floats, split;
+// cols[j] < 0 (chunk padding) gives a zero row
+__global__ void tc_gather_cols_kernel(const double *__restrict__ src, const int *__restrict__ cols, long long n,
+                                      int k, int ld, float *__restrict__ hi, float *__restrict__ lo) {
+    const long long total = n * ld;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(idx / ld), r = (int)(idx - (long long)j * ld);
+        const long long j = idx / ld;
+        const int r = (int)(idx - j * ld);
+        const int c = cols[j];
         float h = 0.f, l = 0.f;
-        if (r < k) tf32_hilo(src[(size_t)cols[j] * k + r], h, l);
+        if (r < k && c >= 0) tf32_hilo(src[(size_t)c * k + r], h, l);
         hi[idx] = h;
         lo[idx] = l;
     }
@@ -1219,6 +1222,76 @@ int record_built(FarField &e, cudaStream_t s) {
 
 }  // namespace
 
+// Tensor-core operands and tile tables of the mixed path's chunked M2L (the levels the
+// dense M2L does not take).  Per group of column chunks two grouped GEMM launches:
+//   stage 1  Z_c = Q_d^T X_c (r_d x 256 per chunk c of offset d), written split into
+//            TF32 hi / lo parts as the next stage's K-major operand (rows of rmax);
+//   stage 2  Y_c = P_d Z_c (k x 256), FP32, reduced per target as on the SIMT path.
+// Every tile is 128 x 128 (rows of the factor x columns of the chunk) over the whole K.
+// The operands (~8 (sum_d r_d k + nslot k rmax) bytes) must fit in 4 GiB, else the
+// SIMT path stays; STKFMM_M2L_TC=0 turns both tensor-core paths off.
+static int setup_m2l_chunks_tc(FarField &F, const std::vector<int> &chunk_slot, int nslot, cudaStream_t s) {
+    F.tcc = false;
+    const char *env_tc = getenv("STKFMM_M2L_TC");
+    if ((env_tc && env_tc[0] == '0') || !umma_available() || F.m2l_chunks == 0) return STK_OK;
+    const int k = F.m2l_rank, k4 = (k + 3) / 4 * 4, rmax = F.m2l_rmax;
+    if (rmax % 4) return STK_OK;  // ranks are padded to multiples of 32
+    long long qrows = 0;
+    for (int sl = 0; sl < nslot; sl++) qrows += F.m2l_r[sl];
+    const size_t bytes = 8 * ((size_t)qrows * k4 + (size_t)nslot * k * rmax);
+    if (bytes > (4ull << 30)) return STK_OK;
+    int rc = F.tcc_q_hi.reserve(sizeof(float) * (size_t)qrows * k4);
+    if (!rc) rc = F.tcc_q_lo.reserve(sizeof(float) * (size_t)qrows * k4);
+    if (!rc) rc = F.tcc_pt_hi.reserve(sizeof(float) * (size_t)nslot * k * rmax);
+    if (!rc) rc = F.tcc_pt_lo.reserve(sizeof(float) * (size_t)nslot * k * rmax);
+    if (!rc && !F.tc_err.ptr) rc = F.tc_err.reserve(sizeof(int) * 4);
+    if (rc) return rc;
+    // Q_d (k x r_d column-major, offsets back to back) read as qrows K-major rows of k
+    tc_rows_kernel<<<grid_for(qrows * k4), 256, 0, s>>>((const double *)F.m2l_q.ptr, k, qrows, k4,
+                                                        (float *)F.tcc_q_hi.ptr, (float *)F.tcc_q_lo.ptr);
+    FCUDA(cudaGetLastError());
+    for (int sl = 0; sl < nslot; sl++) {
+        tc_trows_kernel<<<grid_for((long long)k * rmax), 256, 0, s>>>(
+            (const double *)F.m2l_p.ptr + F.m2l_pq_off[sl], k, F.m2l_r[sl], rmax,
+            (float *)F.tcc_pt_hi.ptr + (size_t)sl * k * rmax, (float *)F.tcc_pt_lo.ptr + (size_t)sl * k * rmax);
+        FCUDA(cudaGetLastError());
+    }
+    FCUDA(cudaMemsetAsync(F.tc_err.ptr, 0, sizeof(int) * 4, s));
+    // tile tables, group by group
+    const int nc = F.m2l_chunks, gc = F.m2l_group_chunks, ngroups = (nc + gc - 1) / gc;
+    std::vector<GroupTile> t1, t2;
+    F.tcc_t1_off.assign(ngroups + 1, 0);
+    F.tcc_t2_off.assign(ngroups + 1, 0);
+    for (int g = 0; g < ngroups; g++) {
+        F.tcc_t1_off[g] = (int)t1.size();
+        F.tcc_t2_off[g] = (int)t2.size();
+        for (int c = g * gc; c < std::min(nc, (g + 1) * gc); c++) {
+            const int sl = chunk_slot[c], r = F.m2l_r[sl];
+            const long long col = (long long)(c - g * gc) * kM2LChunk;  // first column within the group
+            const int qrow0 = (int)(F.m2l_pq_off[sl] / (size_t)k);
+            for (int nt = 0; nt < kM2LChunk / 128; nt++) {
+                const long long cn = col + 128LL * nt;
+                for (int m0 = 0; m0 < r; m0 += 128) {
+                    const int mv = std::min(128, r - m0);
+                    t1.push_back(GroupTile{qrow0 + m0, (int)cn, k, mv, mv, 128, rmax, 0, cn * rmax + m0});
+                }
+                for (int m0 = 0; m0 < k; m0 += 128) {
+                    const int mv = std::min(128, k - m0);
+                    t2.push_back(GroupTile{sl * k + m0, (int)cn, r, mv, mv, 128, k, 0, cn * k + m0});
+                }
+            }
+        }
+    }
+    F.tcc_t1_off[ngroups] = (int)t1.size();
+    F.tcc_t2_off[ngroups] = (int)t2.size();
+    rc = F.tcc_tiles1.upload(t1.data(), sizeof(GroupTile) * t1.size(), s);
+    if (!rc) rc = F.tcc_tiles2.upload(t2.data(), sizeof(GroupTile) * t2.size(), s);
+    if (rc) return rc;
+    F.tcc_q_rows = qrows;
+    F.tcc = true;
+    return STK_OK;
+}
+
 // Dense M2L of the complete levels (M2LDenseLevel).  A level l >= 4 qualifies
 // when all 8^l boxes are present and its V lists hold at least 70% of 189 pairs
 // per box (periodic and deep uniform levels); the stacked factors and the work
@@ -1848,7 +1921,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         rc = F.d_m2l_gstart.upload(gstart.data(), sizeof(int) * gstart.size(), s);
         if (rc) return rc;
         const int rmax = F.m2l_rmax;
-        rc = F.m2l_x.reserve(sizeof(double) * (size_t)k * gcols);
+        // k4 (not k) per column: the tensor-core path keeps split FP32 rows of k4 floats here
+        rc = F.m2l_x.reserve(sizeof(double) * (size_t)((k + 3) / 4 * 4) * gcols);
         if (!rc) rc = F.m2l_y.reserve(sizeof(double) * (size_t)k * gcols);
         if (!rc) rc = F.m2l_z.reserve(sizeof(double) * (size_t)rmax * gcols);
         if (rc) return rc;
@@ -1894,6 +1968,8 @@ int farfield_setup(Stk3DFMM *f, KernelData *kd) {
         if (!rc) rc = F.d_m2l_ptr32[2].upload(c1f.data(), sizeof(void *) * nc, s);
         if (!rc) rc = F.d_m2l_ptr32[3].upload(a2f.data(), sizeof(void *) * nc, s);
         if (!rc) rc = F.d_m2l_ptr32[4].upload(c2f.data(), sizeof(void *) * nc, s);
+        if (rc) return rc;
+        rc = setup_m2l_chunks_tc(F, chunk_slot, nslot, s);
         if (rc) return rc;
         F.m2l_flops = 0;
         for (int c = 0; c < nc; c++) F.m2l_flops += 4.0 * k * F.m2l_r[chunk_slot[c]] * kM2LChunk;
@@ -2136,6 +2212,30 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
         const cudaDataType_t dt = mixed ? CUDA_R_32F : CUDA_R_64F;
         const cublasComputeType_t ct = mixed ? CUBLAS_COMPUTE_32F : CUBLAS_COMPUTE_64F;
         DevBuf *P = mixed ? F.d_m2l_ptr32 : F.d_m2l_ptr;
+        if (mixed && F.tcc) {
+            // tensor cores: split gather, Z = Q_d^T X (split), Y = P_d Z, in two grouped launches
+            const int g = c0 / gc, k4 = (k + 3) / 4 * 4;
+            float *xh = (float *)F.m2l_x.ptr, *xl = xh + (size_t)ncol * k4;
+            float *zh = (float *)F.m2l_z.ptr, *zl = zh + (size_t)ncol * rmax;
+            int *err = (int *)F.tc_err.ptr;
+            t_launches += 3;
+            tc_gather_cols_kernel<<<grid_for(ncol * k4), 256, 0, s>>>(phi_hat, gsrc, ncol, k, k4, xh, xl);
+            FCUDA(cudaGetLastError());
+            FCUDA(umma_grouped_3xtf32(Tf32Rows{(const float *)F.tcc_q_hi.ptr, (const float *)F.tcc_q_lo.ptr,
+                                               (int)F.tcc_q_rows, k, k4},
+                                      Tf32Rows{xh, xl, (int)ncol, k, k4},
+                                      (const GroupTile *)F.tcc_tiles1.ptr + F.tcc_t1_off[g],
+                                      F.tcc_t1_off[g + 1] - F.tcc_t1_off[g], zh, zl, err, s));
+            FCUDA(umma_grouped_3xtf32(Tf32Rows{(const float *)F.tcc_pt_hi.ptr, (const float *)F.tcc_pt_lo.ptr,
+                                               (int)F.m2l_r.size() * k, rmax, rmax},
+                                      Tf32Rows{zh, zl, (int)ncol, rmax, rmax},
+                                      (const GroupTile *)F.tcc_tiles2.ptr + F.tcc_t2_off[g],
+                                      F.tcc_t2_off[g + 1] - F.tcc_t2_off[g], (float *)F.m2l_y.ptr, nullptr, err, s));
+            m2l_reduce_kernel<float><<<grid_for((long long)nn * k), 256, 0, s>>>(
+                (const float *)F.m2l_y.ptr, gbeg, gend, (const int *)F.d_m2l_red_col.ptr, nn, k, col0, psi_hat);
+            FCUDA(cudaGetLastError());
+            continue;
+        }
         if (mixed)
             m2l_gather_kernel<float><<<gg, 256, 0, s>>>(phi_hat, gsrc, k, ncol, (float *)F.m2l_x.ptr);
         else
@@ -2279,7 +2379,7 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
 }
 
 int farfield_status(KernelData *kd) {
-    if (!kd->far || !kd->far->tc || !kd->far->tc_err.ptr) return STK_OK;
+    if (!kd->far || !(kd->far->tc || kd->far->tcc) || !kd->far->tc_err.ptr) return STK_OK;
     int e = 0;
     if (cudaMemcpy(&e, kd->far->tc_err.ptr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return STK_ERR_CUDA;
     if (e == 0) return STK_OK;

@@ -119,6 +119,15 @@ struct FarField {
     DevBuf m2l_x, m2l_y, m2l_z;             // one group of columns: k x, k x, rmax x columns (FP64 or FP32)
     DevBuf d_m2l_ptr[5], d_m2l_ptr32[5];    // per chunk: Q_d, X, Z, P_d, Y (FP64 / FP32 views)
     std::vector<M2LSeg> m2l_seg;            // per group of columns and padded rank: chunks in the pointer arrays
+    // the mixed path's chunked M2L on the tensor cores (grouped 3xTF32 GEMMs, stk_umma.cu):
+    // Q_d^T of every offset as K-major rows (sum_d r_d rows of k4 floats), P_d^T per offset
+    // (k rows of rmax floats each, offset after offset), and per group of columns the tiles
+    // of both stages (Z = Q_d^T X into split Z, Y = P_d Z)
+    bool tcc = false;
+    DevBuf tcc_q_hi, tcc_q_lo, tcc_pt_hi, tcc_pt_lo;
+    long long tcc_q_rows = 0;
+    DevBuf tcc_tiles1, tcc_tiles2;
+    std::vector<int> tcc_t1_off, tcc_t2_off;  // per group: its tiles in the arrays above
     double m2l_flops = 0;                   // flops of one M2L (both stages, padded ranks and chunks)
     double m2l_flops_alg = 0;               // the same at the true ranks over the real pairs, plus the
                                             // two basis products (V^T phi, (DC2DE U) psi_hat)

@@ -11,7 +11,7 @@
 // then drained into FP32 registers with ordinary (round-to-nearest) adds, so the
 // tensor core only ever sums 12 products (4 K-steps x 3 splits) per output.
 //
-// Pipeline of one CTA (one 128 x 128 output tile, the whole K range):
+// Pipeline of one CTA (persistent: 128 x 128 output tiles in turn, each over its whole K range):
 //   warp 0  TMA producer: per K-block the four 128 x 32 FP32 tiles Ah, Al, Bh, Bl
 //           (128-byte swizzle, K-major) into a 3-stage shared-memory ring;
 //   warp 1  TMEM owner and MMA issuer: 12 tcgen05.mma (M = 128, N = 128, K = 8,
@@ -28,6 +28,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -131,18 +132,80 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// One output tile: output rows [0, 128) are rows a_row .. a_row + 127 of A, output
+// columns [0, 128) rows b_row .. b_row + 127 of B (tensor-map coordinates), summed
+// over k < K (K-blocks of 32; the maps zero-fill beyond their inner extent).
+struct TileSpec {
+    int a_row, b_row, K;
+};
+
+// One GEMM C = A B^T over (gx = ceil(M/128)) x ceil(N/128) tiles.
+struct DenseJob {
+    int M, N, K, ldc, beta, gx, ntiles;
+    float *C;
+    __device__ TileSpec tile(int i) const { return {(i % gx) * kBM, (i / gx) * kBN, K}; }
+    __device__ void store(int, const TileSpec &t, int row, const float (&acc)[kBN]) const {
+        const int m = t.a_row + row;
+        if (m >= M) return;
+#pragma unroll
+        for (int j = 0; j < kBN; j++) {
+            const int n = t.b_row + j;
+            if (n < N) {
+                float *p = C + (size_t)n * ldc + m;
+                *p = beta ? *p + acc[j] : acc[j];
+            }
+        }
+    }
+};
+
+// Many small GEMMs in one launch: tile i is described by tiles[i].
+struct GroupJob {
+    const GroupTile *tiles;
+    int ntiles;
+    float *C, *C_lo;
+    __device__ TileSpec tile(int i) const {
+        const GroupTile &g = tiles[i];
+        return {g.a_row, g.b_row, g.K};
+    }
+    __device__ void store(int i, const TileSpec &, int row, const float (&acc)[kBN]) const {
+        const GroupTile &g = tiles[i];
+        if (row >= g.m_store) return;
+        const bool valid = row < g.m_valid;
+        const int nv = g.n_valid;
+        float *c = C + g.c_off + row;
+        float *cl = C_lo ? C_lo + g.c_off + row : nullptr;
+#pragma unroll
+        for (int j = 0; j < kBN; j++) {
+            if (j < nv) {
+                const float v = valid ? acc[j] : 0.0f;
+                if (cl) {
+                    float h, l;
+                    tf32_split_value(v, h, l);
+                    c[(size_t)j * g.ldc] = h;
+                    cl[(size_t)j * g.ldc] = l;
+                } else {
+                    c[(size_t)j * g.ldc] = v;
+                }
+            }
+        }
+    }
+};
+
+// Persistent: CTA b computes tiles b, b + gridDim.x, ...  The three roles walk the
+// same sequence of K-blocks over all of the CTA's tiles; stage, accumulator buffer
+// and barrier parities follow the running K-block count g, so the loads and MMAs
+// of a tile start while the drain warps still finish the previous one.
+template <class Job>
 __global__ void __launch_bounds__(kThreads, 1)
-    umma_gemm_3xtf32_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-                            const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, int M,
-                            int N, int K, float *__restrict__ C, int ldc, int beta, int *err) {
+    umma_3xtf32_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, const Job job,
+                       int *err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = saddr(smem_raw);
     const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
     uint8_t *tiles = smem_raw + pad;  // kStages x {Ah, Al, Bh, Bl}, 1024-byte aligned
     Bars *bars = reinterpret_cast<Bars *>(tiles + kStages * kStageBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
-    const int nkb = (K + kBK - 1) / kBK;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) {
@@ -170,102 +233,103 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         // ---- TMA producer ----
         if (lane == 0) {
-            int issued = 0;
-            for (int kb = 0; kb < nkb && ok; kb++) {
-                const int s = kb % kStages;
-                const uint32_t ph = (uint32_t)(kb / kStages) & 1u;
-                if (!mbar_wait(saddr(&bars->empty[s]), ph ^ 1u)) {
-                    ok = false;
-                    break;
+            long long g = 0;  // K-blocks issued so far
+            for (int t = blockIdx.x; t < job.ntiles && ok; t += gridDim.x) {
+                const TileSpec ts = job.tile(t);
+                const int nkb = (ts.K + kBK - 1) / kBK;
+                for (int kb = 0; kb < nkb; kb++, g++) {
+                    const int s = (int)(g % kStages);
+                    const uint32_t ph = (uint32_t)(g / kStages) & 1u;
+                    if (!mbar_wait(saddr(&bars->empty[s]), ph ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = saddr(&bars->full[s]);
+                    mbar_expect_tx(fb, kStageBytes);
+                    const uint32_t st = saddr(tiles + s * kStageBytes);
+                    tma_load_2d(st, &mAh, fb, kb * kBK, ts.a_row);
+                    tma_load_2d(st + kTileBytes, &mAl, fb, kb * kBK, ts.a_row);
+                    tma_load_2d(st + 2 * kTileBytes, &mBh, fb, kb * kBK, ts.b_row);
+                    tma_load_2d(st + 3 * kTileBytes, &mBl, fb, kb * kBK, ts.b_row);
                 }
-                const uint32_t fb = saddr(&bars->full[s]);
-                mbar_expect_tx(fb, kStageBytes);
-                const uint32_t st = saddr(tiles + s * kStageBytes);
-                tma_load_2d(st, &mAh, fb, kb * kBK, m0);
-                tma_load_2d(st + kTileBytes, &mAl, fb, kb * kBK, m0);
-                tma_load_2d(st + 2 * kTileBytes, &mBh, fb, kb * kBK, n0);
-                tma_load_2d(st + 3 * kTileBytes, &mBl, fb, kb * kBK, n0);
-                issued = kb + 1;
             }
             if (!ok) {
                 atomicExch(err, 1);
                 // let the loads already issued land before the CTA exits
-                if (issued > 0) mbar_wait(saddr(&bars->full[(issued - 1) % kStages]), (uint32_t)((issued - 1) / kStages) & 1u);
+                if (g > 0) mbar_wait(saddr(&bars->full[(g - 1) % kStages]), (uint32_t)((g - 1) / kStages) & 1u);
             }
         }
     } else if (warp == 1) {
         // ---- MMA issuer ----
         if (lane == 0) {
-            int committed = 0;
-            for (int kb = 0; kb < nkb && ok; kb++) {
-                const int s = kb % kStages, b = kb & 1;
-                if (!mbar_wait(saddr(&bars->acce[b]), ((uint32_t)(kb >> 1) & 1u) ^ 1u) ||
-                    !mbar_wait(saddr(&bars->full[s]), (uint32_t)(kb / kStages) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t st = saddr(tiles + s * kStageBytes);
-                const uint32_t d = tmem + (uint32_t)(b * kBN);
+            long long g = 0;  // K-blocks committed so far
+            for (int t = blockIdx.x; t < job.ntiles && ok; t += gridDim.x) {
+                const int nkb = (job.tile(t).K + kBK - 1) / kBK;
+                for (int kb = 0; kb < nkb; kb++) {
+                    const int s = (int)(g % kStages), b = (int)(g & 1);
+                    if (!mbar_wait(saddr(&bars->acce[b]), ((uint32_t)(g >> 1) & 1u) ^ 1u) ||
+                        !mbar_wait(saddr(&bars->full[s]), (uint32_t)(g / kStages) & 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = saddr(tiles + s * kStageBytes);
+                    const uint32_t d = tmem + (uint32_t)(b * kBN);
 #pragma unroll
-                for (int ks = 0; ks < kBK / 8; ks++) {
-                    const uint32_t off = (uint32_t)ks * 32u;  // 8 TF32 = 32 bytes along K
-                    const uint64_t ah = smem_desc(st + off), al = smem_desc(st + kTileBytes + off);
-                    const uint64_t bh = smem_desc(st + 2 * kTileBytes + off), bl = smem_desc(st + 3 * kTileBytes + off);
-                    // small terms first; the block's first product overwrites the buffer
-                    mma_tf32(d, al, bh, ks > 0 ? 1u : 0u);
-                    mma_tf32(d, ah, bl, 1u);
-                    mma_tf32(d, ah, bh, 1u);
+                    for (int ks = 0; ks < kBK / 8; ks++) {
+                        const uint32_t off = (uint32_t)ks * 32u;  // 8 TF32 = 32 bytes along K
+                        const uint64_t ah = smem_desc(st + off), al = smem_desc(st + kTileBytes + off);
+                        const uint64_t bh = smem_desc(st + 2 * kTileBytes + off),
+                                       bl = smem_desc(st + 3 * kTileBytes + off);
+                        // small terms first; the block's first product overwrites the buffer
+                        mma_tf32(d, al, bh, ks > 0 ? 1u : 0u);
+                        mma_tf32(d, ah, bl, 1u);
+                        mma_tf32(d, ah, bh, 1u);
+                    }
+                    mma_commit(saddr(&bars->empty[s]));  // the stage is free once these MMAs are done
+                    mma_commit(saddr(&bars->accf[b]));   // the accumulator is ready
+                    g++;
                 }
-                mma_commit(saddr(&bars->empty[s]));  // the stage is free once these MMAs are done
-                mma_commit(saddr(&bars->accf[b]));   // the accumulator is ready
-                committed = kb + 1;
             }
             if (!ok) atomicExch(err, 2);
             // the MMAs issued last must be complete before the TMEM is freed
-            if (committed > 0)
-                mbar_wait(saddr(&bars->accf[(committed - 1) & 1]), (uint32_t)((committed - 1) >> 1) & 1u);
+            if (g > 0) mbar_wait(saddr(&bars->accf[(g - 1) & 1]), (uint32_t)((g - 1) >> 1) & 1u);
         }
         __syncwarp();
     } else {
         // ---- drain + epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 ----
         const int q = warp & 3;
         const int row = q * 32 + lane;
-        float acc[kBN];
+        long long g = 0;  // K-blocks drained so far
+        for (int t = blockIdx.x; t < job.ntiles && ok; t += gridDim.x) {
+            const TileSpec ts = job.tile(t);
+            const int nkb = (ts.K + kBK - 1) / kBK;
+            float acc[kBN];
 #pragma unroll
-        for (int j = 0; j < kBN; j++) acc[j] = 0.0f;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int b = kb & 1;
-            // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
-            if (!__all_sync(0xffffffffu, mbar_wait(saddr(&bars->accf[b]), (uint32_t)(kb >> 1) & 1u))) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-#pragma unroll
-            for (int c = 0; c < kBN / 32; c++) {
-                uint32_t r[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN + c * 32), r);
-#pragma unroll
-                for (int j = 0; j < 32; j++) acc[c * 32 + j] += __uint_as_float(r[j]);
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(saddr(&bars->acce[b]));
-        }
-        if (!ok) {
-            if (lane == 0) atomicExch(err, 3);
-        } else {
-            const int m = m0 + row;
-            if (m < M) {
-#pragma unroll
-                for (int j = 0; j < kBN; j++) {
-                    const int n = n0 + j;
-                    if (n < N) {
-                        float *p = C + (size_t)n * ldc + m;
-                        *p = beta ? *p + acc[j] : acc[j];
-                    }
+            for (int j = 0; j < kBN; j++) acc[j] = 0.0f;
+            for (int kb = 0; kb < nkb; kb++, g++) {
+                const int b = (int)(g & 1);
+                // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
+                if (!__all_sync(0xffffffffu, mbar_wait(saddr(&bars->accf[b]), (uint32_t)(g >> 1) & 1u))) {
+                    ok = false;
+                    break;
                 }
+                tc_fence_after();
+#pragma unroll
+                for (int c = 0; c < kBN / 32; c++) {
+                    uint32_t r[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN + c * 32), r);
+#pragma unroll
+                    for (int j = 0; j < 32; j++) acc[c * 32 + j] += __uint_as_float(r[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(saddr(&bars->acce[b]));
+            }
+            if (!ok) {
+                if (lane == 0) atomicExch(err, 3);
+            } else {
+                job.store(t, ts, row, acc);
             }
         }
     }
@@ -318,6 +382,27 @@ bool encode(CUtensorMap *m, const float *base, int rows, int K, int ld) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// SMs of the current device (one persistent CTA each; the pipeline's shared memory
+// keeps one CTA per SM)
+int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+// opt-in to the pipeline's dynamic shared memory, once per kernel instance
+template <class Job> cudaError_t smem_attr() {
+    static std::once_flag once;
+    static cudaError_t e = cudaSuccess;
+    std::call_once(once, [] {
+        e = cudaFuncSetAttribute(umma_3xtf32_kernel<Job>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    });
+    return e;
+}
+
 }  // namespace
 
 bool umma_available() {
@@ -340,16 +425,33 @@ cudaError_t umma_gemm_3xtf32(int M, int N, int K, Tf32Split A, Tf32Split B, floa
     if (!encode(&mah, A.hi, M, K, A.ld) || !encode(&mal, A.lo, M, K, A.ld) || !encode(&mbh, B.hi, N, K, B.ld) ||
         !encode(&mbl, B.lo, N, K, B.ld))
         return cudaErrorInvalidValue;
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(umma_gemm_3xtf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kSmemBytes);
-    });
-    if (attr_err != cudaSuccess) return attr_err;
-    const dim3 grid((M + kBM - 1) / kBM, (N + kBN - 1) / kBN);
-    if (grid.y > 65535) return cudaErrorInvalidValue;
-    umma_gemm_3xtf32_kernel<<<grid, kThreads, kSmemBytes, s>>>(mah, mal, mbh, mbl, M, N, K, C, ldc, beta, err);
+    const cudaError_t ae = smem_attr<DenseJob>();
+    if (ae != cudaSuccess) return ae;
+    const int gx = (M + kBM - 1) / kBM, gy = (N + kBN - 1) / kBN;
+    const long long nt = (long long)gx * gy;
+    if (nt > 0x7fffffff) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(nt, sm_count());
+    umma_3xtf32_kernel<DenseJob><<<grid, kThreads, kSmemBytes, s>>>(
+        mah, mal, mbh, mbl, DenseJob{M, N, K, ldc, beta, gx, (int)nt, C}, err);
+    return cudaGetLastError();
+}
+
+cudaError_t umma_grouped_3xtf32(Tf32Rows A, Tf32Rows B, const GroupTile *tiles, int ntiles, float *C, float *C_lo,
+                                int *err, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    auto aligned = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    if (!A.hi || !A.lo || !B.hi || !B.lo || !tiles || !C || !err || A.ld % 4 || B.ld % 4 || A.k > A.ld ||
+        B.k > B.ld || A.k <= 0 || B.k <= 0 || A.rows <= 0 || B.rows <= 0 || !aligned(A.hi) || !aligned(A.lo) ||
+        !aligned(B.hi) || !aligned(B.lo))
+        return cudaErrorInvalidValue;
+    CUtensorMap mah, mal, mbh, mbl;
+    if (!encode(&mah, A.hi, A.rows, A.k, A.ld) || !encode(&mal, A.lo, A.rows, A.k, A.ld) ||
+        !encode(&mbh, B.hi, B.rows, B.k, B.ld) || !encode(&mbl, B.lo, B.rows, B.k, B.ld))
+        return cudaErrorInvalidValue;
+    const cudaError_t ae = smem_attr<GroupJob>();
+    if (ae != cudaSuccess) return ae;
+    umma_3xtf32_kernel<GroupJob><<<std::min(ntiles, sm_count()), kThreads, kSmemBytes, s>>>(
+        mah, mal, mbh, mbl, GroupJob{tiles, ntiles, C, C_lo}, err);
     return cudaGetLastError();
 }
 

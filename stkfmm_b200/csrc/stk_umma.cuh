@@ -23,6 +23,28 @@ struct Tf32Split {
 cudaError_t umma_gemm_3xtf32(int M, int N, int K, Tf32Split A, Tf32Split B, float *C, int ldc, int beta, int *err,
                              cudaStream_t s);
 
+// A K-major operand as one 2-D array of rows: rows x ld floats (ld a multiple of 4),
+// of which the first k columns are read (the tensor map zero-fills columns >= k and
+// rows >= rows).
+struct Tf32Rows {
+    const float *hi = nullptr, *lo = nullptr;
+    int rows = 0, k = 0, ld = 0;
+};
+
+// One 128 x 128 output tile of a grouped GEMM: out[m][n] = sum_{kk < K}
+// A[a_row + m][kk] B[b_row + n][kk]; rows m < m_store, columns n < n_valid are written
+// to C[c_off + n ldc + m] (0 for rows m >= m_valid), split into TF32 hi / lo parts
+// (C, C_lo) when C_lo is given.
+struct GroupTile {
+    int a_row, b_row, K, m_valid, m_store, n_valid, ldc, pad_;
+    long long c_off;
+};
+
+// Many tiles, each of its own small GEMM, in one launch (one CTA per tile; the same
+// 3xTF32 pipeline as umma_gemm_3xtf32).  tiles: device array of ntiles entries.
+cudaError_t umma_grouped_3xtf32(Tf32Rows A, Tf32Rows B, const GroupTile *tiles, int ntiles, float *C, float *C_lo,
+                                int *err, cudaStream_t s);
+
 // v = hi + lo to ~2^-24 relative with both parts exact in TF32: hi = v rounded to
 // TF32 (to nearest, ties away), lo = (v - hi) rounded to TF32 (v - hi is exact in FP32)
 __device__ __forceinline__ void tf32_split_value(float v, float &hi, float &lo) {

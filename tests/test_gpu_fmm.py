@@ -191,3 +191,32 @@ def test_operators_shared_between_handles(torch_cuda, pbc):
     c = handle()  # no holder left: c builds its own
     tc, oc = first_eval(c)
     assert rel_l2(oc, oa) < 1e-13
+
+
+@pytest.mark.parametrize("kernel,p", [(1, 10), (8, 8), (128, 8)])
+def test_mixed_chunked_m2l_tensor_cores(torch_cuda, monkeypatch, kernel, p):
+    """The mixed path's per-offset (chunked) M2L on the tensor cores (grouped 3xTF32
+    tcgen05 GEMMs) is as accurate as the same M2L in SIMT FP32 (STKFMM_M2L_TC=0): the
+    mixed FMM stays within 1e-6 of FP64, on an adaptive clustered tree whose levels
+    all take the chunked path."""
+    import stkfmm_b200 as S
+    pts, slv, dlv, td = fmm_case(kernel, 12000, seed=40 + kernel)
+    res = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("STKFMM_M2L_TC", mode)
+        _, res[mode] = run_fmm(kernel, p, 40, pts, slv, dlv, td, prec=1)
+    _, ref = run_fmm(kernel, p, 40, pts, slv, dlv, td, prec=0)
+    # both FP32-accurate: each within 1e-6 of FP64, the tensor-core one no worse
+    e1, e0 = rel_l2(res["1"], ref), rel_l2(res["0"], ref)
+    assert e1 < 1e-6 and e1 < 1.5 * e0 + 1e-7, (e1, e0)
+    # relative to the part beyond the U-list near field (what the far field computes, plus
+    # the direct W / X pairs), the tensor-core M2L's mixed FMM errs no more than the SIMT one's
+    fmm = S.Stk3DFMM(p, 40, 0, kernel)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts if dlv is not None else None)
+    fmm.setup_tree(kernel)
+    near = np.zeros_like(ref)
+    fmm.evaluate_near(kernel, slv, near, dlv)
+    far = ref - near
+    e_tc, e_simt = rel_l2(res["1"] - ref, far), rel_l2(res["0"] - ref, far)
+    assert e_tc < 1.5 * e_simt + 1e-7, (e_tc, e_simt)
