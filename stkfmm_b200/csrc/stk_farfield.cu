@@ -2190,8 +2190,13 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
     // ---- downward pass: compressed M2L per offset ----
     const int k = F.m2l_rank;
     double *phi_hat = (double *)F.phi_hat.ptr, *psi_hat = (double *)F.psi_hat.ptr;
-    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, nn, N, &one, (const double *)F.m2l_vt.ptr, k, phi, N, &zero,
-                      phi_hat, k));
+    // The basis products phi_hat = V^T phi and psi += (DC2DE U) psi_hat stay FP64 in both
+    // paths.  Their sums cancel strongly: the equivalent densities of the pseudo-inverse
+    // solves are much larger than the fields they stand for.  FP32-accurate products
+    // (3xTF32 on the tensor cores) raised the mixed Stokes FMM's error from 2.8e-7 to
+    // 5.2e-7 (V^T phi alone) and 7.3e-7 (both); p = 8, 12000 clustered points.
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, k, nn, N, &one, (const double *)F.m2l_vt.ptr, k, phi, N,
+                      &zero, phi_hat, k));
     // gather the sources of every (offset, chunk) column, one batched GEMM over the
     // chunks, then each target sums its columns in offset order (deterministic)
     FCUDA(cudaMemsetAsync(psi_hat, 0, sizeof(double) * (size_t)nn * k, s));
@@ -2268,8 +2273,8 @@ int farfield_evaluate(Stk3DFMM *f, KernelData *kd, const double *d_sl, const dou
                                            : m2l_dense_level<double>(F, *Dp, phi_hat, psi_hat, s);
         if (rcd) return rcd;
     }
-    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k, &one,
-                      psi, N));
+    FBLAS(cublasDgemm(F.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, nn, k, &one, (const double *)F.m2l_e.ptr, N, psi_hat, k,
+                      &one, psi, N));
     // triply periodic: the root's far images (FP64)
     if (F.periodic && (!F.split || f->shard_rank == 0))
         FBLAS(cublasDgemv(F.blas, CUBLAS_OP_N, N, N, &one, (const double *)F.m2c_op.ptr, N, phi, 1, &one, psi, 1));
