@@ -401,6 +401,41 @@ def run_one_workload(name, steps, warmup):
     raise SystemExit("unknown workload %s" % name)
 
 
+def run_p2p_only(steps, warmup):
+    """The headline U-list P2P step alone, FP64 then mixed (for kernel profiles): `warmup`
+    untimed launches then `steps` timed ones per precision, one list_p2p_kernel launch each,
+    L2 flushed between timed steps; prints per-precision kernel times as one JSON line."""
+    import torch
+    import stkfmm_b200 as S
+    torch.cuda.set_device(0)
+    K = KERNEL_LAPPGRAD
+    pts, q, d = make_points(0)
+    fmm = S.Stk3DFMM(MULT_ORDER, MAX_PTS, S.PAXIS.NONE, K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts)
+    fmm.setup_tree(K)
+    st = fmm.tree_stats(K)
+    stream = torch.cuda.Stream()
+    qd, dd = torch.as_tensor(q).cuda(), torch.as_tensor(d).cuda()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = torch.zeros((N_POINTS, 4), dtype=torch.float64, device="cuda")
+    res = {"workload": WORKLOAD, "point_pairs_per_step": st["u_pairs_sl"]}
+    for prec, nm in ((S.PRECISION.FP64, "fp64"), (S.PRECISION.MIXED, "mixed")):
+        fmm.set_precision(prec)
+        kern = []
+        with torch.cuda.stream(stream):
+            for i in range(warmup + steps):
+                flush.zero_()
+                out.zero_()
+                fmm.evaluate_near_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), stream.cuda_stream)
+                stream.synchronize()
+                if i >= warmup:
+                    kern.append(fmm.last_kernel_ms(K))
+        res[nm] = {"kernel_ms_median": statistics.median(kern), "kernel_ms": kern}
+    print(json.dumps({"p2p_only": res}), flush=True)
+    return 0
+
+
 def extra_fmm_inputs(cfg, seed):
     """Points, SL values and DL values (or None) of a further workload."""
     rng = np.random.default_rng(seed)
@@ -1105,7 +1140,11 @@ def main():
     ap.add_argument("--fmm-workload", default=None,
                     help="time one further FMM / wall workload alone (%s) and print its block"
                          % ", ".join([c["name"] for c in EXTRA_FMM + WALL_FMM] + [ADJ["name"]]))
+    ap.add_argument("--p2p-only", action="store_true",
+                    help="time the U-list P2P step alone, FP64 then mixed (one kernel launch per step)")
     args = ap.parse_args()
+    if args.p2p_only:
+        return run_p2p_only(args.steps, args.warmup)
     if args.fmm_workload:
         return run_one_workload(args.fmm_workload, args.steps, args.warmup)
     if args.impl == "reference":
