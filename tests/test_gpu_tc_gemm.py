@@ -35,3 +35,25 @@ def test_gemm_3xtf32_fp32_accuracy(torch_cuda, M, N, K, beta):
     err = float(torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref))
     err32 = float(torch.linalg.norm(naive.double() - ref) / torch.linalg.norm(ref))
     assert err < max(4 * err32, 1e-7) and err < 1e-6, (err, err32)
+
+
+def test_gemm_3xtf32_m2l_shape(torch_cuda):
+    """The shape of one dense M2L GEMM of the 2M-point RPY PXYZ workload at p = 8
+    (level 5): M = k = 636 rows of the stacked factor, N = 4096 boxes of one parity
+    type, K = 28672 stacked ranks; operands of ~0.5 GB, larger than L2."""
+    from stkfmm_b200 import lib
+    torch = torch_cuda
+    M, N, K = 636, 4096, 28672
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.randn((M, K), device="cuda", generator=g, dtype=torch.float32)
+    B = torch.randn((N, K), device="cuda", generator=g, dtype=torch.float32)
+    C = torch.zeros((N, M), device="cuda", dtype=torch.float32)
+    rc = lib().stk_gemm_3xtf32(M, N, K, A.data_ptr(), K, B.data_ptr(), K, C.data_ptr(), M, 0,
+                               torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    ref = (A.double() @ B.double().T).T
+    naive = (A @ B.T).T
+    err = float(torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref))
+    err32 = float(torch.linalg.norm(naive.double() - ref) / torch.linalg.norm(ref))
+    assert err < max(4 * err32, 1e-7) and err < 1e-6, (err, err32)
