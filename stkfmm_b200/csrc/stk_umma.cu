@@ -15,13 +15,19 @@
 //   warp 0  TMA producer: per K-block the four 128 x 32 FP32 tiles Ah, Al, Bh, Bl
 //           (128-byte swizzle, K-major) into a 3-stage shared-memory ring;
 //   warp 1  TMEM owner and MMA issuer: 12 tcgen05.mma (M = 128, N = 128, K = 8,
-//           kind::tf32) per K-block into one of two TMEM accumulators
-//           (2 x 128 columns), committed to the stage's "empty" barrier and the
+//           kind::tf32) per K-block into one of four TMEM accumulators
+//           (4 x 128 columns), committed to the stage's "empty" barrier and the
 //           accumulator's "full" barrier;
 //   warps 2-5 drain: tcgen05.ld of the accumulator (each warp its 32 TMEM lanes =
-//           output rows), added into 128 FP32 registers per thread; the buffer is
-//           released to the MMA warp; at the end the rows are written (or added)
-//           to C with coalesced column stores.
+//           output rows, two 32-column loads per wait), added into 128 FP32
+//           registers per thread; the buffer is released to the MMA warp; at the
+//           end the rows are written (or added) to C with coalesced column stores.
+// What bounds it: per K-block the 12 MMAs read 96 KB of operand tiles from shared
+// memory (Ah and Bh twice, Al and Bl once, 16 KB each) and TMA writes 64 KB into
+// it, ~200 bytes per clock at the nominal TF32 rate against ~128 that shared
+// memory delivers; the tensor pipe runs at ~60% of its rate inside a tile.  Wider
+// tiles (N = 256, or M = 256 over a CTA pair) would read each A tile for twice
+// the products.
 // Every mbarrier wait has an iteration limit: on expiry the kernel records an
 // error code, stops issuing work, waits (bounded) for what it issued, frees its
 // TMEM and returns.  TMA loads read this GPU's memory only, without multicast.
@@ -43,12 +49,27 @@ constexpr int kStages = 3;
 constexpr int kTileBytes = kBM * kBK * 4;      // 16 KB (A and B tiles are both 128 x 32 FP32)
 constexpr int kStageBytes = 4 * kTileBytes;    // Ah, Al, Bh, Bl
 constexpr int kThreads = 192;                  // 6 warps
-constexpr uint32_t kTmemCols = 256;            // two 128-column FP32 accumulators
+// FP32 accumulators of 128 columns in TMEM (the MMA warp runs up to kAccBufs - 1
+// K-blocks ahead of the drain); 4 take all 512 columns, which one CTA per SM allows
+// (198 KB of shared memory per CTA).  4 accumulators with two TMEM loads per wait
+// measured 2% faster than 2 with one (mixed M2L of the 2M-point RPY PXYZ FMM,
+// 17.4 against 17.8 ms).
+#ifndef STK_UMMA_ACCBUFS
+#define STK_UMMA_ACCBUFS 4
+#endif
+constexpr int kAccBufs = STK_UMMA_ACCBUFS;
+static_assert(kAccBufs == 2 || kAccBufs == 4, "2 or 4 accumulators");
+constexpr uint32_t kTmemCols = 128 * kAccBufs;
+// TMEM columns per drain load before its wait (32: one load per wait; 64: two)
+#ifndef STK_UMMA_LDCOLS
+#define STK_UMMA_LDCOLS 64
+#endif
+constexpr int kLdCols = STK_UMMA_LDCOLS;
 constexpr long long kSpinLimit = 1LL << 25;    // ~ a second of polling per wait
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /* barriers */ + 1024 /* alignment */;
 
 struct Bars {
-    unsigned long long full[kStages], empty[kStages], accf[2], acce[2];
+    unsigned long long full[kStages], empty[kStages], accf[kAccBufs], acce[kAccBufs];
     uint32_t tmem;
 };
 
@@ -131,6 +152,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "memory");
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // One output tile: output rows [0, 128) are rows a_row .. a_row + 127 of A, output
 // columns [0, 128) rows b_row .. b_row + 127 of B (tensor-map coordinates), summed
@@ -212,13 +245,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(saddr(&bars->full[s]), 1);
             mbar_init(saddr(&bars->empty[s]), 1);
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < kAccBufs; b++) {
             mbar_init(saddr(&bars->accf[b]), 1);
             mbar_init(saddr(&bars->acce[b]), 4);  // one arrival per drain warp
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 1) {  // TMEM: two 128-column accumulators, owned by warp 1
+    if (warp == 1) {  // TMEM: kAccBufs 128-column accumulators, owned by warp 1
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&bars->tmem)),
                      "r"(kTmemCols)
                      : "memory");
@@ -266,8 +299,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int t = blockIdx.x; t < job.ntiles && ok; t += gridDim.x) {
                 const int nkb = (job.tile(t).K + kBK - 1) / kBK;
                 for (int kb = 0; kb < nkb; kb++) {
-                    const int s = (int)(g % kStages), b = (int)(g & 1);
-                    if (!mbar_wait(saddr(&bars->acce[b]), ((uint32_t)(g >> 1) & 1u) ^ 1u) ||
+                    const int s = (int)(g % kStages), b = (int)(g % kAccBufs);
+                    if (!mbar_wait(saddr(&bars->acce[b]), ((uint32_t)(g / kAccBufs) & 1u) ^ 1u) ||
                         !mbar_wait(saddr(&bars->full[s]), (uint32_t)(g / kStages) & 1u)) {
                         ok = false;
                         break;
@@ -293,7 +326,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             if (!ok) atomicExch(err, 2);
             // the MMAs issued last must be complete before the TMEM is freed
-            if (g > 0) mbar_wait(saddr(&bars->accf[(g - 1) & 1]), (uint32_t)((g - 1) >> 1) & 1u);
+            if (g > 0) mbar_wait(saddr(&bars->accf[(g - 1) % kAccBufs]), (uint32_t)((g - 1) / kAccBufs) & 1u);
         }
         __syncwarp();
     } else {
@@ -308,19 +341,35 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int j = 0; j < kBN; j++) acc[j] = 0.0f;
             for (int kb = 0; kb < nkb; kb++, g++) {
-                const int b = (int)(g & 1);
+                const int b = (int)(g % kAccBufs);
                 // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
-                if (!__all_sync(0xffffffffu, mbar_wait(saddr(&bars->accf[b]), (uint32_t)(g >> 1) & 1u))) {
+                if (!__all_sync(0xffffffffu, mbar_wait(saddr(&bars->accf[b]), (uint32_t)(g / kAccBufs) & 1u))) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
+                const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN);
+                if constexpr (kLdCols == 64) {
 #pragma unroll
-                for (int c = 0; c < kBN / 32; c++) {
-                    uint32_t r[32];
-                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN + c * 32), r);
+                    for (int c = 0; c < kBN / 64; c++) {
+                        uint32_t r0[32], r1[32];
+                        tmem_ld32_nowait(tb + (uint32_t)(c * 64), r0);
+                        tmem_ld32_nowait(tb + (uint32_t)(c * 64 + 32), r1);
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < 32; j++) acc[c * 32 + j] += __uint_as_float(r[j]);
+                        for (int j = 0; j < 32; j++) {
+                            acc[c * 64 + j] += __uint_as_float(r0[j]);
+                            acc[c * 64 + 32 + j] += __uint_as_float(r1[j]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < kBN / 32; c++) {
+                        uint32_t r[32];
+                        tmem_ld32(tb + (uint32_t)(c * 32), r);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) acc[c * 32 + j] += __uint_as_float(r[j]);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
