@@ -393,12 +393,60 @@ def run_one_workload(name, steps, warmup):
             r.pop("_acc")
             print(json.dumps({name: r}), flush=True)
             return 0
+    if name == MAIN_FMM_NAME:
+        print(json.dumps({name: time_main_fmm(steps, warmup, flush)}), flush=True)
+        return 0
     if name == ADJ["name"]:
         r = time_adjoint(steps, warmup, 0, 1, flush)
         adjoint_checks(r)
         print(json.dumps({name: r}), flush=True)
         return 0
     raise SystemExit("unknown workload %s" % name)
+
+
+MAIN_FMM_NAME = "lappgrad_1m_clustered"
+
+
+def time_main_fmm(steps, warmup, flush):
+    """The headline workload's whole evaluate_fmm alone (FP64, then mixed): CUDA events
+    around each evaluate_fmm_device, L2 flushed between, per-phase split; timed steps
+    inside torch.cuda.profiler.start/stop."""
+    import torch
+    import stkfmm_b200 as S
+    K = KERNEL_LAPPGRAD
+    pts, q, d = make_points(0)
+    fmm = S.Stk3DFMM(MULT_ORDER, MAX_PTS, S.PAXIS.NONE, K)
+    fmm.set_box(np.zeros(3), 1.0)
+    fmm.set_points(pts, pts, pts)
+    fmm.setup_tree(K)
+    stream = torch.cuda.Stream()
+    qd, dd = torch.as_tensor(q).cuda(), torch.as_tensor(d).cuda()
+    out = torch.zeros((N_POINTS, 4), dtype=torch.float64, device="cuda")
+    res = {"workload": WORKLOAD_FMM}
+    for prec, nm in ((S.PRECISION.FP64, "fp64"), (S.PRECISION.MIXED, "mixed")):
+        fmm.set_precision(prec)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), stream.cuda_stream)
+        stream.synchronize()
+        ms, phases = [], []
+        torch.cuda.profiler.start()
+        with torch.cuda.stream(stream):
+            for _ in range(steps):
+                flush.zero_()
+                out.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fmm.evaluate_fmm_device(K, qd.data_ptr(), out.data_ptr(), dd.data_ptr(), stream.cuda_stream)
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                phases.append(fmm.last_phase_ms(K))
+        torch.cuda.profiler.stop()
+        res[nm] = {"evals_per_s": 1e3 / (sum(ms) / steps), "ms_per_eval": sum(ms) / steps,
+                   "phases_ms": {k: sum(p[k] for p in phases) / steps for k in phases[0]}}
+    res["mixed_over_fp64"] = res["fp64"]["ms_per_eval"] / res["mixed"]["ms_per_eval"]
+    return res
 
 
 def run_p2p_only(steps, warmup):
@@ -1138,8 +1186,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--fmm-workload", default=None,
-                    help="time one further FMM / wall workload alone (%s) and print its block"
-                         % ", ".join([c["name"] for c in EXTRA_FMM + WALL_FMM] + [ADJ["name"]]))
+                    help="time one FMM / wall workload alone (%s) and print its block"
+                         % ", ".join([MAIN_FMM_NAME] + [c["name"] for c in EXTRA_FMM + WALL_FMM] + [ADJ["name"]]))
     ap.add_argument("--p2p-only", action="store_true",
                     help="time the U-list P2P step alone, FP64 then mixed (one kernel launch per step)")
     args = ap.parse_args()
