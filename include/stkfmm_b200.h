@@ -46,7 +46,7 @@ enum stk_status {
     STK_ERR_CUDA = 5,         /* a CUDA runtime call failed                               */
     STK_ERR_NO_DEVICE = 6,    /* no CUDA device: this library has no CPU path             */
     STK_ERR_OUT_OF_BOX = 7,   /* a point lies outside the FMM box on a free axis          */
-    STK_ERR_NOT_SUPPORTED = 8 /* kernel or feature not provided by this build             */
+    STK_ERR_NOT_SUPPORTED = 8 /* kernel or feature not provided by this library           */
 };
 
 /* ---- enums of Lib/include/STKFMM/STKFMM_common.hpp ---------------------- */

@@ -43,7 +43,7 @@ extern "C" const char *stk_status_string(int status) {
     case STK_ERR_CUDA: return "CUDA runtime error";
     case STK_ERR_NO_DEVICE: return "no CUDA device (this library has no CPU path)";
     case STK_ERR_OUT_OF_BOX: return "point outside the FMM box";
-    case STK_ERR_NOT_SUPPORTED: return "not supported by this build";
+    case STK_ERR_NOT_SUPPORTED: return "not supported by this library";
     default: return "unknown status";
     }
 }

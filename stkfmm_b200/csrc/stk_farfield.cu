@@ -124,7 +124,7 @@ __global__ void kernel_matrix_kernel(const double *__restrict__ X, int ni, const
 // (M2L/Laplace/Laplace1D3D.cpp:18-28, M2L/Stokeslet/Stokes1D3D.cpp:37,
 // M2L/SVD_pvfmm.hpp:35), t < 1000000 for stokes_pvel
 // (M2L/StokesPVel/StokesPVel1D3D.cpp:36-46).  Their sums start at t = 3
-// because PVFMM's lists reach two cells; this build's reach one.  The sum
+// because PVFMM's lists reach two cells; this library's reach one.  The sum
 // runs from the farthest images inwards with compensation; for a neutral
 // (and force-free) root density the images' tail decays like a dipole
 // lattice, so the cut-off costs about 1 / kPxImages of a dipole's field.

@@ -102,7 +102,7 @@ inline const KernelInfo *find_kernel(unsigned id) {
     return nullptr;
 }
 
-// A kernel is evaluated by this build when its S2T single-layer slot is filled.
+// A kernel is evaluated by this library when its S2T single-layer slot is filled.
 inline bool kernel_supported(const KernelInfo *k) { return k && k->slot[SLOT_S2T_SL] >= 0; }
 
 }  // namespace stk
