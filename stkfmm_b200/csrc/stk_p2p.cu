@@ -44,8 +44,15 @@ namespace stk {
 
 namespace {
 
-constexpr int kWarpsPerCta = 4;
-constexpr int kThreads = 32 * kWarpsPerCta;
+// Warps per CTA.  Every warp works alone (warp-level synchronisation only), so
+// this only sets the granularity in which registers fill an SM: one warp per CTA
+// lets the FP64 kernels use every register slot (14 warps per SM at 140
+// registers instead of 12 in 4-warp CTAs: the benchmark's FP64 launch 1.1%
+// faster); the mixed kernels measured best at 4.
+template <bool MIXED> struct Cta {
+    static constexpr int warps = MIXED ? 4 : 1;
+    static constexpr int threads = 32 * warps;
+};
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kPadCoord = 1.0e4;  // offset of zero-strength padding sources
 constexpr int kShiftNoneCode = 13;   // list-entry shift code of the unshifted source box
@@ -159,7 +166,9 @@ template <int RS> struct RawStride {
 };
 
 template <int UK, bool MIXED>
-__global__ void __launch_bounds__(kThreads, MinBlocks<UK, MIXED>::value) list_p2p_kernel(const ListP2PArgs a) {
+__global__ void __launch_bounds__(Cta<MIXED>::threads, MinBlocks<UK, MIXED>::value)
+    list_p2p_kernel(const ListP2PArgs a) {
+    constexpr int kWarpsPerCta = Cta<MIXED>::warps;
     using K = Uk<UK>;
     constexpr int TDIM = K::TDIM;
     constexpr int NV = K::NV;
@@ -521,15 +530,17 @@ cudaError_t launch_impl(const ListP2PArgs &a, int num_sms, cudaStream_t stream) 
     static int blocks_per_sm = 0;
     if (blocks_per_sm == 0) {
         cudaError_t err =
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, list_p2p_kernel<UK, MIXED>, kThreads, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, list_p2p_kernel<UK, MIXED>,
+                                                          Cta<MIXED>::threads, 0);
         if (err != cudaSuccess) return err;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
+    constexpr int kWarpsPerCta = Cta<MIXED>::warps;
     long long want = ((long long)a.n_items + kWarpsPerCta - 1) / kWarpsPerCta;
     int grid = (int)std::max(1LL, std::min<long long>((long long)num_sms * blocks_per_sm, want));
     cudaError_t err = cudaMemsetAsync(a.counter, 0, sizeof(unsigned int), stream);
     if (err != cudaSuccess) return err;
-    list_p2p_kernel<UK, MIXED><<<grid, kThreads, 0, stream>>>(a);
+    list_p2p_kernel<UK, MIXED><<<grid, Cta<MIXED>::threads, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
