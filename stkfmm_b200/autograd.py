@@ -150,6 +150,12 @@ class StokesRegVelP2P(torch.autograd.Function):
     @staticmethod
     def forward(ctx, src_xyz, src_val, trg_xyz, plan, precision):
         src, sval, trg = _c(src_xyz), _c(src_val), _c(trg_xyz)
+        if plan.mode == "ulist":
+            # the U list is of one point set: its targets are its sources
+            if len(src) != plan.n or len(sval) != plan.n:
+                raise ValueError("UListPlan of %d points given %d sources" % (plan.n, len(src)))
+            if trg.data_ptr() != src.data_ptr() and not (trg.shape == src.shape and torch.equal(trg, src)):
+                raise ValueError("UListPlan: trg_xyz must be the source points")
         out = torch.zeros((len(trg), 3), dtype=torch.float64, device=src.device)
         plan.forward(src, sval, trg, out, precision)
         ctx.save_for_backward(src, sval, trg)
